@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the giant-impact step at 262,144 particles.
+
+Workload (the full plain impact): 262,144 particles; target 0.9 M_earth, core
+mass fraction 0.3 (7.8 / 3.3 g/cc), crust of 2.7 g/cc on the outer 5 % of
+radius, spun to an 8-hour day; impactor 0.1 M_earth at 45 degrees and 1.0
+v_esc.  The run is taken through the reference's phases (settle, rigid
+approach, first-touch kick, then full steps with a synchronous analysis every
+360 steps, as window.__impact.runTo does) before anything is timed, so the
+timed steps see a mid-impact state: contacts, debris, a Morton order and a
+loose list.
+
+A step is one full-phase step of the reference schedule (contact grid every
+2nd step, 64^3 mesh + P3M every 8th, contacts, heat, kick/drift).
+
+  value    N * K / sum over the K timed steps of each step's CUDA-event time on
+           the library's stream, with L2 flushed (a 256 MiB write) before every
+           step, so each step starts from HBM.  Max over ranks.
+  e2e      the same metric through the host-buffer C-ABI call
+           (ccs_advance_host: pinned host state in, one step, state out).
+  roofline the contact step kernel (k_simulate): algorithmic bytes (92 B per
+           particle: pos, vel, mat, q in; pos, vel, aux, q out) over its mean
+           event-timed duration, against the measured HBM copy bandwidth.
+  cpu_baseline / --impl reference: the CPU oracle (a C restatement of the
+           reference's step, all host cores, OpenMP) on a bounded sample.
+
+Multi-GPU: one process per GPU, independent replicas of the impact (the step
+has no partition worth a data-path collective at this size): weak scaling.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ALG_BYTES_SIM = 92          # bytes per particle per contact-step launch
+L2_FLUSH_BYTES = 256 << 20
+
+
+def impact_opt(N):
+    """The full plain giant impact (second-case variants are parity configs, not bench lines)."""
+    day_frac = 2 * math.pi * 805 / (8 * 3600)     # an 8-hour day as a fraction of breakup spin
+    return dict(N=N, q=0.1, dens=1.0, core=0.3, spin0=day_frac, spin1=0.2, angle=45.0, incl=0.0, vfac=1.0,
+                rest=0.3, mImp=0.1, mTarget=0.9, rhoR=7.8 / 3.3, rhoCrust=2.7 / 3.3, crustFrac=0.05)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        try:
+            d = json.load(open(p))
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """dram bytes per k_simulate launch from the committed ncu summary, scaled to a launch of N particles."""
+    p = os.path.join(ROOT, "profiles", "simulate_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    vals = {}
+    for line in open(p):
+        if ":" in line and not line.startswith("#"):
+            k, v = line.split(":", 1)
+            vals[k.strip()] = v.strip()
+    try:
+        return float(vals["dram_bytes_per_particle"])
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(N, min_seconds=10.0, min_steps=8, threads=None):
+    """The CPU oracle's step (the reference's algorithm restated in C, OpenMP over all host cores) on a
+    bounded sample: the freshly built impact, boxes on the target, full-phase steps."""
+    from oracle import oracle as O
+    O.build()
+    cores = threads or os.cpu_count()
+    O.set_threads(cores)
+    sim, pos, vel, mat, home = O.build_run(O.make_opt(**impact_opt(N)))
+    sim.phase, sim.impactT = 2, sim.t
+    for k in range(3):
+        sim.boxCen[0][k] = sim.cen0[k]
+    sim.boxT[0] = sim.t
+    e = O.Engine(sim, pos, vel, mat)
+    e.step(False, False)           # warm: the pair table, first touches of the arrays
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        e.step(False, False)
+        e.sim.t += e.sim.dt
+        steps += 1
+        el = time.perf_counter() - t0
+        if steps >= min_steps and el >= min_seconds:
+            break
+    return {"value": N * steps / el, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": "%d full-phase steps of the freshly built %d-particle impact (%.1f s, %d OpenMP threads)"
+                      % (steps, N, el, cores)}
+
+
+def prepare(nb, cc, N, prep_steps, log):
+    """build -> settle -> rigid approach -> kick -> prep_steps full steps with runTo's analysis cadence."""
+    t0 = time.perf_counter()
+    nb.build(cc.make_opt(**impact_opt(N)))
+    log("built N=%d in %.1fs (a=%.5f dt=%.3e settle=%d)" % (N, time.perf_counter() - t0, nb.sim.a, nb.sim.dt,
+                                                            nb.sim.settleLeft))
+    while nb.sim.phase == 0:
+        nb.settle_some(64)
+    nb.analyze(True)
+    n_rigid = 0
+    while nb.sim.phase == 1 and n_rigid < 5000:
+        nb.rigid_step(0.01)
+        n_rigid += 1
+    if nb.sim.phase != 2:
+        raise RuntimeError("the bodies never touched")
+    done = 0
+    while done < prep_steps:
+        n = min(360 - (nb.sim.stepNo - nb.analyzed_at), prep_steps - done)
+        n = max(n, 1)
+        nb.steps(n)
+        done += n
+        if nb.sim.stepNo - nb.analyzed_at >= 360:
+            nb.analyze(True)
+    nb.analyze(True)
+    nb.sync()
+    r = nb.report
+    log("prepared in %.1fs: %d rigid steps, %d full steps, t=%.3f, loose=%d (list %d), largest=%.3f"
+        % (time.perf_counter() - t0, n_rigid, done, nb.sim.t, nb.pp["loose"], nb.pp["count"], r.largest))
+
+
+def run_ours(args, rank, world, log):
+    import torch
+    import cosmic_collisions_b200 as cc
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    N = args.n
+    nb = cc.NBody(dev)
+    lib = cc.lib()
+    prepare(nb, cc, N, args.prep, log)
+    nb.steps(args.warmup)
+    nb.sync()
+    buf = nb.device_buffers()
+    stream = torch.cuda.ExternalStream(buf.stream, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(dev)
+    dist = world > 1
+    if dist:
+        import torch.distributed as td
+        td.barrier()
+    torch.cuda.synchronize()
+    lib.ccs_timing(nb.handle, 1)
+    l0 = lib.ccs_launch_count(nb.handle)
+    clocks.start()
+    w0 = time.perf_counter()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+        nb.step(False, False)
+        nb.sim.t += nb.sim.dt
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+    nb.sync()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    clk = clocks.stop()
+    launches = lib.ccs_launch_count(nb.handle) - l0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    import ctypes as C
+    kt = {}
+    for kid, name in enumerate(["simulate", "contact_grid", "deposit", "cell", "pp_force"]):
+        tot, cnt = C.c_double(), C.c_int()
+        lib.ccs_timing_read(nb.handle, kid, C.byref(tot), C.byref(cnt))
+        kt[name] = {"launches": cnt.value, "total_ms": tot.value,
+                    "mean_us": 1e3 * tot.value / cnt.value if cnt.value else None}
+    lib.ccs_timing(nb.handle, 0)
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * N * args.steps / (total_ms / 1e3)
+
+    # the same steps back to back from captured 8-step graphs, state L2-resident (no flush)
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ksteps = max(8, args.steps // 8 * 8)
+    if nb.sim.stepNo % 8:
+        nb.steps(8 - nb.sim.stepNo % 8)
+    nb.sync()
+    with torch.cuda.stream(stream):
+        g0.record(stream)
+    nb.steps(ksteps)
+    with torch.cuda.stream(stream):
+        g1.record(stream)
+    nb.sync()
+    resident_ms = g0.elapsed_time(g1)
+
+    # end to end through the host-buffer plugin call
+    st = nb.read_state()
+    hp = torch.from_numpy(st["pos"]).pin_memory()
+    hv = torch.from_numpy(st["vel"]).pin_memory()
+    hq = torch.from_numpy(st["q"]).pin_memory()
+    ha = torch.empty((N, 4), dtype=torch.float32).pin_memory()
+    P = lambda t: C.c_void_p(t.data_ptr())
+    e2e_steps = max(8, min(args.steps, 256))
+    if dist:
+        td.barrier()
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        rc = lib.ccs_advance_host(nb.handle, P(hp), P(hv), P(hq), 1, P(hp), P(hv), P(ha), P(hq))
+        if rc:
+            raise RuntimeError("ccs_advance_host: %d" % rc)
+    e2e_s = time.perf_counter() - e0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = N * (16 + 16 + 4)
+    d2h = N * (16 + 16 + 16 + 4)
+
+    peak, peak_kind = measured_peaks()
+    sim_mean_us = kt["simulate"]["mean_us"]
+    achieved = ALG_BYTES_SIM * N / (sim_mean_us * 1e-6) / 1e9 if sim_mean_us else None
+    tpp = committed_traffic()
+    line = {
+        "metric": "particle-steps/s @262k, plain P3M step (NN-corrected form not built yet)",
+        "value": value,
+        "unit": "particle-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded builder: src/nbody.js build() with the config's masses and layers)",
+        "config": {
+            "workload": "full plain giant impact, %d particles: 0.9 + 0.1 M_earth, core 0.3, crust 2.7 g/cc "
+                        "outer 5%%, 8 h day, 45 deg, 1.0 v_esc; mid-impact state after %d full steps" % (N, args.prep),
+            "particles": N, "mesh": "64^3 x %d box(es)" % (2 if nb.sim.boxOn[1] else 1),
+            "contact_grid": "%d^3 hashed" % nb.sim.G, "loose_list": nb.pp["count"],
+            "parallelism": "replicas x%d" % world,
+            "l2": "flushed (256 MiB write) before every timed step; value sums per-step event times",
+            "l2_resident_particle_steps_per_s": world * N * ksteps / (resident_ms / 1e3),
+            "wall_s_timed_region": wall,
+            "kernels_us": {k: v["mean_us"] for k, v in kt.items()},
+        },
+        "e2e": {"value": world * N * e2e_steps / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "api": "ccs_advance_host, one step per call, pinned host buffers"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "peak_kind": peak_kind + " hbm_gbs",
+                     "kernel": "k_simulate (contacts + gather + kick/drift)",
+                     "traffic": tpp * N if tpp else None,
+                     "algorithmic_bytes_per_launch": ALG_BYTES_SIM * N},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    nb.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1024)
+    ap.add_argument("--warmup", type=int, default=16)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--prep", type=int, default=720, help="full-phase steps before timing")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    log = (lambda s: print("[bench] " + s, file=sys.stderr, flush=True)) if rank == 0 else (lambda s: None)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        ref = cpu_reference(args.n, min_seconds=args.cpu_seconds)
+        line = {"impl": "reference", "metric": "particle-steps/s @262k, plain P3M step", "value": ref["value"],
+                "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": {"workload": "full plain giant impact, %d particles" % args.n},
+                "cpu_baseline": ref,
+                "e2e": {"value": ref["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    line = run_ours(args, rank, world, log)
+    if rank == 0:
+        if world == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu_reference(args.n, min_seconds=args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as td
+        td.barrier()
+        td.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1160 @@
+// ccs_api.cu -- the C ABI: the engine of src/nbody.js on the B200.
+//
+// The handle owns the device state (the reference's textures as flat arrays),
+// runs the step schedule of src/nbody.js:551-558 (contact grid every 2nd step,
+// mesh + P3M every 8th, gravity as one impulse), the phases (settle, rigid
+// approach, kick) and the analysis hand-off.  Per-step uniforms live in
+// device memory; `ccs_steps` replays captured CUDA graphs of whole 8-step
+// blocks whose uniform slots are refreshed by one memcpy node each replay.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "ccs_internal.h"
+
+using namespace ccs;
+
+namespace {
+
+constexpr double kFL = 6.0;
+constexpr double kFH = 2.0 * kFL / 64.0;
+constexpr double kPPCut = 5.0 * kFH;
+constexpr double kSeatSlack = 0.6;
+constexpr double kCpIron = 450.0, kCpRock = 1200.0;
+constexpr int kRing = 256;        // per-step uniform slots of the direct path
+constexpr int kMaxBlock = 16;     // largest meshEvery a captured block supports
+constexpr int kTimedKernels = 5;  // simulate, contact grid, deposit, cell, P3M force
+
+struct GraphKey {
+  int boxB, pp, seatCur, cur, meshEvery, ping;
+  bool operator<(const GraphKey &o) const {
+    return std::memcmp(this, &o, sizeof *this) < 0;
+  }
+};
+
+struct GraphSlot {
+  cudaGraphExec_t exec = nullptr;
+  ccs_uniforms *dev = nullptr;   // meshEvery slots on the device
+  ccs_uniforms *host = nullptr;  // pinned staging the memcpy node reads at replay
+  cudaEvent_t done = nullptr;    // recorded after the last replay
+  bool used = false;
+};
+
+}  // namespace
+
+struct ccs_handle {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  std::string err;
+  bool built = false;
+  ccs_sim sim{};
+  ccs_uniforms stat{};                  // setStaticUniforms
+  float LA[3] = {0, 0, 0}, LB[3] = {0, 0, 0}, boxB = 0.0f;   // what boxes() last set
+  int N = 0, meshEvery = 8;
+  // per-step uniform ring (direct launches)
+  ccs_uniforms *uniDev = nullptr, *uniHost = nullptr;
+  cudaEvent_t uniEv[kRing] = {};
+  bool uniUsed[kRing] = {};
+  int uniNext = 0;
+  // particle state, double-buffered (sim.src / sim.dst)
+  float4 *pos[2] = {}, *vel[2] = {}, *aux[2] = {};
+  float *q[2] = {};
+  int cur = 0;
+  float *mat = nullptr, *matTmp = nullptr;
+  float4 *home = nullptr, *homeTmp = nullptr;
+  // contact grid: two seat tables used in turn, and the cell each particle went to
+  uint32_t *seats[2] = {}, *hk[2] = {};
+  int seatCur = 0;
+  size_t ncell = 0;
+  MeshBuf pm[2];
+  // P3M
+  int *ppIndex = nullptr, *ppSlot = nullptr;
+  float4 *ppList = nullptr, *ppForce = nullptr;
+  float *ppBox = nullptr;
+  float2 *tab = nullptr;
+  int ppCount = 0, ppLoose = 0;
+  float4 *diag = nullptr;
+  unsigned *status = nullptr;           // kernel status word (kStatus* bits), sticky until the next build
+  // Morton sort scratch
+  uint32_t *keys = nullptr, *keysTmp = nullptr, *hist = nullptr;
+  int32_t *vals = nullptr, *valsTmp = nullptr, *into = nullptr, *permDev = nullptr;
+  // asynchronous read-back
+  float *stageP = nullptr, *stageV = nullptr, *stageD = nullptr;
+  cudaEvent_t readEv = nullptr;
+  bool pending = false;
+  // books
+  double *booksPartial = nullptr, *booksOut = nullptr;
+  // graphs
+  std::map<GraphKey, GraphSlot> graphs;
+  int ping = 0;
+  bool useGraphs = true;
+  // timing of chosen kernels with events on the stream
+  bool timing = false;
+  std::vector<cudaEvent_t> evPool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> evRecs;
+  size_t evNext = 0;
+  double tAcc[kTimedKernels] = {};
+  int tCount[kTimedKernels] = {};
+  int64_t launches = 0;
+};
+
+namespace {
+
+#define CUDA_TRY(h, call)                                                                        \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) {                                                                     \
+      (h)->err = std::string(#call) + ": " + cudaGetErrorString(e_);                             \
+      return CCS_E_CUDA;                                                                         \
+    }                                                                                            \
+  } while (0)
+
+template <class T>
+int dev_alloc(ccs_handle *h, T **p, size_t count) {
+  if (*p) { cudaFree(*p); *p = nullptr; }
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void **)p, sizeof(T) * count);
+  if (e != cudaSuccess) {
+    h->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    *p = nullptr;
+    return CCS_E_NOMEM;
+  }
+  return CCS_OK;
+}
+
+template <class T>
+void dev_free(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+int check_launch(ccs_handle *h) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    h->err = std::string("kernel launch: ") + cudaGetErrorString(e);
+    return CCS_E_CUDA;
+  }
+  return CCS_OK;
+}
+
+// the kernels' status word, read where the host synchronises anyway
+int check_status(ccs_handle *h) {
+  if (!h->status) return CCS_OK;
+  unsigned st = 0;
+  cudaError_t e = cudaMemcpy(&st, h->status, sizeof st, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    h->err = std::string("status read: ") + cudaGetErrorString(e);
+    return CCS_E_CUDA;
+  }
+  if (st & kStatusGrid) {
+    h->err = "contact grid: an insertion gave up after its retry bound (a degenerate pile of particles, "
+             "e.g. non-finite positions)";
+    return CCS_E_KERNEL;
+  }
+  return CCS_OK;
+}
+
+// setStaticUniforms, src/nbody.js:255-336: every per-run value rounded to binary32
+void make_static(ccs_handle *h) {
+  const ccs_sim &s = h->sim;
+  ccs_uniforms &u = h->stat;
+  std::memset(&u, 0, sizeof u);
+  u.N = s.N;
+  u.W = s.W;
+  u.G = s.G;
+  u.SX = s.G == 128 ? 16 : 8;
+  u.GShift = s.G == 128 ? 7 : 6;
+  u.SXShift = u.SX == 16 ? 4 : 3;
+  u.GMask = u.G - 1;
+  u.SXMask = u.SX - 1;
+  u.AW = u.SX * u.G;
+  u.AH = (u.G / u.SX) * u.G;
+  u.invCell = (float)(1.0 / s.cell);
+  u.cell = (float)s.cell;
+  u.link2 = (float)(s.cell * s.cell);
+  u.reach2 = (float)std::pow(s.cell + kSeatSlack * s.a, 2);
+  u.touch = (float)(2 * s.a);
+  u.K = (float)s.k;
+  u.C = (float)s.c;
+  u.invM = (float)(1.0 / s.m);
+  u.damp = (float)s.damp;
+  u.creep = (float)s.creep;
+  u.tK = (float)s.tK;
+  u.kappa = (float)s.kappa;
+  u.cpIron = (float)(kCpIron / kCpRock);
+  u.dt = (float)s.dt;
+  for (int k = 0; k < 3; ++k) {
+    u.spin0[k] = (float)s.spin0[k];
+    u.spin1[k] = (float)s.spin1[k];
+  }
+  u.invH = (float)(1.0 / kFH);
+  u.eps2Mesh = (float)(kFH * kFH);
+  u.eps2Cell = (float)(0.5 * kFH * kFH);
+  u.Gm = (float)s.m;
+  u.cut = (float)kPPCut;
+  u.a2 = (float)(s.a * s.a);
+}
+
+// boxes(), src/nbody.js:342-350
+void set_boxes(ccs_handle *h) {
+  const ccs_sim &s = h->sim;
+  for (int i = 0; i < 2; ++i) {
+    const double dt = s.t - s.boxT[i];
+    float *L = i ? h->LB : h->LA;
+    for (int k = 0; k < 3; ++k) L[k] = (float)(kFL - s.boxCen[i][k] - s.boxVel[i][k] * dt);
+  }
+  h->boxB = s.boxOn[1] ? 1.0f : 0.0f;
+}
+
+// the uniforms of one pass: statics + the boxes as last set + passSim's own
+ccs_uniforms pass_uniforms(const ccs_handle *h, int settle, int kick, double gdt) {
+  ccs_uniforms u = h->stat;
+  std::memcpy(u.LA, h->LA, sizeof u.LA);
+  std::memcpy(u.LB, h->LB, sizeof u.LB);
+  u.boxB = h->boxB;
+  u.settle = settle ? 1.0f : 0.0f;
+  u.kick = kick ? 1.0f : 0.0f;
+  u.gdt = (float)gdt;
+  for (int k = 0; k < 3; ++k) {
+    u.bulk0[k] = (float)h->sim.bulk0[k];
+    u.bulk1[k] = (float)h->sim.bulk1[k];
+    u.cen0[k] = (float)h->sim.cen0[k];
+    u.cen1[k] = (float)h->sim.cen1[k];
+  }
+  u.ppCount = h->ppCount;
+  return u;
+}
+
+// soften(), src/nbody.js:545-550
+void soften(ccs_handle *h) {
+  ccs_sim &s = h->sim;
+  s.soft = 1;
+  s.k *= 0.5;
+  s.c *= std::sqrt(0.5);
+  s.dt *= std::sqrt(2.0);
+  s.damp = std::exp(-s.dt * 12);
+  make_static(h);
+}
+
+// a ring slot holding u on the device (direct path)
+int push_uniforms(ccs_handle *h, const ccs_uniforms &u, const ccs_uniforms **dev) {
+  const int slot = h->uniNext;
+  h->uniNext = (h->uniNext + 1) % kRing;
+  if (h->uniUsed[slot]) CUDA_TRY(h, cudaEventSynchronize(h->uniEv[slot]));
+  h->uniHost[slot] = u;
+  CUDA_TRY(h, cudaMemcpyAsync(h->uniDev + slot, h->uniHost + slot, sizeof(ccs_uniforms), cudaMemcpyHostToDevice,
+                              h->st));
+  CUDA_TRY(h, cudaEventRecord(h->uniEv[slot], h->st));
+  h->uniUsed[slot] = true;
+  *dev = h->uniDev + slot;
+  return CCS_OK;
+}
+
+// timing brackets around chosen kernels
+void time_begin(ccs_handle *h, int kernel, cudaEvent_t *b, cudaEvent_t *e) {
+  *b = *e = nullptr;
+  if (!h->timing) return;
+  if (h->evNext + 2 > h->evPool.size()) {
+    for (int k = 0; k < 256; ++k) {
+      cudaEvent_t ev;
+      if (cudaEventCreate(&ev) == cudaSuccess) h->evPool.push_back(ev);
+    }
+  }
+  if (h->evNext + 2 > h->evPool.size()) return;
+  *b = h->evPool[h->evNext++];
+  *e = h->evPool[h->evNext++];
+  cudaEventRecord(*b, h->st);
+  h->evRecs.push_back({kernel, {*b, *e}});
+}
+void time_end(ccs_handle *h, cudaEvent_t e) {
+  if (e) cudaEventRecord(e, h->st);
+}
+void time_collect(ccs_handle *h) {
+  if (h->evRecs.empty()) return;
+  cudaStreamSynchronize(h->st);
+  for (auto &r : h->evRecs) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, r.second.first, r.second.second) == cudaSuccess) {
+      h->tAcc[r.first] += ms;
+      h->tCount[r.first] += 1;
+    }
+  }
+  h->evRecs.clear();
+  h->evNext = 0;
+}
+
+// ---- the passes, each enqueued on h->st reading uniforms at U ----
+
+void pass_slots(ccs_handle *h, const ccs_uniforms *U) {
+  const int nxt = h->seatCur ^ 1;
+  cudaEvent_t b, e;
+  time_begin(h, 1, &b, &e);
+  h->launches += launch_contact_grid(U, h->N, h->pos[h->cur], h->seats[nxt], h->hk[nxt], h->seats[h->seatCur],
+                                     h->hk[h->seatCur], h->status, h->st);
+  time_end(h, e);
+  h->seatCur = nxt;
+}
+
+void pass_mesh_box(ccs_handle *h, const ccs_uniforms *U, int b) {
+  MeshBuf &m = h->pm[b];
+  cudaMemsetAsync(m.fine, 0, sizeof(float4) * (kFine + 1), h->st);
+  cudaEvent_t eb, ee;
+  time_begin(h, 2, &eb, &ee);
+  h->launches += launch_deposit(U, h->N, b, h->pos[h->cur], h->mat, m.mono, m.fine, h->st);
+  time_end(h, ee);
+  h->launches += launch_coarse(m, h->st);
+  h->launches += launch_far(m, h->st);
+  time_begin(h, 3, &eb, &ee);
+  h->launches += launch_cell(U, m, h->st);
+  time_end(h, ee);
+}
+
+void pass_mesh(ccs_handle *h, const ccs_uniforms *U, int boxB) {
+  pass_mesh_box(h, U, 0);
+  if (boxB) pass_mesh_box(h, U, 1);
+}
+
+void pass_pp(ccs_handle *h, const ccs_uniforms *U, int count) {
+  if (!count) return;
+  h->launches += launch_pp_gather(U, h->pos[h->cur], h->mat, h->ppIndex, CCS_PP_CAP, h->ppList, h->ppBox, h->st);
+  cudaEvent_t b, e;
+  time_begin(h, 4, &b, &e);
+  h->launches += launch_pp_force(U, h->ppList, h->ppBox, CCS_PP_CAP, h->tab, h->ppForce, h->st);
+  time_end(h, e);
+}
+
+void pass_sim(ccs_handle *h, const ccs_uniforms *U) {
+  const int s = h->cur, d = h->cur ^ 1;
+  SimArgs a;
+  a.pos = h->pos[s];
+  a.vel = h->vel[s];
+  a.mat = h->mat;
+  a.q = h->q[s];
+  a.seats = h->seats[h->seatCur];
+  a.forceA = h->pm[0].force;
+  a.monoA = h->pm[0].mono;
+  a.forceB = h->pm[1].force;
+  a.monoB = h->pm[1].mono;
+  a.ppSlot = h->ppSlot;
+  a.ppForce = h->ppForce;
+  a.cap = CCS_PP_CAP;
+  a.posO = h->pos[d];
+  a.velO = h->vel[d];
+  a.auxO = h->aux[d];
+  a.qO = h->q[d];
+  cudaEvent_t b, e;
+  time_begin(h, 0, &b, &e);
+  h->launches += launch_simulate(U, h->N, a, h->st);
+  time_end(h, e);
+  h->cur = d;
+}
+
+void pass_diag_kernel(ccs_handle *h, const ccs_uniforms *U) {
+  DiagArgs a;
+  a.pos = h->pos[h->cur];
+  a.q = h->q[h->cur];
+  a.seats = h->seats[h->seatCur];
+  a.forceA = h->pm[0].force;
+  a.monoA = h->pm[0].mono;
+  a.forceB = h->pm[1].force;
+  a.monoB = h->pm[1].mono;
+  a.ppSlot = h->ppSlot;
+  a.ppForce = h->ppForce;
+  a.cap = CCS_PP_CAP;
+  a.diag = h->diag;
+  h->launches += launch_diag(U, h->N, a, h->st);
+}
+
+// the step's schedule decided on the host (src/nbody.js:551-558); returns the
+// uniforms of this step and what the step runs
+struct StepPlan {
+  ccs_uniforms u;
+  bool slots, mesh;
+};
+StepPlan plan_step(ccs_handle *h, int settle, int kick) {
+  ccs_sim &s = h->sim;
+  if (!settle && !kick && !s.soft && s.t - s.impactT > 1.5) soften(h);
+  const int n = s.stepNo++;
+  StepPlan p;
+  p.slots = n % 2 == 0;
+  p.mesh = n % h->meshEvery == 0;
+  if (p.mesh) set_boxes(h);
+  p.u = pass_uniforms(h, settle, kick, p.mesh ? h->meshEvery * s.dt : 0.0);
+  return p;
+}
+
+void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
+  if (p.slots) pass_slots(h, U);
+  if (p.mesh) {
+    pass_mesh(h, U, p.u.boxB > 0.5f);
+    pass_pp(h, U, p.u.ppCount);
+  }
+  pass_sim(h, U);
+}
+
+int do_step(ccs_handle *h, int settle, int kick) {
+  StepPlan p = plan_step(h, settle, kick);
+  const ccs_uniforms *U;
+  int rc = push_uniforms(h, p.u, &U);
+  if (rc) return rc;
+  enqueue_step(h, p, U);
+  return check_launch(h);
+}
+
+void free_graphs(ccs_handle *h) {
+  for (auto &kv : h->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.dev) cudaFree(kv.second.dev);
+    if (kv.second.host) cudaFreeHost(kv.second.host);
+    if (kv.second.done) cudaEventDestroy(kv.second.done);
+  }
+  h->graphs.clear();
+}
+
+// one block of meshEvery frame-loop steps, starting at stepNo % meshEvery == 0,
+// replayed from a captured graph
+int graph_block(ccs_handle *h) {
+  const int M = h->meshEvery;
+  GraphKey key{(int)(h->boxB > 0.5f), h->ppCount > 0, h->seatCur, h->cur, M, h->ping};
+  // plan the block's steps on the host (the boxes are set at its first step)
+  ccs_uniforms us[kMaxBlock];
+  StepPlan plans[kMaxBlock];
+  for (int k = 0; k < M; ++k) {
+    plans[k] = plan_step(h, 0, 0);
+    us[k] = plans[k].u;
+    h->sim.t += h->sim.dt;   // the frame loop's clock, index.html:372
+  }
+  key.boxB = (int)(us[0].boxB > 0.5f);
+  GraphSlot &g = h->graphs[key];
+  const int seatCur0 = h->seatCur, cur0 = h->cur;
+  if (!g.exec) {
+    CUDA_TRY(h, cudaMalloc(&g.dev, sizeof(ccs_uniforms) * M));
+    CUDA_TRY(h, cudaMallocHost(&g.host, sizeof(ccs_uniforms) * M));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+    std::memcpy(g.host, us, sizeof(ccs_uniforms) * M);
+    cudaGraph_t graph;
+    const bool timing = h->timing;
+    h->timing = false;
+    const int64_t l0 = h->launches;
+    CUDA_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(g.dev, g.host, sizeof(ccs_uniforms) * M, cudaMemcpyHostToDevice, h->st);
+    for (int k = 0; k < M; ++k) enqueue_step(h, plans[k], g.dev + k);
+    cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
+    h->timing = timing;
+    h->launches = l0;
+    if (ce != cudaSuccess) {
+      h->err = std::string("graph capture: ") + cudaGetErrorString(ce);
+      return CCS_E_CUDA;
+    }
+    ce = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) {
+      h->err = std::string("graph instantiate: ") + cudaGetErrorString(ce);
+      g.exec = nullptr;
+      return CCS_E_CUDA;
+    }
+    // capture ran the buffer rotation once on the host; restore it for the replay
+    h->seatCur = seatCur0;
+    h->cur = cur0;
+  }
+  if (g.used) CUDA_TRY(h, cudaEventSynchronize(g.done));
+  std::memcpy(g.host, us, sizeof(ccs_uniforms) * M);
+  CUDA_TRY(h, cudaGraphLaunch(g.exec, h->st));
+  CUDA_TRY(h, cudaEventRecord(g.done, h->st));
+  g.used = true;
+  h->ping ^= 1;
+  // a block does 4 grid rebuilds (the table parity returns) and M swaps
+  h->cur = cur0 ^ (M & 1);
+  h->seatCur = seatCur0 ^ (((M + 1) / 2) & 1);
+  // count the block's launches as the direct path would
+  int per = 0;
+  for (int k = 0; k < M; ++k) {
+    per += 1;                                   // simulate
+    if (plans[k].slots) per += 1;               // contact grid
+    if (plans[k].mesh) {
+      per += 4 * (1 + (us[k].boxB > 0.5f));     // deposit, coarse, far, cell per box
+      if (us[k].ppCount) per += 2;              // gather, force
+    }
+  }
+  h->launches += per;
+  return CCS_OK;
+}
+
+int ensure_built(ccs_handle *h) {
+  if (!h || !h->built) {
+    if (h) h->err = "no run built (ccs_build)";
+    return CCS_E_STATE;
+  }
+  return CCS_OK;
+}
+
+void free_state(ccs_handle *h) {
+  free_graphs(h);
+  for (int b = 0; b < 2; ++b) {
+    dev_free(h->pos[b]); dev_free(h->vel[b]); dev_free(h->aux[b]); dev_free(h->q[b]);
+    dev_free(h->seats[b]); dev_free(h->hk[b]);
+    MeshBuf &m = h->pm[b];
+    dev_free(m.fine); dev_free(m.force); dev_free(m.coarse); dev_free(m.farA); dev_free(m.farT0);
+    dev_free(m.farT1); dev_free(m.mono); dev_free(m.partial); dev_free(m.counter);
+  }
+  dev_free(h->mat); dev_free(h->matTmp); dev_free(h->home); dev_free(h->homeTmp);
+  dev_free(h->ppIndex); dev_free(h->ppSlot); dev_free(h->ppList); dev_free(h->ppForce); dev_free(h->ppBox);
+  dev_free(h->tab); dev_free(h->diag);
+  dev_free(h->keys); dev_free(h->keysTmp); dev_free(h->hist); dev_free(h->vals); dev_free(h->valsTmp);
+  dev_free(h->into); dev_free(h->permDev);
+  dev_free(h->booksPartial); dev_free(h->booksOut); dev_free(h->status);
+  if (h->stageP) cudaFreeHost(h->stageP);
+  if (h->stageV) cudaFreeHost(h->stageV);
+  if (h->stageD) cudaFreeHost(h->stageD);
+  h->stageP = h->stageV = h->stageD = nullptr;
+  h->built = false;
+  h->pending = false;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int ccs_version(void) { return 1; }
+
+const char *ccs_last_error(const ccs_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int ccs_create(int device, ccs_handle **out) {
+  if (!out) return CCS_E_ARG;
+  *out = nullptr;
+  ccs_handle *h = new (std::nothrow) ccs_handle();
+  if (!h) return CCS_E_NOMEM;
+  h->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return CCS_E_CUDA;
+  }
+  if (cudaMalloc(&h->uniDev, sizeof(ccs_uniforms) * kRing) != cudaSuccess ||
+      cudaMallocHost(&h->uniHost, sizeof(ccs_uniforms) * kRing) != cudaSuccess) {
+    cudaStreamDestroy(h->st);
+    delete h;
+    return CCS_E_NOMEM;
+  }
+  for (int k = 0; k < kRing; ++k) cudaEventCreateWithFlags(&h->uniEv[k], cudaEventDisableTiming);
+  if (init_kernels() != cudaSuccess) {
+    h->err = "kernel attributes could not be set";
+  }
+  cudaEventCreateWithFlags(&h->readEv, cudaEventDisableTiming);
+  *out = h;
+  return CCS_OK;
+}
+
+int ccs_destroy(ccs_handle *h) {
+  if (!h) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->st);
+  free_state(h);
+  for (int k = 0; k < kRing; ++k)
+    if (h->uniEv[k]) cudaEventDestroy(h->uniEv[k]);
+  for (auto ev : h->evPool) cudaEventDestroy(ev);
+  if (h->readEv) cudaEventDestroy(h->readEv);
+  if (h->uniDev) cudaFree(h->uniDev);
+  if (h->uniHost) cudaFreeHost(h->uniHost);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+  return CCS_OK;
+}
+
+int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float *vel4, const float *mat,
+              const float *home4) {
+  if (!h || !sim || !pos4 || !vel4 || !mat) return CCS_E_ARG;
+  if (sim->N <= 0 || sim->N > CCS_MAX_N) {
+    h->err = "N must be in 1..262144 (the 18-bit seat index)";
+    return CCS_E_RANGE;
+  }
+  if (sim->G != 64 && sim->G != 128) {
+    h->err = "G must be 64 or 128";
+    return CCS_E_ARG;
+  }
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->st);
+  free_state(h);
+  h->sim = *sim;
+  h->N = sim->N;
+  const size_t N = (size_t)h->N;
+  int rc = 0;
+  for (int b = 0; b < 2; ++b) {
+    rc |= dev_alloc(h, &h->pos[b], N); rc |= dev_alloc(h, &h->vel[b], N);
+    rc |= dev_alloc(h, &h->aux[b], N); rc |= dev_alloc(h, &h->q[b], N);
+  }
+  rc |= dev_alloc(h, &h->mat, N); rc |= dev_alloc(h, &h->matTmp, N);
+  rc |= dev_alloc(h, &h->home, N); rc |= dev_alloc(h, &h->homeTmp, N);
+  make_static(h);
+  h->ncell = (size_t)h->stat.AW * (size_t)h->stat.AH;
+  for (int b = 0; b < 2; ++b) {
+    rc |= dev_alloc(h, &h->seats[b], h->ncell * kSeats);
+    rc |= dev_alloc(h, &h->hk[b], N);
+    MeshBuf &m = h->pm[b];
+    rc |= dev_alloc(h, &m.fine, kFine + 1); rc |= dev_alloc(h, &m.force, kFine + 1);
+    rc |= dev_alloc(h, &m.coarse, kCoarse); rc |= dev_alloc(h, &m.farA, kCoarse);
+    rc |= dev_alloc(h, &m.farT0, kCoarse); rc |= dev_alloc(h, &m.farT1, kCoarse);
+    rc |= dev_alloc(h, &m.mono, 1); rc |= dev_alloc(h, &m.partial, 64); rc |= dev_alloc(h, &m.counter, 1);
+  }
+  rc |= dev_alloc(h, &h->ppIndex, CCS_PP_CAP); rc |= dev_alloc(h, &h->ppSlot, N);
+  rc |= dev_alloc(h, &h->ppList, CCS_PP_CAP); rc |= dev_alloc(h, &h->ppForce, 4 * CCS_PP_CAP);
+  rc |= dev_alloc(h, &h->ppBox, CCS_PP_CAP); rc |= dev_alloc(h, &h->tab, CCS_PP_BINS);
+  rc |= dev_alloc(h, &h->diag, N);
+  rc |= dev_alloc(h, &h->keys, N); rc |= dev_alloc(h, &h->keysTmp, N); rc |= dev_alloc(h, &h->vals, N);
+  rc |= dev_alloc(h, &h->valsTmp, N); rc |= dev_alloc(h, &h->into, N); rc |= dev_alloc(h, &h->permDev, N);
+  rc |= dev_alloc(h, &h->hist, radix_hist_words(h->N));
+  rc |= dev_alloc(h, &h->booksPartial, books_partial_doubles(h->N));
+  rc |= dev_alloc(h, &h->booksOut, CCS_BOOKS);
+  rc |= dev_alloc(h, &h->status, 1);
+  if (rc) { free_state(h); return CCS_E_NOMEM; }
+  if (cudaMallocHost(&h->stageP, 16 * N) != cudaSuccess || cudaMallocHost(&h->stageV, 16 * N) != cudaSuccess ||
+      cudaMallocHost(&h->stageD, 16 * N) != cudaSuccess) {
+    free_state(h);
+    h->err = "pinned staging allocation failed";
+    return CCS_E_NOMEM;
+  }
+  cudaStream_t st = h->st;
+  CUDA_TRY(h, cudaMemcpyAsync(h->pos[0], pos4, 16 * N, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(h, cudaMemcpyAsync(h->vel[0], vel4, 16 * N, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(h, cudaMemcpyAsync(h->mat, mat, 4 * N, cudaMemcpyHostToDevice, st));
+  if (home4) CUDA_TRY(h, cudaMemcpyAsync(h->home, home4, 16 * N, cudaMemcpyHostToDevice, st));
+  else CUDA_TRY(h, cudaMemsetAsync(h->home, 0, 16 * N, st));
+  for (int b = 0; b < 2; ++b) {
+    CUDA_TRY(h, cudaMemsetAsync(h->aux[b], 0, 16 * N, st));
+    CUDA_TRY(h, cudaMemsetAsync(h->q[b], 0, 4 * N, st));
+    if (b) {
+      CUDA_TRY(h, cudaMemsetAsync(h->pos[b], 0, 16 * N, st));
+      CUDA_TRY(h, cudaMemsetAsync(h->vel[b], 0, 16 * N, st));
+    }
+    h->launches += launch_fill_u32(h->seats[b], h->ncell * kSeats, kEmpty, st);
+    h->launches += launch_fill_u32(h->hk[b], N, kNoCell, st);
+    MeshBuf &m = h->pm[b];
+    CUDA_TRY(h, cudaMemsetAsync(m.fine, 0, sizeof(float4) * (kFine + 1), st));
+    CUDA_TRY(h, cudaMemsetAsync(m.force, 0, sizeof(float4) * (kFine + 1), st));
+    CUDA_TRY(h, cudaMemsetAsync(m.coarse, 0, sizeof(float4) * kCoarse, st));
+    CUDA_TRY(h, cudaMemsetAsync(m.farA, 0, sizeof(float4) * kCoarse, st));
+    CUDA_TRY(h, cudaMemsetAsync(m.farT0, 0, sizeof(float4) * kCoarse, st));
+    CUDA_TRY(h, cudaMemsetAsync(m.farT1, 0, sizeof(float4) * kCoarse, st));
+    CUDA_TRY(h, cudaMemsetAsync(m.mono, 0, sizeof(float4), st));
+    CUDA_TRY(h, cudaMemsetAsync(m.counter, 0, sizeof(unsigned), st));
+  }
+  h->launches += launch_fill_u32((uint32_t *)h->ppIndex, CCS_PP_CAP, 0xFFFFFFFFu, st);
+  h->launches += launch_fill_u32((uint32_t *)h->ppSlot, N, 0xFFFFFFFFu, st);
+  CUDA_TRY(h, cudaMemsetAsync(h->ppList, 0, sizeof(float4) * CCS_PP_CAP, st));
+  CUDA_TRY(h, cudaMemsetAsync(h->ppForce, 0, sizeof(float4) * 4 * CCS_PP_CAP, st));
+  CUDA_TRY(h, cudaMemsetAsync(h->ppBox, 0, sizeof(float) * CCS_PP_CAP, st));
+  CUDA_TRY(h, cudaMemsetAsync(h->booksPartial, 0, sizeof(double) * books_partial_doubles(h->N), st));
+  CUDA_TRY(h, cudaMemsetAsync(h->status, 0, sizeof(unsigned), st));
+  float f[CCS_PP_BINS], p[CCS_PP_BINS];
+  ccs_pair_table(CCS_PP_BINS, kPPCut, f, p);
+  float2 tab[CCS_PP_BINS];
+  for (int k = 0; k < CCS_PP_BINS; ++k) tab[k] = make_float2(f[k], p[k]);
+  CUDA_TRY(h, cudaMemcpyAsync(h->tab, tab, sizeof tab, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  h->cur = 0;
+  h->seatCur = 0;
+  h->ppCount = h->ppLoose = 0;
+  h->LA[0] = h->LA[1] = h->LA[2] = 0;
+  h->LB[0] = h->LB[1] = h->LB[2] = 0;
+  h->boxB = 0;
+  h->built = true;
+  return check_launch(h);
+}
+
+ccs_sim *ccs_sim_ptr(ccs_handle *h) { return h ? &h->sim : nullptr; }
+
+int ccs_set_static(ccs_handle *h) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  make_static(h);
+  return CCS_OK;
+}
+
+int ccs_get_uniforms(ccs_handle *h, ccs_uniforms *out) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!out) return CCS_E_ARG;
+  *out = pass_uniforms(h, 0, 0, 0.0);
+  return CCS_OK;
+}
+
+int ccs_set_mesh_every(ccs_handle *h, int n) {
+  if (!h || n < 1 || n > kMaxBlock) return CCS_E_ARG;
+  h->meshEvery = n;
+  return CCS_OK;
+}
+
+int ccs_step(ccs_handle *h, int settle, int kick) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  return do_step(h, settle, kick);
+}
+
+int ccs_steps(ccs_handle *h, int n) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (n < 0) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  while (n > 0) {
+    const bool aligned = h->sim.stepNo % h->meshEvery == 0;
+    const bool graphOk = h->useGraphs && !h->timing && aligned && n >= h->meshEvery && h->meshEvery % 2 == 0;
+    if (graphOk) {
+      rc = graph_block(h);
+      if (rc) return rc;
+      n -= h->meshEvery;
+    } else {
+      rc = do_step(h, 0, 0);
+      if (rc) return rc;
+      h->sim.t += h->sim.dt;
+      --n;
+    }
+  }
+  return check_launch(h);
+}
+
+int ccs_settle_some(ccs_handle *h, int n) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (n < 0) return CCS_E_ARG;
+  ccs_sim &s = h->sim;
+  n = n < s.settleLeft ? n : s.settleLeft;
+  for (int i = 0; i < n; ++i) {
+    rc = do_step(h, 1, 0);
+    if (rc) return rc;
+  }
+  s.settleLeft -= n;
+  if (s.settleLeft == 0 && s.phase == 0) s.phase = 1;
+  return CCS_OK;
+}
+
+static void turn_matrix(const double w[3], double dt, float o[9]) {
+  const double m = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  if (m < 1e-12) {
+    const float I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    std::memcpy(o, I, sizeof I);
+    return;
+  }
+  const double x = w[0] / m, y = w[1] / m, z = w[2] / m, th = m * dt, c = std::cos(th), s = std::sin(th), t = 1 - c;
+  const double r[9] = {t * x * x + c,     t * x * y + s * z, t * x * z - s * y,
+                       t * x * y - s * z, t * y * y + c,     t * y * z + s * x,
+                       t * x * z + s * y, t * y * z - s * x, t * z * z + c};
+  for (int k = 0; k < 9; ++k) o[k] = (float)r[k];
+}
+
+int ccs_rigid_step(ccs_handle *h, double dtF) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!(dtF > 0)) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  ccs_sim &s = h->sim;
+  double *r = s.relr, *v = s.relv;
+  const double M = s.M, M1 = s.M1, M2 = s.M2;
+  const double r0[3] = {r[0], r[1], r[2]};
+  const int n = 8;
+  const double hh = dtF / n;
+  double a[3];
+  auto acc = [&]() {
+    const double d2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    const double f = -M * std::pow(d2, -1.5);
+    a[0] = r[0] * f; a[1] = r[1] * f; a[2] = r[2] * f;
+  };
+  const double cen[2][3] = {{-r0[0] * M2 / M, -r0[1] * M2 / M, -r0[2] * M2 / M},
+                            {r0[0] * M1 / M, r0[1] * M1 / M, r0[2] * M1 / M}};
+  acc();
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) v[k] += a[k] * hh * 0.5;
+    for (int k = 0; k < 3; ++k) r[k] += v[k] * hh;
+    acc();
+    for (int k = 0; k < 3; ++k) v[k] += a[k] * hh * 0.5;
+  }
+  const double mv[3] = {(r[0] - r0[0]) / dtF, (r[1] - r0[1]) / dtF, (r[2] - r0[2]) / dtF};
+  for (int k = 0; k < 3; ++k) {
+    s.bulk0[k] = -mv[k] * M2 / M;
+    s.bulk1[k] = mv[k] * M1 / M;
+  }
+  ccs_uniforms u = pass_uniforms(h, 0, 0, 0.0);
+  for (int k = 0; k < 3; ++k) {
+    u.cen0[k] = (float)cen[0][k];
+    u.cen1[k] = (float)cen[1][k];
+  }
+  turn_matrix(s.spin0, dtF, u.rot0);
+  turn_matrix(s.spin1, dtF, u.rot1);
+  u.rdt = (float)dtF;
+  const ccs_uniforms *U;
+  rc = push_uniforms(h, u, &U);
+  if (rc) return rc;
+  const int src = h->cur, dst = h->cur ^ 1;
+  h->launches += launch_rigid(U, h->N, h->pos[src], h->vel[src], h->aux[src], h->q[src], h->pos[dst], h->vel[dst],
+                              h->aux[dst], h->q[dst], h->st);
+  h->cur = dst;
+  s.t += dtF;
+  if (std::hypot(std::hypot(r[0], r[1]), r[2]) <= s.Re1 + s.Re2 + 2 * s.a) {   // the equators touch
+    for (int k = 0; k < 3; ++k) {
+      s.bulk0[k] = -v[k] * M2 / M;
+      s.bulk1[k] = v[k] * M1 / M;
+      s.cen0[k] = -r[k] * M2 / M;
+      s.cen1[k] = r[k] * M1 / M;
+      s.boxCen[0][k] = s.cen0[k];
+      s.boxVel[0][k] = s.bulk0[k];
+    }
+    s.boxOn[0] = 1;
+    s.boxT[0] = s.t;
+    s.boxOn[1] = 0;
+    s.stepNo = 0;
+    rc = do_step(h, 0, 1);
+    if (rc) return rc;
+    s.t += s.dt;
+    s.phase = 2;
+    s.impactT = s.t;
+  }
+  return check_launch(h);
+}
+
+int ccs_set_pp(ccs_handle *h, const int32_t *list, int n, int loose) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (n < 0 || n > CCS_PP_CAP || (n > 0 && !list)) return CCS_E_ARG;
+  for (int k = 0; k < n; ++k)
+    if (list[k] < 0 || list[k] >= h->N) {
+      h->err = "loose-list index out of range";
+      return CCS_E_ARG;
+    }
+  cudaSetDevice(h->device);
+  std::vector<int32_t> slot((size_t)h->N, -1), index(CCS_PP_CAP, -1);
+  for (int k = 0; k < n; ++k) {
+    slot[(size_t)list[k]] = k;
+    index[(size_t)k] = list[k];
+  }
+  // synchronous copies: the vectors die with this call
+  CUDA_TRY(h, cudaMemcpyAsync(h->ppSlot, slot.data(), 4 * (size_t)h->N, cudaMemcpyHostToDevice, h->st));
+  CUDA_TRY(h, cudaMemcpyAsync(h->ppIndex, index.data(), 4 * (size_t)CCS_PP_CAP, cudaMemcpyHostToDevice, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  h->ppCount = n;
+  h->ppLoose = loose;
+  if (n) {
+    const ccs_uniforms *U;
+    rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+    if (rc) return rc;
+    pass_pp(h, U, n);
+  }
+  return check_launch(h);
+}
+
+int ccs_prime_mono(ccs_handle *h, int box, const float mono[4]) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (box < 0 || box > 1 || !mono) return CCS_E_ARG;
+  float4 m = make_float4(mono[0], mono[1], mono[2], mono[3]);
+  CUDA_TRY(h, cudaMemcpyAsync(h->pm[box].mono, &m, sizeof m, cudaMemcpyHostToDevice, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  return CCS_OK;
+}
+
+static int apply_perm_device(ccs_handle *h, const int32_t *permDev) {
+  const int s = h->cur, d = h->cur ^ 1;
+  h->launches += launch_permute(h->N, permDev, h->pos[s], h->vel[s], h->aux[s], h->q[s], h->mat, h->home, h->pos[d],
+                                h->vel[d], h->aux[d], h->q[d], h->matTmp, h->homeTmp, h->st);
+  std::swap(h->mat, h->matTmp);
+  std::swap(h->home, h->homeTmp);
+  h->cur = d;
+  // the old cells name particles by their old places: fresh ones
+  const ccs_uniforms *U;
+  int rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+  if (rc) return rc;
+  pass_slots(h, U);
+  return check_launch(h);
+}
+
+int ccs_apply_perm(ccs_handle *h, const int32_t *perm) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!perm) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  std::vector<char> seen((size_t)h->N, 0);
+  for (int i = 0; i < h->N; ++i) {
+    if (perm[i] < 0 || perm[i] >= h->N || seen[(size_t)perm[i]]) {
+      h->err = "perm is not a permutation of 0..N-1";
+      return CCS_E_ARG;
+    }
+    seen[(size_t)perm[i]] = 1;
+  }
+  CUDA_TRY(h, cudaMemcpyAsync(h->permDev, perm, 4 * (size_t)h->N, cudaMemcpyHostToDevice, h->st));
+  rc = apply_perm_device(h, h->permDev);
+  if (rc) return rc;
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  return CCS_OK;
+}
+
+int ccs_sort_morton(ccs_handle *h, const double core[3], int32_t *perm_out, int32_t *into_out) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!core) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  const int N = h->N;
+  h->launches += launch_morton_keys(N, h->pos[h->cur], core[0], core[1], core[2], h->keys, h->vals, h->st);
+  h->launches += launch_radix_sort(N, 21, h->keys, h->vals, h->keysTmp, h->valsTmp, h->hist, h->st);
+  CUDA_TRY(h, cudaMemcpyAsync(h->permDev, h->vals, 4 * (size_t)N, cudaMemcpyDeviceToDevice, h->st));
+  h->launches += launch_invert_perm(N, h->permDev, h->into, h->st);
+  if (perm_out) CUDA_TRY(h, cudaMemcpyAsync(perm_out, h->permDev, 4 * (size_t)N, cudaMemcpyDeviceToHost, h->st));
+  if (into_out) CUDA_TRY(h, cudaMemcpyAsync(into_out, h->into, 4 * (size_t)N, cudaMemcpyDeviceToHost, h->st));
+  rc = apply_perm_device(h, h->permDev);
+  if (rc) return rc;
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  return CCS_OK;
+}
+
+// passDiag, src/nbody.js:488-507
+static int diag_pass(ccs_handle *h) {
+  set_boxes(h);
+  const ccs_uniforms *U;
+  int rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+  if (rc) return rc;
+  pass_slots(h, U);
+  pass_mesh(h, U, h->boxB > 0.5f);
+  pass_pp(h, U, h->ppCount);
+  pass_diag_kernel(h, U);
+  return check_launch(h);
+}
+
+int ccs_diag_async(ccs_handle *h) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  rc = diag_pass(h);
+  if (rc) return rc;
+  const size_t b = 16 * (size_t)h->N;
+  CUDA_TRY(h, cudaMemcpyAsync(h->stageD, h->diag, b, cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaMemcpyAsync(h->stageP, h->pos[h->cur], b, cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaMemcpyAsync(h->stageV, h->vel[h->cur], b, cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaEventRecord(h->readEv, h->st));
+  h->pending = true;
+  return CCS_OK;
+}
+
+int ccs_poll(ccs_handle *h, float *P, float *V, float *D) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!h->pending) {
+    h->err = "no read-back pending";
+    return CCS_E_STATE;
+  }
+  const cudaError_t q = cudaEventQuery(h->readEv);
+  if (q == cudaErrorNotReady) return CCS_NOT_READY;
+  if (q != cudaSuccess) {
+    h->err = std::string("read-back: ") + cudaGetErrorString(q);
+    return CCS_E_CUDA;
+  }
+  const size_t b = 16 * (size_t)h->N;
+  if (P) std::memcpy(P, h->stageP, b);
+  if (V) std::memcpy(V, h->stageV, b);
+  if (D) std::memcpy(D, h->stageD, b);
+  h->pending = false;
+  return check_status(h);
+}
+
+int ccs_read_state(ccs_handle *h, float *pos4, float *vel4, float *aux4, float *q, float *mat) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  const size_t N = (size_t)h->N;
+  if (pos4) CUDA_TRY(h, cudaMemcpyAsync(pos4, h->pos[h->cur], 16 * N, cudaMemcpyDeviceToHost, h->st));
+  if (vel4) CUDA_TRY(h, cudaMemcpyAsync(vel4, h->vel[h->cur], 16 * N, cudaMemcpyDeviceToHost, h->st));
+  if (aux4) CUDA_TRY(h, cudaMemcpyAsync(aux4, h->aux[h->cur], 16 * N, cudaMemcpyDeviceToHost, h->st));
+  if (q) CUDA_TRY(h, cudaMemcpyAsync(q, h->q[h->cur], 4 * N, cudaMemcpyDeviceToHost, h->st));
+  if (mat) CUDA_TRY(h, cudaMemcpyAsync(mat, h->mat, 4 * N, cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  return check_status(h);
+}
+
+int ccs_write_state(ccs_handle *h, const float *pos4, const float *vel4, const float *aux4, const float *q,
+                    const float *mat) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  const size_t N = (size_t)h->N;
+  if (pos4) CUDA_TRY(h, cudaMemcpyAsync(h->pos[h->cur], pos4, 16 * N, cudaMemcpyHostToDevice, h->st));
+  if (vel4) CUDA_TRY(h, cudaMemcpyAsync(h->vel[h->cur], vel4, 16 * N, cudaMemcpyHostToDevice, h->st));
+  if (aux4) CUDA_TRY(h, cudaMemcpyAsync(h->aux[h->cur], aux4, 16 * N, cudaMemcpyHostToDevice, h->st));
+  if (q) CUDA_TRY(h, cudaMemcpyAsync(h->q[h->cur], q, 4 * N, cudaMemcpyHostToDevice, h->st));
+  if (mat) CUDA_TRY(h, cudaMemcpyAsync(h->mat, mat, 4 * N, cudaMemcpyHostToDevice, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  return CCS_OK;
+}
+
+int ccs_device_ptrs(ccs_handle *h, ccs_device_buffers *out) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!out) return CCS_E_ARG;
+  out->pos4 = h->pos[h->cur];
+  out->vel4 = h->vel[h->cur];
+  out->aux4 = h->aux[h->cur];
+  out->q = h->q[h->cur];
+  out->mat = h->mat;
+  out->home4 = h->home;
+  for (int b = 0; b < 2; ++b) {
+    out->force[b] = h->pm[b].force;
+    out->mono[b] = h->pm[b].mono;
+  }
+  out->stream = (void *)h->st;
+  return CCS_OK;
+}
+
+int ccs_books(ccs_handle *h, int with_diag, double out[CCS_BOOKS]) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!out) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  if (with_diag) {
+    rc = diag_pass(h);
+    if (rc) return rc;
+  }
+  h->launches += launch_books(h->N, h->sim.m, h->pos[h->cur], h->vel[h->cur], h->mat, h->diag, h->booksPartial,
+                              h->booksOut, with_diag, h->st);
+  CUDA_TRY(h, cudaMemcpyAsync(out, h->booksOut, sizeof(double) * CCS_BOOKS, cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  out[10] /= h->N;
+  out[11] /= h->N;
+  if (!with_diag) out[8] = out[9] = out[10] = out[11] = 0.0;
+  return check_launch(h);
+}
+
+int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!dst) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  const void *src = nullptr;
+  size_t n = 0;
+  const size_t N = (size_t)h->N;
+  switch (which) {
+    case CCS_BUF_SEATS: src = h->seats[h->seatCur]; n = 4 * h->ncell * kSeats; break;
+    case CCS_BUF_FINE_A: src = h->pm[0].fine; n = 16 * (size_t)(kFine + 1); break;
+    case CCS_BUF_FORCE_A: src = h->pm[0].force; n = 16 * (size_t)(kFine + 1); break;
+    case CCS_BUF_MONO_A: src = h->pm[0].mono; n = 16; break;
+    case CCS_BUF_COARSE_A: src = h->pm[0].coarse; n = 16 * (size_t)kCoarse; break;
+    case CCS_BUF_FAR_A: src = h->pm[0].farA; n = 16 * (size_t)kCoarse; break;
+    case CCS_BUF_FINE_B: src = h->pm[1].fine; n = 16 * (size_t)(kFine + 1); break;
+    case CCS_BUF_FORCE_B: src = h->pm[1].force; n = 16 * (size_t)(kFine + 1); break;
+    case CCS_BUF_MONO_B: src = h->pm[1].mono; n = 16; break;
+    case CCS_BUF_PP_LIST: src = h->ppList; n = 16 * (size_t)CCS_PP_CAP; break;
+    case CCS_BUF_PP_FORCE: src = h->ppForce; n = 64 * (size_t)CCS_PP_CAP; break;
+    case CCS_BUF_PP_BOX: src = h->ppBox; n = 4 * (size_t)CCS_PP_CAP; break;
+    case CCS_BUF_PP_SLOT: src = h->ppSlot; n = 4 * N; break;
+    case CCS_BUF_DIAG: src = h->diag; n = 16 * N; break;
+    case CCS_BUF_CELL_OF: src = h->hk[h->seatCur]; n = 4 * N; break;
+    default: h->err = "unknown buffer"; return CCS_E_ARG;
+  }
+  if (bytes != n) {
+    h->err = "buffer size mismatch: expected " + std::to_string(n);
+    return CCS_E_ARG;
+  }
+  CUDA_TRY(h, cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  return check_status(h);
+}
+
+int ccs_pass_slots(ccs_handle *h) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  const ccs_uniforms *U;
+  rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+  if (rc) return rc;
+  pass_slots(h, U);
+  return check_launch(h);
+}
+
+int ccs_pass_mesh(ccs_handle *h) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  set_boxes(h);
+  const ccs_uniforms *U;
+  rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+  if (rc) return rc;
+  pass_mesh(h, U, h->boxB > 0.5f);
+  return check_launch(h);
+}
+
+int ccs_pass_pp(ccs_handle *h) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  const ccs_uniforms *U;
+  rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+  if (rc) return rc;
+  pass_pp(h, U, h->ppCount);
+  return check_launch(h);
+}
+
+int ccs_pass_sim(ccs_handle *h, int settle, int kick, double gdt) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  const ccs_uniforms *U;
+  rc = push_uniforms(h, pass_uniforms(h, settle, kick, gdt), &U);
+  if (rc) return rc;
+  pass_sim(h, U);
+  return check_launch(h);
+}
+
+int ccs_pass_diag(ccs_handle *h) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  return diag_pass(h);
+}
+
+int ccs_advance_host(ccs_handle *h, const float *pos4, const float *vel4, const float *q, int nsteps, float *pos4_out,
+                     float *vel4_out, float *aux4_out, float *q_out) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (nsteps < 0) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  const size_t N = (size_t)h->N;
+  if (pos4) CUDA_TRY(h, cudaMemcpyAsync(h->pos[h->cur], pos4, 16 * N, cudaMemcpyHostToDevice, h->st));
+  if (vel4) CUDA_TRY(h, cudaMemcpyAsync(h->vel[h->cur], vel4, 16 * N, cudaMemcpyHostToDevice, h->st));
+  if (q) CUDA_TRY(h, cudaMemcpyAsync(h->q[h->cur], q, 4 * N, cudaMemcpyHostToDevice, h->st));
+  rc = ccs_steps(h, nsteps);
+  if (rc) return rc;
+  if (pos4_out) CUDA_TRY(h, cudaMemcpyAsync(pos4_out, h->pos[h->cur], 16 * N, cudaMemcpyDeviceToHost, h->st));
+  if (vel4_out) CUDA_TRY(h, cudaMemcpyAsync(vel4_out, h->vel[h->cur], 16 * N, cudaMemcpyDeviceToHost, h->st));
+  if (aux4_out) CUDA_TRY(h, cudaMemcpyAsync(aux4_out, h->aux[h->cur], 16 * N, cudaMemcpyDeviceToHost, h->st));
+  if (q_out) CUDA_TRY(h, cudaMemcpyAsync(q_out, h->q[h->cur], 4 * N, cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  return check_launch(h);
+}
+
+int ccs_sync(ccs_handle *h) {
+  if (!h) return CCS_E_ARG;
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  int rc = check_launch(h);
+  return rc ? rc : (h->built ? check_status(h) : CCS_OK);
+}
+
+int ccs_timing(ccs_handle *h, int enable) {
+  if (!h) return CCS_E_ARG;
+  time_collect(h);
+  h->timing = enable != 0;
+  for (int k = 0; k < kTimedKernels; ++k) {
+    h->tAcc[k] = 0;
+    h->tCount[k] = 0;
+  }
+  return CCS_OK;
+}
+
+int ccs_timing_read(ccs_handle *h, int kernel, double *total_ms, int *launches) {
+  if (!h || kernel < 0 || kernel >= kTimedKernels || !total_ms || !launches) return CCS_E_ARG;
+  time_collect(h);
+  *total_ms = h->tAcc[kernel];
+  *launches = h->tCount[kernel];
+  return CCS_OK;
+}
+
+int64_t ccs_launch_count(ccs_handle *h) { return h ? h->launches : -1; }
+
+}  // extern "C"

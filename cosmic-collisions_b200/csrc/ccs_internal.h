@@ -1,0 +1,91 @@
+// ccs_internal.h -- the handle and the kernel launchers shared by the API.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/ccstep.h"
+
+namespace ccs {
+
+constexpr uint32_t kEmpty = CCS_SEAT_EMPTY;   // -1.0f bit pattern: an empty seat
+constexpr uint32_t kNoCell = 0xFFFFFFFFu;     // no cell recorded for this particle
+constexpr int kFine = 64 * 64 * 64;           // 64^3 mesh; index kFine is the scratch texel
+constexpr int kCoarse = 4096;                 // 16^3 blocks
+constexpr int kSeats = CCS_SEATS;
+constexpr unsigned kStatusGrid = 1u;          // a contact-cell insertion gave up (degenerate pile)
+
+// One gravity mesh box: the textures of meshBox(), src/nbody.js:1050-1068,
+// as plain float4 arrays.  fine/force hold 64^3 cells in [z][y][x] order
+// plus the scratch texel at index 64^3 (the atlas row y = 512 of the reference).
+struct MeshBuf {
+  float4 *fine = nullptr, *force = nullptr;
+  float4 *coarse = nullptr, *farA = nullptr, *farT0 = nullptr, *farT1 = nullptr;
+  float4 *mono = nullptr;
+  float4 *partial = nullptr;   // per-block partial sums for the monopole
+  unsigned *counter = nullptr; // last-block-done counter of the coarse pass
+};
+
+// Arguments of the contact step (simFS, src/glsl-sim.js:354-512).
+struct SimArgs {
+  const float4 *pos, *vel;
+  const float *mat, *q;
+  const uint32_t *seats;
+  const float4 *forceA, *monoA, *forceB, *monoB;
+  const int *ppSlot;
+  const float4 *ppForce;
+  int cap;
+  float4 *posO, *velO, *auxO;
+  float *qO;
+};
+
+struct DiagArgs {
+  const float4 *pos;
+  const float *q;
+  const uint32_t *seats;
+  const float4 *forceA, *monoA, *forceB, *monoB;
+  const int *ppSlot;
+  const float4 *ppForce;
+  int cap;
+  float4 *diag;
+};
+
+// per-device kernel attributes (dynamic shared memory limits); call once per
+// device before the first launch and never during a stream capture
+cudaError_t init_kernels();
+
+// kernel launchers (ccs_kernels.cu); all enqueue on `st` and return the
+// number of kernels launched.
+int launch_fill_u32(uint32_t *p, size_t n, uint32_t v, cudaStream_t st);
+int launch_contact_grid(const ccs_uniforms *u, int N, const float4 *pos, uint32_t *seats, uint32_t *hk,
+                        uint32_t *seatsOld, const uint32_t *hkOld, unsigned *status, cudaStream_t st);
+int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st);
+int launch_deposit(const ccs_uniforms *u, int N, int box, const float4 *pos, const float *mat, const float4 *monoPrev,
+                   float4 *fine, cudaStream_t st);
+int launch_coarse(const MeshBuf &m, cudaStream_t st);
+int launch_far(const MeshBuf &m, cudaStream_t st);
+int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st);
+int launch_pp_gather(const ccs_uniforms *u, const float4 *pos, const float *mat, const int *index, int cap,
+                     float4 *list, float *box, cudaStream_t st);
+int launch_pp_force(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,
+                    float4 *force, cudaStream_t st);
+int launch_diag(const ccs_uniforms *u, int N, const DiagArgs &a, cudaStream_t st);
+int launch_rigid(const ccs_uniforms *u, int N, const float4 *pos, const float4 *vel, const float4 *aux,
+                 const float *q, float4 *posO, float4 *velO, float4 *auxO, float *qO, cudaStream_t st);
+int launch_permute(int N, const int32_t *perm, const float4 *pos, const float4 *vel, const float4 *aux,
+                   const float *q, const float *mat, const float4 *home, float4 *posO, float4 *velO, float4 *auxO,
+                   float *qO, float *matO, float4 *homeO, cudaStream_t st);
+int launch_morton_keys(int N, const float4 *pos, double cx, double cy, double cz, uint32_t *keys, int32_t *idx,
+                       cudaStream_t st);
+// stable LSD radix sort of (key, value) pairs on `bits` key bits; tmp buffers
+// hold N entries each, hist holds radix_hist_words(N) words
+size_t radix_hist_words(int N);
+int launch_radix_sort(int N, int bits, uint32_t *keys, int32_t *vals, uint32_t *keysTmp, int32_t *valsTmp,
+                      uint32_t *hist, cudaStream_t st);
+int launch_invert_perm(int N, const int32_t *perm, int32_t *into, cudaStream_t st);
+int launch_books(int N, double mref, const float4 *pos, const float4 *vel, const float *mat, const float4 *diag,
+                 double *partial, double *out, int withDiag, cudaStream_t st);
+size_t books_partial_doubles(int N);
+
+}  // namespace ccs

@@ -1,0 +1,208 @@
+/*
+ * ccstep.h -- C ABI of the B200 simulation step for cosmic-collisions.
+ *
+ * This library is a drop-in for the engine object `CC.nbody` that
+ * src/nbody.js:1095-1118 hands the pages (index.html, src/view.js).  Each entry
+ * point below names the reference function it replaces.  All functions return
+ * an int status (CCS_OK, CCS_NOT_READY, or a negative CCS_E_* code); no C++
+ * exception crosses this boundary.  A handle belongs to one host thread at a
+ * time.  The handle owns every device buffer; the caller owns every host array
+ * it passes.  Particle arrays are row-major: pos4/vel4/aux4/home4 are N x 4
+ * float (x, y, z, w), mat and q are N floats -- the reference's RGBA32F / R32F
+ * textures laid out by texel index i = y * W + x.
+ *
+ * Units are the reference's: G = M_earth = R_earth = 1 (src/nbody.js:7-10).
+ */
+#ifndef CCSTEP_H
+#define CCSTEP_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCS_OK 0
+#define CCS_NOT_READY 1      /* an async read-back is still in flight (src/nbody.js:1012-1013) */
+#define CCS_E_ARG (-1)       /* bad argument, size or pointer */
+#define CCS_E_CUDA (-2)      /* a CUDA call failed; ccs_last_error() says which */
+#define CCS_E_STATE (-3)     /* call out of order (nothing built, nothing pending, ...) */
+#define CCS_E_NOMEM (-4)     /* host or device allocation failed */
+#define CCS_E_RANGE (-5)     /* size beyond a documented maximum */
+#define CCS_E_KERNEL (-6)    /* a kernel reported an error through its status word */
+
+#define CCS_SEATS 8          /* body-particles a contact cell holds: CC.SLOTS, src/shell.js:131 */
+#define CCS_PP_CAP 8192      /* loose-list capacity: PP_CAP, src/nbody.js:38 */
+#define CCS_PP_BINS 64       /* mesh pair table bins: src/nbody.js:109 */
+#define CCS_MAX_N 262144     /* the 18-bit seat index: src/glsl-sim.js:96-109, CC.N_CHOICES */
+#define CCS_SEAT_EMPTY 0xBF800000u /* -1.0f, the cleared seat (src/nbody.js:385) */
+
+typedef struct ccs_handle ccs_handle;
+
+/* The per-pass uniforms, rounded to binary32 as gl.uniform* rounds them
+ * (src/nbody.js:255-336 setStaticUniforms, 342-350 boxes, 458-484 passSim). */
+typedef struct {
+  int N, W;
+  int G, GShift, GMask, SX, SXShift, SXMask, AW, AH; /* contact grid, src/gl.js:73-75 */
+  float invCell, cell, link2, reach2, touch;
+  float K, C, invM, damp, creep, tK, kappa, cpIron;
+  float dt, gdt, settle, kick;
+  float bulk0[3], bulk1[3], cen0[3], cen1[3], spin0[3], spin1[3];
+  float invH, eps2Mesh, eps2Cell, Gm;               /* eps2Mesh = FH^2, eps2Cell = FH^2/2 */
+  float LA[3], LB[3], boxB;                         /* the two mesh boxes, src/glsl-sim.js:25-37 */
+  float cut, a2;                                    /* P3M cut-off and particle radius^2 */
+  int ppCount;                                      /* loose-list length (pp.count) */
+  float rot0[9], rot1[9], rdt;                      /* rigid carry (src/glsl-sim.js:537-570) */
+} ccs_uniforms;
+
+/* The run's scalars: the fields of the reference's `sim` object
+ * (src/nbody.js:212-234) that the step, the phases and the pages read. */
+typedef struct {
+  int N, W, H, n1, n2, G, settleLeft, settleTotal, stepNo, soft, phase; /* phase: 0 settle, 1 approach, 2 full */
+  double m, a, cell, dt, k, c, creep, damp, tK, kappa;
+  double R1, R2, Re1, Re2, M1, M2, M, vc, vesc, t, impactT;
+  double spin0[3], spin1[3], cen0[3], cen1[3], bulk0[3], bulk1[3];
+  double relr[3], relv[3];                          /* impactor relative to target (sim.rel) */
+  int boxOn[2];                                     /* sim.boxes[b].on */
+  double boxCen[2][3], boxVel[2][3], boxT[2];       /* sim.boxes[b].cen/vel/t */
+} ccs_sim;
+
+/* build(opt) options (src/nbody.js:114, index.html:250).  The last four fields
+ * are extensions the reference fixes; 0 keeps the reference's value.
+ * coreImp < 0 means "undefined" (use core). */
+typedef struct {
+  int N;
+  double q, dens, core, coreImp, spin0, spin1, angle, incl, vfac, rest;
+  int n2;
+  double mImp;
+  double mTarget;   /* target mass in M_earth (reference: 1) */
+  double rhoR;      /* core/mantle density ratio (reference: 2.5, src/nbody.js:118) */
+  double rhoCrust;  /* crust/mantle density ratio (reference: 1, src/nbody.js:155) */
+  double crustFrac; /* crust = outer fraction of radius (reference: the outermost shell) */
+} ccs_build_opt;
+
+/* The analysis report of fof() (src/nbody.js:888-892), binary64. */
+typedef struct {
+  double largest, largestImp, largestIron, day, tilt, axis[3], bodyVel[3], orbit, escape;
+  int hasSecond;
+  double secMass, secDist, secImp, secIron, secCom[3], secCore[3], secVel[3], secR;
+  int secBound;
+  double com[3], core[3], vel[3], R, Redge, Tsurf, hotCom[3], hotR, impMass, impCom[3], impRms;
+  double M, iron, drift, L, KE, PE, EL, Q, unseated, full, jD, moon;
+  int ppCount, ppLoose;
+} ccs_report;
+
+/* Headless device buffers in place of the GL textures src/view.js reads
+ * (sim.src.pos/vel/aux/q, sim.mat, sim.home: src/view.js:216-220,566-569). */
+typedef struct {
+  void *pos4, *vel4, *aux4, *q, *mat, *home4;
+  void *force[2], *mono[2];                         /* pm[b].force (64^3 + scratch), pm[b].mono */
+  void *stream;                                     /* the cudaStream_t every kernel runs on */
+} ccs_device_buffers;
+
+/* ---- lifecycle: CC.nbody.init (src/nbody.js:1032-1092) ---- */
+int ccs_create(int device, ccs_handle **out);
+int ccs_destroy(ccs_handle *h);
+const char *ccs_last_error(const ccs_handle *h);
+int ccs_version(void);
+
+/* ---- building a run ---- */
+/* Host-side builder: build() of src/nbody.js:114-250 with ball/relax/maclaurin
+ * of src/bodies.js:23-160 and mulberry of src/math.js:8-15.  Fills sim and the
+ * particle arrays (pos4, vel4, home4: N*4 floats; mat: N floats). */
+int ccs_make_bodies(const ccs_build_opt *opt, ccs_sim *sim, float *pos4, float *vel4, float *mat, float *home4);
+/* Upload a run: the texture uploads and setStaticUniforms of src/nbody.js:208-249.
+ * home4 may be NULL. */
+int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float *vel4, const float *mat,
+              const float *home4);
+/* The live run scalars (CC.nbody.sim): the caller may advance sim->t as the
+ * frame loop does (index.html:372).  After changing static fields (k, c, dt,
+ * damp, spins ...) call ccs_set_static (setStaticUniforms, src/nbody.js:255). */
+ccs_sim *ccs_sim_ptr(ccs_handle *h);
+int ccs_set_static(ccs_handle *h);
+int ccs_get_uniforms(ccs_handle *h, ccs_uniforms *out);
+/* meshEvery setter, src/nbody.js:1115 (default 8) */
+int ccs_set_mesh_every(ccs_handle *h, int n);
+
+/* ---- the step: src/nbody.js:551-558 step(settle, kick) ---- */
+int ccs_step(ccs_handle *h, int settle, int kick);
+/* n frame-loop steps: { step(false,false); sim.t += sim.dt } (index.html:372),
+ * replayed from captured CUDA graphs in blocks of meshEvery steps. */
+int ccs_steps(ccs_handle *h, int n);
+/* settleSome(n), src/nbody.js:561-566 */
+int ccs_settle_some(ccs_handle *h, int n);
+/* rigidStep(dtF), src/nbody.js:591-636: CPU two-body leapfrog + GPU rigid carry,
+ * and the first-touch kick step */
+int ccs_rigid_step(ccs_handle *h, double dtF);
+
+/* ---- the analysis hand-off: applyReport (src/nbody.js:912-966) ---- */
+/* setPP: the loose list (particle indices), then its pairwise pass at once */
+int ccs_set_pp(ccs_handle *h, const int32_t *list, int n, int loose);
+/* placeBoxes' priming of a box's mono texel (src/nbody.js:368-370) */
+int ccs_prime_mono(ccs_handle *h, int box, const float mono[4]);
+/* applyPerm(perm): state, mat and home gathered by perm, then fresh contact cells */
+int ccs_apply_perm(ccs_handle *h, const int32_t *perm);
+/* The Morton order of src/nbody.js:871-887 computed on the device (keys in
+ * binary64, stable radix sort), applied as applyPerm.  perm_out and into_out
+ * (N int32 each) may be NULL; into_out renames a loose list. */
+int ccs_sort_morton(ccs_handle *h, const double core[3], int32_t *perm_out, int32_t *into_out);
+/* analyze(): passDiag (src/nbody.js:488-507) and the asynchronous read-back of
+ * diag, pos and vel (src/nbody.js:977-993) into pinned staging ... */
+int ccs_diag_async(ccs_handle *h);
+/* ... collected without blocking (src/nbody.js:1011-1025): CCS_NOT_READY until
+ * the copy has landed.  P, V, D: N*4 floats each (any may be NULL). */
+int ccs_poll(ccs_handle *h, float *P, float *V, float *D);
+/* The host analysis, fof() of src/nbody.js:646-893 (CPU, binary64): groups,
+ * books, loose list (cap entries) and, with sort, the Morton permutation. */
+int ccs_fof(int N, double mref, double a, const float *P, const float *V, const float *R, const float *D,
+            double spring, double touch, int cap, int sort, ccs_report *rep, int32_t *list, int32_t *perm);
+/* The mesh's own pair force and potential by distance, meshPairTable of
+ * src/nbody.js:56-108 (host, binary64 -> binary32). */
+int ccs_pair_table(int bins, double cut, float *f, float *p);
+
+/* ---- read-outs ---- */
+int ccs_read_state(ccs_handle *h, float *pos4, float *vel4, float *aux4, float *q, float *mat);
+int ccs_write_state(ccs_handle *h, const float *pos4, const float *vel4, const float *aux4, const float *q,
+                    const float *mat);
+int ccs_device_ptrs(ccs_handle *h, ccs_device_buffers *out);
+/* Conservation books on the device in binary64 (the sums of src/nbody.js:837-850):
+ * out[0] M, [1..3] momentum, [4..6] angular momentum about the origin, [7] KE,
+ * [8] PE (needs a diag pass), [9] Q/2, [10] unseated fraction, [11] full fraction */
+#define CCS_BOOKS 12
+int ccs_books(ccs_handle *h, int with_diag, double out[CCS_BOOKS]);
+/* Internal buffers, for tests and the console checks of index.html:531-556:
+ * which = CCS_BUF_* below; bytes must equal the buffer's size. */
+enum {
+  CCS_BUF_SEATS = 5, CCS_BUF_FINE_A = 6, CCS_BUF_FORCE_A = 7, CCS_BUF_MONO_A = 8, CCS_BUF_COARSE_A = 9,
+  CCS_BUF_FAR_A = 10, CCS_BUF_FINE_B = 11, CCS_BUF_FORCE_B = 12, CCS_BUF_MONO_B = 13, CCS_BUF_PP_LIST = 14,
+  CCS_BUF_PP_FORCE = 15, CCS_BUF_PP_BOX = 16, CCS_BUF_PP_SLOT = 17, CCS_BUF_DIAG = 18, CCS_BUF_CELL_OF = 19
+};
+int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes);
+
+/* ---- single passes: CC.nbody.passes (src/nbody.js:1105) ---- */
+int ccs_pass_slots(ccs_handle *h);
+int ccs_pass_mesh(ccs_handle *h);            /* boxes() + passMesh() */
+int ccs_pass_pp(ccs_handle *h);
+int ccs_pass_sim(ccs_handle *h, int settle, int kick, double gdt);
+int ccs_pass_diag(ccs_handle *h);
+
+/* ---- host-buffer step (the plugin call a host without device memory makes):
+ * upload pos/vel/q from host arrays, run nsteps frame-loop steps, read
+ * pos/vel/aux/q back.  Any output pointer may be NULL. ---- */
+int ccs_advance_host(ccs_handle *h, const float *pos4, const float *vel4, const float *q, int nsteps,
+                     float *pos4_out, float *vel4_out, float *aux4_out, float *q_out);
+
+/* ---- timing helpers for the benchmark ---- */
+int ccs_sync(ccs_handle *h);
+/* average device time (ms) of the kernels named by `kernel` launched since the
+ * last reset, measured with CUDA events on the handle's stream; kernel ids:
+ * 0 contact step (simulate), 1 contact grid, 2 deposit, 3 cell, 4 P3M force */
+int ccs_timing(ccs_handle *h, int enable);
+int ccs_timing_read(ccs_handle *h, int kernel, double *total_ms, int *launches);
+/* kernels launched by this handle since creation (the benchmark's gpu_launches) */
+int64_t ccs_launch_count(ccs_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
