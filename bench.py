@@ -201,6 +201,19 @@ def run_ours(args, rank, world, log):
     prepare(nb, cc, N, args.prep, log)
     nb.steps(args.warmup)
     nb.sync()
+    if args.profile:
+        # for `ncu --profile-from-start off`: only these steps are profiled
+        l0 = lib.ccs_launch_count(nb.handle)
+        torch.cuda.profiler.start()
+        for _ in range(args.steps):
+            nb.step(False, False)
+            nb.sim.t += nb.sim.dt
+        nb.sync()
+        torch.cuda.profiler.stop()
+        out = {"profile": True, "steps": args.steps, "gpu_launches": int(lib.ccs_launch_count(nb.handle) - l0),
+               "stepNo": nb.sim.stepNo, "loose_list": nb.pp["count"]}
+        nb.close()
+        return out
     buf = nb.device_buffers()
     stream = torch.cuda.ExternalStream(buf.stream, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -334,6 +347,9 @@ def main():
     ap.add_argument("--prep", type=int, default=720, help="full-phase steps before timing")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="prepare, warm up, then run --steps steps inside cudaProfilerStart/Stop and exit "
+                         "(for ncu --profile-from-start off); prints no bench line")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
@@ -363,7 +379,7 @@ def main():
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     line = run_ours(args, rank, world, log)
     if rank == 0:
-        if world == 1 and not args.no_cpu:
+        if world == 1 and not args.no_cpu and not args.profile:
             line["cpu_baseline"] = cpu_reference(args.n, min_seconds=args.cpu_seconds)
         print(json.dumps(line), flush=True)
     if world > 1:

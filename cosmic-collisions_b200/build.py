@@ -1,9 +1,9 @@
 """Builds libccstep.so (the sm_100a step library) in place, beside this file.
 
-nvcc cross-compiles for sm_100a without a GPU.  Device code is compiled with
--fmad=false and IEEE division/square root so each GLSL expression of the
-reference rounds once per operation; host code with -ffp-contract=off for the
-same reason on the binary64 side.
+nvcc cross-compiles for sm_100a without a GPU.  Device code that decides an
+integer outcome uses non-fusing _rn intrinsics (see csrc/ccs_device.cuh); the
+rest may fuse.  Host code is compiled with -ffp-contract=off so the binary64
+routines round once per operation, as the reference's JavaScript does.
 """
 import os
 import subprocess
@@ -12,14 +12,14 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libccstep.so")
-SOURCES = ["ccs_kernels.cu", "ccs_api.cu", "ccs_host.cpp"]
+SOURCES = ["ccs_step.cu", "ccs_mesh.cu", "ccs_pp.cu", "ccs_order.cu", "ccs_api.cu", "ccs_host.cpp"]
 HEADERS = ["ccs_device.cuh", "ccs_internal.h", os.path.join("..", "..", "include", "ccstep.h")]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo",
-    "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
+    "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
     "-shared",
 ]

@@ -75,7 +75,7 @@ struct ccs_handle {
   MeshBuf pm[2];
   // P3M
   int *ppIndex = nullptr, *ppSlot = nullptr;
-  float4 *ppList = nullptr, *ppForce = nullptr;
+  float4 *ppList = nullptr, *ppForce = nullptr, *ppPart = nullptr;
   float *ppBox = nullptr;
   float2 *tab = nullptr;
   int ppCount = 0, ppLoose = 0;
@@ -325,7 +325,7 @@ void pass_pp(ccs_handle *h, const ccs_uniforms *U, int count) {
   h->launches += launch_pp_gather(U, h->pos[h->cur], h->mat, h->ppIndex, CCS_PP_CAP, h->ppList, h->ppBox, h->st);
   cudaEvent_t b, e;
   time_begin(h, 4, &b, &e);
-  h->launches += launch_pp_force(U, h->ppList, h->ppBox, CCS_PP_CAP, h->tab, h->ppForce, h->st);
+  h->launches += launch_pp_force(U, h->ppList, h->ppBox, CCS_PP_CAP, h->tab, h->ppPart, h->ppForce, h->st);
   time_end(h, e);
 }
 
@@ -502,9 +502,11 @@ void free_state(ccs_handle *h) {
     MeshBuf &m = h->pm[b];
     dev_free(m.fine); dev_free(m.force); dev_free(m.coarse); dev_free(m.farA); dev_free(m.farT0);
     dev_free(m.farT1); dev_free(m.mono); dev_free(m.partial); dev_free(m.counter);
+    dev_free(m.occ); dev_free(m.occIdx); dev_free(m.occN);
   }
   dev_free(h->mat); dev_free(h->matTmp); dev_free(h->home); dev_free(h->homeTmp);
   dev_free(h->ppIndex); dev_free(h->ppSlot); dev_free(h->ppList); dev_free(h->ppForce); dev_free(h->ppBox);
+  dev_free(h->ppPart);
   dev_free(h->tab); dev_free(h->diag);
   dev_free(h->keys); dev_free(h->keysTmp); dev_free(h->hist); dev_free(h->vals); dev_free(h->valsTmp);
   dev_free(h->into); dev_free(h->permDev);
@@ -603,10 +605,13 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
     rc |= dev_alloc(h, &m.coarse, kCoarse); rc |= dev_alloc(h, &m.farA, kCoarse);
     rc |= dev_alloc(h, &m.farT0, kCoarse); rc |= dev_alloc(h, &m.farT1, kCoarse);
     rc |= dev_alloc(h, &m.mono, 1); rc |= dev_alloc(h, &m.partial, 64); rc |= dev_alloc(h, &m.counter, 1);
+    rc |= dev_alloc(h, &m.occ, (size_t)kCoarse * 64); rc |= dev_alloc(h, &m.occIdx, (size_t)kCoarse * 64);
+    rc |= dev_alloc(h, &m.occN, kCoarse);
   }
   rc |= dev_alloc(h, &h->ppIndex, CCS_PP_CAP); rc |= dev_alloc(h, &h->ppSlot, N);
   rc |= dev_alloc(h, &h->ppList, CCS_PP_CAP); rc |= dev_alloc(h, &h->ppForce, 4 * CCS_PP_CAP);
   rc |= dev_alloc(h, &h->ppBox, CCS_PP_CAP); rc |= dev_alloc(h, &h->tab, CCS_PP_BINS);
+  rc |= dev_alloc(h, &h->ppPart, pp_partial_float4s());
   rc |= dev_alloc(h, &h->diag, N);
   rc |= dev_alloc(h, &h->keys, N); rc |= dev_alloc(h, &h->keysTmp, N); rc |= dev_alloc(h, &h->vals, N);
   rc |= dev_alloc(h, &h->valsTmp, N); rc |= dev_alloc(h, &h->into, N); rc |= dev_alloc(h, &h->permDev, N);
@@ -645,6 +650,7 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
     CUDA_TRY(h, cudaMemsetAsync(m.farT1, 0, sizeof(float4) * kCoarse, st));
     CUDA_TRY(h, cudaMemsetAsync(m.mono, 0, sizeof(float4), st));
     CUDA_TRY(h, cudaMemsetAsync(m.counter, 0, sizeof(unsigned), st));
+    CUDA_TRY(h, cudaMemsetAsync(m.occN, 0, sizeof(int) * kCoarse, st));
   }
   h->launches += launch_fill_u32((uint32_t *)h->ppIndex, CCS_PP_CAP, 0xFFFFFFFFu, st);
   h->launches += launch_fill_u32((uint32_t *)h->ppSlot, N, 0xFFFFFFFFu, st);

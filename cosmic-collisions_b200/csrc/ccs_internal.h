@@ -25,6 +25,9 @@ struct MeshBuf {
   float4 *mono = nullptr;
   float4 *partial = nullptr;   // per-block partial sums for the monopole
   unsigned *counter = nullptr; // last-block-done counter of the coarse pass
+  float4 *occ = nullptr;       // per coarse block: its occupied fine cells (centre of mass, mass), 64 slots
+  uint8_t *occIdx = nullptr;   // ... and their place in the block
+  int *occN = nullptr;         // ... and how many there are
 };
 
 // Arguments of the contact step (simFS, src/glsl-sim.js:354-512).
@@ -68,8 +71,10 @@ int launch_far(const MeshBuf &m, cudaStream_t st);
 int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st);
 int launch_pp_gather(const ccs_uniforms *u, const float4 *pos, const float *mat, const int *index, int cap,
                      float4 *list, float *box, cudaStream_t st);
+// the pairwise partials of the P3M pass: 4 quarters x chunks x cap float4
+size_t pp_partial_float4s();
 int launch_pp_force(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,
-                    float4 *force, cudaStream_t st);
+                    float4 *part, float4 *force, cudaStream_t st);
 int launch_diag(const ccs_uniforms *u, int N, const DiagArgs &a, cudaStream_t st);
 int launch_rigid(const ccs_uniforms *u, int N, const float4 *pos, const float4 *vel, const float4 *aux,
                  const float *q, float4 *posO, float4 *velO, float4 *auxO, float *qO, cudaStream_t st);

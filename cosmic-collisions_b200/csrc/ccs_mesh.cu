@@ -1,0 +1,302 @@
+// ccs_mesh.cu -- the 64^3 particle mesh of one box: cloud-in-cell deposit,
+// coarse sums and the monopole, the block-to-block far field, and the gravity
+// at every occupied fine cell (src/glsl-sim.js:158-352).
+#include "ccs_device.cuh"
+#include "ccs_internal.h"
+
+namespace ccs {
+
+namespace {
+constexpr int kBlock = 256;
+inline int blocks_for(long n, int b = kBlock) { return (int)((n + b - 1) / b); }
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// deposit: src/glsl-sim.js:168-211 (DEP_VS) with src/nbody.js:402-416.
+// Each particle's eight cloud-in-cell corners carry (w m x, w m); particles in
+// the other box are left out; a stray (in neither) adds its pull toward last
+// time's monopole into the scratch texel.  Lanes of a warp whose particles
+// share a base cell (the common case in Morton order) reduce-scatter their 32
+// values (8 corners x 4 components) with 31 shuffles, so the warp issues 32
+// scalar L2 atomics instead of 256 vector ones; mixed warps fall back to
+// per-lane float4 atomics.  The box a particle is in and its base cell are
+// exact; the summation order is unspecified, as the reference's blending is.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void reduce_scatter32(float (&v)[32], int lane) {
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool upper = (lane & s) != 0;
+#pragma unroll
+    for (int j = 0; j < s; ++j) {
+      const float send = upper ? v[j] : v[j + s];
+      const float keep = upper ? v[j + s] : v[j];
+      v[j] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, s);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_deposit(const ccs_uniforms *__restrict__ U, int box,
+                                                    const float4 *__restrict__ pos, const float *__restrict__ mat,
+                                                    const float4 *__restrict__ monoPrev, float4 *fine) {
+  const ccs_uniforms &u = *U;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  bool in = false, stray = false;
+  int bx = 0, by = 0, bz = 0;
+  f3 t = mk(0, 0, 0), p = mk(0, 0, 0);
+  float mr = 0.0f;
+  float4 sw = make_float4(0, 0, 0, 0);
+  if (i < u.N) {
+    const float4 P = pos[i];
+    p = xyz(P);
+    mr = mat[i];
+    f3 g;
+    const int mine = box_of(u, p, g);
+    if (mine == box) {
+      in = true;
+      const float fx = floorf(g.x), fy = floorf(g.y), fz = floorf(g.z);
+      t = mk(g.x - fx, g.y - fy, g.z - fz);
+      bx = (int)fx;
+      by = (int)fy;
+      bz = (int)fz;
+    } else if (mine < 0) {
+      stray = true;
+      const float4 mono = *monoPrev;
+      const f3 r = xyz(mono) * fdiv(1.0f, fmaxf(mono.w, 1e-6f)) - p;
+      const float inv = rsqrtf(dot(r, r) + u.eps2Mesh);
+      const f3 w = r * (mr * inv * inv * inv);
+      sw = make_float4(w.x, w.y, w.z, mr);
+    }
+  }
+  if (__any_sync(0xFFFFFFFFu, stray)) {   // the strays' reaction: one float4 atomic per warp
+    float4 s = sw;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      s.x += __shfl_xor_sync(0xFFFFFFFFu, s.x, o);
+      s.y += __shfl_xor_sync(0xFFFFFFFFu, s.y, o);
+      s.z += __shfl_xor_sync(0xFFFFFFFFu, s.z, o);
+      s.w += __shfl_xor_sync(0xFFFFFFFFu, s.w, o);
+    }
+    if (lane == 0) atomicAdd(fine + kFine, s);
+  }
+  const unsigned inMask = __ballot_sync(0xFFFFFFFFu, in);
+  if (inMask == 0u) return;
+  const int key = in ? (bz << 16) | (by << 8) | bx : -1 - lane;
+  const int key0 = __shfl_sync(0xFFFFFFFFu, key, __ffs(inMask) - 1);
+  const bool uniform = __all_sync(0xFFFFFFFFu, !in || key == key0) && __popc(inMask) > 1;
+  float v[32];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
+    const bool ok = in && bx + ox <= 63 && by + oy <= 63 && bz + oz <= 63;
+    const float w = ok ? (ox ? t.x : 1.0f - t.x) * (oy ? t.y : 1.0f - t.y) * (oz ? t.z : 1.0f - t.z) * mr : 0.0f;
+    v[4 * k + 0] = p.x * w;
+    v[4 * k + 1] = p.y * w;
+    v[4 * k + 2] = p.z * w;
+    v[4 * k + 3] = w;
+  }
+  if (uniform) {
+    reduce_scatter32(v, lane);
+    const int k = lane >> 2, comp = lane & 3;
+    const int cx = (key0 & 0xFF) + (k & 1), cy = ((key0 >> 8) & 0xFF) + ((k >> 1) & 1), cz = (key0 >> 16) + (k >> 2);
+    if (cx <= 63 && cy <= 63 && cz <= 63 && v[0] != 0.0f)
+      atomicAdd(reinterpret_cast<float *>(fine + fine_index(cx, cy, cz)) + comp, v[0]);
+  } else if (in) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int cx = bx + (k & 1), cy = by + ((k >> 1) & 1), cz = bz + (k >> 2);
+      if (cx > 63 || cy > 63 || cz > 63) continue;
+      atomicAdd(fine + fine_index(cx, cy, cz), make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]));
+    }
+  }
+}
+
+int launch_deposit(const ccs_uniforms *u, int N, int box, const float4 *pos, const float *mat, const float4 *monoPrev,
+                   float4 *fine, cudaStream_t st) {
+  k_deposit<<<blocks_for(N), kBlock, 0, st>>>(u, box, pos, mat, monoPrev, fine);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// coarse and monopole: src/glsl-sim.js:222-251.  One thread per coarse block
+// sums its 4^3 fine cells in the reference's loop order (bit for bit); the
+// monopole is a fixed-shape tree over the 4096 sums finished by the last CTA
+// to arrive (deterministic, unlike the reference's single serial fragment).
+// ---------------------------------------------------------------------------
+// The same thread also writes its block's occupied fine cells, in that loop
+// order, as (centre of mass, mass) plus their place in the block: the source
+// list the cell pass walks instead of all 64 cells of every neighbour block.
+__global__ void __launch_bounds__(kBlock) k_coarse(const float4 *__restrict__ fine, float4 *__restrict__ coarse,
+                                                   float4 *partial, unsigned *counter, float4 *mono,
+                                                   float4 *__restrict__ occ, uint8_t *__restrict__ occIdx,
+                                                   int *__restrict__ occN) {
+  __shared__ float4 red[kBlock];
+  __shared__ bool last;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cx = b & 15, cy = (b >> 4) & 15, cz = b >> 8;
+  float4 s = make_float4(0, 0, 0, 0);
+  int n = 0;
+  for (int z = 0; z < 4; z++)
+    for (int y = 0; y < 4; y++)
+      for (int x = 0; x < 4; x++) {
+        const float4 f = fine[fine_index(cx * 4 + x, cy * 4 + y, cz * 4 + z)];
+        s.x = xadd(s.x, f.x);
+        s.y = xadd(s.y, f.y);
+        s.z = xadd(s.z, f.z);
+        s.w = xadd(s.w, f.w);
+        if (f.w > 0.0f) {
+          const float iw = fdiv(1.0f, f.w);
+          occ[b * 64 + n] = make_float4(f.x * iw, f.y * iw, f.z * iw, f.w);
+          occIdx[b * 64 + n] = (uint8_t)((z * 4 + y) * 4 + x);
+          ++n;
+        }
+      }
+  occN[b] = n;
+  coarse[b] = s;
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = kBlock / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      float4 a = red[threadIdx.x];
+      const float4 c = red[threadIdx.x + o];
+      a.x += c.x; a.y += c.y; a.z += c.z; a.w += c.w;
+      red[threadIdx.x] = a;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = red[0];
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    float4 m = make_float4(0, 0, 0, 0);
+    for (int k = 0; k < (int)gridDim.x; ++k) {
+      const float4 c = __ldcg(partial + k);
+      m.x += c.x; m.y += c.y; m.z += c.z; m.w += c.w;
+    }
+    *mono = m;
+    *counter = 0u;
+  }
+}
+
+int launch_coarse(const MeshBuf &m, cudaStream_t st) {
+  k_coarse<<<kCoarse / kBlock, kBlock, 0, st>>>(m.fine, m.coarse, m.partial, m.counter, m.mono, m.occ, m.occIdx,
+                                               m.occN);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// far field: src/glsl-sim.js:263-295.  One warp per coarse block; its lanes
+// split the 4096 source blocks (lane, lane + 32, ...) and the warp reduces the
+// ten sums.  Occupancy (mass > 0) and the "more than two away" test are exact.
+// ---------------------------------------------------------------------------
+constexpr int kFarWarps = 8;
+
+__global__ void __launch_bounds__(32 * kFarWarps) k_far(const float4 *__restrict__ coarse, float4 *__restrict__ farA,
+                                                       float4 *__restrict__ farT0, float4 *__restrict__ farT1) {
+  const int lane = threadIdx.x & 31;
+  const int b = blockIdx.x * kFarWarps + (threadIdx.x >> 5);
+  const float4 mc = __ldg(coarse + b);
+  if (!(mc.w > 0.0f)) {
+    if (lane == 0) farA[b] = farT0[b] = farT1[b] = make_float4(0, 0, 0, 0);
+    return;
+  }
+  const int cx = b & 15, cy = (b >> 4) & 15, cz = b >> 8;
+  const f3 x = xyz(mc) * fdiv(1.0f, mc.w);
+  float s[10];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) s[k] = 0.0f;
+  for (int k = lane; k < kCoarse; k += 32) {
+    const int kx = k & 15, ky = (k >> 4) & 15, kz = k >> 8;
+    if (max(abs(kx - cx), max(abs(ky - cy), abs(kz - cz))) <= 2) continue;
+    const float4 m = __ldg(coarse + k);
+    if (!(m.w > 0.0f)) continue;
+    const f3 r = xyz(m) * fdiv(1.0f, m.w) - x;
+    const float inv = rsqrtf(dot(r, r)), inv2 = inv * inv, inv3 = inv * inv2, inv5 = inv3 * inv2;
+    const float a3 = m.w * inv3, a5 = 3.0f * m.w * inv5;
+    s[0] += r.x * a3; s[1] += r.y * a3; s[2] += r.z * a3;
+    s[3] -= m.w * inv;
+    s[4] += a5 * r.x * r.x - a3; s[5] += a5 * r.y * r.y - a3; s[6] += a5 * r.z * r.z - a3;
+    s[7] += a5 * r.x * r.y; s[8] += a5 * r.x * r.z; s[9] += a5 * r.y * r.z;
+  }
+#pragma unroll
+  for (int k = 0; k < 10; ++k)
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s[k] += __shfl_xor_sync(0xFFFFFFFFu, s[k], o);
+  if (lane == 0) {
+    farA[b] = make_float4(s[0], s[1], s[2], s[3]);
+    farT0[b] = make_float4(s[4], s[5], s[6], s[7]);
+    farT1[b] = make_float4(s[8], s[9], 0.0f, 0.0f);
+  }
+}
+
+cudaError_t init_kernels() { return cudaSuccess; }
+
+int launch_far(const MeshBuf &m, cudaStream_t st) {
+  k_far<<<kCoarse / kFarWarps, 32 * kFarWarps, 0, st>>>(m.coarse, m.farA, m.farT0, m.farT1);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// cell gravity: src/glsl-sim.js:303-352.  One thread per fine cell, 64 to a
+// CTA per coarse block (a cell can hold mass only if its block does); empty
+// cells leave at once.  An occupied cell walks the 5^3 blocks around its own
+// in the reference's order and, within each, only the occupied cells the
+// coarse pass listed (centre of mass and mass, already divided out), skipping
+// itself -- every thread of a CTA reads the same entries, so each load is a
+// broadcast.  Then the block's far field is carried to the cell by the tidal
+// tensor.  The pull of a cell on a cell is fast arithmetic (rsqrt, FMA).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U, const float4 *__restrict__ fine,
+                                             const float4 *__restrict__ coarse, const float4 *__restrict__ occ,
+                                             const uint8_t *__restrict__ occIdx, const int *__restrict__ occN,
+                                             const float4 *__restrict__ farA, const float4 *__restrict__ farT0,
+                                             const float4 *__restrict__ farT1, float4 *__restrict__ force) {
+  const int blk = blockIdx.x;
+  const int ccx = blk & 15, ccy = (blk >> 4) & 15, ccz = blk >> 8;
+  const int tx = threadIdx.x & 3, ty = (threadIdx.x >> 2) & 3, tz = threadIdx.x >> 4;
+  const int c = fine_index(ccx * 4 + tx, ccy * 4 + ty, ccz * 4 + tz);
+  if (blk == 0 && threadIdx.x == 0) force[kFine] = fine[kFine];   // the scratch texel, carried through
+  const float4 mc = fine[c];
+  if (!(mc.w > 0.0f)) {
+    force[c] = make_float4(0, 0, 0, 0);
+    return;
+  }
+  const f3 x = xyz(mc) * fdiv(1.0f, mc.w);
+  const float eps2 = U->eps2Cell, Gm = U->Gm;
+  f3 acc = mk(0, 0, 0);
+  float pot = 0.0f;
+  for (int kz = max(ccz - 2, 0); kz <= min(ccz + 2, 15); kz++)
+    for (int ky = max(ccy - 2, 0); ky <= min(ccy + 2, 15); ky++)
+      for (int kx = max(ccx - 2, 0); kx <= min(ccx + 2, 15); kx++) {
+        const int k = coarse_index(kx, ky, kz);
+        const int n = __ldg(occN + k);
+        const float4 *src = occ + (size_t)k * 64;
+        const int self = k == blk ? (int)threadIdx.x : -1;
+        for (int i = 0; i < n; ++i) {
+          if (self >= 0 && __ldg(occIdx + (size_t)k * 64 + i) == self) continue;   // a cell does not pull itself
+          const float4 mf = __ldg(src + i);
+          const f3 r = xyz(mf) - x;
+          const float inv = rsqrtf(dot(r, r) + eps2);
+          acc = acc + r * (mf.w * inv * inv * inv);
+          pot -= mf.w * inv;
+        }
+      }
+  const float4 mb = coarse[blk], fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
+  const f3 d = x - xyz(mb) * fdiv(1.0f, mb.w);
+  const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
+                   t1.x * d.x + t1.y * d.y + t0.z * d.z);
+  acc = acc + (xyz(fa) + Td);
+  pot += fa.w - dot(xyz(fa), d) - 0.5f * dot(d, Td);
+  force[c] = make_float4(acc.x * Gm, acc.y * Gm, acc.z * Gm, pot * Gm);
+}
+
+int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st) {
+  k_cell<<<kCoarse, 64, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.farA, m.farT0, m.farT1, m.force);
+  return 1;
+}
+
+}  // namespace ccs

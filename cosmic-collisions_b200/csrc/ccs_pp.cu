@@ -1,0 +1,142 @@
+// ccs_pp.cu -- the P3M pairwise correction for the loose list
+// (src/glsl-sim.js:669-754, src/nbody.js:509-528).
+//
+// The reference gathers the list into a 128x64 texture and runs 4 x 8192
+// fragments, each walking a quarter of the list.  Here the list is tiled two
+// ways: a CTA takes 128 seats (i) against one 128-wide chunk (j) of one
+// quarter, with the chunk staged in shared memory, so a list of 8192 keeps
+// 4096 CTAs busy instead of 32K threads walking 2048 pairs each.  A second
+// kernel sums each quarter's chunks in a fixed order: the four slices the
+// contact step adds are the reference's four slices, and the result is
+// deterministic.  The cut-off test and the box comparison are exact; the
+// force arithmetic is fast (FMA, rsqrt).
+#include "ccs_device.cuh"
+#include "ccs_internal.h"
+
+namespace ccs {
+
+namespace {
+constexpr int kBlock = 256;
+inline int blocks_for(long n, int b = kBlock) { return (int)((n + b - 1) / b); }
+constexpr int kPPI = 128;                                  // seats per CTA
+constexpr int kPPJ = 128;                                  // list entries per chunk
+constexpr int kMaxChunks = (CCS_PP_CAP / 4 + kPPJ - 1) / kPPJ;   // chunks per quarter at full capacity
+}  // namespace
+
+size_t pp_partial_float4s() { return (size_t)4 * kMaxChunks * CCS_PP_CAP; }
+
+__global__ void __launch_bounds__(kBlock) k_pp_gather(const ccs_uniforms *__restrict__ U,
+                                                      const float4 *__restrict__ pos, const float *__restrict__ mat,
+                                                      const int *__restrict__ index, int cap,
+                                                      float4 *__restrict__ list, float *__restrict__ box) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= cap) return;
+  const int i = index[s];
+  if (i < 0) {
+    list[s] = make_float4(0, 0, 0, 0);
+    box[s] = -1.0f;
+    return;
+  }
+  const float4 P = pos[i];
+  f3 g;
+  box[s] = (float)box_of(*U, xyz(P), g);
+  list[s] = make_float4(P.x, P.y, P.z, mat[i]);
+}
+
+int launch_pp_gather(const ccs_uniforms *u, const float4 *pos, const float *mat, const int *index, int cap,
+                     float4 *list, float *box, cudaStream_t st) {
+  k_pp_gather<<<blocks_for(cap), kBlock, 0, st>>>(u, pos, mat, index, cap, list, box);
+  return 1;
+}
+
+__global__ void __launch_bounds__(kPPI) k_pp_pairs(const ccs_uniforms *__restrict__ U,
+                                                   const float4 *__restrict__ list, const float *__restrict__ box,
+                                                   int cap, const float2 *__restrict__ tab,
+                                                   float4 *__restrict__ part) {
+  __shared__ float4 sq[kPPJ];
+  __shared__ float sb[kPPJ];
+  __shared__ float2 stab[CCS_PP_BINS];
+  const ccs_uniforms &u = *U;
+  const int count = u.ppCount;
+  const int slice = blockIdx.y / kMaxChunks, chunk = blockIdx.y % kMaxChunks;
+  const int share = (count + 3) >> 2;
+  const int s0 = slice * share, s1 = min(s0 + share, count);
+  const int j0 = s0 + chunk * kPPJ, j1 = min(j0 + kPPJ, s1);
+  const int i0 = blockIdx.x * kPPI;
+  if (i0 >= count || j0 >= j1) return;   // never read by the reduction
+  const int me = i0 + threadIdx.x;
+  if (threadIdx.x < CCS_PP_BINS) stab[threadIdx.x] = tab[threadIdx.x];
+  if (j0 + (int)threadIdx.x < j1) {
+    sq[threadIdx.x] = list[j0 + threadIdx.x];
+    sb[threadIdx.x] = box[j0 + threadIdx.x];
+  }
+  __syncthreads();
+  const float4 P = me < cap ? list[me] : make_float4(0, 0, 0, 0);
+  const bool active = me < count && P.w != 0.0f;
+  const float myBox = me < cap ? box[me] : -1.0f;
+  const float cut = u.cut, a2 = u.a2, cut2 = xmul(cut, cut), a = fsqrt(a2);
+  const float binScale = fdiv(64.0f, cut), taperScale = fdiv(1.0f, 0.8f * cut - cut);
+  f3 acc = mk(0, 0, 0);
+  float pot = 0.0f;
+  if (active) {
+    const int n = j1 - j0;
+#pragma unroll 4
+    for (int jj = 0; jj < n; ++jj) {
+      if (j0 + jj == me) continue;
+      const float4 Q = sq[jj];
+      const f3 d = xsub3(xyz(Q), xyz(P));
+      const float r2 = xdot(d, d);
+      if (r2 >= cut2) continue;
+      const float r = fsqrt(r2);
+      const float xx = clampf(r * binScale - 0.5f, 0.0f, 63.0f);
+      const int k = (int)xx, k1 = min(k + 1, 63);
+      const float tt = xx - (float)k;
+      const float invN = rsqrtf(r2 + a2);
+      const float ts = clampf((r - cut) * taperScale, 0.0f, 1.0f);
+      const float taper = ts * ts * (3.0f - 2.0f * ts);
+      const float same = (myBox >= 0.0f && sb[jj] == myBox) ? 1.0f : 0.0f;
+      const float2 ta = stab[k], tb = stab[k1];
+      const float Tx = (ta.x + (tb.x - ta.x) * tt) * same;
+      const float Ty = (ta.y + (tb.y - ta.y) * tt) * same;
+      const float fn = invN * invN * invN * r - fdiv(Tx, fmaxf(r2, a2));
+      const float mj = Q.w;
+      acc = acc + d * (fdiv(1.0f, fmaxf(r, 1e-6f)) * mj * fn * taper);
+      pot += mj * (-invN - fdiv(Ty, fmaxf(r, a))) * taper;
+    }
+  }
+  part[((size_t)slice * kMaxChunks + chunk) * cap + me] = make_float4(acc.x, acc.y, acc.z, pot);
+}
+
+__global__ void __launch_bounds__(kBlock) k_pp_reduce(const ccs_uniforms *__restrict__ U,
+                                                      const float4 *__restrict__ list,
+                                                      const float4 *__restrict__ part, int cap,
+                                                      float4 *__restrict__ force) {
+  const int me = blockIdx.x * blockDim.x + threadIdx.x;
+  const int slice = blockIdx.y;
+  if (me >= cap) return;
+  const ccs_uniforms &u = *U;
+  const int count = u.ppCount;
+  float4 o = make_float4(0, 0, 0, 0);
+  if (me < count && list[me].w != 0.0f) {
+    const int share = (count + 3) >> 2;
+    const int s0 = slice * share, s1 = min(s0 + share, count);
+    const int nChunks = s1 > s0 ? (s1 - s0 + kPPJ - 1) / kPPJ : 0;
+    for (int c = 0; c < nChunks; ++c) {
+      const float4 v = part[((size_t)slice * kMaxChunks + c) * cap + me];
+      o.x += v.x; o.y += v.y; o.z += v.z; o.w += v.w;
+    }
+    o = make_float4(o.x * u.Gm, o.y * u.Gm, o.z * u.Gm, o.w * u.Gm);
+  }
+  force[(size_t)slice * cap + me] = o;
+}
+
+int launch_pp_force(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,
+                    float4 *part, float4 *force, cudaStream_t st) {
+  dim3 g1((cap + kPPI - 1) / kPPI, 4 * kMaxChunks);
+  k_pp_pairs<<<g1, kPPI, 0, st>>>(u, list, box, cap, tab, part);
+  dim3 g2(blocks_for(cap), 4);
+  k_pp_reduce<<<g2, kBlock, 0, st>>>(u, list, part, cap, force);
+  return 2;
+}
+
+}  // namespace ccs
