@@ -233,59 +233,81 @@ __global__ void __launch_bounds__(32 * kFarWarps) k_far(const float4 *__restrict
   }
 }
 
-cudaError_t init_kernels() { return cudaSuccess; }
-
 int launch_far(const MeshBuf &m, cudaStream_t st) {
   k_far<<<kCoarse / kFarWarps, 32 * kFarWarps, 0, st>>>(m.coarse, m.farA, m.farT0, m.farT1);
   return 1;
 }
 
 // ---------------------------------------------------------------------------
-// cell gravity: src/glsl-sim.js:303-352.  One thread per fine cell, 64 to a
-// CTA per coarse block (a cell can hold mass only if its block does); empty
-// cells leave at once.  An occupied cell walks the 5^3 blocks around its own
-// in the reference's order and, within each, only the occupied cells the
-// coarse pass listed (centre of mass and mass, already divided out), skipping
-// itself -- every thread of a CTA reads the same entries, so each load is a
-// broadcast.  Then the block's far field is carried to the cell by the tidal
-// tensor.  The pull of a cell on a cell is fast arithmetic (rsqrt, FMA).
+// cell gravity: src/glsl-sim.js:303-352.  One 64-thread CTA per coarse block,
+// a thread per fine cell (a cell can hold mass only if its block does).  The
+// CTA first reads how many occupied cells each of the 5^3 blocks around it
+// holds; then, block by block in the reference's order, it stages that
+// block's occupied cells -- centre of mass and mass, as the coarse pass listed
+// them -- in shared memory with one coalesced load, and every occupied thread
+// sums them for its own cell, skipping itself.  Then the block's far field is
+// carried to the cell by the tidal tensor.  Cell-on-cell pulls are fast
+// arithmetic (rsqrt, FMA).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U, const float4 *__restrict__ fine,
                                              const float4 *__restrict__ coarse, const float4 *__restrict__ occ,
                                              const uint8_t *__restrict__ occIdx, const int *__restrict__ occN,
                                              const float4 *__restrict__ farA, const float4 *__restrict__ farT0,
                                              const float4 *__restrict__ farT1, float4 *__restrict__ force) {
-  const int blk = blockIdx.x;
+  __shared__ int nbK[125], nbN[125];
+  __shared__ float4 src[64];
+  __shared__ uint8_t sidx[64];
+  const int blk = blockIdx.x, t = threadIdx.x;
   const int ccx = blk & 15, ccy = (blk >> 4) & 15, ccz = blk >> 8;
-  const int tx = threadIdx.x & 3, ty = (threadIdx.x >> 2) & 3, tz = threadIdx.x >> 4;
-  const int c = fine_index(ccx * 4 + tx, ccy * 4 + ty, ccz * 4 + tz);
-  if (blk == 0 && threadIdx.x == 0) force[kFine] = fine[kFine];   // the scratch texel, carried through
-  const float4 mc = fine[c];
-  if (!(mc.w > 0.0f)) {
+  const int c = fine_index(ccx * 4 + (t & 3), ccy * 4 + ((t >> 2) & 3), ccz * 4 + (t >> 4));
+  if (blk == 0 && t == 0) force[kFine] = fine[kFine];   // the scratch texel, carried through
+  const float4 mb = coarse[blk];
+  if (!(mb.w > 0.0f)) {   // an empty block: the same for the whole CTA
     force[c] = make_float4(0, 0, 0, 0);
     return;
   }
-  const f3 x = xyz(mc) * fdiv(1.0f, mc.w);
+  for (int o = t; o < 125; o += 64) {   // o = kx + 5 ky + 25 kz: the reference's loop order
+    const int kx = ccx + o % 5 - 2, ky = ccy + (o / 5) % 5 - 2, kz = ccz + o / 25 - 2;
+    const bool in = kx >= 0 && ky >= 0 && kz >= 0 && kx <= 15 && ky <= 15 && kz <= 15;
+    const int k = in ? coarse_index(kx, ky, kz) : 0;
+    nbK[o] = k;
+    nbN[o] = in ? __ldg(occN + k) : 0;
+  }
+  const float4 mc = fine[c];
+  const bool mine = mc.w > 0.0f;
+  const f3 x = mine ? xyz(mc) * fdiv(1.0f, mc.w) : mk(0, 0, 0);
   const float eps2 = U->eps2Cell, Gm = U->Gm;
   f3 acc = mk(0, 0, 0);
   float pot = 0.0f;
-  for (int kz = max(ccz - 2, 0); kz <= min(ccz + 2, 15); kz++)
-    for (int ky = max(ccy - 2, 0); ky <= min(ccy + 2, 15); ky++)
-      for (int kx = max(ccx - 2, 0); kx <= min(ccx + 2, 15); kx++) {
-        const int k = coarse_index(kx, ky, kz);
-        const int n = __ldg(occN + k);
-        const float4 *src = occ + (size_t)k * 64;
-        const int self = k == blk ? (int)threadIdx.x : -1;
-        for (int i = 0; i < n; ++i) {
-          if (self >= 0 && __ldg(occIdx + (size_t)k * 64 + i) == self) continue;   // a cell does not pull itself
-          const float4 mf = __ldg(src + i);
-          const f3 r = xyz(mf) - x;
-          const float inv = rsqrtf(dot(r, r) + eps2);
-          acc = acc + r * (mf.w * inv * inv * inv);
-          pot -= mf.w * inv;
-        }
+  __syncthreads();
+  for (int o = 0; o < 125; ++o) {
+    const int n = nbN[o];
+    if (n == 0) continue;   // an empty block is nothing: most of the 125 are
+    const int k = nbK[o];
+    if (t < n) {
+      src[t] = __ldg(occ + (size_t)k * 64 + t);
+      sidx[t] = __ldg(occIdx + (size_t)k * 64 + t);
+    }
+    __syncthreads();
+    if (mine) {
+      const int self = k == blk ? t : -1;   // a cell does not pull itself
+#pragma unroll 4
+      for (int i = 0; i < n; ++i) {
+        if ((int)sidx[i] == self) continue;
+        const float4 mf = src[i];
+        const f3 r = xyz(mf) - x;
+        const float inv = rsqrtf(dot(r, r) + eps2);
+        acc = acc + r * (mf.w * inv * inv * inv);
+        pot -= mf.w * inv;
       }
-  const float4 mb = coarse[blk], fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
+    }
+    __syncthreads();
+  }
+  if (!mine) {
+    force[c] = make_float4(0, 0, 0, 0);
+    return;
+  }
+  const float4 fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
   const f3 d = x - xyz(mb) * fdiv(1.0f, mb.w);
   const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
                    t1.x * d.x + t1.y * d.y + t0.z * d.z);

@@ -1524,3 +1524,27 @@ void orc_fof(int N, double mref, double a, const float *P, const float *V, const
   rep->ppCount = len; rep->ppLoose = nLoose;
   free(cx); free(cy); free(cz); free(key); free(cnt); free(fill); free(order); free(uf); free(size); free(members);
 }
+
+/* ------------------------------------------------------------------ */
+/* FP64 direct sum (the gravity checker of the error sweep)            */
+/* ------------------------------------------------------------------ */
+void orc_direct_sum(int N, const float *P, const double *m, double eps, int nt, const int32_t *idx, double *acc,
+                    double *pot) {
+  double e2 = eps * eps;
+#pragma omp parallel for schedule(dynamic, 8)
+  for (int t = 0; t < nt; t++) {
+    int i = idx[t];
+    double xi = P[4 * (size_t)i], yi = P[4 * (size_t)i + 1], zi = P[4 * (size_t)i + 2];
+    double ax = 0, ay = 0, az = 0, ph = 0;
+    for (int j = 0; j < N; j++) {
+      if (j == i) continue;
+      double dx = P[4 * (size_t)j] - xi, dy = P[4 * (size_t)j + 1] - yi, dz = P[4 * (size_t)j + 2] - zi;
+      double r2 = dx * dx + dy * dy + dz * dz + e2;
+      double inv = 1.0 / sqrt(r2), inv3 = inv * inv * inv * m[j];
+      ax += dx * inv3; ay += dy * inv3; az += dz * inv3;
+      ph -= m[j] * inv;
+    }
+    acc[3 * t] = ax; acc[3 * t + 1] = ay; acc[3 * t + 2] = az;
+    pot[t] = ph;
+  }
+}

@@ -135,6 +135,13 @@ void orc_engine_diag(orc_engine *e, float *diag4);
 const void *orc_engine_buf(orc_engine *e, int which, long *bytes);
 void orc_engine_set_threads(int n);
 
+/* ---- the FP64 direct-sum gravity oracle ----
+ * acceleration and potential at the targets idx[0..nt), from all N particles
+ * (mass m[j], G = 1), Newton softened at eps (the P3M pass's own softening,
+ * src/glsl-sim.js:745), the self term excluded; acc: nt*3, pot: nt */
+void orc_direct_sum(int N, const float *pos4, const double *m, double eps, int nt, const int32_t *idx,
+                    double *acc, double *pot);
+
 /* ---- the analysis (src/nbody.js:646-893) ---- */
 typedef struct {
   double largest, largestImp, largestIron, day, tilt, axis[3], bodyVel[3], orbit, escape;

@@ -161,6 +161,7 @@ def lib():
         L.orc_engine_set_threads.argtypes = [C.c_int]
         L.orc_fof.argtypes = [C.c_int, C.c_double, C.c_double, P, P, P, P, C.c_double, C.c_double, C.c_int,
                               C.c_int, C.POINTER(Report), P, P]
+        L.orc_direct_sum.argtypes = [C.c_int, P, P, C.c_double, C.c_int, P, P, P]
         _lib = L
     return _lib
 
@@ -246,6 +247,17 @@ def morton(pos4, core):
     core = np.asarray(core, np.float64)
     lib().orc_morton(N, ptr(pos4), ptr(core), ptr(keys), ptr(perm), ptr(into))
     return keys, perm, into
+
+
+def direct_sum(pos4, masses, eps, idx):
+    """FP64 direct-sum acceleration and potential at particles idx (G = 1, softening eps, no self term)."""
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    m = np.ascontiguousarray(masses, np.float64)
+    idx = np.ascontiguousarray(idx, np.int32)
+    acc = np.zeros((len(idx), 3), np.float64)
+    pot = np.zeros(len(idx), np.float64)
+    lib().orc_direct_sum(len(pos4), ptr(pos4), ptr(m), float(eps), len(idx), ptr(idx), ptr(acc), ptr(pot))
+    return acc, pot
 
 
 def fof(N, mref, a, P, V, R, D, spring, touch, cap=PP_CAP, sort=False):
