@@ -159,6 +159,34 @@ def cpu_reference(N, min_seconds=10.0, min_steps=8, threads=None):
                       % (steps, N, el, cores)}
 
 
+def force_error(cc, dev, N, sample=2048, seed=3):
+    """The gravity-only sweep (Plummer sphere + 10 % debris, equal masses, 1 M_earth): one force evaluation
+    of the plain P3M step against the library's binary64 direct sum at a seeded sample of particles."""
+    import numpy as np
+    from cosmic_collisions_b200 import configs
+    sim, pos, vel, mat = configs.gravity_sweep(N=N)
+    nb = cc.NBody(dev)
+    try:
+        nb.upload(sim, pos, vel, mat)
+        nb.pass_slots()
+        nb.pass_diag()
+        D = nb.buffer("diag")
+        s = nb.sim
+        rep, lst, _ = cc.fof(s.N, s.m, s.a, pos, vel, mat, D, s.k, 2 * s.a)
+        nb.set_pp(lst, rep.ppLoose)
+        nb.pass_sim(False, False, 0.0)
+        g = nb.read_state()["aux"][:, :3].astype(np.float64)
+        idx = np.sort(np.random.default_rng(seed).choice(N, sample, replace=False)).astype(np.int32)
+        ref, _ = nb.direct_sum(idx)
+    finally:
+        nb.close()
+    rel = np.linalg.norm(g[idx] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    return {"median": float(np.median(rel)), "p99": float(np.percentile(rel, 99)), "sample": sample,
+            "workload": "gravity sweep, %d equal masses: Plummer sphere (scale 1 R_earth) + 10%% uniform debris" % N,
+            "loose_list": int(rep.ppCount), "loose_total": int(rep.ppLoose),
+            "reference": "binary64 direct sum, softening a, self term excluded"}
+
+
 def prepare(nb, cc, N, prep_steps, log):
     """build -> settle -> rigid approach -> kick -> prep_steps full steps with runTo's analysis cadence."""
     t0 = time.perf_counter()
@@ -295,6 +323,7 @@ def run_ours(args, rank, world, log):
     h2d = N * (16 + 16 + 4)
     d2h = N * (16 + 16 + 16 + 4)
 
+    ferr = force_error(cc, dev, N) if rank == 0 else None
     peak, peak_kind = measured_peaks()
     sim_mean_us = kt["simulate"]["mean_us"]
     achieved = ALG_BYTES_SIM * N / (sim_mean_us * 1e-6) / 1e9 if sim_mean_us else None
@@ -332,6 +361,7 @@ def run_ours(args, rank, world, log):
                      "algorithmic_bytes_per_launch": ALG_BYTES_SIM * N},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "force_error": ferr,
     }
     nb.close()
     return line

@@ -1033,6 +1033,37 @@ int ccs_books(ccs_handle *h, int with_diag, double out[CCS_BOOKS]) {
   return check_launch(h);
 }
 
+int ccs_direct_sum(ccs_handle *h, const int32_t *idx, int n, double *acc3, double *pot) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (n <= 0 || !idx || !acc3 || !pot) return CCS_E_ARG;
+  for (int k = 0; k < n; ++k)
+    if (idx[k] < 0 || idx[k] >= h->N) {
+      h->err = "direct sum: index out of range";
+      return CCS_E_ARG;
+    }
+  cudaSetDevice(h->device);
+  int32_t *dIdx = nullptr;
+  double *dAcc = nullptr, *dPot = nullptr;
+  if (cudaMalloc(&dIdx, 4 * (size_t)n) != cudaSuccess || cudaMalloc(&dAcc, 24 * (size_t)n) != cudaSuccess ||
+      cudaMalloc(&dPot, 8 * (size_t)n) != cudaSuccess) {
+    cudaFree(dIdx); cudaFree(dAcc); cudaFree(dPot);
+    h->err = "direct sum: device allocation failed";
+    return CCS_E_NOMEM;
+  }
+  cudaMemcpyAsync(dIdx, idx, 4 * (size_t)n, cudaMemcpyHostToDevice, h->st);
+  h->launches += launch_direct_sum(h->N, h->pos[h->cur], h->mat, h->sim.m, h->sim.a, dIdx, n, dAcc, dPot, h->st);
+  cudaMemcpyAsync(acc3, dAcc, 24 * (size_t)n, cudaMemcpyDeviceToHost, h->st);
+  cudaMemcpyAsync(pot, dPot, 8 * (size_t)n, cudaMemcpyDeviceToHost, h->st);
+  const cudaError_t e = cudaStreamSynchronize(h->st);
+  cudaFree(dIdx); cudaFree(dAcc); cudaFree(dPot);
+  if (e != cudaSuccess) {
+    h->err = std::string("direct sum: ") + cudaGetErrorString(e);
+    return CCS_E_CUDA;
+  }
+  return check_launch(h);
+}
+
 int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes) {
   int rc = ensure_built(h);
   if (rc) return rc;

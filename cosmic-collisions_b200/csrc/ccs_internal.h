@@ -89,6 +89,8 @@ size_t radix_hist_words(int N);
 int launch_radix_sort(int N, int bits, uint32_t *keys, int32_t *vals, uint32_t *keysTmp, int32_t *valsTmp,
                       uint32_t *hist, cudaStream_t st);
 int launch_invert_perm(int N, const int32_t *perm, int32_t *into, cudaStream_t st);
+int launch_direct_sum(int N, const float4 *pos, const float *mat, double mref, double eps, const int32_t *idx,
+                      int nt, double *acc, double *pot, cudaStream_t st);
 int launch_books(int N, double mref, const float4 *pos, const float4 *vel, const float *mat, const float4 *diag,
                  double *partial, double *out, int withDiag, cudaStream_t st);
 size_t books_partial_doubles(int N);

@@ -273,9 +273,13 @@ __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U,
     nbK[o] = k;
     nbN[o] = in ? __ldg(occN + k) : 0;
   }
-  const float4 mc = fine[c];
-  const bool mine = mc.w > 0.0f;
-  const f3 x = mine ? xyz(mc) * fdiv(1.0f, mc.w) : mk(0, 0, 0);
+  if (!(fine[c].w > 0.0f)) force[c] = make_float4(0, 0, 0, 0);   // this thread's own place, when empty
+  // thread t sums for the block's t-th occupied cell, so the busy lanes sit together
+  const int nOwn = __ldg(occN + blk);
+  const bool mine = t < nOwn;
+  const float4 tc = mine ? __ldg(occ + (size_t)blk * 64 + t) : make_float4(0, 0, 0, 0);
+  const int tl = mine ? (int)__ldg(occIdx + (size_t)blk * 64 + t) : -1;
+  const f3 x = xyz(tc);
   const float eps2 = U->eps2Cell, Gm = U->Gm;
   f3 acc = mk(0, 0, 0);
   float pot = 0.0f;
@@ -290,7 +294,7 @@ __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U,
     }
     __syncthreads();
     if (mine) {
-      const int self = k == blk ? t : -1;   // a cell does not pull itself
+      const int self = k == blk ? tl : -1;   // a cell does not pull itself
 #pragma unroll 4
       for (int i = 0; i < n; ++i) {
         if ((int)sidx[i] == self) continue;
@@ -303,17 +307,15 @@ __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U,
     }
     __syncthreads();
   }
-  if (!mine) {
-    force[c] = make_float4(0, 0, 0, 0);
-    return;
-  }
+  if (!mine) return;
   const float4 fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
   const f3 d = x - xyz(mb) * fdiv(1.0f, mb.w);
   const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
                    t1.x * d.x + t1.y * d.y + t0.z * d.z);
   acc = acc + (xyz(fa) + Td);
   pot += fa.w - dot(xyz(fa), d) - 0.5f * dot(d, Td);
-  force[c] = make_float4(acc.x * Gm, acc.y * Gm, acc.z * Gm, pot * Gm);
+  force[fine_index(ccx * 4 + (tl & 3), ccy * 4 + ((tl >> 2) & 3), ccz * 4 + (tl >> 4))] =
+      make_float4(acc.x * Gm, acc.y * Gm, acc.z * Gm, pot * Gm);
 }
 
 int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st) {

@@ -267,3 +267,69 @@ int launch_books(int N, double mref, const float4 *pos, const float4 *vel, const
 }
 
 }  // namespace ccs
+
+namespace ccs {
+
+// ---------------------------------------------------------------------------
+// FP64 direct sum: the exact pull at chosen particles, for the force-error
+// measurement and for the learned correction's training labels.  Targets are
+// tiled 128 to a CTA and the sources split across gridDim.y chunks staged in
+// shared memory; chunks add into the result with double atomics.  Newton is
+// softened at eps (the P3M pass's own softening), the self term left out.
+// ---------------------------------------------------------------------------
+constexpr int kDsTile = 128;
+
+__global__ void __launch_bounds__(kDsTile) k_direct_sum(int N, const float4 *__restrict__ pos,
+                                                        const float *__restrict__ mat, double mref, double eps2,
+                                                        const int32_t *__restrict__ idx, int nt, int chunk,
+                                                        double *__restrict__ acc, double *__restrict__ pot) {
+  __shared__ double sx[kDsTile], sy[kDsTile], sz[kDsTile], sm[kDsTile];
+  const int t = blockIdx.x * kDsTile + threadIdx.x;
+  const int i = t < nt ? idx[t] : -1;
+  double xi = 0, yi = 0, zi = 0;
+  if (i >= 0) {
+    const float4 P = pos[i];
+    xi = P.x; yi = P.y; zi = P.z;
+  }
+  const int j0 = blockIdx.y * chunk, j1 = min(j0 + chunk, N);
+  double ax = 0, ay = 0, az = 0, ph = 0;
+  for (int base = j0; base < j1; base += kDsTile) {
+    __syncthreads();
+    const int j = base + threadIdx.x;
+    if (j < j1) {
+      const float4 Q = pos[j];
+      sx[threadIdx.x] = Q.x; sy[threadIdx.x] = Q.y; sz[threadIdx.x] = Q.z;
+      sm[threadIdx.x] = mref * (double)mat[j];
+    }
+    __syncthreads();
+    const int n = min(kDsTile, j1 - base);
+    if (i < 0) continue;
+    for (int k = 0; k < n; ++k) {
+      if (base + k == i) continue;
+      const double dx = sx[k] - xi, dy = sy[k] - yi, dz = sz[k] - zi;
+      const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+      const double inv = 1.0 / sqrt(r2), w = sm[k] * inv * inv * inv;
+      ax += dx * w; ay += dy * w; az += dz * w;
+      ph -= sm[k] * inv;
+    }
+  }
+  if (i >= 0) {
+    atomicAdd(acc + 3 * t, ax);
+    atomicAdd(acc + 3 * t + 1, ay);
+    atomicAdd(acc + 3 * t + 2, az);
+    atomicAdd(pot + t, ph);
+  }
+}
+
+int launch_direct_sum(int N, const float4 *pos, const float *mat, double mref, double eps, const int32_t *idx,
+                      int nt, double *acc, double *pot, cudaStream_t st) {
+  const int chunks = 32;
+  const int chunk = (N + chunks - 1) / chunks;
+  cudaMemsetAsync(acc, 0, sizeof(double) * 3 * nt, st);
+  cudaMemsetAsync(pot, 0, sizeof(double) * nt, st);
+  dim3 g((nt + kDsTile - 1) / kDsTile, chunks);
+  k_direct_sum<<<g, kDsTile, 0, st>>>(N, pos, mat, mref, eps * eps, idx, nt, chunk, acc, pot);
+  return 1;
+}
+
+}  // namespace ccs

@@ -214,6 +214,14 @@ class NBody:
         self._check(lib().ccs_device_ptrs(self._h, C.byref(d)), "ccs_device_ptrs")
         return d
 
+    def direct_sum(self, idx):
+        """The exact pull (binary64 direct sum, softening a) at particles idx: (acc n x 3, pot n)."""
+        idx = np.ascontiguousarray(idx, np.int32)
+        acc = np.zeros((len(idx), 3), np.float64)
+        pot = np.zeros(len(idx), np.float64)
+        self._check(lib().ccs_direct_sum(self._h, ptr(idx), len(idx), ptr(acc), ptr(pot)), "ccs_direct_sum")
+        return acc, pot
+
     def books(self, with_diag=True):
         """The conservation books on the device in binary64 (src/nbody.js:837-850)."""
         out = np.zeros(L.BOOKS, np.float64)

@@ -170,6 +170,13 @@ int ccs_device_ptrs(ccs_handle *h, ccs_device_buffers *out);
  * [8] PE (needs a diag pass), [9] Q/2, [10] unseated fraction, [11] full fraction */
 #define CCS_BOOKS 12
 int ccs_books(ccs_handle *h, int with_diag, double out[CCS_BOOKS]);
+/* The exact pull, for the force-error measurement and the learned correction's
+ * labels (no counterpart in the reference, which has no direct sum): binary64
+ * acceleration (n*3) and potential (n) at the particles idx[0..n), from all N,
+ * Newton softened at the particle radius a (the P3M pass's softening,
+ * src/glsl-sim.js:745), self term excluded, G = 1. */
+int ccs_direct_sum(ccs_handle *h, const int32_t *idx, int n, double *acc3, double *pot);
+
 /* Internal buffers, for tests and the console checks of index.html:531-556:
  * which = CCS_BUF_* below; bytes must equal the buffer's size. */
 enum {

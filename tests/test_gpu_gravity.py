@@ -40,6 +40,22 @@ def force_error(cc, orc, N, sample=1024, seed=3):
     return rel, loose[idx], rep
 
 
+def test_device_direct_sum_matches_oracle(ccmod, orc):
+    """The library's binary64 direct sum (used by the benchmark's error line) against the oracle's."""
+    from cosmic_collisions_b200 import configs
+    sim, pos, vel, mat = configs.gravity_sweep(N=16384)
+    nb = ccmod.NBody(0)
+    try:
+        nb.upload(sim, pos, vel, mat)
+        idx = np.arange(0, 16384, 37, dtype=np.int32)
+        acc, pot = nb.direct_sum(idx)
+    finally:
+        nb.close()
+    ref, rpot = orc.direct_sum(pos, sim.m * mat.astype(np.float64), sim.a, idx)
+    assert np.allclose(acc, ref, rtol=1e-10, atol=1e-13)
+    assert np.allclose(pot, rpot, rtol=1e-10)
+
+
 def test_force_error_vs_direct_sum(ccmod, orc):
     rel, loose, rep = force_error(ccmod, orc, 65536)
     med, p99 = np.median(rel), np.percentile(rel, 99)
