@@ -34,7 +34,7 @@ EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_ma
            "ccs_sort_morton", "ccs_diag_async", "ccs_poll", "ccs_fof", "ccs_pair_table", "ccs_read_state",
            "ccs_write_state", "ccs_device_ptrs", "ccs_books", "ccs_read_buffer", "ccs_pass_slots",
            "ccs_pass_mesh", "ccs_pass_pp", "ccs_pass_sim", "ccs_pass_diag", "ccs_advance_host", "ccs_sync",
-           "ccs_timing", "ccs_timing_read", "ccs_launch_count", "ccs_direct_sum"]
+           "ccs_timing", "ccs_timing_read", "ccs_launch_count", "ccs_direct_sum", "ccs_pp_force_static"]
 
 
 class Uniforms(C.Structure):
@@ -168,6 +168,7 @@ def lib():
         "ccs_timing_read": (I, [H, I, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
         "ccs_launch_count": (C.c_int64, [H]),
         "ccs_direct_sum": (I, [H, P, I, P, P]),
+        "ccs_pp_force_static": (I, [P, P, I, P, C.c_float, C.c_float, C.c_float, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

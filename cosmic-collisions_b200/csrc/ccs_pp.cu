@@ -140,3 +140,71 @@ int launch_pp_force(const ccs_uniforms *u, const float4 *list, const float *box,
 }
 
 }  // namespace ccs
+
+// ---------------------------------------------------------------------------
+// The pairwise pass without allocation: ccs_pp_force_static.
+//
+// Some callers cannot call cudaMalloc at the point they need this pass: a
+// host that runs the step inside a device-memory budget owned by someone
+// else (a JavaScript or game engine's arena, a framework's caching pool),
+// code that must not trigger the device-wide synchronisation cudaMalloc and
+// cudaFree imply, or a loop that may not fail on an out-of-memory halfway
+// through a frame.  They hand over the list, the boxes, the table and the
+// output in memory they already own; the pass's only scratch -- the partial
+// sums of the 2-D tiling -- lives here, in a file-scope device array sized for
+// lists of up to CCS_PP_STATIC_MAX entries (2 MiB, held by every GPU that
+// loads the library until the process exits).  Its uniforms live in a second
+// static device struct, filled by an asynchronous copy on the caller's stream.
+// Every call shares both: two calls that overlap on the GPU (different
+// streams, or another thread) race and must be ordered by the caller.
+// Nothing in the scratch has to start at zero -- every partial the reduction
+// reads is written earlier in the same call.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+constexpr int kStaticMaxDevices = 64;
+constexpr size_t kStaticScratch = (size_t)4 * ccs::kMaxChunks * CCS_PP_STATIC_MAX;   // float4 partials: 2 MiB
+}  // namespace
+
+static __device__ __align__(256) float4 g_pp_scratch[kStaticScratch];
+static __device__ __align__(256) ccs_uniforms g_pp_uniforms;
+
+namespace {
+std::mutex g_pp_static_mutex;
+float4 *g_pp_scratch_at[kStaticMaxDevices] = {};
+ccs_uniforms *g_pp_uniforms_at[kStaticMaxDevices] = {};
+}  // namespace
+
+extern "C" int ccs_pp_force_static(const float *list4, const float *box, int n, const float *tab2, float cut,
+                                   float a2, float gm, float *force4, void *stream) {
+  if (n < 0 || (n > 0 && (!list4 || !box || !tab2 || !force4))) return CCS_E_ARG;
+  if (n > CCS_PP_STATIC_MAX) return CCS_E_RANGE;
+  if (n == 0) return CCS_OK;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kStaticMaxDevices) return CCS_E_CUDA;
+  {
+    // set-up, once per device, with that device current: the arrays' device addresses (in host code
+    // their names stand for host-side shadows, never for device memory)
+    std::lock_guard<std::mutex> lock(g_pp_static_mutex);
+    if (!g_pp_scratch_at[dev]) {
+      void *s = nullptr, *u = nullptr;
+      if (cudaGetSymbolAddress(&s, g_pp_scratch) != cudaSuccess || !s) return CCS_E_CUDA;
+      if (cudaGetSymbolAddress(&u, g_pp_uniforms) != cudaSuccess || !u) return CCS_E_CUDA;
+      g_pp_uniforms_at[dev] = static_cast<ccs_uniforms *>(u);
+      g_pp_scratch_at[dev] = static_cast<float4 *>(s);
+    }
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  ccs_uniforms u{};
+  u.cut = cut;
+  u.a2 = a2;
+  u.Gm = gm;
+  u.ppCount = n;
+  if (cudaMemcpyAsync(g_pp_uniforms_at[dev], &u, sizeof u, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return CCS_E_CUDA;
+  ccs::launch_pp_force(g_pp_uniforms_at[dev], reinterpret_cast<const float4 *>(list4), box, n,
+                       reinterpret_cast<const float2 *>(tab2), g_pp_scratch_at[dev],
+                       reinterpret_cast<float4 *>(force4), st);
+  return cudaGetLastError() == cudaSuccess ? CCS_OK : CCS_E_CUDA;
+}

@@ -177,6 +177,24 @@ int ccs_books(ccs_handle *h, int with_diag, double out[CCS_BOOKS]);
  * src/glsl-sim.js:745), self term excluded, G = 1. */
 int ccs_direct_sum(ccs_handle *h, const int32_t *idx, int n, double *acc3, double *pot);
 
+/* The P3M pairwise pass with no allocation at all, for callers that may not
+ * call cudaMalloc (a host running inside a device-memory budget it does not
+ * own, or code that must not pay cudaMalloc's device-wide synchronisation).
+ * No counterpart in the reference.  Every pointer is caller-owned device
+ * memory: list4 (n x float4: position, mass ratio; 0 mass = empty seat), box
+ * (n floats: the box each entry reads, -1 for neither), tab2 (64 x 2 floats:
+ * the mesh pair table of ccs_pair_table), force4 (out: 4 x n float4, the four
+ * quarter-list slices, slice-major, as the contact step adds them).  cut, a2
+ * and gm are the uniforms uCut, uA2, uGm.  stream is a cudaStream_t (NULL:
+ * the legacy default stream).  n may not exceed CCS_PP_STATIC_MAX
+ * (CCS_E_RANGE otherwise).  The scratch is one static 2 MiB device array
+ * shared by all calls: calls that overlap on the GPU race.  The first call on
+ * a device looks the array up on that device; make it before any stream
+ * capture. */
+#define CCS_PP_STATIC_MAX 2048
+int ccs_pp_force_static(const float *list4, const float *box, int n, const float *tab2, float cut, float a2,
+                        float gm, float *force4, void *stream);
+
 /* Internal buffers, for tests and the console checks of index.html:531-556:
  * which = CCS_BUF_* below; bytes must equal the buffer's size. */
 enum {
