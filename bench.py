@@ -52,6 +52,19 @@ def impact_opt(N):
                 rest=0.3, mImp=0.1, mTarget=0.9, rhoR=7.8 / 3.3, rhoCrust=2.7 / 3.3, crustFrac=0.05)
 
 
+def max_over_ranks(x):
+    """The largest of x over the ranks of the process group (x itself without one): the job's time is
+    its slowest rank's."""
+    import torch
+    import torch.distributed as td
+    if not (td.is_available() and td.is_initialized()) or td.get_world_size() == 1:
+        return x
+    dev = "cuda" if td.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -217,13 +230,70 @@ def prepare(nb, cc, N, prep_steps, log):
         % (time.perf_counter() - t0, n_rigid, done, nb.sim.t, nb.pp["loose"], nb.pp["count"], r.largest))
 
 
+def run_ensemble(args, log):
+    """The batched ensemble: `args.ensemble` impacts of uneven size (seeded: N over the page's counts,
+    impactor 0.02-1 M_earth, 0-75 degrees, 1.0-2.6 v_esc), each prepared to first touch, then advanced
+    `args.ens_steps` steps each.  Every instance is a handle on its own stream; the host interleaves one
+    captured 8-step graph per instance per round, so the instances run concurrently on the GPU.
+    Reports the aggregate particle-steps/s and the p50/p99 of the per-instance step time."""
+    import numpy as np
+    import torch
+    import cosmic_collisions_b200 as cc
+    from cosmic_collisions_b200 import configs
+    opts = configs.ensemble_opts(args.ensemble)
+    runs = []
+    t0 = time.perf_counter()
+    for opt in opts:
+        nb = cc.NBody(0)
+        nb.build(cc.make_opt(**opt))
+        while nb.sim.phase == 0:
+            nb.settle_some(256)
+        n_rigid = 0
+        while nb.sim.phase == 1 and n_rigid < 5000:
+            nb.rigid_step(0.01)
+            n_rigid += 1
+        if nb.sim.stepNo % 8:
+            nb.steps(8 - nb.sim.stepNo % 8)
+        runs.append(nb)
+    for nb in runs:
+        nb.sync()
+    log("ensemble of %d prepared in %.1fs (%d particles)" % (len(runs), time.perf_counter() - t0,
+                                                             sum(nb.sim.N for nb in runs)))
+    blocks = max(1, args.ens_steps // 8)
+    streams = [torch.cuda.ExternalStream(nb.device_buffers().stream) for nb in runs]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in runs]
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    for k, (nb, s) in enumerate(zip(runs, streams)):
+        with torch.cuda.stream(s):
+            ev[k][0].record(s)
+    for _ in range(blocks):
+        for nb in runs:
+            nb.steps(8)
+    for k, (nb, s) in enumerate(zip(runs, streams)):
+        with torch.cuda.stream(s):
+            ev[k][1].record(s)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    per_step_ms = np.array([a.elapsed_time(b) / (8 * blocks) for a, b in ev])
+    total = sum(nb.sim.N for nb in runs) * 8 * blocks
+    line = {"metric": "ensemble aggregate particle-steps/s", "value": total / wall, "unit": "particle-steps/s",
+            "instances": len(runs), "steps_each": 8 * blocks, "particles": int(sum(nb.sim.N for nb in runs)),
+            "per_instance_step_ms": {"p50": float(np.percentile(per_step_ms, 50)),
+                                     "p99": float(np.percentile(per_step_ms, 99))},
+            "wall_s": wall, "mode": "one handle and stream per impact, captured 8-step graphs interleaved"}
+    for nb in runs:
+        nb.close()
+    return line
+
+
 def run_ours(args, rank, world, log):
     import torch
     import cosmic_collisions_b200 as cc
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    N = args.n
+    N = args.particles
     nb = cc.NBody(dev)
     lib = cc.lib()
     prepare(nb, cc, N, args.prep, log)
@@ -278,11 +348,7 @@ def run_ours(args, rank, world, log):
         kt[name] = {"launches": cnt.value, "total_ms": tot.value,
                     "mean_us": 1e3 * tot.value / cnt.value if cnt.value else None}
     lib.ccs_timing(nb.handle, 0)
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms))
     value = world * N * args.steps / (total_ms / 1e3)
 
     # the same steps back to back from captured 8-step graphs, state L2-resident (no flush)
@@ -297,7 +363,7 @@ def run_ours(args, rank, world, log):
     with torch.cuda.stream(stream):
         g1.record(stream)
     nb.sync()
-    resident_ms = g0.elapsed_time(g1)
+    resident_ms = max_over_ranks(g0.elapsed_time(g1))
 
     # end to end through the host-buffer plugin call
     st = nb.read_state()
@@ -315,11 +381,7 @@ def run_ours(args, rank, world, log):
         rc = lib.ccs_advance_host(nb.handle, P(hp), P(hv), P(hq), 1, P(hp), P(hv), P(ha), P(hq))
         if rc:
             raise RuntimeError("ccs_advance_host: %d" % rc)
-    e2e_s = time.perf_counter() - e0
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - e0)
     h2d = N * (16 + 16 + 4)
     d2h = N * (16 + 16 + 16 + 4)
 
@@ -373,10 +435,13 @@ def main():
     ap.add_argument("--steps", type=int, default=1024)
     ap.add_argument("--warmup", type=int, default=16)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--particles", type=int, default=262144)
     ap.add_argument("--prep", type=int, default=720, help="full-phase steps before timing")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="run the batched ensemble of this many impacts instead and print its line")
+    ap.add_argument("--ens-steps", type=int, default=2000)
     ap.add_argument("--profile", action="store_true",
                     help="prepare, warm up, then run --steps steps inside cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no bench line")
@@ -390,15 +455,20 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        ref = cpu_reference(args.n, min_seconds=args.cpu_seconds)
+        ref = cpu_reference(args.particles, min_seconds=args.cpu_seconds)
         line = {"impl": "reference", "metric": "particle-steps/s @262k, plain P3M step", "value": ref["value"],
                 "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": {"workload": "full plain giant impact, %d particles" % args.n},
+                "data": "synthetic", "config": {"workload": "full plain giant impact, %d particles" % args.particles},
                 "cpu_baseline": ref,
                 "e2e": {"value": ref["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
+        return
+
+    if args.ensemble:
+        if rank == 0:
+            print(json.dumps(run_ensemble(args, log)), flush=True)
         return
 
     if world > 1:
@@ -410,7 +480,7 @@ def main():
     line = run_ours(args, rank, world, log)
     if rank == 0:
         if world == 1 and not args.no_cpu and not args.profile:
-            line["cpu_baseline"] = cpu_reference(args.n, min_seconds=args.cpu_seconds)
+            line["cpu_baseline"] = cpu_reference(args.particles, min_seconds=args.cpu_seconds)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as td

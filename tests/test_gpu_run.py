@@ -1,0 +1,96 @@
+"""A whole run: the small giant impact (16,384 particles, 0.9 + 0.1 M_earth,
+45 degrees, 1.0 v_esc) taken through settle, the rigid approach, first touch
+and the full phase with runTo's analysis every 360 steps, on the GPU and on
+the CPU oracle.
+
+The books -- angular momentum against the first look, and the energy balance
+(KE + PE + elastic + heat) as a fraction of KE - PE -- must be kept to a
+fraction of a percent, as the reference's readout states (README.md:72,187).
+Particle trajectories of two float implementations part ways in a collision,
+so the two runs are compared in aggregate: the same clock and step count, and
+the same books and largest body to small tolerances.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+T_END = 4.0
+
+
+def balance(r, ref):
+    return ((r.KE + r.PE + r.EL + r.Q) - ref["EQ"]) / ref["scale"]
+
+
+def test_concurrent_handles_match_a_lone_run(ccmod):
+    """An ensemble's instances are handles on their own streams: interleaved, they step as one alone does.
+
+    The contact forces are summed with float atomics, so two runs of the same
+    state differ by rounding in every step, and from an unsettled packing that
+    difference grows by orders of magnitude within a few dozen steps.  The
+    comparison is therefore one 8-step graph block (the window the oracle
+    parity holds at 1e-4) with the handles' blocks in flight together; a
+    handle that read another's buffers or uniforms would be off by O(1).
+    """
+    from cosmic_collisions_b200 import configs
+    opt = configs.small_impact_opt(16384)
+    runs = [ccmod.NBody(0) for _ in range(3)]
+    try:
+        for nb in runs:
+            nb.build(opt)
+            nb.settle_some(64)
+            nb.sync()
+        runs[0].steps(8)                # two handles' blocks enqueued back to back, no sync between
+        runs[1].steps(8)
+        runs[0].sync()
+        runs[1].sync()
+        runs[2].steps(8)                # one alone
+        states = [nb.read_state() for nb in runs]
+        clocks = [(nb.sim.stepNo, nb.sim.t) for nb in runs]
+    finally:
+        for nb in runs:
+            nb.close()
+    assert clocks[0] == clocks[1] == clocks[2]
+    ref = states[2]
+    for st in states[:2]:
+        for k in ("pos", "vel"):
+            a, b = st[k][:, :3].astype(np.float64), ref[k][:, :3].astype(np.float64)
+            assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max(), k
+
+
+def test_small_impact_run_keeps_its_books(ccmod):
+    from cosmic_collisions_b200 import configs
+    from oracle_run import OracleRun
+    opt = configs.small_impact_opt(16384)
+    nb = ccmod.NBody(0)
+    try:
+        nb.build(opt)
+        nb.run_to(T_END)
+        g, gref, gs = nb.report, nb.ref, nb.sim
+        steps, t, soft = gs.stepNo, gs.t, gs.soft
+        books = nb.books(with_diag=False)
+    finally:
+        nb.close()
+    oc = OracleRun(opt)
+    oc.run_to(T_END)
+    o, oref = oc.report, oc.ref
+    print("GPU: L %.6f (first look %.6f) balance %.4f drift %.3e largest %.4f | oracle: L %.6f balance %.4f "
+          "largest %.4f | steps %d" % (g.L, gref["L"], balance(g, gref), g.drift, g.largest, o.L,
+                                       balance(o, oref), o.largest, steps))
+    # the same schedule on both sides
+    assert steps == oc.sim.stepNo and t == oc.sim.t and soft == oc.sim.soft == 1
+    # the books, kept to a fraction of a percent
+    assert abs(g.L - gref["L"]) / gref["L"] < 1e-3
+    assert abs(balance(g, gref)) < 1e-2
+    assert g.drift < 1e-4
+    # and the same run in aggregate
+    assert abs(g.L - o.L) / o.L < 1e-3
+    assert abs(g.largest - o.largest) < 0.01
+    assert abs(balance(g, gref) - balance(o, oref)) < 5e-3
+    # the device's binary64 books agree with the host analysis's
+    assert abs(books["M"] - g.M) < 1e-9
+    assert abs(np.sqrt(books["Lx"] ** 2 + books["Ly"] ** 2 + books["Lz"] ** 2) - g.L) < 1e-6 * g.L
