@@ -18,7 +18,7 @@ A step is one full-phase step of the reference schedule (contact grid every
            step, so each step starts from HBM.  Max over ranks.
   e2e      the same metric through the host-buffer C-ABI call
            (ccs_advance_host: pinned host state in, one step, state out).
-  roofline the contact step kernel (k_simulate): algorithmic bytes (92 B per
+  roofline the contact step kernel (k_contact_step): algorithmic bytes (92 B per
            particle: pos, vel, mat, q in; pos, vel, aux, q out) over its mean
            event-timed duration, against the measured HBM copy bandwidth.
   cpu_baseline / --impl reference: the CPU oracle (a C restatement of the
@@ -77,8 +77,8 @@ def measured_peaks():
 
 
 def committed_traffic():
-    """dram bytes per k_simulate launch from the committed ncu summary, scaled to a launch of N particles."""
-    p = os.path.join(ROOT, "profiles", "simulate_traffic.txt")
+    """dram bytes per k_contact_step launch from the committed ncu summary, scaled to a launch of N particles."""
+    p = os.path.join(ROOT, "profiles", "contact_step_traffic.txt")
     if not os.path.exists(p):
         return None
     vals = {}
@@ -418,7 +418,7 @@ def run_ours(args, rank, world, log):
                 "d2h_bytes_per_step": d2h, "api": "ccs_advance_host, one step per call, pinned host buffers"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "peak_kind": peak_kind + " hbm_gbs",
-                     "kernel": "k_simulate (contacts + gather + kick/drift)",
+                     "kernel": "k_contact_step (contacts + gather + kick/drift)",
                      "traffic": tpp * N if tpp else None,
                      "algorithmic_bytes_per_launch": ALG_BYTES_SIM * N},
         "gpu_launches": int(launches),
