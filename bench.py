@@ -23,6 +23,11 @@ A step is one full-phase step of the reference schedule (contact grid every
            event-timed duration, against the measured HBM copy bandwidth.
   cpu_baseline / --impl reference: the CPU oracle (a C restatement of the
            reference's step, all host cores, OpenMP) on a bounded sample.
+  nn_corrected  the same timed steps with the learned pairwise correction
+           attached (BF16 network on the tensor cores, half the plain cut),
+           after training it on the device on pairs drawn from the same impact
+           at full-phase steps 0, 1000 and 3000; its force error on the same
+           gravity sweep as force_error.
 
 Multi-GPU: one process per GPU, independent replicas of the impact (the step
 has no partition worth a data-path collective at this size): weak scaling.
@@ -172,15 +177,18 @@ def cpu_reference(N, min_seconds=10.0, min_steps=8, threads=None):
                       % (steps, N, el, cores)}
 
 
-def force_error(cc, dev, N, sample=2048, seed=3):
+def force_error(cc, dev, N, sample=2048, seed=3, net=None):
     """The gravity-only sweep (Plummer sphere + 10 % debris, equal masses, 1 M_earth): one force evaluation
-    of the plain P3M step against the library's binary64 direct sum at a seeded sample of particles."""
+    of the P3M step (plain, or with the learned correction `net`) against the library's binary64 direct sum
+    at a seeded sample of particles."""
     import numpy as np
     from cosmic_collisions_b200 import configs
     sim, pos, vel, mat = configs.gravity_sweep(N=N)
     nb = cc.NBody(dev)
     try:
         nb.upload(sim, pos, vel, mat)
+        if net is not None:
+            nb.set_pp_nn(net)
         nb.pass_slots()
         nb.pass_diag()
         D = nb.buffer("diag")
@@ -194,7 +202,10 @@ def force_error(cc, dev, N, sample=2048, seed=3):
     finally:
         nb.close()
     rel = np.linalg.norm(g[idx] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    on = np.isin(idx, np.asarray(lst, np.int64))
     return {"median": float(np.median(rel)), "p99": float(np.percentile(rel, 99)), "sample": sample,
+            "loose_list_members_in_sample": int(on.sum()),
+            "loose_list_median": float(np.median(rel[on])) if on.any() else None,
             "workload": "gravity sweep, %d equal masses: Plummer sphere (scale 1 R_earth) + 10%% uniform debris" % N,
             "loose_list": int(rep.ppCount), "loose_total": int(rep.ppLoose),
             "reference": "binary64 direct sum, softening a, self term excluded"}
@@ -215,9 +226,18 @@ def prepare(nb, cc, N, prep_steps, log):
         n_rigid += 1
     if nb.sim.phase != 2:
         raise RuntimeError("the bodies never touched")
+    done = advance(nb, prep_steps)
+    r = nb.report
+    log("prepared in %.1fs: %d rigid steps, %d full steps, t=%.3f, loose=%d (list %d), largest=%.3f"
+        % (time.perf_counter() - t0, n_rigid, done, nb.sim.t, nb.pp["loose"], nb.pp["count"], r.largest))
+
+
+def advance(nb, steps):
+    """steps full-phase steps with runTo's synchronous analysis every 360 steps (index.html:592-600), then a
+    closing analysis."""
     done = 0
-    while done < prep_steps:
-        n = min(360 - (nb.sim.stepNo - nb.analyzed_at), prep_steps - done)
+    while done < steps:
+        n = min(360 - (nb.sim.stepNo - nb.analyzed_at), steps - done)
         n = max(n, 1)
         nb.steps(n)
         done += n
@@ -225,9 +245,50 @@ def prepare(nb, cc, N, prep_steps, log):
             nb.analyze(True)
     nb.analyze(True)
     nb.sync()
-    r = nb.report
-    log("prepared in %.1fs: %d rigid steps, %d full steps, t=%.3f, loose=%d (list %d), largest=%.3f"
-        % (time.perf_counter() - t0, n_rigid, done, nb.sim.t, nb.pp["loose"], nb.pp["count"], r.largest))
+    return done
+
+
+def learned_correction(cc, dev, N, log, pairs=9_000_000, epochs=8, snaps=(0, 1000, 3000), held=262_144):
+    """The learned P3M correction (config 4): a network trained on the device on pairs drawn from the full
+    plain impact at full-phase steps 0, 1000 and 3000, labelled by the binary64 mesh arithmetic of the
+    isolated pair.  Returns the network and what its training and a held-out set say."""
+    import numpy as np
+    from cosmic_collisions_b200.learned import LearnedCorrection
+    net = LearnedCorrection(dev, seed=2024)
+    nb = cc.NBody(dev)
+    t0 = time.perf_counter()
+    try:
+        prepare(nb, cc, N, 0, log)
+        done = 0
+        for k, s in enumerate(snaps):
+            done += advance(nb, s - done) if s > done else 0
+            net.sample_state(nb, pairs // len(snaps), seed=1000 + k)
+        net.sample_state(nb, held, seed=9999)              # held out: the last snapshot, another draw
+    finally:
+        nb.close()
+    t_sample = time.perf_counter() - t0
+    n_train = pairs // len(snaps) * len(snaps)
+    t1 = time.perf_counter()
+    loss = net.train(0, n_train, epochs=epochs, tiles_per_cta=4, lr=2e-3)
+    t_train = time.perf_counter() - t1
+    rec, lab = net.read_pool(n_train, held)
+    live = np.isfinite(rec[:, 0])
+    rec, lab = rec[live], lab[live]
+    y = net.forward(rec)
+    r = np.linalg.norm(rec[:, :3], axis=1)
+    near = r < 1.7
+    rms = lambda v: float(np.sqrt((v ** 2).sum(1).mean())) if len(v) else None
+    info = {"pairs": int(n_train), "epochs": epochs, "snapshots_full_steps": list(snaps),
+            "loss_first_epoch": float(loss[0]), "loss_last_epoch": float(loss[-1]),
+            "sample_s": t_sample, "train_s": t_train,
+            "held_out": {"pairs": int(len(rec)), "near_pairs_r_lt_1p7_cells": int(near.sum()),
+                         "table_rms_near": rms(lab[near]), "network_rms_near": rms((y - lab)[near]),
+                         "table_rms_all": rms(lab), "network_rms_all": rms(y - lab),
+                         "unit": "mesh pair force, cells^-2 (the table's error is the label itself)"}}
+    log("learned correction: %d pairs, loss %.3e -> %.3e in %.1fs; held-out near rms table %.3e net %.3e"
+        % (n_train, loss[0], loss[-1], t_train, info["held_out"]["table_rms_near"] or 0,
+           info["held_out"]["network_rms_near"] or 0))
+    return net, info
 
 
 def run_ensemble(args, log):
@@ -287,6 +348,45 @@ def run_ensemble(args, log):
     return line
 
 
+def timed_steps(nb, lib, stream, flush, steps, dev, dist):
+    """steps direct-launch steps, L2 flushed before each, each bracketed by CUDA events on the library's
+    stream; kernel times from the library's own events; clocks sampled meanwhile."""
+    import ctypes as C
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    clocks = Clocks(dev)
+    if dist:
+        import torch.distributed as td
+        td.barrier()
+    torch.cuda.synchronize()
+    lib.ccs_timing(nb.handle, 1)
+    l0 = lib.ccs_launch_count(nb.handle)
+    clocks.start()
+    w0 = time.perf_counter()
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+        nb.step(False, False)
+        nb.sim.t += nb.sim.dt
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+    nb.sync()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    clk = clocks.stop()
+    launches = lib.ccs_launch_count(nb.handle) - l0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    kt = {}
+    for kid, name in enumerate(["simulate", "contact_grid", "deposit", "cell", "pp_force"]):
+        tot, cnt = C.c_double(), C.c_int()
+        lib.ccs_timing_read(nb.handle, kid, C.byref(tot), C.byref(cnt))
+        kt[name] = {"launches": cnt.value, "total_ms": tot.value,
+                    "mean_us": 1e3 * tot.value / cnt.value if cnt.value else None}
+    lib.ccs_timing(nb.handle, 0)
+    return step_ms, kt, launches, wall, clk
+
+
 def run_ours(args, rank, world, log):
     import torch
     import cosmic_collisions_b200 as cc
@@ -312,42 +412,14 @@ def run_ours(args, rank, world, log):
                "stepNo": nb.sim.stepNo, "loose_list": nb.pp["count"]}
         nb.close()
         return out
+    import ctypes as C
     buf = nb.device_buffers()
     stream = torch.cuda.ExternalStream(buf.stream, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    clocks = Clocks(dev)
     dist = world > 1
     if dist:
         import torch.distributed as td
-        td.barrier()
-    torch.cuda.synchronize()
-    lib.ccs_timing(nb.handle, 1)
-    l0 = lib.ccs_launch_count(nb.handle)
-    clocks.start()
-    w0 = time.perf_counter()
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(float(k))
-            ev[k][0].record(stream)
-        nb.step(False, False)
-        nb.sim.t += nb.sim.dt
-        with torch.cuda.stream(stream):
-            ev[k][1].record(stream)
-    nb.sync()
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - w0
-    clk = clocks.stop()
-    launches = lib.ccs_launch_count(nb.handle) - l0
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    import ctypes as C
-    kt = {}
-    for kid, name in enumerate(["simulate", "contact_grid", "deposit", "cell", "pp_force"]):
-        tot, cnt = C.c_double(), C.c_int()
-        lib.ccs_timing_read(nb.handle, kid, C.byref(tot), C.byref(cnt))
-        kt[name] = {"launches": cnt.value, "total_ms": tot.value,
-                    "mean_us": 1e3 * tot.value / cnt.value if cnt.value else None}
-    lib.ccs_timing(nb.handle, 0)
+    step_ms, kt, launches, wall, clk = timed_steps(nb, lib, stream, flush, args.steps, dev, dist)
     total_ms = max_over_ranks(sum(step_ms))
     value = world * N * args.steps / (total_ms / 1e3)
 
@@ -386,12 +458,31 @@ def run_ours(args, rank, world, log):
     d2h = N * (16 + 16 + 16 + 4)
 
     ferr = force_error(cc, dev, N) if rank == 0 else None
+
+    # the learned correction (config 4): train, attach, the same timed steps, the same force sweep
+    nn_line = None
+    if not args.no_nn:
+        net, info = learned_correction(cc, dev, N, log, pairs=args.nn_pairs, epochs=args.nn_epochs)
+        nb.set_pp_nn(net)
+        for _ in range(args.warmup):
+            nb.step(False, False)
+            nb.sim.t += nb.sim.dt
+        nb.sync()
+        nn_ms, nn_kt, nn_launches, nn_wall, nn_clk = timed_steps(nb, lib, stream, flush, args.steps, dev, dist)
+        nn_total = max_over_ranks(sum(nn_ms))
+        nn_err = force_error(cc, dev, N, net=net) if rank == 0 else None
+        nb.set_pp_nn(None)
+        net.close()
+        nn_line = {"value": world * N * args.steps / (nn_total / 1e3), "unit": "particle-steps/s",
+                   "ms_per_step": nn_total / args.steps, "pp_cut_cells": 2.5, "loose_list": nb.pp["count"],
+                   "kernels_us": {k: v["mean_us"] for k, v in nn_kt.items()}, "gpu_launches": int(nn_launches),
+                   "clocks": nn_clk, "wall_s_timed_region": nn_wall, "force_error": nn_err, "training": info}
     peak, peak_kind = measured_peaks()
     sim_mean_us = kt["simulate"]["mean_us"]
     achieved = ALG_BYTES_SIM * N / (sim_mean_us * 1e-6) / 1e9 if sim_mean_us else None
     tpp = committed_traffic()
     line = {
-        "metric": "particle-steps/s @262k, plain P3M step (NN-corrected form not built yet)",
+        "metric": "particle-steps/s @262k, plain P3M step (value) and the NN-corrected P3M step (nn_corrected)",
         "value": value,
         "unit": "particle-steps/s",
         "n_gpus": world,
@@ -424,6 +515,7 @@ def run_ours(args, rank, world, log):
         "gpu_launches": int(launches),
         "clocks": clk,
         "force_error": ferr,
+        "nn_corrected": nn_line,
     }
     nb.close()
     return line
@@ -442,6 +534,9 @@ def main():
     ap.add_argument("--ensemble", type=int, default=0,
                     help="run the batched ensemble of this many impacts instead and print its line")
     ap.add_argument("--ens-steps", type=int, default=2000)
+    ap.add_argument("--no-nn", action="store_true", help="skip the learned-correction leg")
+    ap.add_argument("--nn-pairs", type=int, default=9_000_000, help="training pairs (three snapshots)")
+    ap.add_argument("--nn-epochs", type=int, default=8)
     ap.add_argument("--profile", action="store_true",
                     help="prepare, warm up, then run --steps steps inside cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no bench line")

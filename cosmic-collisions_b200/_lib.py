@@ -34,7 +34,12 @@ EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_ma
            "ccs_sort_morton", "ccs_diag_async", "ccs_poll", "ccs_fof", "ccs_pair_table", "ccs_read_state",
            "ccs_write_state", "ccs_device_ptrs", "ccs_books", "ccs_read_buffer", "ccs_pass_slots",
            "ccs_pass_mesh", "ccs_pass_pp", "ccs_pass_sim", "ccs_pass_diag", "ccs_advance_host", "ccs_sync",
-           "ccs_timing", "ccs_timing_read", "ccs_launch_count", "ccs_direct_sum", "ccs_pp_force_static"]
+           "ccs_timing", "ccs_timing_read", "ccs_launch_count", "ccs_direct_sum", "ccs_pp_force_static",
+           "ccs_nn_create", "ccs_nn_destroy", "ccs_nn_last_error", "ccs_nn_set_params", "ccs_nn_get_params",
+           "ccs_nn_clear", "ccs_nn_pool_size", "ccs_nn_sample_state", "ccs_nn_sample_uniform", "ccs_nn_read_pool",
+           "ccs_nn_train", "ccs_nn_forward", "ccs_nn_labels", "ccs_nn_grad", "ccs_set_pp_nn"]
+NN_PARAMS = 4803
+NN_CUT_CELLS = 2.5
 
 
 class Uniforms(C.Structure):
@@ -169,6 +174,21 @@ def lib():
         "ccs_launch_count": (C.c_int64, [H]),
         "ccs_direct_sum": (I, [H, P, I, P, P]),
         "ccs_pp_force_static": (I, [P, P, I, P, C.c_float, C.c_float, C.c_float, P, P]),
+        "ccs_nn_create": (I, [I, C.c_uint32, C.POINTER(C.c_void_p)]),
+        "ccs_nn_destroy": (I, [H]),
+        "ccs_nn_last_error": (C.c_char_p, [H]),
+        "ccs_nn_set_params": (I, [H, P]),
+        "ccs_nn_get_params": (I, [H, P]),
+        "ccs_nn_clear": (I, [H]),
+        "ccs_nn_pool_size": (C.c_int64, [H]),
+        "ccs_nn_sample_state": (I, [H, H, C.c_int64, C.c_uint32]),
+        "ccs_nn_sample_uniform": (I, [H, C.c_int64, C.c_uint32]),
+        "ccs_nn_read_pool": (I, [H, C.c_int64, C.c_int64, P, P]),
+        "ccs_nn_train": (I, [H, C.c_int64, C.c_int64, I, I, C.c_float, P]),
+        "ccs_nn_forward": (I, [H, P, C.c_int64, P]),
+        "ccs_nn_labels": (I, [H, P, C.c_int64, P]),
+        "ccs_nn_grad": (I, [H, P, P, C.c_int64, P, P]),
+        "ccs_set_pp_nn": (I, [H, H]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

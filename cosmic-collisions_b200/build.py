@@ -12,8 +12,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libccstep.so")
-SOURCES = ["ccs_step.cu", "ccs_contact.cu", "ccs_mesh.cu", "ccs_pp.cu", "ccs_order.cu", "ccs_api.cu", "ccs_host.cpp"]
-HEADERS = ["ccs_device.cuh", "ccs_internal.h", os.path.join("..", "..", "include", "ccstep.h")]
+SOURCES = ["ccs_step.cu", "ccs_contact.cu", "ccs_mesh.cu", "ccs_pp.cu", "ccs_nn.cu", "ccs_order.cu", "ccs_api.cu",
+           "ccs_host.cpp"]
+HEADERS = ["ccs_device.cuh", "ccs_internal.h", "ccs_umma.cuh", os.path.join("..", "..", "include", "ccstep.h")]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17",

@@ -79,6 +79,12 @@ struct ccs_handle {
   float *ppBox = nullptr;
   float2 *tab = nullptr;
   int ppCount = 0, ppLoose = 0;
+  // the learned form of the P3M pass (borrowed network; pair buffers sized for the list)
+  ccs_nn *nn = nullptr;
+  int *nnCounts = nullptr, *nnOffs = nullptr, *nnTotal = nullptr;
+  int2 *nnPairs = nullptr;
+  float4 *nnMesh = nullptr;
+  long nnPairCap = 0;
   float4 *diag = nullptr;
   unsigned *status = nullptr;           // kernel status word (kStatus* bits), sticky until the next build
   // Morton sort scratch
@@ -155,6 +161,10 @@ int check_status(ccs_handle *h) {
   if (st & kStatusGrid) {
     h->err = "contact grid: an insertion gave up after its retry bound (a degenerate pile of particles, "
              "e.g. non-finite positions)";
+    return CCS_E_KERNEL;
+  }
+  if (st & kStatusNN) {
+    h->err = "learned P3M pass: a tensor-core wait gave up";
     return CCS_E_KERNEL;
   }
   return CCS_OK;
@@ -325,7 +335,12 @@ void pass_pp(ccs_handle *h, const ccs_uniforms *U, int count) {
   h->launches += launch_pp_gather(U, h->pos[h->cur], h->mat, h->ppIndex, CCS_PP_CAP, h->ppList, h->ppBox, h->st);
   cudaEvent_t b, e;
   time_begin(h, 4, &b, &e);
-  h->launches += launch_pp_force(U, h->ppList, h->ppBox, CCS_PP_CAP, h->tab, h->ppPart, h->ppForce, h->st);
+  if (h->nn)
+    h->launches += launch_pp_nn(U, h->ppList, h->ppBox, CCS_PP_CAP, h->tab, nn_image(h->nn),
+                                h->nnCounts, h->nnOffs, h->nnTotal, h->nnPairs, h->nnMesh, h->ppForce, h->status,
+                                h->st);
+  else
+    h->launches += launch_pp_force(U, h->ppList, h->ppBox, CCS_PP_CAP, h->tab, h->ppPart, h->ppForce, h->st);
   time_end(h, e);
 }
 
@@ -494,6 +509,31 @@ int ensure_built(ccs_handle *h) {
   return CCS_OK;
 }
 
+// pair buffers of the learned pass, sized for the worst case of an n-entry list (every pair inside the cut)
+int ensure_nn_buffers(ccs_handle *h, int n) {
+  if (!h->nn) return CCS_OK;
+  int rc = CCS_OK;
+  if (!h->nnCounts) {
+    free_graphs(h);
+    rc |= dev_alloc(h, &h->nnCounts, nn_pp_count_ints());
+    rc |= dev_alloc(h, &h->nnOffs, nn_pp_count_ints());
+    rc |= dev_alloc(h, &h->nnTotal, 1);
+    if (rc) return CCS_E_NOMEM;
+  }
+  const long need = std::max<long>(1, (long)n * (long)(n - 1));
+  if (need > h->nnPairCap) {
+    free_graphs(h);   // captured launches hold the old pointers
+    rc |= dev_alloc(h, &h->nnPairs, (size_t)need);
+    rc |= dev_alloc(h, &h->nnMesh, (size_t)need);
+    if (rc) {
+      h->nnPairCap = 0;
+      return CCS_E_NOMEM;
+    }
+    h->nnPairCap = need;
+  }
+  return CCS_OK;
+}
+
 void free_state(ccs_handle *h) {
   free_graphs(h);
   for (int b = 0; b < 2; ++b) {
@@ -507,6 +547,8 @@ void free_state(ccs_handle *h) {
   dev_free(h->mat); dev_free(h->matTmp); dev_free(h->home); dev_free(h->homeTmp);
   dev_free(h->ppIndex); dev_free(h->ppSlot); dev_free(h->ppList); dev_free(h->ppForce); dev_free(h->ppBox);
   dev_free(h->ppPart);
+  dev_free(h->nnCounts); dev_free(h->nnOffs); dev_free(h->nnTotal); dev_free(h->nnPairs); dev_free(h->nnMesh);
+  h->nnPairCap = 0;
   dev_free(h->tab); dev_free(h->diag);
   dev_free(h->keys); dev_free(h->keysTmp); dev_free(h->hist); dev_free(h->vals); dev_free(h->valsTmp);
   dev_free(h->into); dev_free(h->permDev);
@@ -829,6 +871,8 @@ int ccs_set_pp(ccs_handle *h, const int32_t *list, int n, int loose) {
   int rc = ensure_built(h);
   if (rc) return rc;
   if (n < 0 || n > CCS_PP_CAP || (n > 0 && !list)) return CCS_E_ARG;
+  rc = ensure_nn_buffers(h, n);
+  if (rc) return rc;
   for (int k = 0; k < n; ++k)
     if (list[k] < 0 || list[k] >= h->N) {
       h->err = "loose-list index out of range";
@@ -853,6 +897,41 @@ int ccs_set_pp(ccs_handle *h, const int32_t *list, int n, int loose) {
     pass_pp(h, U, n);
   }
   return check_launch(h);
+}
+
+int ccs_set_pp_nn(ccs_handle *h, ccs_nn *nn) {
+  if (!h) return CCS_E_ARG;
+  if (nn && nn_device(nn) != h->device) {
+    h->err = "the network lives on another device";
+    return CCS_E_ARG;
+  }
+  cudaSetDevice(h->device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  free_graphs(h);   // the captured P3M launches change
+  h->nn = nn;
+  if (nn && h->built) return ensure_nn_buffers(h, h->ppCount);
+  return CCS_OK;
+}
+
+int ccs_nn_sample_state(ccs_nn *nn, ccs_handle *h, int64_t count, uint32_t seed) {
+  if (!nn || !h || count < 0) return CCS_E_ARG;
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (nn_device(nn) != h->device) {
+    h->err = "the network lives on another device";
+    return CCS_E_ARG;
+  }
+  cudaSetDevice(h->device);
+  const ccs_uniforms *U;
+  rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);   // the boxes where they are now
+  if (rc) return rc;
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  float4 *D, *S;
+  cudaStream_t st;
+  rc = nn_reserve(nn, count, &D, &S, &st);
+  if (rc) return rc;
+  launch_nn_sample_state(U, h->pos[h->cur], h->N, (long)count, seed, (float)CCS_NN_CUT_CELLS, D, S, st);
+  return nn_commit(nn, count);
 }
 
 int ccs_prime_mono(ccs_handle *h, int box, const float mono[4]) {

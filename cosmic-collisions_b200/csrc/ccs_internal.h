@@ -15,6 +15,7 @@ constexpr int kFine = 64 * 64 * 64;           // 64^3 mesh; index kFine is the s
 constexpr int kCoarse = 4096;                 // 16^3 blocks
 constexpr int kSeats = CCS_SEATS;
 constexpr unsigned kStatusGrid = 1u;          // a contact-cell insertion gave up (degenerate pile)
+constexpr unsigned kStatusNN = 2u;            // a tensor-core wait of the learned P3M pass gave up
 
 // One gravity mesh box: the textures of meshBox(), src/nbody.js:1050-1068,
 // as plain float4 arrays.  fine/force hold 64^3 cells in [z][y][x] order
@@ -75,6 +76,21 @@ int launch_pp_gather(const ccs_uniforms *u, const float4 *pos, const float *mat,
 size_t pp_partial_float4s();
 int launch_pp_force(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,
                     float4 *part, float4 *force, cudaStream_t st);
+// the learned P3M pass (ccs_nn.cu): count / scan / fill the pairs inside half
+// the cut, the network on the tensor cores, the per-target sums
+size_t nn_pp_count_ints();
+int launch_pp_nn(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,
+                 const uint8_t *img, int *counts, int *offs, int *total, int2 *pairs, float4 *mesh, float4 *force,
+                 unsigned *status, cudaStream_t st);
+int launch_nn_sample_state(const ccs_uniforms *u, const float4 *pos, int N, long count, uint32_t seed, float cutG,
+                           float4 *D, float4 *S, cudaStream_t st);
+cudaError_t init_nn_kernels();
+// the network object's engine-facing half: room for count records in its pool,
+// then label them and count them in; its operand image; its device
+int nn_reserve(ccs_nn *nn, int64_t count, float4 **D, float4 **S, cudaStream_t *st);
+int nn_commit(ccs_nn *nn, int64_t count);
+const uint8_t *nn_image(const ccs_nn *nn);
+int nn_device(const ccs_nn *nn);
 int launch_diag(const ccs_uniforms *u, int N, const DiagArgs &a, cudaStream_t st);
 int launch_rigid(const ccs_uniforms *u, int N, const float4 *pos, const float4 *vel, const float4 *aux,
                  const float *q, float4 *posO, float4 *velO, float4 *auxO, float *qO, cudaStream_t st);

@@ -361,6 +361,12 @@ class NBody:
                     "ccs_set_pp")
         self.pp = {"count": n, "loose": int(loose if loose is not None else n)}
 
+    def set_pp_nn(self, net):
+        """Attach a LearnedCorrection to the P3M pass (None: back to the plain table).  The network must outlive
+        the attachment."""
+        self._check(lib().ccs_set_pp_nn(self._h, net.handle if net is not None else None), "ccs_set_pp_nn")
+        self.nn = net
+
     # ---- the scripted driver: window.__impact.runTo, index.html:592-600 ------
     def run_to(self, t, analyze_every=360):
         s = self.sim

@@ -195,6 +195,51 @@ int ccs_direct_sum(ccs_handle *h, const int32_t *idx, int n, double *acc3, doubl
 int ccs_pp_force_static(const float *list4, const float *box, int n, const float *tab2, float cut, float a2,
                         float gm, float *force4, void *stream);
 
+/* ---- the learned pairwise correction ----
+ * No counterpart in the reference.  The plain pass subtracts the mesh's pair
+ * force as the placement-averaged table of meshPairTable (src/nbody.js:48-109;
+ * PPFORCE_FS's T.f, src/glsl-sim.js:738-750).  A network R(d, s) learns what
+ * that table misses: the isolated pair's mesh force less T(r) d / r^3, d the
+ * pair offset in mesh cells (source - target), s the source's position in its
+ * cell; 6 -> 64 -> 64 -> 3 with SiLU, BF16 weights, FP32 accumulation, run and
+ * trained on the tensor cores.  With a network attached, the P3M pass of an
+ * engine corrects the loose pairs inside CCS_NN_CUT_CELLS cells (half the
+ * plain pass's 5) by the plain pass's correction less m_j R(d, s) / FH^2;
+ * detaching it restores the plain pass.  Flat parameter order: W1[64][6]
+ * b1[64] W2[64][64] b2[64] W3[3][64] b3[3]. */
+#define CCS_NN_PARAMS 4803
+#define CCS_NN_CUT_CELLS 2.5
+typedef struct ccs_nn ccs_nn;
+int ccs_nn_create(int device, uint32_t seed, ccs_nn **out);
+int ccs_nn_destroy(ccs_nn *nn);   /* detach it from every engine first */
+const char *ccs_nn_last_error(const ccs_nn *nn);
+int ccs_nn_set_params(ccs_nn *nn, const float *params);   /* also resets the optimiser */
+int ccs_nn_get_params(ccs_nn *nn, float *params);
+/* The pair pool the network trains on: records (d in cells, s in [0,1)) with
+ * their labels, the mesh arithmetic of meshPairTable's field() for the
+ * isolated pair in binary64 less the table's model (cells^-2, unit masses). */
+int ccs_nn_clear(ccs_nn *nn);
+int64_t ccs_nn_pool_size(const ccs_nn *nn);
+/* count pairs of the engine's particles inside the cut, both in box 0; odd
+ * records pair Morton neighbours (index within 128), even ones any two */
+int ccs_nn_sample_state(ccs_nn *nn, ccs_handle *h, int64_t count, uint32_t seed);
+/* count synthetic pairs: s uniform, d uniform in the ball or in distance */
+int ccs_nn_sample_uniform(ccs_nn *nn, int64_t count, uint32_t seed);
+/* records n x 6 floats (NaN offsets mark a dead record), labels n x 3 */
+int ccs_nn_read_pool(ccs_nn *nn, int64_t first, int64_t n, float *rec6, float *label3);
+/* Adam on the mean squared error over pool records [first, first + n):
+ * batches of (SMs x tilesPerCta x 128) pairs, cosine decay from lr to lr/20;
+ * epochLoss (epochs floats, may be NULL) gets each epoch's mean loss */
+int ccs_nn_train(ccs_nn *nn, int64_t first, int64_t n, int epochs, int tilesPerCta, float lr, float *epochLoss);
+/* host records in, the network's output (n x 3) / the label (n x 3) out */
+int ccs_nn_forward(ccs_nn *nn, const float *rec6, int64_t n, float *out3);
+int ccs_nn_labels(ccs_nn *nn, const float *rec6, int64_t n, float *label3);
+/* the gradient (CCS_NN_PARAMS floats) and loss of the mean squared error over
+ * n host records, through the training kernel, without a step */
+int ccs_nn_grad(ccs_nn *nn, const float *rec6, const float *label3, int64_t n, float *grad, float *loss);
+/* attach (or, with NULL, detach) a network to an engine's P3M pass */
+int ccs_set_pp_nn(ccs_handle *h, ccs_nn *nn);
+
 /* Internal buffers, for tests and the console checks of index.html:531-556:
  * which = CCS_BUF_* below; bytes must equal the buffer's size. */
 enum {

@@ -428,10 +428,13 @@ static void pair_field(const double parts[][3], int np, const double at[3], doub
       nodes[f].m += w[k]; nodes[f].x += w[k] * parts[i][0]; nodes[f].y += w[k] * parts[i][1]; nodes[f].z += w[k] * parts[i][2];
     }
   }
-  for (int q = 0; q < nn; q++) { nodes[q].x /= nodes[q].m; nodes[q].y /= nodes[q].m; nodes[q].z /= nodes[q].m; }
+  /* a node of zero weight (a particle exactly on a cell face) carries nothing; the table's random
+   * placings never make one */
+  for (int q = 0; q < nn; q++)
+    if (nodes[q].m > 0) { nodes[q].x /= nodes[q].m; nodes[q].y /= nodes[q].m; nodes[q].z /= nodes[q].m; }
   for (int c = 0; c < nn; c++)
     for (int o = 0; o < nn; o++) {
-      if (o == c) continue;
+      if (o == c || !(nodes[o].m > 0) || !(nodes[c].m > 0)) continue;
       double rx = nodes[o].x - nodes[c].x, ry = nodes[o].y - nodes[c].y, rz = nodes[o].z - nodes[c].z;
       double inv = 1 / sqrt(rx * rx + ry * ry + rz * rz + eps2), inv3 = inv * inv * inv;
       nodes[c].fx += rx * nodes[o].m * inv3; nodes[c].fy += ry * nodes[o].m * inv3; nodes[c].fz += rz * nodes[o].m * inv3;
@@ -447,6 +450,24 @@ static void pair_field(const double parts[][3], int np, const double at[3], doub
     if (f < 0) continue;
     out[0] += w[k] * nodes[f].fx; out[1] += w[k] * nodes[f].fy; out[2] += w[k] * nodes[f].fz; out[3] += w[k] * nodes[f].pot;
   }
+}
+
+/* The label of the learned correction: the mesh's force on a target from a
+ * unit source, field() of meshPairTable (src/nbody.js:60-91) for the isolated
+ * pair, both minus alone, in mesh cells: d = source - target in cells, s the
+ * source's position in its cell (the GLSL_BOX g with its half-cell shift, as
+ * the deposit uses it).  The pair is placed mid-mesh; out in cells^-2. */
+void orc_nn_label(const double d[3], const double s[3], double out[3]) {
+  double q[3], p[3], both[4], alone[4];
+  for (int k = 0; k < 3; k++) {
+    q[k] = (s[k] + 32.0 + 0.5) * FH - FL;
+    p[k] = q[k] - d[k] * FH;
+  }
+  const double two[2][3] = {{p[0], p[1], p[2]}, {q[0], q[1], q[2]}};
+  const double one[1][3] = {{p[0], p[1], p[2]}};
+  pair_field(two, 2, p, both);
+  pair_field(one, 1, p, alone);
+  for (int k = 0; k < 3; k++) out[k] = (both[k] - alone[k]) * (FH * FH);
 }
 
 void orc_pair_table(int bins, double cut, float *f, float *pt) {

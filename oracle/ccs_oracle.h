@@ -87,6 +87,7 @@ double orc_approach_time(const double relr[3], const double relv[3], double M, d
 /* build(): fills sim and the four particle arrays (pos4, vel4 N*4; mat N; home4 N*4) */
 int orc_build(const orc_opt *opt, orc_sim *sim, float *pos4, float *vel4, float *mat, float *home4);
 void orc_pair_table(int bins, double cut, float *f, float *p);
+void orc_nn_label(const double d[3], const double s[3], double out[3]);   /* learned-correction label */
 
 /* ---- uniforms ---- */
 void orc_make_uni(const orc_sim *sim, orc_uni *u);

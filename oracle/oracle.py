@@ -162,6 +162,7 @@ def lib():
         L.orc_fof.argtypes = [C.c_int, C.c_double, C.c_double, P, P, P, P, C.c_double, C.c_double, C.c_int,
                               C.c_int, C.POINTER(Report), P, P]
         L.orc_direct_sum.argtypes = [C.c_int, P, P, C.c_double, C.c_int, P, P, P]
+        L.orc_nn_label.argtypes = [P, P, P]
         _lib = L
     return _lib
 
@@ -247,6 +248,27 @@ def morton(pos4, core):
     core = np.asarray(core, np.float64)
     lib().orc_morton(N, ptr(pos4), ptr(core), ptr(keys), ptr(perm), ptr(into))
     return keys, perm, into
+
+
+def nn_labels(rec):
+    """The learned correction's labels (cells^-2) of records (d.xyz, s.xyz): orc_nn_label per record."""
+    rec = np.asarray(rec, np.float64)
+    out = np.empty((len(rec), 3))
+    o = np.empty(3)
+    for k in range(len(rec)):
+        d = np.ascontiguousarray(rec[k, :3])
+        s = np.ascontiguousarray(rec[k, 3:6])
+        lib().orc_nn_label(ptr(d), ptr(s), ptr(o))
+        out[k] = o
+    return out
+
+
+def box_of(u, p):
+    """GLSL_BOX boxOf for one position: (box, g as float32[3])."""
+    p = np.ascontiguousarray(p, np.float32)
+    g = np.empty(3, np.float32)
+    b = lib().orc_box_of(C.byref(u), ptr(p), ptr(g))
+    return b, g
 
 
 def direct_sum(pos4, masses, eps, idx):

@@ -1,0 +1,149 @@
+"""The learned pairwise correction on the GPU against its CPU oracle.
+
+* labels: the device's binary64 mesh arithmetic of the isolated pair less the
+  table's model equals the oracle's (orc_nn_label, the restatement of
+  meshPairTable's field(), src/nbody.js:60-91);
+* the network's forward pass and its gradients, both through the tensor-core
+  kernels, equal the numpy oracle's with the BF16 roundings at the same places;
+* training on the device learns what the pair table misses, and the trained
+  network gains over the table where the two particles' mesh nodes overlap;
+* the learned P3M pass over a loose list equals the oracle's pass.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import nn_oracle as NO
+
+pytestmark = pytest.mark.gpu
+
+
+def records(n, seed, rmax=2.5):
+    rng = np.random.default_rng(seed)
+    u = rng.normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    r = rmax * rng.random(n) ** (1.0 / 3.0)
+    return np.concatenate([u * r[:, None], rng.random((n, 3))], axis=1).astype(np.float32)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def net(ccmod):
+    from cosmic_collisions_b200.learned import LearnedCorrection
+    n = LearnedCorrection(0, seed=11)
+    yield n
+    n.close()
+
+
+def test_labels_match_the_oracle(net, orc):
+    rec = records(512, 1)
+    got = net.labels(rec)
+    f, _ = orc.pair_table()
+    mesh = orc.nn_labels(rec)
+    want = NO.target(rec, f, mesh)
+    # float32 of a binary64 difference: rounding relative to the mesh force itself
+    assert np.abs(got - want).max() <= 2e-7 * np.abs(mesh).max() + 1e-9
+    near = np.linalg.norm(rec[:, :3], axis=1) < 1.5
+    assert np.abs(want[near]).max() > 1e-2          # the table misses something where nodes overlap
+
+
+def test_forward_matches_the_oracle(net):
+    p = net.params()
+    rec = records(1000, 2)
+    got = net.forward(rec)
+    want = NO.forward(p, rec)
+    assert got.shape == want.shape
+    assert rel_l2(got, want) < 1e-2
+    assert np.abs(got - want).max() < 3e-2 * np.abs(want).max()
+
+
+def test_gradient_matches_the_oracle(net):
+    p = net.params()
+    rec = records(1000, 3)                          # 7 full tiles and a ragged one
+    lab = (np.random.default_rng(4).normal(size=(1000, 3)) * 0.1).astype(np.float32)
+    g, loss = net.grad(rec, lab)
+    gw, lw = NO.grad(p, rec, lab)
+    assert abs(loss - lw) <= 1e-3 * lw
+    for name, (o, shape) in NO.SL.items():
+        n = int(np.prod(shape))
+        assert rel_l2(g[o:o + n], gw[o:o + n]) < 3e-2, name
+    assert rel_l2(g, gw) < 2e-2
+
+
+def test_training_learns_what_the_table_misses(net):
+    p0 = net.params()
+    try:
+        net.clear()
+        net.sample_uniform(262144, seed=5)
+        net.sample_uniform(16384, seed=6)           # held out
+        prec, plab = net.read_pool(0, 262144)
+        assert np.isfinite(prec).all() and np.isfinite(plab).all()
+        g, l0 = net.grad(prec[:37888], plab[:37888])
+        assert np.isfinite(g).all() and np.isfinite(l0)
+        loss = net.train(0, 262144, epochs=40, tiles_per_cta=2, lr=3e-3)
+        print("epoch losses", loss[:4], loss[-4:])
+        assert np.isfinite(net.params()).all()
+        rec, lab = net.read_pool(262144, 16384)
+        y = net.forward(rec)
+        r = np.linalg.norm(rec[:, :3], axis=1)
+        near = r < 1.7
+        err_nn = np.sqrt(((y - lab) ** 2).sum(1))
+        err_tab = np.sqrt((lab ** 2).sum(1))          # the table's error is the label itself
+        print("loss %.3e -> %.3e; near pairs: table rms %.3e, network rms %.3e" %
+              (loss[0], loss[-1], np.sqrt((err_tab[near] ** 2).mean()), np.sqrt((err_nn[near] ** 2).mean())))
+        assert loss[-1] < loss[0] / 10
+        assert np.sqrt((err_nn[near] ** 2).mean()) < 0.25 * np.sqrt((err_tab[near] ** 2).mean())
+    finally:
+        net.set_params(p0)
+        net.clear()
+
+
+def test_learned_pass_matches_the_oracle(net, ccmod, orc):
+    osim, pos, vel, mat, home = orc.build_run(orc.make_opt(16384))
+    rng = np.random.default_rng(8)
+    pos = pos.copy()
+    sel = np.sort(rng.choice(osim.N, 600, replace=False)).astype(np.int32)
+    pos[sel, :3] *= np.float32(1.6)                 # spread out: pairs inside and beyond the cut
+    com = (pos[:, :3].astype(np.float64) * mat[:, None]).sum(0) / mat.sum()
+    osim.boxOn[0] = 1
+    for k in range(3):
+        osim.boxCen[0][k] = com[k]
+    osim.boxT[0] = osim.t
+    nb = ccmod.NBody(0)
+    try:
+        nb.upload(ccmod._lib.Sim.from_buffer_copy(bytes(osim)), pos, vel, mat, home)
+        nb.pass_mesh()                              # boxes()
+        nb.set_pp_nn(net)
+        nb.set_pp(sel)
+        got = nb.buffer("ppforce")
+        lst = nb.buffer("pplist")
+        box = nb.buffer("ppbox")
+        lu = ccmod._lib.Uniforms()
+        ccmod._lib.check(ccmod._lib.lib().ccs_get_uniforms(nb.handle, C.byref(lu)), nb.handle, "uniforms")
+        nb.set_pp_nn(None)
+        nb.set_pp(sel)
+        plain = nb.buffer("ppforce")
+    finally:
+        nb.close()
+    u = orc.Uni.from_buffer_copy(bytes(lu))
+    f, pt = orc.pair_table()
+    tab = np.stack([f, pt], 1).astype(np.float32)
+    n = len(sel)
+    want = NO.pp_nn(u, lst[:n], box[:n], n, tab, net.params(), orc.box_of)
+    g0 = got.reshape(4, -1, 4)
+    assert np.abs(g0[1:]).max() == 0.0              # one slice
+    acc = g0[0, :n, :3].astype(np.float64)
+    scale = np.abs(want[:, :3]).max()
+    assert scale > 0
+    # the network's BF16 activations round the same way on both sides except at ties the FP32 sums
+    # land on differently: a few 1e-3 of the learned term, far below the Newton term
+    assert np.abs(acc - want[:, :3]).max() < 5e-3 * scale
+    assert np.abs(g0[0, :n, 3] - want[:, 3]).max() < 1e-4 * np.abs(want[:, 3]).max()
+    # detached, the plain pass is back: four slices again
+    assert np.abs(plain.reshape(4, -1, 4)[1:]).max() > 0
