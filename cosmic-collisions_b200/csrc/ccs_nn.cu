@@ -4,25 +4,26 @@
 // force between two particles as a function of distance alone: the placement-
 // averaged table of src/nbody.js:48-109 (meshPairTable).  Where the two
 // particles' cloud-in-cell nodes are apart (beyond about 1.7 cells) the mesh's
-// pair force is the node-softened Newton force and the table is exact; where
-// their nodes overlap it depends on the direction against the grid axes and
-// on where the particles sit in their cells, and the table keeps only its
-// average.  A small network learns what the table misses:
+// pair force is the node-to-node Newton force with CELL_FS's 0.5 FH^2
+// softening, exactly; where their nodes overlap it depends on the direction
+// against the grid axes and on where the particles sit in their cells, and the
+// table keeps only its average.  A small network learns that part:
 //
-//   R(d, s) = M(d, s) - T(|d|) d / |d|^3 ~ MLP(d, s - 1/2),
+//   R(d, s) = M(d, s) - d / (|d|^2 + 1/2)^(3/2) ~ MLP(d, s - 1/2),
 //   6 -> 64 -> 64 -> 3, SiLU, BF16 weights, FP32 accumulation,
 //
 // d the pair offset in mesh cells (source - target), s the source's fractional
 // position in its cell, M the mesh's force on the target from a unit source
-// and T the table's f (both in cells^-2).  The learned pass corrects a loose
-// pair by m_j (N_a(d) - T/max(r^2, a^2) d^ - R(d, s)) taper -- the plain
-// pass's correction less the network's residual -- at half the plain cut.
+// (cells^-2).  The learned pass corrects a loose pair inside half the plain
+// cut by m_j (N_a(d) - d/(r^2 + FH^2/2)^(3/2) - R(d, s)/FH^2) taper; the
+// potential keeps the table's.
 //
 // Labels are the mesh arithmetic of meshPairTable's field() for the isolated
 // pair -- cloud-in-cell deposit, node centres of mass, node-to-node Newton
 // with 0.5 FH^2 softening and the own node left out, cloud-in-cell gather --
-// in binary64 on the device (k_nn_label), less the table's model.  Training
-// pairs are drawn from a running impact's particles (k_nn_sample_state).
+// in binary64 on the device (k_nn_label), less the softened Newton force.
+// Training pairs are drawn from a running impact's particles
+// (k_nn_sample_state).
 //
 // The three layers run on the 5th-generation tensor cores: 128 pairs per
 // tile are the MMA's M, operands are staged in shared memory in the
@@ -176,23 +177,11 @@ __device__ void pair_field(double px, double py, double pz, double qx, double qy
   }
 }
 
-// the table's model of the same force: T(r) d / r^3 in cells, T the linear
-// interpolation of the 64-bin table over [0, 5 cells) as PPFORCE_FS reads it
-__device__ __forceinline__ void table_model(const float *__restrict__ tabF, double dx, double dy, double dz,
-                                            double o[3]) {
-  const double r = sqrt(dx * dx + dy * dy + dz * dz);
-  const double xx = fmin(fmax(r * (64.0 / 5.0) - 0.5, 0.0), 63.0);
-  const int k = (int)xx, k1 = min(k + 1, 63);
-  const double T = (double)tabF[k] + ((double)tabF[k1] - (double)tabF[k]) * (xx - (double)k);
-  const double s = r > 0.0 ? T / (r * r * r) : 0.0;
-  o[0] = dx * s;
-  o[1] = dy * s;
-  o[2] = dz * s;
-}
-
-// the network's target: the isolated pair's mesh force less the table's model
+// the network's target: the isolated pair's mesh force less the node-softened Newton force
+// d / (r^2 + 1/2)^(3/2) (cells, the 0.5 FH^2 softening of CELL_FS), which it equals once the two
+// particles' nodes are apart
 __global__ void k_nn_label(const float4 *__restrict__ D, const float4 *__restrict__ S, long n,
-                           const float *__restrict__ tabF, float4 *__restrict__ L) {
+                           float4 *__restrict__ L) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const float4 d = D[k], s = S[k];
@@ -200,11 +189,11 @@ __global__ void k_nn_label(const float4 *__restrict__ D, const float4 *__restric
     L[k] = make_float4(0, 0, 0, 0);
     return;
   }
-  const double qx = s.x, qy = s.y, qz = s.z;
-  double o[3], b[3];
-  pair_field(qx - (double)d.x, qy - (double)d.y, qz - (double)d.z, qx, qy, qz, o);
-  table_model(tabF, d.x, d.y, d.z, b);
-  L[k] = make_float4((float)(o[0] - b[0]), (float)(o[1] - b[1]), (float)(o[2] - b[2]), 0.0f);
+  const double qx = s.x, qy = s.y, qz = s.z, dx = d.x, dy = d.y, dz = d.z;
+  double o[3];
+  pair_field(qx - dx, qy - dy, qz - dz, qx, qy, qz, o);
+  const double q = 1.0 / sqrt((dx * dx + dy * dy + dz * dz) + 0.5), b = q * q * q;
+  L[k] = make_float4((float)(o[0] - dx * b), (float)(o[1] - dy * b), (float)(o[2] - dz * b), 0.0f);
 }
 
 // ---------------------------------------------------------------------------
@@ -807,7 +796,7 @@ __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__rest
     const float myBox = box[me];
     const float cutN = xmul(0.5f, u.cut), a2 = u.a2, a = fsqrt(a2);
     const float binScale = fdiv(64.0f, u.cut), taperScale = fdiv(1.0f, 0.8f * cutN - cutN);
-    const float invH2 = u.invH * u.invH;
+    const float invH2 = u.invH * u.invH, eps2Cell = u.eps2Cell;
     f3 acc = mk(0, 0, 0);
     float pot = 0.0f;
     const int q0 = offs[me * kChunks], q1 = offs[me * kChunks + kChunks];
@@ -821,18 +810,16 @@ __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__rest
       const float ts = clampf((r - cutN) * taperScale, 0.0f, 1.0f);
       const float taper = ts * ts * (3.0f - 2.0f * ts);
       const bool same = myBox >= 0.0f && box[j] == myBox;
-      float fn = invN * invN * invN * r, Ty = 0.0f;
-      f3 learned = mk(0, 0, 0);
-      if (same) {
+      f3 f = d * (invN * invN * invN);
+      float Ty = 0.0f;
+      if (same) {   // the mesh's own pull: node-softened Newton plus what the network learned
+        const float qn = rsqrtf(r2 + eps2Cell);
+        const float4 R = mesh[q];
+        f = f - d * (qn * qn * qn) - mk(R.x, R.y, R.z) * invH2;
         const float xx = clampf(r * binScale - 0.5f, 0.0f, 63.0f);
         const int k = (int)xx, k1 = min(k + 1, 63);
-        const float tt = xx - (float)k;
-        fn -= fdiv(tab[k].x + (tab[k1].x - tab[k].x) * tt, fmaxf(r2, a2));
-        Ty = tab[k].y + (tab[k1].y - tab[k].y) * tt;
-        const float4 R = mesh[q];
-        learned = mk(R.x, R.y, R.z) * invH2;
+        Ty = tab[k].y + (tab[k1].y - tab[k].y) * (xx - (float)k);
       }
-      const f3 f = d * (fdiv(1.0f, fmaxf(r, 1e-6f)) * fn) - learned;
       acc = acc + f * (Q.w * taper);
       pot += Q.w * (-invN - fdiv(Ty, fmaxf(r, a))) * taper;
     }
@@ -907,7 +894,6 @@ struct ccs_nn {
   uint8_t *img = nullptr;
   unsigned *status = nullptr;
   float4 *D = nullptr, *S = nullptr, *L = nullptr, *out = nullptr;
-  float *tabF = nullptr;   // the pair table's force column (64 bins to 5 cells)
   long capPairs = 0, nPairs = 0;
   int partCap = 0, steps = 0;
 };
@@ -1049,7 +1035,7 @@ int nn_reserve(ccs_nn *nn, int64_t count, float4 **D, float4 **S, cudaStream_t *
 int nn_commit(ccs_nn *nn, int64_t count) {
   float4 *D = nn->D + nn->nPairs, *S = nn->S + nn->nPairs, *L = nn->L + nn->nPairs;
   if (count) {
-    nn::k_nn_label<<<(unsigned)((count + 255) / 256), 256, 0, nn->st>>>(D, S, count, nn->tabF, L);
+    nn::k_nn_label<<<(unsigned)((count + 255) / 256), 256, 0, nn->st>>>(D, S, count, L);
     NN_TRY(nn, cudaGetLastError());
   }
   int rc = nn_check(nn);
@@ -1090,12 +1076,6 @@ int ccs_nn_create(int device, uint32_t seed, ccs_nn **out) {
   rc |= nn_alloc(nn, &nn->loss, 1 << 16);
   rc |= nn_alloc(nn, &nn->img, nn::kImgTotal);
   rc |= nn_alloc(nn, &nn->status, 1);
-  rc |= nn_alloc(nn, &nn->tabF, CCS_PP_BINS);
-  if (!rc) {
-    std::vector<float> f(CCS_PP_BINS), p(CCS_PP_BINS);
-    ccs_pair_table(CCS_PP_BINS, 5.0 * 12.0 / 64.0, f.data(), p.data());
-    if (cudaMemcpy(nn->tabF, f.data(), 4 * CCS_PP_BINS, cudaMemcpyHostToDevice) != cudaSuccess) rc = CCS_E_CUDA;
-  }
   if (rc) {
     ccs_nn_destroy(nn);
     return rc < 0 ? rc : CCS_E_NOMEM;
@@ -1128,7 +1108,7 @@ int ccs_nn_destroy(ccs_nn *nn) {
   if (nn->st) cudaStreamSynchronize(nn->st);
   cudaFree(nn->params); cudaFree(nn->m1); cudaFree(nn->m2); cudaFree(nn->grad); cudaFree(nn->loss);
   cudaFree(nn->partial); cudaFree(nn->img); cudaFree(nn->status);
-  cudaFree(nn->D); cudaFree(nn->S); cudaFree(nn->L); cudaFree(nn->out); cudaFree(nn->tabF);
+  cudaFree(nn->D); cudaFree(nn->S); cudaFree(nn->L); cudaFree(nn->out);
   if (nn->st) cudaStreamDestroy(nn->st);
   delete nn;
   return CCS_OK;
@@ -1174,7 +1154,7 @@ int ccs_nn_sample_uniform(ccs_nn *nn, int64_t count, uint32_t seed) {
     float4 *D = nn->D + nn->nPairs, *S = nn->S + nn->nPairs, *L = nn->L + nn->nPairs;
     const unsigned g = (unsigned)((count + 255) / 256);
     nn::k_nn_sample_uniform<<<g, 256, 0, nn->st>>>(count, seed, (float)(CCS_NN_CUT_CELLS), D, S);
-    nn::k_nn_label<<<g, 256, 0, nn->st>>>(D, S, count, nn->tabF, L);
+    nn::k_nn_label<<<g, 256, 0, nn->st>>>(D, S, count, L);
     NN_TRY(nn, cudaGetLastError());
   }
   rc = nn_check(nn);
@@ -1213,7 +1193,7 @@ int ccs_nn_labels(ccs_nn *nn, const float *rec6, int64_t n, float *label3) {
   int rc = scratch(nn, n, &D, &S, &L);
   if (!rc) rc = upload_records(nn, rec6, n, D, S);
   if (rc) return rc;
-  nn::k_nn_label<<<(unsigned)((n + 255) / 256), 256, 0, nn->st>>>(D, S, n, nn->tabF, L);
+  nn::k_nn_label<<<(unsigned)((n + 255) / 256), 256, 0, nn->st>>>(D, S, n, L);
   NN_TRY(nn, cudaGetLastError());
   std::vector<float4> l((size_t)n);
   NN_TRY(nn, cudaMemcpyAsync(l.data(), L, 16 * (size_t)n, cudaMemcpyDeviceToHost, nn->st));

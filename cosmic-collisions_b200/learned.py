@@ -2,12 +2,12 @@
 
 No counterpart in the reference, which subtracts the placement-averaged table
 of meshPairTable (src/nbody.js:48-109) inside PPFORCE_FS (src/glsl-sim.js:
-738-750).  The network R(d, s) -- d the pair offset in mesh cells, s the
-source's position in its cell -- learns what that table misses of the mesh's
-pair force (the part that depends on direction and placement where the two
-particles' mesh nodes overlap); with it attached to an engine the P3M pass
-corrects loose pairs inside NN_CUT_CELLS cells (half the plain cut) by the
-plain pass's correction less m_j R(d, s).  Everything runs on the device:
+738-750).  Here the mesh's pair force is the node-softened Newton force (what
+it is exactly once the two particles' mesh nodes are apart) plus a network
+R(d, s) -- d the pair offset in mesh cells, s the source's position in its
+cell -- for the part that depends on direction and placement where the nodes
+overlap; with it attached to an engine the P3M pass corrects loose pairs
+inside NN_CUT_CELLS cells (half the plain cut) by m_j (N_a(d) - that) taper.  Everything runs on the device:
 labels (binary64 mesh arithmetic of the isolated pair), sampling, training
 (forward, backward and weight gradients on the tensor cores, Adam) and
 inference inside the P3M pass.
@@ -121,10 +121,16 @@ class LearnedCorrection:
         return g, float(loss.value)
 
 
-def table_model(rec, f_table, cut_cells=5.0):
-    """The plain pass's model of the mesh pair force: T(r) d / r^3 in cells^-2, the pair table's force column
-    read as PPFORCE_FS reads it (src/glsl-sim.js:738-744; the a^2 clamp left out).  The network learns the
-    isolated pair's mesh force less this."""
+def softened_newton(rec):
+    """d / (r^2 + 1/2)^1.5 in cells^-2: the mesh's pair force once the two particles' nodes are apart (the
+    0.5 FH^2 softening of CELL_FS); the network learns the isolated pair's mesh force less this."""
+    d = np.asarray(rec, np.float64)[:, :3]
+    return d / (((d * d).sum(1) + 0.5) ** 1.5)[:, None]
+
+
+def table_model(rec, f_table, a_cells, cut_cells=5.0):
+    """The plain pass's model of the mesh pair force in cells^-2: T.f / max(r^2, a^2) along d (PPFORCE_FS,
+    src/glsl-sim.js:738-744), the pair table's force column read over 64 bins to the cut."""
     d = np.asarray(rec, np.float64)[:, :3]
     r = np.sqrt((d * d).sum(1))
     n = len(f_table)
@@ -133,7 +139,7 @@ def table_model(rec, f_table, cut_cells=5.0):
     k1 = np.minimum(k + 1, n - 1)
     f = np.asarray(f_table, np.float64)
     T = f[k] + (f[k1] - f[k]) * (xx - k)
-    return d * np.where(r > 0, T / np.maximum(r, 1e-300) ** 3, 0.0)[:, None]
+    return d * (T / np.maximum(r * r, a_cells * a_cells) / np.maximum(r, 1e-300))[:, None]
 
 
-__all__ = ["LearnedCorrection", "unpack", "table_model", "NN_CUT_CELLS", "NN_PARAMS"]
+__all__ = ["LearnedCorrection", "unpack", "softened_newton", "table_model", "NN_CUT_CELLS", "NN_PARAMS"]

@@ -198,15 +198,17 @@ int ccs_pp_force_static(const float *list4, const float *box, int n, const float
 /* ---- the learned pairwise correction ----
  * No counterpart in the reference.  The plain pass subtracts the mesh's pair
  * force as the placement-averaged table of meshPairTable (src/nbody.js:48-109;
- * PPFORCE_FS's T.f, src/glsl-sim.js:738-750).  A network R(d, s) learns what
- * that table misses: the isolated pair's mesh force less T(r) d / r^3, d the
- * pair offset in mesh cells (source - target), s the source's position in its
- * cell; 6 -> 64 -> 64 -> 3 with SiLU, BF16 weights, FP32 accumulation, run and
- * trained on the tensor cores.  With a network attached, the P3M pass of an
- * engine corrects the loose pairs inside CCS_NN_CUT_CELLS cells (half the
- * plain pass's 5) by the plain pass's correction less m_j R(d, s) / FH^2;
- * detaching it restores the plain pass.  Flat parameter order: W1[64][6]
- * b1[64] W2[64][64] b2[64] W3[3][64] b3[3]. */
+ * PPFORCE_FS's T.f, src/glsl-sim.js:738-750).  Here the mesh's pair force is
+ * the node-softened Newton force d / (r^2 + FH^2/2)^(3/2) (what it is exactly
+ * once the two particles' mesh nodes are apart) plus a network R(d, s) for
+ * the rest: d the pair offset in mesh cells (source - target), s the source's
+ * position in its cell; 6 -> 64 -> 64 -> 3 with SiLU, BF16 weights, FP32
+ * accumulation, run and trained on the tensor cores.  With a network
+ * attached, the P3M pass of an engine corrects the loose pairs inside
+ * CCS_NN_CUT_CELLS cells (half the plain pass's 5) by m_j (N_a(d) -
+ * d/(r^2 + FH^2/2)^(3/2) - R(d, s)/FH^2) taper (the potential keeps the
+ * table's); detaching it restores the plain pass.  Flat parameter order:
+ * W1[64][6] b1[64] W2[64][64] b2[64] W3[3][64] b3[3]. */
 #define CCS_NN_PARAMS 4803
 #define CCS_NN_CUT_CELLS 2.5
 typedef struct ccs_nn ccs_nn;
@@ -217,7 +219,8 @@ int ccs_nn_set_params(ccs_nn *nn, const float *params);   /* also resets the opt
 int ccs_nn_get_params(ccs_nn *nn, float *params);
 /* The pair pool the network trains on: records (d in cells, s in [0,1)) with
  * their labels, the mesh arithmetic of meshPairTable's field() for the
- * isolated pair in binary64 less the table's model (cells^-2, unit masses). */
+ * isolated pair in binary64 less the softened Newton force (cells^-2, unit
+ * masses). */
 int ccs_nn_clear(ccs_nn *nn);
 int64_t ccs_nn_pool_size(const ccs_nn *nn);
 /* count pairs of the engine's particles inside the cut, both in box 0; odd

@@ -13,13 +13,12 @@ gradients and the learned P3M pass can be checked against it:
           dH1 = bf16((dH2 W2) * silu'(h1)); weight gradients are sums over rows
           of the BF16 operands (FP32 on the device, binary64 here).
 
-The network's target is what the pair table misses: the isolated pair's mesh
-force (meshPairTable's field(), src/nbody.js:60-91; orc_nn_label) less the
-table's model T(r) d / r^3 (table_model).  The learned P3M pass follows
-src/glsl-sim.js:676-754 at half the cut, less the network's output: for loose
-pairs inside 2.5 cells, acc += m_j (d^ fn - same * y(d, s) / FH^2) taper with
-fn the plain pass's r/(r^2 + a^2)^1.5 - same * T.f / max(r^2, a^2); pot is
-the plain pass's; times Gm; one slice.
+The network's target is the isolated pair's mesh force (meshPairTable's
+field(), src/nbody.js:60-91; orc_nn_label) less the node-softened Newton
+force d / (r^2 + 1/2)^1.5 in cells (softened_newton).  The learned P3M pass
+follows src/glsl-sim.js:676-754 at half the cut: for loose pairs inside 2.5
+cells, acc += m_j (d / (r^2 + a^2)^1.5 - same * (d / (r^2 + FH^2/2)^1.5 +
+y(d, s) / FH^2)) taper; pot is the plain pass's; times Gm; one slice.
 """
 import numpy as np
 
@@ -100,9 +99,15 @@ def grad(params, rec, lab, exact=False):
     return g, loss
 
 
-def table_model(rec, f):
-    """T(r) d / r^3 in cells^-2: the pair table's force column f read as PPFORCE_FS reads it (64 bins to
-    5 cells, linear), binary64."""
+def softened_newton(rec):
+    """d / (r^2 + 1/2)^1.5 in cells: the mesh's pair force once the two particles' nodes are apart."""
+    d = np.asarray(rec, np.float64)[:, :3]
+    return d / (((d * d).sum(1) + 0.5) ** 1.5)[:, None]
+
+
+def table_model(rec, f, a_cells):
+    """The plain pass's model of the mesh pair force in cells^-2: T.f / max(r^2, a^2) along d (PPFORCE_FS,
+    src/glsl-sim.js:738-744), the table's force column read over 64 bins to 5 cells."""
     d = np.asarray(rec, np.float64)[:, :3]
     r = np.sqrt((d * d).sum(1))
     xx = np.clip(r * (64.0 / 5.0) - 0.5, 0.0, 63.0)
@@ -110,12 +115,12 @@ def table_model(rec, f):
     k1 = np.minimum(k + 1, 63)
     f = np.asarray(f, np.float64)
     T = f[k] + (f[k1] - f[k]) * (xx - k)
-    return d * np.where(r > 0, T / np.maximum(r, 1e-300) ** 3, 0.0)[:, None]
+    return d * (T / np.maximum(r * r, a_cells * a_cells) / np.maximum(r, 1e-300))[:, None]
 
 
-def target(rec, f, mesh):
-    """The network's label: the mesh force (orc_nn_label) less the table's model."""
-    return np.asarray(mesh, np.float64) - table_model(rec, f)
+def target(rec, mesh):
+    """The network's label: the mesh force (orc_nn_label) less the softened Newton force."""
+    return np.asarray(mesh, np.float64) - softened_newton(rec)
 
 
 def pp_nn(u, list4, box, count, tab, params, box_of):
@@ -160,17 +165,14 @@ def pp_nn(u, list4, box, count, tab, params, box_of):
             ts = min(max((r - cutN) / (0.8 * cutN - cutN), 0.0), 1.0)
             taper = ts * ts * (3.0 - 2.0 * ts)
             same = box[i] >= 0 and box[j] == box[i]
-            fn = invN ** 3 * r
+            f = d * invN ** 3
             Ty = 0.0
-            learned = np.zeros(3)
             if same:
+                f = f - d / (r2 + float(u.eps2Cell)) ** 1.5 - y[q] * invH * invH
                 xx = min(max(r * 64.0 / cut - 0.5, 0.0), 63.0)
                 k = int(xx)
                 k1 = min(k + 1, 63)
-                fn -= (tab[k, 0] + (tab[k1, 0] - tab[k, 0]) * (xx - k)) / max(r2, a2)
                 Ty = tab[k, 1] + (tab[k1, 1] - tab[k, 1]) * (xx - k)
-                learned = y[q] * invH * invH
-            f = d / max(r, 1e-6) * fn - learned
             acc += f * (Q[3] * taper)
             pot += Q[3] * (-invN - Ty / max(r, a)) * taper
         out[i, :3] = acc * u.Gm

@@ -31,14 +31,13 @@ def test_concurrent_handles_match_a_lone_run(ccmod):
 
     The contact forces are summed with float atomics, so two runs of the same
     state differ by rounding in every step, and from an unsettled packing that
-    difference grows by orders of magnitude within a few dozen steps.  The
-    comparison is therefore one 8-step graph block (the window the oracle
-    parity holds at 1e-4) with the handles' blocks in flight together; a
-    handle that read another's buffers or uniforms would be off by O(1).
+    difference grows quickly.  So the interleaved handles are held to the
+    spread of two lone runs of the same state: a handle that read another's
+    buffers or uniforms would be off by O(1) of the state's scale.
     """
     from cosmic_collisions_b200 import configs
     opt = configs.small_impact_opt(16384)
-    runs = [ccmod.NBody(0) for _ in range(3)]
+    runs = [ccmod.NBody(0) for _ in range(4)]
     try:
         for nb in runs:
             nb.build(opt)
@@ -48,18 +47,22 @@ def test_concurrent_handles_match_a_lone_run(ccmod):
         runs[1].steps(8)
         runs[0].sync()
         runs[1].sync()
-        runs[2].steps(8)                # one alone
+        runs[2].steps(8)                # two alone
+        runs[2].sync()
+        runs[3].steps(8)
         states = [nb.read_state() for nb in runs]
         clocks = [(nb.sim.stepNo, nb.sim.t) for nb in runs]
     finally:
         for nb in runs:
             nb.close()
-    assert clocks[0] == clocks[1] == clocks[2]
-    ref = states[2]
-    for st in states[:2]:
-        for k in ("pos", "vel"):
-            a, b = st[k][:, :3].astype(np.float64), ref[k][:, :3].astype(np.float64)
-            assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max(), k
+    assert clocks[0] == clocks[1] == clocks[2] == clocks[3]
+    for k in ("pos", "vel"):
+        ref = states[2][k][:, :3].astype(np.float64)
+        scale = np.abs(ref).max()
+        lone = np.abs(states[3][k][:, :3] - ref).max()
+        for st in states[:2]:
+            diff = np.abs(st[k][:, :3] - ref).max()
+            assert diff <= max(10 * lone, 1e-4 * scale) and diff <= 2e-2 * scale, (k, diff, lone, scale)
 
 
 def test_small_impact_run_keeps_its_books(ccmod):
