@@ -3,11 +3,12 @@
 // The reference subtracts, for every loose pair inside the cut, the mesh's own
 // force between two particles as a function of distance alone: the placement-
 // averaged table of src/nbody.js:48-109 (meshPairTable).  Where the two
-// particles' cloud-in-cell nodes are apart (beyond about 1.7 cells) the mesh's
-// pair force is the node-to-node Newton force with CELL_FS's 0.5 FH^2
-// softening, exactly; where their nodes overlap it depends on the direction
-// against the grid axes and on where the particles sit in their cells, and the
-// table keeps only its average.  A small network learns that part:
+// particles share no cloud-in-cell node (certainly once they are two cells
+// apart along an axis) the mesh's pair force is the node-to-node Newton force
+// with CELL_FS's 0.5 FH^2 softening, exactly; where they share nodes (possible
+// out to 2 sqrt(3) cells) it depends on the direction against the grid axes
+// and on where the particles sit in their cells, and the table keeps only its
+// average.  A small network learns that part:
 //
 //   R(d, s) = M(d, s) - d / (|d|^2 + 1/2)^(3/2) ~ MLP(d, s - 1/2),
 //   6 -> 64 -> 64 -> 3, SiLU, BF16 weights, FP32 accumulation,
@@ -178,8 +179,8 @@ __device__ void pair_field(double px, double py, double pz, double qx, double qy
 }
 
 // the network's target: the isolated pair's mesh force less the node-softened Newton force
-// d / (r^2 + 1/2)^(3/2) (cells, the 0.5 FH^2 softening of CELL_FS), which it equals once the two
-// particles' nodes are apart
+// d / (r^2 + 1/2)^(3/2) (cells, the 0.5 FH^2 softening of CELL_FS), which it equals when the two
+// particles share no node
 __global__ void k_nn_label(const float4 *__restrict__ D, const float4 *__restrict__ S, long n,
                            float4 *__restrict__ L) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -3,10 +3,10 @@
 No counterpart in the reference, which subtracts the placement-averaged table
 of meshPairTable (src/nbody.js:48-109) inside PPFORCE_FS (src/glsl-sim.js:
 738-750).  Here the mesh's pair force is the node-softened Newton force (what
-it is exactly once the two particles' mesh nodes are apart) plus a network
+it is exactly when the two particles share no mesh node) plus a network
 R(d, s) -- d the pair offset in mesh cells, s the source's position in its
-cell -- for the part that depends on direction and placement where the nodes
-overlap; with it attached to an engine the P3M pass corrects loose pairs
+cell -- for the part that depends on direction and placement where they share
+nodes; with it attached to an engine the P3M pass corrects loose pairs
 inside NN_CUT_CELLS cells (half the plain cut) by m_j (N_a(d) - that) taper.  Everything runs on the device:
 labels (binary64 mesh arithmetic of the isolated pair), sampling, training
 (forward, backward and weight gradients on the tensor cores, Adam) and
@@ -122,7 +122,7 @@ class LearnedCorrection:
 
 
 def softened_newton(rec):
-    """d / (r^2 + 1/2)^1.5 in cells^-2: the mesh's pair force once the two particles' nodes are apart (the
+    """d / (r^2 + 1/2)^1.5 in cells^-2: the mesh's pair force when the two particles share no node (the
     0.5 FH^2 softening of CELL_FS); the network learns the isolated pair's mesh force less this."""
     d = np.asarray(rec, np.float64)[:, :3]
     return d / (((d * d).sum(1) + 0.5) ** 1.5)[:, None]

@@ -200,7 +200,7 @@ int ccs_pp_force_static(const float *list4, const float *box, int n, const float
  * force as the placement-averaged table of meshPairTable (src/nbody.js:48-109;
  * PPFORCE_FS's T.f, src/glsl-sim.js:738-750).  Here the mesh's pair force is
  * the node-softened Newton force d / (r^2 + FH^2/2)^(3/2) (what it is exactly
- * once the two particles' mesh nodes are apart) plus a network R(d, s) for
+ * when the two particles share no mesh node) plus a network R(d, s) for
  * the rest: d the pair offset in mesh cells (source - target), s the source's
  * position in its cell; 6 -> 64 -> 64 -> 3 with SiLU, BF16 weights, FP32
  * accumulation, run and trained on the tensor cores.  With a network

@@ -100,7 +100,7 @@ def grad(params, rec, lab, exact=False):
 
 
 def softened_newton(rec):
-    """d / (r^2 + 1/2)^1.5 in cells: the mesh's pair force once the two particles' nodes are apart."""
+    """d / (r^2 + 1/2)^1.5 in cells: the mesh's pair force when the two particles share no mesh node."""
     d = np.asarray(rec, np.float64)[:, :3]
     return d / (((d * d).sum(1) + 0.5) ** 1.5)[:, None]
 

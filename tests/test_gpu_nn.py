@@ -6,7 +6,7 @@
 * the network's forward pass and its gradients, both through the tensor-core
   kernels, equal the numpy oracle's with the BF16 roundings at the same places;
 * training on the device learns the mesh's pair force where the two
-  particles' mesh nodes overlap, and gains over the pair table there;
+  particles share a mesh node, and gains over the pair table there;
 * the learned P3M pass over a loose list equals the oracle's pass.
 """
 import ctypes as C
@@ -25,6 +25,13 @@ def records(n, seed, rmax=2.5):
     u /= np.linalg.norm(u, axis=1)[:, None]
     r = rmax * rng.random(n) ** (1.0 / 3.0)
     return np.concatenate([u * r[:, None], rng.random((n, 3))], axis=1).astype(np.float32)
+
+
+def shares_a_node(rec):
+    """Whether the target's and the source's cloud-in-cell nodes overlap: the target's cell (floor(s - d))
+    within one cell of the source's (cell 0) along every axis."""
+    rec = np.asarray(rec, np.float64)
+    return (np.abs(np.floor(rec[:, 3:6] - rec[:, :3])) <= 1).all(axis=1)
 
 
 def rel_l2(a, b):
@@ -48,9 +55,9 @@ def test_labels_match_the_oracle(net, orc):
     want = NO.target(rec, mesh)
     # float32 of a binary64 difference: rounding relative to the mesh force itself
     assert np.abs(got - want).max() <= 2e-7 * np.abs(mesh).max() + 1e-9
-    r = np.linalg.norm(rec[:, :3], axis=1)
-    assert np.abs(want[r < 1.5]).max() > 1e-2       # where the nodes overlap there is something to learn
-    assert np.abs(want[r > 2.0]).max() < 1e-5       # apart, the mesh's pair force is the softened Newton force
+    share = shares_a_node(rec)
+    assert np.abs(want[share]).max() > 1e-2         # where the two share a mesh node there is something to learn
+    assert np.abs(want[~share]).max() < 1e-5        # apart, the mesh's pair force is the softened Newton force
 
 
 def test_forward_matches_the_oracle(net):
@@ -89,13 +96,13 @@ def test_training_learns_the_mesh_pair_force(net, orc):
         rec, lab = net.read_pool(262144, 16384)
         y = net.forward(rec)
         r = np.linalg.norm(rec[:, :3], axis=1)
-        near = (r > 0.1) & (r < 1.7)
+        near = shares_a_node(rec) & (r > 0.1)
         mesh = lab + NO.softened_newton(rec)        # the isolated pair's mesh force
         f, _ = orc.pair_table()
         tab = NO.table_model(rec, f, 0.075)         # the plain pass's model (a = 0.075 cells at 262k)
         rms = lambda v: float(np.sqrt((v ** 2).sum(1).mean()))
         e_net, e_tab = rms((y - lab)[near]), rms((mesh - tab)[near])
-        print("loss %.3e -> %.3e; near pairs: label rms %.3e, table error %.3e, network error %.3e"
+        print("loss %.3e -> %.3e; pairs sharing a node: label rms %.3e, table error %.3e, network error %.3e"
               % (loss[0], loss[-1], rms(lab[near]), e_tab, e_net))
         assert loss[-1] < loss[0] / 5
         assert e_net < 0.25 * e_tab
