@@ -130,7 +130,7 @@ __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const Si
   if (two) push_near(u, a, spc, w, near1, e1, r21, lane, nn);
 }
 
-__global__ void __launch_bounds__(kThreads) k_contact_step(const ccs_uniforms *__restrict__ U, const SimArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) k_contact_step(const ccs_uniforms *__restrict__ U, const SimArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ float spc[16];   // seatPos(q) * uCell, exact
   const ccs_uniforms &u = *U;

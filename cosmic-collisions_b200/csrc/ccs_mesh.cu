@@ -241,22 +241,25 @@ int launch_far(const MeshBuf &m, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // cell gravity: src/glsl-sim.js:303-352.  One 64-thread CTA per coarse block,
 // a thread per fine cell (a cell can hold mass only if its block does).  The
-// CTA first reads how many occupied cells each of the 5^3 blocks around it
-// holds; then, block by block in the reference's order, it stages that
-// block's occupied cells -- centre of mass and mass, as the coarse pass listed
-// them -- in shared memory with one coalesced load, and every occupied thread
-// sums them for its own cell, skipping itself.  Then the block's far field is
+// CTA reads how many occupied cells each of the 5^3 blocks around it holds,
+// then copies the occupied cells of all of them -- centre of mass and mass, as
+// the coarse pass listed them, block by block in the reference's order -- into
+// shared memory in one pass of independent loads (in batches of kCellBatch
+// when the neighbourhood holds more), and every occupied thread sums them for
+// its own cell in that order, skipping itself.  Then the block's far field is
 // carried to the cell by the tidal tensor.  Cell-on-cell pulls are fast
 // arithmetic (rsqrt, FMA).
 // ---------------------------------------------------------------------------
+constexpr int kCellBatch = 1024;
+
 __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U, const float4 *__restrict__ fine,
                                              const float4 *__restrict__ coarse, const float4 *__restrict__ occ,
                                              const uint8_t *__restrict__ occIdx, const int *__restrict__ occN,
                                              const float4 *__restrict__ farA, const float4 *__restrict__ farT0,
                                              const float4 *__restrict__ farT1, float4 *__restrict__ force) {
-  __shared__ int nbK[125], nbN[125];
-  __shared__ float4 src[64];
-  __shared__ uint8_t sidx[64];
+  __shared__ int nbK[125], nbOff[126];
+  __shared__ float4 src[kCellBatch];
+  __shared__ uint8_t sidx[kCellBatch];   // a source's place in its block; 255 for another block's cells
   const int blk = blockIdx.x, t = threadIdx.x;
   const int ccx = blk & 15, ccy = (blk >> 4) & 15, ccz = blk >> 8;
   const int c = fine_index(ccx * 4 + (t & 3), ccy * 4 + ((t >> 2) & 3), ccz * 4 + (t >> 4));
@@ -271,7 +274,7 @@ __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U,
     const bool in = kx >= 0 && ky >= 0 && kz >= 0 && kx <= 15 && ky <= 15 && kz <= 15;
     const int k = in ? coarse_index(kx, ky, kz) : 0;
     nbK[o] = k;
-    nbN[o] = in ? __ldg(occN + k) : 0;
+    nbOff[o + 1] = in ? __ldg(occN + k) : 0;
   }
   if (!(fine[c].w > 0.0f)) force[c] = make_float4(0, 0, 0, 0);   // this thread's own place, when empty
   // thread t sums for the block's t-th occupied cell, so the busy lanes sit together
@@ -284,20 +287,31 @@ __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U,
   f3 acc = mk(0, 0, 0);
   float pot = 0.0f;
   __syncthreads();
-  for (int o = 0; o < 125; ++o) {
-    const int n = nbN[o];
-    if (n == 0) continue;   // an empty block is nothing: most of the 125 are
-    const int k = nbK[o];
-    if (t < n) {
-      src[t] = __ldg(occ + (size_t)k * 64 + t);
-      sidx[t] = __ldg(occIdx + (size_t)k * 64 + t);
+  if (t == 0) {   // where each neighbour block's cells start in the neighbourhood's list
+    nbOff[0] = 0;
+    for (int o = 0; o < 125; ++o) nbOff[o + 1] += nbOff[o];
+  }
+  __syncthreads();
+  const int total = nbOff[125];
+  for (int b0 = 0; b0 < total; b0 += kCellBatch) {
+    const int b1 = min(b0 + kCellBatch, total);
+    // the neighbour blocks' cells in [b0, b1): every load independent of the others
+    for (int o = 0; o < 125; ++o) {
+      const int lo = max(nbOff[o], b0), hi = min(nbOff[o + 1], b1);
+      if (lo >= hi) continue;
+      const int k = nbK[o];
+      for (int e = lo + t; e < hi; e += 64) {
+        const int i = e - nbOff[o];
+        src[e - b0] = __ldg(occ + (size_t)k * 64 + i);
+        sidx[e - b0] = k == blk ? __ldg(occIdx + (size_t)k * 64 + i) : (uint8_t)255;
+      }
     }
     __syncthreads();
     if (mine) {
-      const int self = k == blk ? tl : -1;   // a cell does not pull itself
+      const int n = b1 - b0;
 #pragma unroll 4
       for (int i = 0; i < n; ++i) {
-        if ((int)sidx[i] == self) continue;
+        if ((int)sidx[i] == tl) continue;   // a cell does not pull itself
         const float4 mf = src[i];
         const f3 r = xyz(mf) - x;
         const float inv = rsqrtf(dot(r, r) + eps2);
