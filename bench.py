@@ -405,7 +405,16 @@ def run_ours(args, rank, world, log):
     nb.steps(args.warmup)
     nb.sync()
     if args.profile:
-        # for `ncu --profile-from-start off`: only these steps are profiled
+        # for `ncu --profile-from-start off`: only these steps are profiled; without --no-nn the learned
+        # pass is attached (a network trained briefly on the same impact)
+        net = None
+        if not args.no_nn:
+            net, _ = learned_correction(cc, dev, N, log, pairs=300_000, epochs=2, snaps=(0,), held=16384)
+            nb.set_pp_nn(net)
+            for _ in range(args.warmup):
+                nb.step(False, False)
+                nb.sim.t += nb.sim.dt
+            nb.sync()
         l0 = lib.ccs_launch_count(nb.handle)
         torch.cuda.profiler.start()
         for _ in range(args.steps):
@@ -414,8 +423,11 @@ def run_ours(args, rank, world, log):
         nb.sync()
         torch.cuda.profiler.stop()
         out = {"profile": True, "steps": args.steps, "gpu_launches": int(lib.ccs_launch_count(nb.handle) - l0),
-               "stepNo": nb.sim.stepNo, "loose_list": nb.pp["count"]}
+               "stepNo": nb.sim.stepNo, "loose_list": nb.pp["count"], "learned": net is not None}
+        nb.set_pp_nn(None)
         nb.close()
+        if net is not None:
+            net.close()
         return out
     import ctypes as C
     buf = nb.device_buffers()

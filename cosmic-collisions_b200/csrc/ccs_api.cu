@@ -494,7 +494,7 @@ int graph_block(ccs_handle *h) {
     if (plans[k].slots) per += 1;               // contact grid
     if (plans[k].mesh) {
       per += 4 * (1 + (us[k].boxB > 0.5f));     // deposit, coarse, far, cell per box
-      if (us[k].ppCount) per += 2;              // gather, force
+      if (us[k].ppCount) per += h->nn ? 6 : 3;  // gather, then pairs + reduce (or the learned pass's five)
     }
   }
   h->launches += per;

@@ -239,49 +239,57 @@ int launch_far(const MeshBuf &m, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// cell gravity: src/glsl-sim.js:303-352.  One 64-thread CTA per coarse block,
-// a thread per fine cell (a cell can hold mass only if its block does).  The
-// CTA reads how many occupied cells each of the 5^3 blocks around it holds,
-// then copies the occupied cells of all of them -- centre of mass and mass, as
-// the coarse pass listed them, block by block in the reference's order -- into
-// shared memory in one pass of independent loads (in batches of kCellBatch
-// when the neighbourhood holds more), and every occupied thread sums them for
-// its own cell in that order, skipping itself.  Then the block's far field is
-// carried to the cell by the tidal tensor.  Cell-on-cell pulls are fast
-// arithmetic (rsqrt, FMA).
+// cell gravity: src/glsl-sim.js:303-352.  One CTA per coarse block; its 64
+// fine cells each get kCellSplit threads (a cell can hold mass only if its
+// block does).  The CTA reads how many occupied cells each of the 5^3 blocks
+// around it holds, then copies the occupied cells of all of them -- centre of
+// mass and mass, as the coarse pass listed them, block by block in the
+// reference's order -- into shared memory in one pass of independent loads
+// (in batches of kCellBatch when the neighbourhood holds more).  A block in
+// the bodies sees thousands of sources, so each occupied cell's sum is split
+// over its kCellSplit threads (every kCellSplit-th source), and the partial
+// sums are added in a fixed order: the result is deterministic.  A cell skips
+// itself.  Then the block's far field is carried to the cell by the tidal
+// tensor.  Cell-on-cell pulls are fast arithmetic (rsqrt, FMA).
 // ---------------------------------------------------------------------------
 constexpr int kCellBatch = 1024;
+constexpr int kCellSplit = 4;
+constexpr int kCellThreads = 64 * kCellSplit;
 
-__global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U, const float4 *__restrict__ fine,
-                                             const float4 *__restrict__ coarse, const float4 *__restrict__ occ,
-                                             const uint8_t *__restrict__ occIdx, const int *__restrict__ occN,
-                                             const float4 *__restrict__ farA, const float4 *__restrict__ farT0,
-                                             const float4 *__restrict__ farT1, float4 *__restrict__ force) {
+__global__ void __launch_bounds__(kCellThreads) k_cell(const ccs_uniforms *__restrict__ U,
+                                                       const float4 *__restrict__ fine,
+                                                       const float4 *__restrict__ coarse,
+                                                       const float4 *__restrict__ occ,
+                                                       const uint8_t *__restrict__ occIdx,
+                                                       const int *__restrict__ occN, const float4 *__restrict__ farA,
+                                                       const float4 *__restrict__ farT0,
+                                                       const float4 *__restrict__ farT1, float4 *__restrict__ force) {
   __shared__ int nbK[125], nbOff[126];
   __shared__ float4 src[kCellBatch];
   __shared__ uint8_t sidx[kCellBatch];   // a source's place in its block; 255 for another block's cells
-  const int blk = blockIdx.x, t = threadIdx.x;
+  __shared__ float4 part[kCellSplit][64];
+  const int blk = blockIdx.x, t = threadIdx.x, cellT = t & 63, q = t >> 6;
   const int ccx = blk & 15, ccy = (blk >> 4) & 15, ccz = blk >> 8;
-  const int c = fine_index(ccx * 4 + (t & 3), ccy * 4 + ((t >> 2) & 3), ccz * 4 + (t >> 4));
+  const int c = fine_index(ccx * 4 + (cellT & 3), ccy * 4 + ((cellT >> 2) & 3), ccz * 4 + (cellT >> 4));
   if (blk == 0 && t == 0) force[kFine] = fine[kFine];   // the scratch texel, carried through
   const float4 mb = coarse[blk];
   if (!(mb.w > 0.0f)) {   // an empty block: the same for the whole CTA
-    force[c] = make_float4(0, 0, 0, 0);
+    if (q == 0) force[c] = make_float4(0, 0, 0, 0);
     return;
   }
-  for (int o = t; o < 125; o += 64) {   // o = kx + 5 ky + 25 kz: the reference's loop order
+  for (int o = t; o < 125; o += kCellThreads) {   // o = kx + 5 ky + 25 kz: the reference's loop order
     const int kx = ccx + o % 5 - 2, ky = ccy + (o / 5) % 5 - 2, kz = ccz + o / 25 - 2;
     const bool in = kx >= 0 && ky >= 0 && kz >= 0 && kx <= 15 && ky <= 15 && kz <= 15;
     const int k = in ? coarse_index(kx, ky, kz) : 0;
     nbK[o] = k;
     nbOff[o + 1] = in ? __ldg(occN + k) : 0;
   }
-  if (!(fine[c].w > 0.0f)) force[c] = make_float4(0, 0, 0, 0);   // this thread's own place, when empty
-  // thread t sums for the block's t-th occupied cell, so the busy lanes sit together
+  if (q == 0 && !(fine[c].w > 0.0f)) force[c] = make_float4(0, 0, 0, 0);   // an empty place of this block
+  // the cellT-th occupied cell of the block, so the busy lanes sit together
   const int nOwn = __ldg(occN + blk);
-  const bool mine = t < nOwn;
-  const float4 tc = mine ? __ldg(occ + (size_t)blk * 64 + t) : make_float4(0, 0, 0, 0);
-  const int tl = mine ? (int)__ldg(occIdx + (size_t)blk * 64 + t) : -1;
+  const bool mine = cellT < nOwn;
+  const float4 tc = mine ? __ldg(occ + (size_t)blk * 64 + cellT) : make_float4(0, 0, 0, 0);
+  const int tl = mine ? (int)__ldg(occIdx + (size_t)blk * 64 + cellT) : -1;
   const f3 x = xyz(tc);
   const float eps2 = U->eps2Cell, Gm = U->Gm;
   f3 acc = mk(0, 0, 0);
@@ -300,7 +308,7 @@ __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U,
       const int lo = max(nbOff[o], b0), hi = min(nbOff[o + 1], b1);
       if (lo >= hi) continue;
       const int k = nbK[o];
-      for (int e = lo + t; e < hi; e += 64) {
+      for (int e = lo + t; e < hi; e += kCellThreads) {
         const int i = e - nbOff[o];
         src[e - b0] = __ldg(occ + (size_t)k * 64 + i);
         sidx[e - b0] = k == blk ? __ldg(occIdx + (size_t)k * 64 + i) : (uint8_t)255;
@@ -310,7 +318,7 @@ __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U,
     if (mine) {
       const int n = b1 - b0;
 #pragma unroll 4
-      for (int i = 0; i < n; ++i) {
+      for (int i = q; i < n; i += kCellSplit) {
         if ((int)sidx[i] == tl) continue;   // a cell does not pull itself
         const float4 mf = src[i];
         const f3 r = xyz(mf) - x;
@@ -321,7 +329,15 @@ __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U,
     }
     __syncthreads();
   }
-  if (!mine) return;
+  part[q][cellT] = make_float4(acc.x, acc.y, acc.z, pot);
+  __syncthreads();
+  if (!mine || q != 0) return;
+#pragma unroll
+  for (int k = 1; k < kCellSplit; ++k) {
+    const float4 p = part[k][cellT];
+    acc = acc + mk(p.x, p.y, p.z);
+    pot += p.w;
+  }
   const float4 fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
   const f3 d = x - xyz(mb) * fdiv(1.0f, mb.w);
   const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
@@ -333,7 +349,7 @@ __global__ void __launch_bounds__(64) k_cell(const ccs_uniforms *__restrict__ U,
 }
 
 int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st) {
-  k_cell<<<kCoarse, 64, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.farA, m.farT0, m.farT1, m.force);
+  k_cell<<<kCoarse, kCellThreads, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.farA, m.farT0, m.farT1, m.force);
   return 1;
 }
 
