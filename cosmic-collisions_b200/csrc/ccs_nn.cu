@@ -782,13 +782,14 @@ __global__ void __launch_bounds__(1024) k_nn_pp_scan(const ccs_uniforms *__restr
   }
 }
 
+// one warp per target: the lanes take every 32nd of its pairs, then a fixed shuffle tree adds the lanes
 __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__restrict__ U,
                                                       const float4 *__restrict__ list, const float *__restrict__ box,
                                                       int cap, const float2 *__restrict__ tab,
                                                       const int2 *__restrict__ pairs, const int *__restrict__ offs,
                                                       const float4 *__restrict__ mesh, float4 *__restrict__ force) {
-  const int me = blockIdx.x * blockDim.x + threadIdx.x;
-  if (me >= cap) return;
+  const int me = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (me >= cap) return;   // whole warps
   const ccs_uniforms &u = *U;
   const int count = u.ppCount;
   float4 o = make_float4(0, 0, 0, 0);
@@ -801,7 +802,7 @@ __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__rest
     f3 acc = mk(0, 0, 0);
     float pot = 0.0f;
     const int q0 = offs[me * kChunks], q1 = offs[me * kChunks + kChunks];
-    for (int q = q0; q < q1; ++q) {
+    for (int q = q0 + lane; q < q1; q += 32) {
       const int j = pairs[q].y;
       const float4 Q = list[j];
       const f3 d = xsub3(xyz(Q), xyz(P));
@@ -824,12 +825,16 @@ __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__rest
       acc = acc + f * (Q.w * taper);
       pot += Q.w * (-invN - fdiv(Ty, fmaxf(r, a))) * taper;
     }
+#pragma unroll
+    for (int sh = 16; sh >= 1; sh >>= 1) {
+      acc.x += __shfl_xor_sync(0xFFFFFFFFu, acc.x, sh);
+      acc.y += __shfl_xor_sync(0xFFFFFFFFu, acc.y, sh);
+      acc.z += __shfl_xor_sync(0xFFFFFFFFu, acc.z, sh);
+      pot += __shfl_xor_sync(0xFFFFFFFFu, pot, sh);
+    }
     o = make_float4(acc.x * u.Gm, acc.y * u.Gm, acc.z * u.Gm, pot * u.Gm);
   }
-  force[me] = o;
-  force[(size_t)cap + me] = make_float4(0, 0, 0, 0);
-  force[(size_t)2 * cap + me] = make_float4(0, 0, 0, 0);
-  force[(size_t)3 * cap + me] = make_float4(0, 0, 0, 0);
+  if (lane < 4) force[(size_t)lane * cap + me] = lane == 0 ? o : make_float4(0, 0, 0, 0);
 }
 
 int forward_grid() {
@@ -859,7 +864,7 @@ int launch_pp_nn(const ccs_uniforms *u, const float4 *list, const float *box, in
   nn::k_nn_pp_pairs<<<g, 128, 0, st>>>(u, list, cap, offs, counts, pairs);
   nn::LoosePairs rows{u, list, pairs, total};
   nn::k_nn_forward<nn::LoosePairs><<<nn::forward_grid(), nn::kRows, nn::kFwdSmem, st>>>(rows, img, mesh, status);
-  nn::k_nn_pp_reduce<<<(cap + 255) / 256, 256, 0, st>>>(u, list, box, cap, tab, pairs, offs, mesh, force);
+  nn::k_nn_pp_reduce<<<(cap * 32 + 255) / 256, 256, 0, st>>>(u, list, box, cap, tab, pairs, offs, mesh, force);
   return 5;
 }
 
