@@ -699,59 +699,50 @@ __global__ void k_nn_image(const float *__restrict__ params, uint8_t *__restrict
 // ---------------------------------------------------------------------------
 // the learned P3M pass over the loose list (the pass of src/glsl-sim.js:
 // 676-754 with the table's force replaced): pairs inside half the cut are
-// enumerated in (target, chunk, source) order, the network evaluates the mesh
-// part of every pair, and each target sums its pairs in that order.
+// enumerated in (target, source) order, the network evaluates the mesh part of
+// every pair, and each target's pairs are summed by one warp.
 // ---------------------------------------------------------------------------
-constexpr int kChunk = 1024, kChunks = CCS_PP_CAP / kChunk;
-
-// count pass (pairs == nullptr) and fill pass
-__global__ void __launch_bounds__(128) k_nn_pp_pairs(const ccs_uniforms *__restrict__ U,
+// count pass (pairs == nullptr) and fill pass: one warp per target, the lanes test 32 consecutive sources
+// at a time; ballot prefix sums keep each target's pairs in ascending source order
+__global__ void __launch_bounds__(256) k_nn_pp_pairs(const ccs_uniforms *__restrict__ U,
                                                      const float4 *__restrict__ list, int cap,
                                                      const int *__restrict__ offs, int *__restrict__ counts,
                                                      int2 *__restrict__ pairs) {
-  __shared__ float4 sq[128];
+  const int me = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   const ccs_uniforms &u = *U;
   const int count = u.ppCount;
-  const int chunk = blockIdx.y, j0 = chunk * kChunk, i0 = blockIdx.x * 128;
-  if (j0 >= count || i0 >= count) return;
-  const int me = i0 + threadIdx.x;
-  const float4 P = me < cap ? list[me] : make_float4(0, 0, 0, 0);
-  const bool active = me < count && P.w != 0.0f;
+  if (me >= count || me >= cap) return;   // whole warps
+  const float4 P = list[me];
+  const bool active = P.w != 0.0f;
   const float cutN = xmul(0.5f, u.cut), cut2 = xmul(cutN, cutN);
-  const int j1 = min(j0 + kChunk, count);
   int n = 0;
-  const int at = pairs && active ? offs[me * kChunks + chunk] : 0;
-  for (int sub = j0; sub < j1; sub += 128) {
-    __syncthreads();
-    if (sub + (int)threadIdx.x < j1) sq[threadIdx.x] = list[sub + threadIdx.x];
-    __syncthreads();
-    if (!active) continue;
-    const int m = min(128, j1 - sub);
-    for (int jj = 0; jj < m; ++jj) {
-      const int j = sub + jj;
-      if (j == me) continue;
-      const f3 d = xsub3(xyz(sq[jj]), xyz(P));
-      if (xdot(d, d) >= cut2) continue;
-      if (pairs) pairs[at + n] = make_int2(me, j);
-      ++n;
+  const int at = pairs ? offs[me] : 0;
+  if (active) {
+    for (int j0 = 0; j0 < count; j0 += 32) {
+      const int j = j0 + lane;
+      bool near = false;
+      if (j < count && j != me) {
+        const f3 d = xsub3(xyz(list[j]), xyz(P));
+        near = xdot(d, d) < cut2;
+      }
+      const unsigned bal = __ballot_sync(0xFFFFFFFFu, near);
+      if (pairs && near) pairs[at + n + __popc(bal & ((1u << lane) - 1u))] = make_int2(me, j);
+      n += __popc(bal);
     }
   }
-  if (!pairs && me < count) counts[me * kChunks + chunk] = active ? n : 0;
+  if (!pairs && lane == 0) counts[me] = n;
 }
 
-// exclusive scan of the (target, chunk) counts, chunks past the list's end read as 0
+// exclusive scan of the targets' pair counts: offs[0..count], total = offs[count]
 __global__ void __launch_bounds__(1024) k_nn_pp_scan(const ccs_uniforms *__restrict__ U,
                                                      const int *__restrict__ counts, int *__restrict__ offs,
                                                      int *__restrict__ total) {
   __shared__ int warpSum[32];
-  const int count = U->ppCount;
-  const int nc = (count + kChunk - 1) / kChunk;
-  const int E = count * kChunks;
+  const int E = U->ppCount;
   const int per = (E + 1023) / 1024;
   const int e0 = threadIdx.x * per, e1 = min(e0 + per, E);
   int s = 0;
-  for (int e = e0; e < e1; ++e) s += (e % kChunks) < nc ? counts[e] : 0;
-  // block-wide exclusive scan of s
+  for (int e = e0; e < e1; ++e) s += counts[e];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int x = s;
 #pragma unroll
@@ -774,7 +765,7 @@ __global__ void __launch_bounds__(1024) k_nn_pp_scan(const ccs_uniforms *__restr
   int run = x - s + (w > 0 ? warpSum[w - 1] : 0);
   for (int e = e0; e < e1; ++e) {
     offs[e] = run;
-    run += (e % kChunks) < nc ? counts[e] : 0;
+    run += counts[e];
   }
   if (threadIdx.x == 1023) {
     offs[E] = run;
@@ -801,7 +792,7 @@ __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__rest
     const float invH2 = u.invH * u.invH, eps2Cell = u.eps2Cell;
     f3 acc = mk(0, 0, 0);
     float pot = 0.0f;
-    const int q0 = offs[me * kChunks], q1 = offs[me * kChunks + kChunks];
+    const int q0 = offs[me], q1 = offs[me + 1];
     for (int q = q0 + lane; q < q1; q += 32) {
       const int j = pairs[q].y;
       const float4 Q = list[j];
@@ -853,15 +844,15 @@ int forward_grid() {
 // ---------------------------------------------------------------------------
 // launchers used by the engine
 // ---------------------------------------------------------------------------
-size_t nn_pp_count_ints() { return (size_t)CCS_PP_CAP * nn::kChunks + 1; }
+size_t nn_pp_count_ints() { return (size_t)CCS_PP_CAP + 1; }
 
 int launch_pp_nn(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,
                  const uint8_t *img, int *counts, int *offs, int *total, int2 *pairs, float4 *mesh, float4 *force,
                  unsigned *status, cudaStream_t st) {
-  dim3 g((cap + 127) / 128, nn::kChunks);
-  nn::k_nn_pp_pairs<<<g, 128, 0, st>>>(u, list, cap, nullptr, counts, nullptr);
+  const int g = (cap * 32 + 255) / 256;   // a warp per list entry
+  nn::k_nn_pp_pairs<<<g, 256, 0, st>>>(u, list, cap, nullptr, counts, nullptr);
   nn::k_nn_pp_scan<<<1, 1024, 0, st>>>(u, counts, offs, total);
-  nn::k_nn_pp_pairs<<<g, 128, 0, st>>>(u, list, cap, offs, counts, pairs);
+  nn::k_nn_pp_pairs<<<g, 256, 0, st>>>(u, list, cap, offs, counts, pairs);
   nn::LoosePairs rows{u, list, pairs, total};
   nn::k_nn_forward<nn::LoosePairs><<<nn::forward_grid(), nn::kRows, nn::kFwdSmem, st>>>(rows, img, mesh, status);
   nn::k_nn_pp_reduce<<<(cap * 32 + 255) / 256, 256, 0, st>>>(u, list, box, cap, tab, pairs, offs, mesh, force);

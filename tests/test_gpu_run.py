@@ -97,3 +97,32 @@ def test_small_impact_run_keeps_its_books(ccmod):
     # the device's binary64 books agree with the host analysis's
     assert abs(books["M"] - g.M) < 1e-9
     assert abs(np.sqrt(books["Lx"] ** 2 + books["Ly"] ** 2 + books["Lz"] ** 2) - g.L) < 1e-6 * g.L
+
+
+def test_hit_and_run_raises_the_second_box(ccmod):
+    """The full impact's case B (0.15 M_earth at 30 degrees and 1.4 v_esc): the impactor survives a hit
+    & run, and the second mesh box is seen going up on it (placeBoxes, src/nbody.js:357-373: a second
+    body above 0.05 M_earth whose core is beyond FL - 1.3 R of the largest's), at 65,536 particles."""
+    from cosmic_collisions_b200 import configs
+    nb = ccmod.NBody(0)
+    seen = None
+    try:
+        nb.build(configs.full_impact_opt(65536, case="B"))
+        t = 0.0
+        while t < 24.0 and seen is None:
+            t += 0.5
+            nb.run_to(t)
+            if nb.sim.boxOn[1]:
+                r = nb.report
+                seen = {"t": nb.sim.t, "steps": nb.sim.stepNo, "second": r.secMass, "largest": r.largest,
+                        "cen": [nb.sim.boxCen[1][k] for k in range(3)], "drift": r.drift}
+        if seen is not None:
+            nb.steps(64)                                # the step with both boxes up
+            nb.sync()
+            st = nb.read_state()
+            assert np.isfinite(st["pos"]).all() and np.isfinite(st["vel"]).all()
+    finally:
+        nb.close()
+    print("second box up:", seen)
+    assert seen is not None, "the second box never went up"
+    assert seen["second"] > 0.05 and seen["drift"] < 1e-3
