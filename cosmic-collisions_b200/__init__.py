@@ -6,4 +6,4 @@ the host-side mirror of the reference engine object `CC.nbody`
 (src/nbody.js:1095-1118).  Import it as ``cosmic_collisions_b200``.
 """
 from ._lib import CCSError, lib, make_bodies, make_opt, fof, pair_table  # noqa: F401
-from .nbody import NBody, mean_k  # noqa: F401
+from .nbody import Ensemble, NBody, mean_k  # noqa: F401

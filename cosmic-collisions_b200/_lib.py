@@ -37,7 +37,9 @@ EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_ma
            "ccs_timing", "ccs_timing_read", "ccs_launch_count", "ccs_direct_sum", "ccs_pp_force_static",
            "ccs_nn_create", "ccs_nn_destroy", "ccs_nn_last_error", "ccs_nn_set_params", "ccs_nn_get_params",
            "ccs_nn_clear", "ccs_nn_pool_size", "ccs_nn_sample_state", "ccs_nn_sample_uniform", "ccs_nn_read_pool",
-           "ccs_nn_train", "ccs_nn_forward", "ccs_nn_labels", "ccs_nn_grad", "ccs_set_pp_nn"]
+           "ccs_nn_train", "ccs_nn_forward", "ccs_nn_labels", "ccs_nn_grad", "ccs_set_pp_nn", "ccs_autotune",
+           "ccs_ensemble_create", "ccs_ensemble_destroy", "ccs_ensemble_last_error", "ccs_ensemble_steps",
+           "ccs_ensemble_sync"]
 NN_PARAMS = 4803
 NN_CUT_CELLS = 2.5
 
@@ -189,6 +191,12 @@ def lib():
         "ccs_nn_labels": (I, [H, P, C.c_int64, P]),
         "ccs_nn_grad": (I, [H, P, P, C.c_int64, P, P]),
         "ccs_set_pp_nn": (I, [H, H]),
+        "ccs_autotune": (I, [H, I, P]),
+        "ccs_ensemble_create": (I, [P, I, C.POINTER(C.c_void_p)]),
+        "ccs_ensemble_destroy": (I, [H]),
+        "ccs_ensemble_last_error": (C.c_char_p, [H]),
+        "ccs_ensemble_steps": (I, [H, I]),
+        "ccs_ensemble_sync": (I, [H]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

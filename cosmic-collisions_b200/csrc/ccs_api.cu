@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -100,6 +101,8 @@ struct ccs_handle {
   std::map<GraphKey, GraphSlot> graphs;
   int ping = 0;
   bool useGraphs = true;
+  // launch shapes chosen by ccs_autotune: contact-step warps per CTA, cell-gravity threads per cell
+  int tuneWarps = 8, tuneSplit = 4;
   // timing of chosen kernels with events on the stream
   bool timing = false;
   std::vector<cudaEvent_t> evPool;
@@ -321,7 +324,7 @@ void pass_mesh_box(ccs_handle *h, const ccs_uniforms *U, int b) {
   h->launches += launch_coarse(m, h->st);
   h->launches += launch_far(m, h->st);
   time_begin(h, 3, &eb, &ee);
-  h->launches += launch_cell(U, m, h->st);
+  h->launches += launch_cell(U, m, h->st, h->tuneSplit);
   time_end(h, ee);
 }
 
@@ -344,7 +347,8 @@ void pass_pp(ccs_handle *h, const ccs_uniforms *U, int count) {
   time_end(h, e);
 }
 
-void pass_sim(ccs_handle *h, const ccs_uniforms *U) {
+// the contact step's arguments: state `s` in, the other buffers out
+SimArgs sim_args(const ccs_handle *h) {
   const int s = h->cur, d = h->cur ^ 1;
   SimArgs a;
   a.pos = h->pos[s];
@@ -363,11 +367,16 @@ void pass_sim(ccs_handle *h, const ccs_uniforms *U) {
   a.velO = h->vel[d];
   a.auxO = h->aux[d];
   a.qO = h->q[d];
+  return a;
+}
+
+void pass_sim(ccs_handle *h, const ccs_uniforms *U) {
+  const SimArgs a = sim_args(h);
   cudaEvent_t b, e;
   time_begin(h, 0, &b, &e);
-  h->launches += launch_simulate(U, h->N, a, h->st);
+  h->launches += launch_simulate(U, h->N, a, h->st, h->tuneWarps);
   time_end(h, e);
-  h->cur = d;
+  h->cur ^= 1;
 }
 
 void pass_diag_kernel(ccs_handle *h, const ccs_uniforms *U) {
@@ -402,6 +411,20 @@ StepPlan plan_step(ccs_handle *h, int settle, int kick) {
   if (p.mesh) set_boxes(h);
   p.u = pass_uniforms(h, settle, kick, p.mesh ? h->meshEvery * s.dt : 0.0);
   return p;
+}
+
+// a block's launches counted as the direct path would count them
+int block_launches(const ccs_handle *h, const StepPlan *plans, int M) {
+  int per = 0;
+  for (int k = 0; k < M; ++k) {
+    per += 1;                                       // contact step
+    if (plans[k].slots) per += 1;                   // contact grid
+    if (plans[k].mesh) {
+      per += 4 * (1 + (plans[k].u.boxB > 0.5f));    // deposit, coarse, far, cell per box
+      if (plans[k].u.ppCount) per += h->nn ? 6 : 3; // gather, then pairs + reduce (or the learned pass's five)
+    }
+  }
+  return per;
 }
 
 void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
@@ -487,17 +510,7 @@ int graph_block(ccs_handle *h) {
   // a block does 4 grid rebuilds (the table parity returns) and M swaps
   h->cur = cur0 ^ (M & 1);
   h->seatCur = seatCur0 ^ (((M + 1) / 2) & 1);
-  // count the block's launches as the direct path would
-  int per = 0;
-  for (int k = 0; k < M; ++k) {
-    per += 1;                                   // simulate
-    if (plans[k].slots) per += 1;               // contact grid
-    if (plans[k].mesh) {
-      per += 4 * (1 + (us[k].boxB > 0.5f));     // deposit, coarse, far, cell per box
-      if (us[k].ppCount) per += h->nn ? 6 : 3;  // gather, then pairs + reduce (or the learned pass's five)
-    }
-  }
-  h->launches += per;
+  h->launches += block_launches(h, plans, M);
   return CCS_OK;
 }
 
@@ -767,6 +780,301 @@ int ccs_steps(ccs_handle *h, int n) {
     }
   }
   return check_launch(h);
+}
+
+}  // extern "C"
+
+// ---- the autotuner: launch shapes by measurement on the run's own state ----
+namespace {
+std::mutex g_tuneMu;
+std::map<std::pair<int, int>, std::pair<int, int>> g_tuned;   // (N, G) -> (warps, split)
+
+// mean device time (ms) of `reps` launches of f on the handle's stream, after one warm launch
+template <class F>
+int time_launches(ccs_handle *h, int reps, F f, float *ms) {
+  cudaEvent_t a, b;
+  CUDA_TRY(h, cudaEventCreate(&a));
+  CUDA_TRY(h, cudaEventCreate(&b));
+  f();
+  cudaEventRecord(a, h->st);
+  for (int r = 0; r < reps; ++r) f();
+  cudaEventRecord(b, h->st);
+  cudaError_t e = cudaEventSynchronize(b);
+  float t = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (e != cudaSuccess) {
+    h->err = std::string("autotune timing: ") + cudaGetErrorString(e);
+    return CCS_E_CUDA;
+  }
+  *ms = t / (float)reps;
+  return CCS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int ccs_autotune(ccs_handle *h, int reps, int choice[2]) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (reps < 0) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  const std::pair<int, int> key(h->N, h->sim.G);
+  int warps = 8, split = 4;
+  if (reps == 0) {
+    std::lock_guard<std::mutex> lk(g_tuneMu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      warps = it->second.first;
+      split = it->second.second;
+    }
+  } else {
+    CUDA_TRY(h, cudaStreamSynchronize(h->st));
+    const ccs_uniforms *U;
+    rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+    if (rc) return rc;
+    const bool timing = h->timing;
+    h->timing = false;
+    const int64_t l0 = h->launches;
+    // the contact step into the spare buffers (no state changes), at each CTA width
+    const SimArgs a = sim_args(h);
+    float best = 1e30f;
+    for (int w : {8, 4}) {
+      float ms = 0.0f;
+      rc = time_launches(h, reps, [&] { launch_simulate(U, h->N, a, h->st, w); }, &ms);
+      if (rc) break;
+      if (ms < best) { best = ms; warps = w; }
+    }
+    // the cell gravity of box 0 over the last mesh step's inputs (it rewrites the same force), at each split
+    best = 1e30f;
+    for (int sp : {2, 4, 8}) {
+      if (rc) break;
+      float ms = 0.0f;
+      rc = time_launches(h, reps, [&] { launch_cell(U, h->pm[0], h->st, sp); }, &ms);
+      if (rc) break;
+      if (ms < best) { best = ms; split = sp; }
+    }
+    if (!rc) launch_cell(U, h->pm[0], h->st, split);
+    h->timing = timing;
+    h->launches = l0;
+    if (rc) return rc;
+    CUDA_TRY(h, cudaStreamSynchronize(h->st));
+    std::lock_guard<std::mutex> lk(g_tuneMu);
+    g_tuned[key] = std::make_pair(warps, split);
+  }
+  if (warps != h->tuneWarps || split != h->tuneSplit) {
+    CUDA_TRY(h, cudaStreamSynchronize(h->st));
+    free_graphs(h);   // captured blocks hold the old shapes
+    h->tuneWarps = warps;
+    h->tuneSplit = split;
+  }
+  if (choice) {
+    choice[0] = warps;
+    choice[1] = split;
+  }
+  return check_launch(h);
+}
+
+}  // extern "C"
+
+// ---- the batched ensemble: every member's block from one graph ----
+namespace {
+struct EnsembleGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<ccs_uniforms *> dev, host;   // per member: meshEvery uniform slots, and their pinned staging
+  cudaEvent_t done = nullptr;
+  bool used = false;
+};
+}  // namespace
+
+struct ccs_ensemble {
+  int device = 0, M = 8;
+  std::vector<ccs_handle *> m;
+  cudaStream_t st = nullptr;
+  cudaEvent_t fork = nullptr, after = nullptr;
+  std::vector<cudaEvent_t> join, ready;
+  std::map<std::vector<GraphKey>, EnsembleGraph> graphs;
+  std::string err;
+};
+
+namespace {
+void free_ensemble_graphs(ccs_ensemble *e) {
+  for (auto &kv : e->graphs) {
+    EnsembleGraph &g = kv.second;
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto p : g.dev) cudaFree(p);
+    for (auto p : g.host) cudaFreeHost(p);
+    if (g.done) cudaEventDestroy(g.done);
+  }
+  e->graphs.clear();
+}
+
+#define ENS_TRY(e, call)                                                                         \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) {                                                                     \
+      (e)->err = std::string(#call) + ": " + cudaGetErrorString(e_);                             \
+      return CCS_E_CUDA;                                                                         \
+    }                                                                                            \
+  } while (0)
+
+// one round: every member's next meshEvery steps, one graph launch
+int ensemble_block(ccs_ensemble *e) {
+  const int n = (int)e->m.size(), M = e->M;
+  std::vector<GraphKey> keys(n);
+  std::vector<std::vector<StepPlan>> plans(n, std::vector<StepPlan>(M));
+  std::vector<int> seat0(n), cur0(n);
+  for (int i = 0; i < n; ++i) {
+    ccs_handle *h = e->m[i];
+    for (int k = 0; k < M; ++k) {
+      plans[i][k] = plan_step(h, 0, 0);
+      h->sim.t += h->sim.dt;   // the frame loop's clock, index.html:372
+    }
+    keys[i] = GraphKey{(int)(plans[i][0].u.boxB > 0.5f), h->ppCount > 0, h->seatCur, h->cur, M, h->ping};
+    seat0[i] = h->seatCur;
+    cur0[i] = h->cur;
+  }
+  EnsembleGraph &g = e->graphs[keys];
+  if (!g.exec) {
+    g.dev.assign(n, nullptr);
+    g.host.assign(n, nullptr);
+    for (int i = 0; i < n; ++i) {
+      ENS_TRY(e, cudaMalloc(&g.dev[i], sizeof(ccs_uniforms) * M));
+      ENS_TRY(e, cudaMallocHost(&g.host[i], sizeof(ccs_uniforms) * M));
+    }
+    ENS_TRY(e, cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+    cudaGraph_t graph;
+    ENS_TRY(e, cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecord(e->fork, e->st);
+    for (int i = 0; i < n; ++i) {   // every member's block on its own stream: parallel branches
+      ccs_handle *h = e->m[i];
+      const bool timing = h->timing;
+      const int64_t l0 = h->launches;
+      h->timing = false;
+      cudaStreamWaitEvent(h->st, e->fork, 0);
+      cudaMemcpyAsync(g.dev[i], g.host[i], sizeof(ccs_uniforms) * M, cudaMemcpyHostToDevice, h->st);
+      for (int k = 0; k < M; ++k) enqueue_step(h, plans[i][k], g.dev[i] + k);
+      cudaEventRecord(e->join[i], h->st);
+      cudaStreamWaitEvent(e->st, e->join[i], 0);
+      h->timing = timing;
+      h->launches = l0;
+      h->seatCur = seat0[i];   // capture ran the buffer rotation on the host; the replay redoes it
+      h->cur = cur0[i];
+    }
+    cudaError_t ce = cudaStreamEndCapture(e->st, &graph);
+    if (ce != cudaSuccess) {
+      e->err = std::string("ensemble capture: ") + cudaGetErrorString(ce);
+      return CCS_E_CUDA;
+    }
+    ce = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) {
+      e->err = std::string("ensemble instantiate: ") + cudaGetErrorString(ce);
+      g.exec = nullptr;
+      return CCS_E_CUDA;
+    }
+  }
+  if (g.used) ENS_TRY(e, cudaEventSynchronize(g.done));
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < M; ++k) g.host[i][k] = plans[i][k].u;
+  for (int i = 0; i < n; ++i) {   // after whatever each member has queued
+    ENS_TRY(e, cudaEventRecord(e->ready[i], e->m[i]->st));
+    ENS_TRY(e, cudaStreamWaitEvent(e->st, e->ready[i], 0));
+  }
+  ENS_TRY(e, cudaGraphLaunch(g.exec, e->st));
+  ENS_TRY(e, cudaEventRecord(g.done, e->st));
+  ENS_TRY(e, cudaEventRecord(e->after, e->st));
+  for (int i = 0; i < n; ++i) {   // and whatever they queue next comes after it
+    ccs_handle *h = e->m[i];
+    ENS_TRY(e, cudaStreamWaitEvent(h->st, e->after, 0));
+    h->ping ^= 1;
+    h->cur = cur0[i] ^ (M & 1);
+    h->seatCur = seat0[i] ^ (((M + 1) / 2) & 1);
+    h->launches += block_launches(h, plans[i].data(), M);
+  }
+  return CCS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int ccs_ensemble_create(ccs_handle *const *members, int count, ccs_ensemble **out) {
+  if (!out || !members || count <= 0) return CCS_E_ARG;
+  *out = nullptr;
+  for (int i = 0; i < count; ++i) {
+    if (!members[i] || !members[i]->built) return CCS_E_STATE;
+    if (members[i]->device != members[0]->device || members[i]->meshEvery != members[0]->meshEvery ||
+        members[i]->meshEvery % 2)
+      return CCS_E_ARG;
+    for (int j = 0; j < i; ++j)
+      if (members[j] == members[i]) return CCS_E_ARG;
+  }
+  cudaSetDevice(members[0]->device);
+  ccs_ensemble *e = new (std::nothrow) ccs_ensemble();
+  if (!e) return CCS_E_NOMEM;
+  e->device = members[0]->device;
+  e->M = members[0]->meshEvery;
+  e->m.assign(members, members + count);
+  e->join.assign(count, nullptr);
+  e->ready.assign(count, nullptr);
+  bool ok = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->after, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; ok && i < count; ++i)
+    ok = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&e->ready[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    ccs_ensemble_destroy(e);
+    return CCS_E_CUDA;
+  }
+  *out = e;
+  return CCS_OK;
+}
+
+int ccs_ensemble_destroy(ccs_ensemble *e) {
+  if (!e) return CCS_OK;
+  cudaSetDevice(e->device);
+  if (e->st) cudaStreamSynchronize(e->st);
+  free_ensemble_graphs(e);
+  for (auto ev : e->join) if (ev) cudaEventDestroy(ev);
+  for (auto ev : e->ready) if (ev) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->after) cudaEventDestroy(e->after);
+  if (e->st) cudaStreamDestroy(e->st);
+  delete e;
+  return CCS_OK;
+}
+
+const char *ccs_ensemble_last_error(const ccs_ensemble *e) { return e ? e->err.c_str() : "null ensemble"; }
+
+int ccs_ensemble_steps(ccs_ensemble *e, int n) {
+  if (!e || n < 0 || n % e->M) return CCS_E_ARG;
+  for (ccs_handle *h : e->m)
+    if (h->sim.stepNo % e->M || h->meshEvery != e->M || h->timing) {
+      e->err = "every member must sit at a block boundary (stepNo % meshEvery == 0) with timing off";
+      return CCS_E_STATE;
+    }
+  cudaSetDevice(e->device);
+  for (int b = 0; b < n / e->M; ++b) {
+    int rc = ensemble_block(e);
+    if (rc) return rc;
+  }
+  return CCS_OK;
+}
+
+int ccs_ensemble_sync(ccs_ensemble *e) {
+  if (!e) return CCS_E_ARG;
+  cudaSetDevice(e->device);
+  ENS_TRY(e, cudaStreamSynchronize(e->st));
+  for (ccs_handle *h : e->m) {
+    int rc = check_status(h);
+    if (rc) {
+      e->err = h->err;
+      return rc;
+    }
+  }
+  return CCS_OK;
 }
 
 int ccs_settle_some(ccs_handle *h, int n) {

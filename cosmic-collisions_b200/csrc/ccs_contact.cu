@@ -26,8 +26,6 @@
 namespace ccs {
 
 namespace {
-constexpr int kWarps = 8;                    // warps per CTA
-constexpr int kThreads = 32 * kWarps;
 constexpr int kQCap = 32 * kSeats + 64;      // seat candidates: one stage-1 round plus what is left
 constexpr int kNCap = 64;                    // neighbours: one stage-2 round plus what is left
 inline int blocks_for(long n, int b) { return (int)((n + b - 1) / b); }
@@ -130,7 +128,11 @@ __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const Si
   if (two) push_near(u, a, spc, w, near1, e1, r21, lane, nn);
 }
 
-__global__ void __launch_bounds__(kThreads, 4) k_contact_step(const ccs_uniforms *__restrict__ U, const SimArgs a) {
+// W warps per CTA (8 or 4: the autotuner's choice; 4 CTAs of 8 or 8 of 4 share an SM)
+template <int W>
+__global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_uniforms *__restrict__ U,
+                                                                 const SimArgs a) {
+  constexpr int kThreads = 32 * W;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ float spc[16];   // seatPos(q) * uCell, exact
   const ccs_uniforms &u = *U;
@@ -273,14 +275,21 @@ __global__ void __launch_bounds__(kThreads, 4) k_contact_step(const ccs_uniforms
   a.qO[me] = Q;
 }
 
-size_t contact_smem_bytes() { return sizeof(ContactWarp) * kWarps; }
+size_t contact_smem_bytes(int warps) { return sizeof(ContactWarp) * warps; }
 
 cudaError_t init_kernels() {
-  return cudaFuncSetAttribute(k_contact_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)contact_smem_bytes());
+  cudaError_t e = cudaFuncSetAttribute(k_contact_step<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)contact_smem_bytes(8));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_contact_step<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)contact_smem_bytes(4));
 }
 
-int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st) {
-  k_contact_step<<<blocks_for(N, kThreads), kThreads, contact_smem_bytes(), st>>>(u, a);
+int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st, int warps) {
+  if (warps == 4)
+    k_contact_step<4><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+  else
+    k_contact_step<8><<<blocks_for(N, 256), 256, contact_smem_bytes(8), st>>>(u, a);
   return 1;
 }
 

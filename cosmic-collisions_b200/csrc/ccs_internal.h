@@ -64,12 +64,14 @@ cudaError_t init_kernels();
 int launch_fill_u32(uint32_t *p, size_t n, uint32_t v, cudaStream_t st);
 int launch_contact_grid(const ccs_uniforms *u, int N, const float4 *pos, uint32_t *seats, uint32_t *hk,
                         uint32_t *seatsOld, const uint32_t *hkOld, unsigned *status, cudaStream_t st);
-int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st);
+// warps: CTA width of the contact step, 8 or 4
+int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st, int warps = 8);
 int launch_deposit(const ccs_uniforms *u, int N, int box, const float4 *pos, const float *mat, const float4 *monoPrev,
                    float4 *fine, cudaStream_t st);
 int launch_coarse(const MeshBuf &m, cudaStream_t st);
 int launch_far(const MeshBuf &m, cudaStream_t st);
-int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st);
+// split: threads per fine cell in the cell-gravity sums, 2, 4 or 8
+int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int split = 4);
 int launch_pp_gather(const ccs_uniforms *u, const float4 *pos, const float *mat, const int *index, int cap,
                      float4 *list, float *box, cudaStream_t st);
 // the pairwise partials of the P3M pass: 4 quarters x chunks x cap float4

@@ -240,23 +240,23 @@ int launch_far(const MeshBuf &m, cudaStream_t st) {
 
 // ---------------------------------------------------------------------------
 // cell gravity: src/glsl-sim.js:303-352.  One CTA per coarse block; its 64
-// fine cells each get kCellSplit threads (a cell can hold mass only if its
+// fine cells each get SPLIT threads (a cell can hold mass only if its
 // block does).  The CTA reads how many occupied cells each of the 5^3 blocks
 // around it holds, then copies the occupied cells of all of them -- centre of
 // mass and mass, as the coarse pass listed them, block by block in the
 // reference's order -- into shared memory in one pass of independent loads
 // (in batches of kCellBatch when the neighbourhood holds more).  A block in
 // the bodies sees thousands of sources, so each occupied cell's sum is split
-// over its kCellSplit threads (every kCellSplit-th source), and the partial
-// sums are added in a fixed order: the result is deterministic.  A cell skips
+// over its SPLIT threads (every SPLIT-th source; 2, 4 or 8, the autotuner's
+// choice), and the partial sums are added in a fixed order: the result is
+// deterministic for a given SPLIT.  A cell skips
 // itself.  Then the block's far field is carried to the cell by the tidal
 // tensor.  Cell-on-cell pulls are fast arithmetic (rsqrt, FMA).
 // ---------------------------------------------------------------------------
 constexpr int kCellBatch = 1024;
-constexpr int kCellSplit = 4;
-constexpr int kCellThreads = 64 * kCellSplit;
 
-__global__ void __launch_bounds__(kCellThreads) k_cell(const ccs_uniforms *__restrict__ U,
+template <int SPLIT>
+__global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restrict__ U,
                                                        const float4 *__restrict__ fine,
                                                        const float4 *__restrict__ coarse,
                                                        const float4 *__restrict__ occ,
@@ -267,7 +267,8 @@ __global__ void __launch_bounds__(kCellThreads) k_cell(const ccs_uniforms *__res
   __shared__ int nbK[125], nbOff[126];
   __shared__ float4 src[kCellBatch];
   __shared__ uint8_t sidx[kCellBatch];   // a source's place in its block; 255 for another block's cells
-  __shared__ float4 part[kCellSplit][64];
+  constexpr int kCellThreads = 64 * SPLIT;
+  __shared__ float4 part[SPLIT][64];
   const int blk = blockIdx.x, t = threadIdx.x, cellT = t & 63, q = t >> 6;
   const int ccx = blk & 15, ccy = (blk >> 4) & 15, ccz = blk >> 8;
   const int c = fine_index(ccx * 4 + (cellT & 3), ccy * 4 + ((cellT >> 2) & 3), ccz * 4 + (cellT >> 4));
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(kCellThreads) k_cell(const ccs_uniforms *__res
     if (mine) {
       const int n = b1 - b0;
 #pragma unroll 4
-      for (int i = q; i < n; i += kCellSplit) {
+      for (int i = q; i < n; i += SPLIT) {
         if ((int)sidx[i] == tl) continue;   // a cell does not pull itself
         const float4 mf = src[i];
         const f3 r = xyz(mf) - x;
@@ -333,7 +334,7 @@ __global__ void __launch_bounds__(kCellThreads) k_cell(const ccs_uniforms *__res
   __syncthreads();
   if (!mine || q != 0) return;
 #pragma unroll
-  for (int k = 1; k < kCellSplit; ++k) {
+  for (int k = 1; k < SPLIT; ++k) {
     const float4 p = part[k][cellT];
     acc = acc + mk(p.x, p.y, p.z);
     pot += p.w;
@@ -348,8 +349,16 @@ __global__ void __launch_bounds__(kCellThreads) k_cell(const ccs_uniforms *__res
       make_float4(acc.x * Gm, acc.y * Gm, acc.z * Gm, pot * Gm);
 }
 
-int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st) {
-  k_cell<<<kCoarse, kCellThreads, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.farA, m.farT0, m.farT1, m.force);
+int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int split) {
+  if (split == 2)
+    k_cell<2><<<kCoarse, 128, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.farA, m.farT0, m.farT1,
+                                       m.force);
+  else if (split == 8)
+    k_cell<8><<<kCoarse, 512, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.farA, m.farT0, m.farT1,
+                                       m.force);
+  else
+    k_cell<4><<<kCoarse, 256, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.farA, m.farT0, m.farT1,
+                                       m.force);
   return 1;
 }
 

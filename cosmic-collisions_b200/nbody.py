@@ -361,6 +361,13 @@ class NBody:
                     "ccs_set_pp")
         self.pp = {"count": n, "loose": int(loose if loose is not None else n)}
 
+    def autotune(self, reps=8):
+        """ccs_autotune: measure the contact step's CTA width and the cell gravity's threads per cell on this run's
+        state (reps > 0) or apply what an earlier run of the same size measured (reps = 0); returns the choice."""
+        ch = (C.c_int * 2)()
+        self._check(lib().ccs_autotune(self._h, int(reps), ch), "ccs_autotune")
+        return {"warps": ch[0], "cell_split": ch[1]}
+
     def set_pp_nn(self, net):
         """Attach a LearnedCorrection to the P3M pass (None: back to the plain table).  The network must outlive
         the attachment."""
@@ -401,3 +408,40 @@ class NBody:
     @property
     def analyzedAt(self):
         return self.analyzed_at
+
+
+class Ensemble:
+    """ccs_ensemble: several engines advanced together, each round of meshEvery steps one CUDA graph with every
+    member's block as a parallel branch.  The members stay usable engines and must outlive the ensemble."""
+
+    def __init__(self, members):
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.handle.value for m in self.members])
+        h = C.c_void_p()
+        rc = lib().ccs_ensemble_create(arr, len(self.members), C.byref(h))
+        if rc != 0:
+            raise L.CCSError("ccs_ensemble_create failed: %s" % L.CCS_E.get(rc, rc))
+        self._h = h
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise L.CCSError("%s failed: %s %s" % (what, L.CCS_E.get(rc, rc),
+                                                   lib().ccs_ensemble_last_error(self._h).decode()))
+
+    def steps(self, n):
+        """n frame-loop steps of every member (n a multiple of meshEvery; members at a block boundary)."""
+        self._check(lib().ccs_ensemble_steps(self._h, int(n)), "ccs_ensemble_steps")
+
+    def sync(self):
+        self._check(lib().ccs_ensemble_sync(self._h), "ccs_ensemble_sync")
+
+    def close(self):
+        if self._h:
+            lib().ccs_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

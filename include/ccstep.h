@@ -243,6 +243,35 @@ int ccs_nn_grad(ccs_nn *nn, const float *rec6, const float *label3, int64_t n, f
 /* attach (or, with NULL, detach) a network to an engine's P3M pass */
 int ccs_set_pp_nn(ccs_handle *h, ccs_nn *nn);
 
+/* ---- launch shapes by measurement ----
+ * No counterpart in the reference (WebGL fixes its own shapes).  Times the
+ * contact step at 8 and 4 warps per CTA and the cell gravity at 2, 4 and 8
+ * threads per fine cell, `reps` launches each, on the run's current state
+ * (the contact step writes only the spare state buffers; the cell gravity
+ * rewrites the last mesh step's force from the same inputs), keeps the fastest
+ * of each for this run and for every later run of the same particle count and
+ * grid in the process.  reps = 0 measures nothing: it applies what an earlier
+ * call measured for this size (or the defaults 8 and 4).  choice (may be NULL)
+ * gets {warps, threads per cell}.  Tune a state that has taken a mesh step. */
+int ccs_autotune(ccs_handle *h, int reps, int choice[2]);
+
+/* ---- the batched ensemble ----
+ * No counterpart in the reference, which runs one impact per page.  An
+ * ensemble advances several engines (impacts of any sizes, on one device)
+ * together: each round of meshEvery steps is one CUDA graph holding every
+ * member's block as a parallel branch, replayed with one launch.  The members
+ * stay ordinary engines (their own streams, buffers and read-outs); work a
+ * caller queues on a member is ordered before and after the ensemble's
+ * rounds.  Members must outlive the ensemble, share one meshEvery, and sit at
+ * a block boundary (stepNo % meshEvery == 0) when ccs_ensemble_steps is
+ * called; n is a multiple of meshEvery. */
+typedef struct ccs_ensemble ccs_ensemble;
+int ccs_ensemble_create(ccs_handle *const *members, int count, ccs_ensemble **out);
+int ccs_ensemble_destroy(ccs_ensemble *e);
+const char *ccs_ensemble_last_error(const ccs_ensemble *e);
+int ccs_ensemble_steps(ccs_ensemble *e, int n);
+int ccs_ensemble_sync(ccs_ensemble *e);   /* waits for the rounds; reports any member's kernel status */
+
 /* Internal buffers, for tests and the console checks of index.html:531-556:
  * which = CCS_BUF_* below; bytes must equal the buffer's size. */
 enum {

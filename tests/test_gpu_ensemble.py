@@ -1,0 +1,87 @@
+"""The batched ensemble and the autotuner on the GPU.
+
+* ccs_autotune measures launch shapes without moving the run: the state is
+  bit-for-bit the same after it, and the chosen shapes step the run as the
+  defaults do (to the spread of two lone runs: float atomics sum in any order);
+* an ensemble round (one graph with every member's block as a branch) steps
+  each member as ccs_steps steps it alone, for members of different sizes, and
+  the members stay usable engines afterwards.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def settled(ccmod, N, steps=64):
+    from cosmic_collisions_b200 import configs
+    nb = ccmod.NBody(0)
+    nb.build(configs.small_impact_opt(N))
+    nb.settle_some(steps)
+    nb.steps(8)
+    nb.sync()
+    return nb
+
+
+def spread_ok(a, b, lone, scale):
+    return np.abs(a - b).max() <= max(10 * lone, 1e-4 * scale) and np.abs(a - b).max() <= 2e-2 * scale
+
+
+def test_autotune_measures_without_moving_the_run(ccmod):
+    runs = [settled(ccmod, 16384) for _ in range(3)]
+    try:
+        before = runs[0].read_state()
+        choice = runs[0].autotune(reps=4)
+        after = runs[0].read_state()
+        assert choice["warps"] in (4, 8) and choice["cell_split"] in (2, 4, 8)
+        for k in ("pos", "vel", "q"):
+            assert np.array_equal(before[k], after[k])
+        again = runs[1].autotune(reps=0)              # the same size: what was measured, no timing
+        assert again == choice
+        for nb in runs:
+            nb.steps(16)
+        st = [nb.read_state() for nb in runs]
+    finally:
+        for nb in runs:
+            nb.close()
+    for k in ("pos", "vel"):
+        ref = st[2][k][:, :3].astype(np.float64)      # default shapes
+        lone = np.abs(st[1][k][:, :3] - ref).max()    # tuned: the same shapes as run 0
+        assert spread_ok(st[0][k][:, :3], ref, max(lone, 1e-7), np.abs(ref).max()), k
+
+
+def test_ensemble_round_steps_members_as_alone(ccmod):
+    sizes = [16384, 32768, 16384]
+    members = [settled(ccmod, N) for N in sizes]
+    lone = [settled(ccmod, N) for N in sizes]
+    lone2 = settled(ccmod, 16384)
+    try:
+        ens = ccmod.Ensemble(members)
+        ens.steps(16)
+        ens.sync()
+        for nb in lone + [lone2]:
+            nb.steps(16)
+            nb.sync()
+        assert [nb.sim.stepNo for nb in members] == [nb.sim.stepNo for nb in lone]
+        spread = np.abs(lone2.read_state()["vel"][:, :3] - lone[0].read_state()["vel"][:, :3]).max()
+        for a, b in zip(members, lone):
+            sa, sb = a.read_state(), b.read_state()
+            for k in ("pos", "vel"):
+                ref = sb[k][:, :3].astype(np.float64)
+                assert spread_ok(sa[k][:, :3], ref, max(spread, 1e-7), np.abs(ref).max()), k
+        # the members stay engines: a direct step, then another round
+        members[0].step(False, False)
+        members[0].sim.t += members[0].sim.dt
+        with pytest.raises(ccmod.CCSError):
+            ens.steps(8)                              # member 0 is off the block boundary
+        for _ in range(7):
+            members[0].step(False, False)
+            members[0].sim.t += members[0].sim.dt
+        ens.steps(8)
+        ens.sync()
+        for nb in members:
+            assert np.isfinite(nb.read_state()["pos"]).all()
+        ens.close()
+    finally:
+        for nb in members + lone + [lone2]:
+            nb.close()
