@@ -365,7 +365,7 @@ def run_ensemble(args, log):
     ens.close()
     line = {"metric": "ensemble aggregate particle-steps/s", "value": total / wall_graph, "unit": "particle-steps/s",
             "instances": len(runs), "steps_each": 8 * blocks, "particles": int(sum(nb.sim.N for nb in runs)),
-            "mode": "one CUDA graph per 8-step round holding every instance's block as a parallel branch "
+            "mode": "one CUDA graph per four 8-step rounds holding every instance's steps as a parallel branch "
                     "(ccs_ensemble); wall clock over the rounds",
             "per_handle_streams": {"value": total / wall, "wall_s": wall,
                                    "per_instance_step_ms": {"p50": float(np.percentile(per_step_ms, 50)),

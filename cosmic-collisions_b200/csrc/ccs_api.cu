@@ -321,6 +321,7 @@ void pass_mesh_box(ccs_handle *h, const ccs_uniforms *U, int b) {
   time_begin(h, 2, &eb, &ee);
   h->launches += launch_deposit(U, h->N, b, h->pos[h->cur], h->mat, m.mono, m.fine, h->st);
   time_end(h, ee);
+  cudaMemsetAsync(m.occCount, 0, sizeof(int), h->st);
   h->launches += launch_coarse(m, h->st);
   h->launches += launch_far(m, h->st);
   time_begin(h, 3, &eb, &ee);
@@ -555,7 +556,7 @@ void free_state(ccs_handle *h) {
     MeshBuf &m = h->pm[b];
     dev_free(m.fine); dev_free(m.force); dev_free(m.coarse); dev_free(m.farA); dev_free(m.farT0);
     dev_free(m.farT1); dev_free(m.mono); dev_free(m.partial); dev_free(m.counter);
-    dev_free(m.occ); dev_free(m.occIdx); dev_free(m.occN);
+    dev_free(m.occ); dev_free(m.occIdx); dev_free(m.occN); dev_free(m.occBlocks); dev_free(m.occCount);
   }
   dev_free(h->mat); dev_free(h->matTmp); dev_free(h->home); dev_free(h->homeTmp);
   dev_free(h->ppIndex); dev_free(h->ppSlot); dev_free(h->ppList); dev_free(h->ppForce); dev_free(h->ppBox);
@@ -662,6 +663,7 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
     rc |= dev_alloc(h, &m.mono, 1); rc |= dev_alloc(h, &m.partial, 64); rc |= dev_alloc(h, &m.counter, 1);
     rc |= dev_alloc(h, &m.occ, (size_t)kCoarse * 64); rc |= dev_alloc(h, &m.occIdx, (size_t)kCoarse * 64);
     rc |= dev_alloc(h, &m.occN, kCoarse);
+    rc |= dev_alloc(h, &m.occBlocks, kCoarse); rc |= dev_alloc(h, &m.occCount, 1);
   }
   rc |= dev_alloc(h, &h->ppIndex, CCS_PP_CAP); rc |= dev_alloc(h, &h->ppSlot, N);
   rc |= dev_alloc(h, &h->ppList, CCS_PP_CAP); rc |= dev_alloc(h, &h->ppForce, 4 * CCS_PP_CAP);
@@ -706,6 +708,8 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
     CUDA_TRY(h, cudaMemsetAsync(m.mono, 0, sizeof(float4), st));
     CUDA_TRY(h, cudaMemsetAsync(m.counter, 0, sizeof(unsigned), st));
     CUDA_TRY(h, cudaMemsetAsync(m.occN, 0, sizeof(int) * kCoarse, st));
+    CUDA_TRY(h, cudaMemsetAsync(m.occCount, 0, sizeof(int), st));
+    CUDA_TRY(h, cudaMemsetAsync(m.force, 0, sizeof(float4) * (kFine + 1), st));
   }
   h->launches += launch_fill_u32((uint32_t *)h->ppIndex, CCS_PP_CAP, 0xFFFFFFFFu, st);
   h->launches += launch_fill_u32((uint32_t *)h->ppSlot, N, 0xFFFFFFFFu, st);
@@ -894,9 +898,11 @@ struct ccs_ensemble {
   cudaStream_t st = nullptr;
   cudaEvent_t fork = nullptr, after = nullptr;
   std::vector<cudaEvent_t> join, ready;
-  std::map<std::vector<GraphKey>, EnsembleGraph> graphs;
+  std::map<std::pair<int, std::vector<GraphKey>>, EnsembleGraph> graphs;   // (rounds, members' keys)
   std::string err;
 };
+
+constexpr int kEnsRounds = 4;   // rounds of meshEvery steps one ensemble graph holds
 
 namespace {
 void free_ensemble_graphs(ccs_ensemble *e) {
@@ -919,9 +925,9 @@ void free_ensemble_graphs(ccs_ensemble *e) {
     }                                                                                            \
   } while (0)
 
-// one round: every member's next meshEvery steps, one graph launch
-int ensemble_block(ccs_ensemble *e) {
-  const int n = (int)e->m.size(), M = e->M;
+// R rounds: every member's next R x meshEvery steps, one graph launch
+int ensemble_block(ccs_ensemble *e, int R) {
+  const int n = (int)e->m.size(), M = e->M * R;
   std::vector<GraphKey> keys(n);
   std::vector<std::vector<StepPlan>> plans(n, std::vector<StepPlan>(M));
   std::vector<int> seat0(n), cur0(n);
@@ -931,11 +937,11 @@ int ensemble_block(ccs_ensemble *e) {
       plans[i][k] = plan_step(h, 0, 0);
       h->sim.t += h->sim.dt;   // the frame loop's clock, index.html:372
     }
-    keys[i] = GraphKey{(int)(plans[i][0].u.boxB > 0.5f), h->ppCount > 0, h->seatCur, h->cur, M, h->ping};
+    keys[i] = GraphKey{(int)(plans[i][0].u.boxB > 0.5f), h->ppCount > 0, h->seatCur, h->cur, e->M, h->ping};
     seat0[i] = h->seatCur;
     cur0[i] = h->cur;
   }
-  EnsembleGraph &g = e->graphs[keys];
+  EnsembleGraph &g = e->graphs[std::make_pair(R, keys)];
   if (!g.exec) {
     g.dev.assign(n, nullptr);
     g.host.assign(n, nullptr);
@@ -1056,9 +1062,11 @@ int ccs_ensemble_steps(ccs_ensemble *e, int n) {
       return CCS_E_STATE;
     }
   cudaSetDevice(e->device);
-  for (int b = 0; b < n / e->M; ++b) {
-    int rc = ensemble_block(e);
+  for (int blocks = n / e->M; blocks > 0;) {
+    const int R = blocks < kEnsRounds ? blocks : kEnsRounds;
+    int rc = ensemble_block(e, R);
     if (rc) return rc;
+    blocks -= R;
   }
   return CCS_OK;
 }

@@ -29,6 +29,8 @@ struct MeshBuf {
   float4 *occ = nullptr;       // per coarse block: its occupied fine cells (centre of mass, mass), 64 slots
   uint8_t *occIdx = nullptr;   // ... and their place in the block
   int *occN = nullptr;         // ... and how many there are
+  int *occBlocks = nullptr;    // the occupied coarse blocks (any order) ...
+  int *occCount = nullptr;     // ... and how many
 };
 
 // Arguments of the contact step (simFS, src/glsl-sim.js:354-512).

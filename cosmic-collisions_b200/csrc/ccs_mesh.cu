@@ -129,7 +129,8 @@ int launch_deposit(const ccs_uniforms *u, int N, int box, const float4 *pos, con
 __global__ void __launch_bounds__(kBlock) k_coarse(const float4 *__restrict__ fine, float4 *__restrict__ coarse,
                                                    float4 *partial, unsigned *counter, float4 *mono,
                                                    float4 *__restrict__ occ, uint8_t *__restrict__ occIdx,
-                                                   int *__restrict__ occN) {
+                                                   int *__restrict__ occN, int *__restrict__ occBlocks,
+                                                   int *__restrict__ occCount) {
   __shared__ float4 red[kBlock];
   __shared__ bool last;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -152,6 +153,7 @@ __global__ void __launch_bounds__(kBlock) k_coarse(const float4 *__restrict__ fi
         }
       }
   occN[b] = n;
+  if (n) occBlocks[atomicAdd(occCount, 1)] = b;   // the cell pass visits these only
   coarse[b] = s;
   red[threadIdx.x] = s;
   __syncthreads();
@@ -184,7 +186,7 @@ __global__ void __launch_bounds__(kBlock) k_coarse(const float4 *__restrict__ fi
 
 int launch_coarse(const MeshBuf &m, cudaStream_t st) {
   k_coarse<<<kCoarse / kBlock, kBlock, 0, st>>>(m.fine, m.coarse, m.partial, m.counter, m.mono, m.occ, m.occIdx,
-                                               m.occN);
+                                               m.occN, m.occBlocks, m.occCount);
   return 1;
 }
 
@@ -239,126 +241,140 @@ int launch_far(const MeshBuf &m, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// cell gravity: src/glsl-sim.js:303-352.  One CTA per coarse block; its 64
-// fine cells each get SPLIT threads (a cell can hold mass only if its
-// block does).  The CTA reads how many occupied cells each of the 5^3 blocks
-// around it holds, then copies the occupied cells of all of them -- centre of
-// mass and mass, as the coarse pass listed them, block by block in the
-// reference's order -- into shared memory in one pass of independent loads
-// (in batches of kCellBatch when the neighbourhood holds more).  A block in
-// the bodies sees thousands of sources, so each occupied cell's sum is split
-// over its SPLIT threads (every SPLIT-th source; 2, 4 or 8, the autotuner's
-// choice), and the partial sums are added in a fixed order: the result is
-// deterministic for a given SPLIT.  A cell skips
-// itself.  Then the block's far field is carried to the cell by the tidal
-// tensor.  Cell-on-cell pulls are fast arithmetic (rsqrt, FMA).
+// cell gravity: src/glsl-sim.js:303-352.  A persistent grid walks the
+// occupied coarse blocks the coarse pass listed (the force mesh is cleared
+// before, so empty blocks and empty cells read zero); a CTA takes one block
+// at a time and gives each of its 64 fine cells SPLIT threads.  It reads how
+// many occupied cells each of the 5^3 blocks around it holds, then copies the
+// occupied cells of all of them -- centre of mass and mass, as the coarse pass
+// listed them, block by block in the reference's order -- into shared memory
+// in one pass of independent loads (in batches of kCellBatch when the
+// neighbourhood holds more).  A block in the bodies sees thousands of
+// sources, so each occupied cell's sum is split over its SPLIT threads (every
+// SPLIT-th source; 2, 4 or 8, the autotuner's choice), and the partial sums
+// are added in a fixed order: the result is deterministic for a given SPLIT.
+// A cell skips itself.  Then the block's far field is carried to the cell by
+// the tidal tensor.  Cell-on-cell pulls are fast arithmetic (rsqrt, FMA).
 // ---------------------------------------------------------------------------
 constexpr int kCellBatch = 1024;
 
 template <int SPLIT>
 __global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restrict__ U,
-                                                       const float4 *__restrict__ fine,
-                                                       const float4 *__restrict__ coarse,
-                                                       const float4 *__restrict__ occ,
-                                                       const uint8_t *__restrict__ occIdx,
-                                                       const int *__restrict__ occN, const float4 *__restrict__ farA,
-                                                       const float4 *__restrict__ farT0,
-                                                       const float4 *__restrict__ farT1, float4 *__restrict__ force) {
+                                                     const float4 *__restrict__ fine,
+                                                     const float4 *__restrict__ coarse,
+                                                     const float4 *__restrict__ occ,
+                                                     const uint8_t *__restrict__ occIdx,
+                                                     const int *__restrict__ occN,
+                                                     const int *__restrict__ occBlocks,
+                                                     const int *__restrict__ occCount,
+                                                     const float4 *__restrict__ farA,
+                                                     const float4 *__restrict__ farT0,
+                                                     const float4 *__restrict__ farT1, float4 *__restrict__ force) {
+  constexpr int kCellThreads = 64 * SPLIT;
   __shared__ int nbK[125], nbOff[126];
   __shared__ float4 src[kCellBatch];
   __shared__ uint8_t sidx[kCellBatch];   // a source's place in its block; 255 for another block's cells
-  constexpr int kCellThreads = 64 * SPLIT;
   __shared__ float4 part[SPLIT][64];
-  const int blk = blockIdx.x, t = threadIdx.x, cellT = t & 63, q = t >> 6;
-  const int ccx = blk & 15, ccy = (blk >> 4) & 15, ccz = blk >> 8;
-  const int c = fine_index(ccx * 4 + (cellT & 3), ccy * 4 + ((cellT >> 2) & 3), ccz * 4 + (cellT >> 4));
-  if (blk == 0 && t == 0) force[kFine] = fine[kFine];   // the scratch texel, carried through
-  const float4 mb = coarse[blk];
-  if (!(mb.w > 0.0f)) {   // an empty block: the same for the whole CTA
-    if (q == 0) force[c] = make_float4(0, 0, 0, 0);
-    return;
-  }
-  for (int o = t; o < 125; o += kCellThreads) {   // o = kx + 5 ky + 25 kz: the reference's loop order
-    const int kx = ccx + o % 5 - 2, ky = ccy + (o / 5) % 5 - 2, kz = ccz + o / 25 - 2;
-    const bool in = kx >= 0 && ky >= 0 && kz >= 0 && kx <= 15 && ky <= 15 && kz <= 15;
-    const int k = in ? coarse_index(kx, ky, kz) : 0;
-    nbK[o] = k;
-    nbOff[o + 1] = in ? __ldg(occN + k) : 0;
-  }
-  if (q == 0 && !(fine[c].w > 0.0f)) force[c] = make_float4(0, 0, 0, 0);   // an empty place of this block
-  // the cellT-th occupied cell of the block, so the busy lanes sit together
-  const int nOwn = __ldg(occN + blk);
-  const bool mine = cellT < nOwn;
-  const float4 tc = mine ? __ldg(occ + (size_t)blk * 64 + cellT) : make_float4(0, 0, 0, 0);
-  const int tl = mine ? (int)__ldg(occIdx + (size_t)blk * 64 + cellT) : -1;
-  const f3 x = xyz(tc);
+  const int t = threadIdx.x, cellT = t & 63, q = t >> 6;
+  if (blockIdx.x == 0 && t == 0) force[kFine] = fine[kFine];   // the scratch texel, carried through
   const float eps2 = U->eps2Cell, Gm = U->Gm;
-  f3 acc = mk(0, 0, 0);
-  float pot = 0.0f;
-  __syncthreads();
-  if (t == 0) {   // where each neighbour block's cells start in the neighbourhood's list
-    nbOff[0] = 0;
-    for (int o = 0; o < 125; ++o) nbOff[o + 1] += nbOff[o];
-  }
-  __syncthreads();
-  const int total = nbOff[125];
-  for (int b0 = 0; b0 < total; b0 += kCellBatch) {
-    const int b1 = min(b0 + kCellBatch, total);
-    // the neighbour blocks' cells in [b0, b1): every load independent of the others
-    for (int o = 0; o < 125; ++o) {
-      const int lo = max(nbOff[o], b0), hi = min(nbOff[o + 1], b1);
-      if (lo >= hi) continue;
-      const int k = nbK[o];
-      for (int e = lo + t; e < hi; e += kCellThreads) {
-        const int i = e - nbOff[o];
-        src[e - b0] = __ldg(occ + (size_t)k * 64 + i);
-        sidx[e - b0] = k == blk ? __ldg(occIdx + (size_t)k * 64 + i) : (uint8_t)255;
-      }
+  const int nBlocks = *occCount;
+  for (int bi = blockIdx.x; bi < nBlocks; bi += gridDim.x) {
+    const int blk = occBlocks[bi];
+    const int ccx = blk & 15, ccy = (blk >> 4) & 15, ccz = blk >> 8;
+    const float4 mb = coarse[blk];
+    for (int o = t; o < 125; o += kCellThreads) {   // o = kx + 5 ky + 25 kz: the reference's loop order
+      const int kx = ccx + o % 5 - 2, ky = ccy + (o / 5) % 5 - 2, kz = ccz + o / 25 - 2;
+      const bool in = kx >= 0 && ky >= 0 && kz >= 0 && kx <= 15 && ky <= 15 && kz <= 15;
+      const int k = in ? coarse_index(kx, ky, kz) : 0;
+      nbK[o] = k;
+      nbOff[o + 1] = in ? __ldg(occN + k) : 0;
+    }
+    // the cellT-th occupied cell of the block, so the busy lanes sit together
+    const int nOwn = __ldg(occN + blk);
+    const bool mine = cellT < nOwn;
+    const float4 tc = mine ? __ldg(occ + (size_t)blk * 64 + cellT) : make_float4(0, 0, 0, 0);
+    const int tl = mine ? (int)__ldg(occIdx + (size_t)blk * 64 + cellT) : -1;
+    const f3 x = xyz(tc);
+    f3 acc = mk(0, 0, 0);
+    float pot = 0.0f;
+    __syncthreads();
+    if (t == 0) {   // where each neighbour block's cells start in the neighbourhood's list
+      nbOff[0] = 0;
+      for (int o = 0; o < 125; ++o) nbOff[o + 1] += nbOff[o];
     }
     __syncthreads();
-    if (mine) {
-      const int n = b1 - b0;
+    const int total = nbOff[125];
+    for (int b0 = 0; b0 < total; b0 += kCellBatch) {
+      const int b1 = min(b0 + kCellBatch, total);
+      // the neighbour blocks' cells in [b0, b1): every load independent of the others
+      for (int o = 0; o < 125; ++o) {
+        const int lo = max(nbOff[o], b0), hi = min(nbOff[o + 1], b1);
+        if (lo >= hi) continue;
+        const int k = nbK[o];
+        for (int e = lo + t; e < hi; e += kCellThreads) {
+          const int i = e - nbOff[o];
+          src[e - b0] = __ldg(occ + (size_t)k * 64 + i);
+          sidx[e - b0] = k == blk ? __ldg(occIdx + (size_t)k * 64 + i) : (uint8_t)255;
+        }
+      }
+      __syncthreads();
+      if (mine) {
+        const int n = b1 - b0;
 #pragma unroll 4
-      for (int i = q; i < n; i += SPLIT) {
-        if ((int)sidx[i] == tl) continue;   // a cell does not pull itself
-        const float4 mf = src[i];
-        const f3 r = xyz(mf) - x;
-        const float inv = rsqrtf(dot(r, r) + eps2);
-        acc = acc + r * (mf.w * inv * inv * inv);
-        pot -= mf.w * inv;
+        for (int i = q; i < n; i += SPLIT) {
+          if ((int)sidx[i] == tl) continue;   // a cell does not pull itself
+          const float4 mf = src[i];
+          const f3 r = xyz(mf) - x;
+          const float inv = rsqrtf(dot(r, r) + eps2);
+          acc = acc + r * (mf.w * inv * inv * inv);
+          pot -= mf.w * inv;
+        }
       }
+      __syncthreads();
     }
+    part[q][cellT] = make_float4(acc.x, acc.y, acc.z, pot);
     __syncthreads();
-  }
-  part[q][cellT] = make_float4(acc.x, acc.y, acc.z, pot);
-  __syncthreads();
-  if (!mine || q != 0) return;
+    if (mine && q == 0) {
 #pragma unroll
-  for (int k = 1; k < SPLIT; ++k) {
-    const float4 p = part[k][cellT];
-    acc = acc + mk(p.x, p.y, p.z);
-    pot += p.w;
+      for (int k = 1; k < SPLIT; ++k) {
+        const float4 p = part[k][cellT];
+        acc = acc + mk(p.x, p.y, p.z);
+        pot += p.w;
+      }
+      const float4 fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
+      const f3 d = x - xyz(mb) * fdiv(1.0f, mb.w);
+      const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
+                       t1.x * d.x + t1.y * d.y + t0.z * d.z);
+      acc = acc + (xyz(fa) + Td);
+      pot += fa.w - dot(xyz(fa), d) - 0.5f * dot(d, Td);
+      force[fine_index(ccx * 4 + (tl & 3), ccy * 4 + ((tl >> 2) & 3), ccz * 4 + (tl >> 4))] =
+          make_float4(acc.x * Gm, acc.y * Gm, acc.z * Gm, pot * Gm);
+    }
+    __syncthreads();   // the shared arrays are the next block's
   }
-  const float4 fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
-  const f3 d = x - xyz(mb) * fdiv(1.0f, mb.w);
-  const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
-                   t1.x * d.x + t1.y * d.y + t0.z * d.z);
-  acc = acc + (xyz(fa) + Td);
-  pot += fa.w - dot(xyz(fa), d) - 0.5f * dot(d, Td);
-  force[fine_index(ccx * 4 + (tl & 3), ccy * 4 + ((tl >> 2) & 3), ccz * 4 + (tl >> 4))] =
-      make_float4(acc.x * Gm, acc.y * Gm, acc.z * Gm, pot * Gm);
 }
 
 int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int split) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  // a persistent grid: four CTAs of 512 threads fill an SM, proportionally more of smaller ones
+  const int grid = sms * (split == 2 ? 16 : split == 4 ? 8 : 4);
+  cudaMemsetAsync(m.force, 0, sizeof(float4) * kFine, st);
   if (split == 2)
-    k_cell<2><<<kCoarse, 128, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.farA, m.farT0, m.farT1,
-                                       m.force);
+    k_cell<2><<<grid, 128, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount, m.farA,
+                                    m.farT0, m.farT1, m.force);
   else if (split == 8)
-    k_cell<8><<<kCoarse, 512, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.farA, m.farT0, m.farT1,
-                                       m.force);
+    k_cell<8><<<grid, 512, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount, m.farA,
+                                    m.farT0, m.farT1, m.force);
   else
-    k_cell<4><<<kCoarse, 256, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.farA, m.farT0, m.farT1,
-                                       m.force);
+    k_cell<4><<<grid, 256, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount, m.farA,
+                                    m.farT0, m.farT1, m.force);
   return 1;
 }
 

@@ -258,8 +258,8 @@ int ccs_autotune(ccs_handle *h, int reps, int choice[2]);
 /* ---- the batched ensemble ----
  * No counterpart in the reference, which runs one impact per page.  An
  * ensemble advances several engines (impacts of any sizes, on one device)
- * together: each round of meshEvery steps is one CUDA graph holding every
- * member's block as a parallel branch, replayed with one launch.  The members
+ * together: up to four rounds of meshEvery steps are one CUDA graph holding
+ * every member's steps as a parallel branch, replayed with one launch.  The members
  * stay ordinary engines (their own streams, buffers and read-outs); work a
  * caller queues on a member is ordered before and after the ensemble's
  * rounds.  Members must outlive the ensemble, share one meshEvery, and sit at

@@ -99,23 +99,22 @@ def test_small_impact_run_keeps_its_books(ccmod):
     assert abs(np.sqrt(books["Lx"] ** 2 + books["Ly"] ** 2 + books["Lz"] ** 2) - g.L) < 1e-6 * g.L
 
 
-def test_hit_and_run_raises_the_second_box(ccmod):
-    """The full impact's case B (0.15 M_earth at 30 degrees and 1.4 v_esc): the impactor survives a hit
-    & run, and the second mesh box is seen going up on it (placeBoxes, src/nbody.js:357-373: a second
-    body above 0.05 M_earth whose core is beyond FL - 1.3 R of the largest's), at 65,536 particles."""
-    from cosmic_collisions_b200 import configs
+def _watch_second_box(ccmod, opt, t_max):
+    """Run an impact with runTo's cadence in half-unit pieces until the second box goes up; the analyses seen."""
     nb = ccmod.NBody(0)
-    seen = None
+    seen, log = None, []
     try:
-        nb.build(configs.full_impact_opt(65536, case="B"))
+        nb.build(opt)
         t = 0.0
-        while t < 24.0 and seen is None:
+        while t < t_max and seen is None:
             t += 0.5
             nb.run_to(t)
+            r = nb.report
+            log.append((round(nb.sim.t, 2), round(r.largest, 3), r.hasSecond, round(r.secMass, 3),
+                        round(r.secDist, 2)))
             if nb.sim.boxOn[1]:
-                r = nb.report
                 seen = {"t": nb.sim.t, "steps": nb.sim.stepNo, "second": r.secMass, "largest": r.largest,
-                        "cen": [nb.sim.boxCen[1][k] for k in range(3)], "drift": r.drift}
+                        "drift": r.drift}
         if seen is not None:
             nb.steps(64)                                # the step with both boxes up
             nb.sync()
@@ -123,6 +122,20 @@ def test_hit_and_run_raises_the_second_box(ccmod):
             assert np.isfinite(st["pos"]).all() and np.isfinite(st["vel"]).all()
     finally:
         nb.close()
-    print("second box up:", seen)
+    return seen, log
+
+
+def test_case_b_outcome_and_the_second_box(ccmod):
+    """The full impact's case B (0.15 M_earth at 30 degrees and 1.4 v_esc) is run at 65,536 particles and its
+    outcome recorded; a grazing variant (60 degrees) is a hit & run whose survivor must raise the second mesh
+    box (placeBoxes, src/nbody.js:357-373: a second body above 0.05 M_earth whose core is beyond FL - 1.3 R of
+    the largest's), and the step then runs with both boxes."""
+    from cosmic_collisions_b200 import configs
+    seen_b, log_b = _watch_second_box(ccmod, configs.full_impact_opt(65536, case="B"), 16.0)
+    print("case B: second box", seen_b, "| (t, largest, hasSecond, secMass, secDist):", log_b[::4])
+    opt = configs.full_impact_opt(65536, case="B")
+    opt["angle"] = 60.0
+    seen, log = _watch_second_box(ccmod, opt, 24.0)
+    print("grazing variant: second box", seen, "|", log[::4])
     assert seen is not None, "the second box never went up"
     assert seen["second"] > 0.05 and seen["drift"] < 1e-3
