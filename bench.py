@@ -328,6 +328,8 @@ def run_ensemble(args, log):
     # launch shapes by measurement: the first instance of each size measures, the rest take its choice
     tuned = {}
     for nb in runs:
+        if args.no_tune:
+            break
         N = nb.sim.N
         ch = nb.autotune(reps=0 if N in tuned else 8)
         tuned.setdefault(N, ch)
@@ -577,6 +579,7 @@ def main():
                     help="run the batched ensemble of this many impacts instead and print its line")
     ap.add_argument("--ens-steps", type=int, default=2000)
     ap.add_argument("--no-nn", action="store_true", help="skip the learned-correction leg")
+    ap.add_argument("--no-tune", action="store_true", help="ensemble: keep the default launch shapes")
     ap.add_argument("--nn-pairs", type=int, default=9_000_000, help="training pairs (three snapshots)")
     ap.add_argument("--nn-epochs", type=int, default=8)
     ap.add_argument("--profile", action="store_true",

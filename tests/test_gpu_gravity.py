@@ -26,6 +26,7 @@ def force_error(cc, orc, N, sample=1024, seed=3):
         nb.pass_diag()          # boxes(), contact cells, mesh, and the read-outs the analysis uses
         D = nb.buffer("diag")
         s = nb.sim
+        m, a = float(s.m), float(s.a)   # copies: the view dies with the engine
         rep, lst, _ = cc.fof(s.N, s.m, s.a, pos, vel, mat, D, s.k, 2 * s.a)
         nb.set_pp(lst, rep.ppLoose)
         nb.pass_sim(False, False, 0.0)   # aux.xyz: the gravity each particle feels
@@ -33,7 +34,7 @@ def force_error(cc, orc, N, sample=1024, seed=3):
     finally:
         nb.close()
     idx = np.sort(np.random.default_rng(seed).choice(N, sample, replace=False)).astype(np.int32)
-    ref, _ = orc.direct_sum(pos, s.m * mat.astype(np.float64), s.a, idx)
+    ref, _ = orc.direct_sum(pos, m * mat.astype(np.float64), a, idx)
     rel = np.linalg.norm(g[idx] - ref, axis=1) / np.linalg.norm(ref, axis=1)
     loose = np.zeros(N, bool)
     loose[lst] = True
