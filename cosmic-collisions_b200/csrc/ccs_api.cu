@@ -1071,6 +1071,73 @@ int ccs_ensemble_steps(ccs_ensemble *e, int n) {
   return CCS_OK;
 }
 
+int ccs_ensemble_autotune(ccs_ensemble *e, int rounds, int choice[2]) {
+  if (!e || rounds <= 0) return CCS_E_ARG;
+  for (ccs_handle *h : e->m)
+    if (h->sim.stepNo % e->M || h->timing) {
+      e->err = "every member must sit at a block boundary (stepNo % meshEvery == 0) with timing off";
+      return CCS_E_STATE;
+    }
+  cudaSetDevice(e->device);
+  const int R = rounds < kEnsRounds ? rounds : kEnsRounds;
+  int bestW = 8, bestS = 4;
+  double best = 1e300;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ENS_TRY(e, cudaEventCreate(&a));
+  ENS_TRY(e, cudaEventCreate(&b));
+  int rc = CCS_OK;
+  for (int w : {8, 4}) {
+    for (int sp : {2, 4, 8}) {
+      for (ccs_handle *h : e->m) {
+        if (h->tuneWarps != w || h->tuneSplit != sp) {
+          cudaStreamSynchronize(h->st);
+          free_graphs(h);
+          h->tuneWarps = w;
+          h->tuneSplit = sp;
+        }
+      }
+      ENS_TRY(e, cudaStreamSynchronize(e->st));
+      free_ensemble_graphs(e);
+      rc = ensemble_block(e, R);   // captures this shape's graph
+      if (rc) break;
+      ENS_TRY(e, cudaEventRecord(a, e->st));
+      for (int r = 0; r < rounds; r += R) {
+        rc = ensemble_block(e, R);
+        if (rc) break;
+      }
+      if (rc) break;
+      ENS_TRY(e, cudaEventRecord(b, e->st));
+      ENS_TRY(e, cudaEventSynchronize(b));
+      float ms = 0.0f;
+      ENS_TRY(e, cudaEventElapsedTime(&ms, a, b));
+      if (ms < best) {
+        best = ms;
+        bestW = w;
+        bestS = sp;
+      }
+    }
+    if (rc) break;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc) return rc;
+  for (ccs_handle *h : e->m) {
+    if (h->tuneWarps != bestW || h->tuneSplit != bestS) {
+      cudaStreamSynchronize(h->st);
+      free_graphs(h);
+      h->tuneWarps = bestW;
+      h->tuneSplit = bestS;
+    }
+  }
+  ENS_TRY(e, cudaStreamSynchronize(e->st));
+  free_ensemble_graphs(e);
+  if (choice) {
+    choice[0] = bestW;
+    choice[1] = bestS;
+  }
+  return CCS_OK;
+}
+
 int ccs_ensemble_sync(ccs_ensemble *e) {
   if (!e) return CCS_E_ARG;
   cudaSetDevice(e->device);

@@ -435,6 +435,13 @@ class Ensemble:
     def sync(self):
         self._check(lib().ccs_ensemble_sync(self._h), "ccs_ensemble_sync")
 
+    def autotune(self, rounds=4):
+        """ccs_ensemble_autotune: every launch-shape combination on all members, timed over real rounds (the
+        members advance); the fastest aggregate is kept.  Returns the choice."""
+        ch = (C.c_int * 2)()
+        self._check(lib().ccs_ensemble_autotune(self._h, int(rounds), ch), "ccs_ensemble_autotune")
+        return {"warps": ch[0], "cell_split": ch[1]}
+
     def close(self):
         if self._h:
             lib().ccs_ensemble_destroy(self._h)

@@ -271,6 +271,15 @@ int ccs_ensemble_destroy(ccs_ensemble *e);
 const char *ccs_ensemble_last_error(const ccs_ensemble *e);
 int ccs_ensemble_steps(ccs_ensemble *e, int n);
 int ccs_ensemble_sync(ccs_ensemble *e);   /* waits for the rounds; reports any member's kernel status */
+/* The ensemble's launch shapes by measurement: every combination of the
+ * contact step's CTA width (8, 4 warps) and the cell gravity's threads per
+ * cell (2, 4, 8) is applied to all members and timed over `rounds` real
+ * rounds of the ensemble after one round that captures its graph (the
+ * members advance: 6 x (rounds + 1) x meshEvery steps when rounds <= 4); the
+ * fastest aggregate is kept.  Shapes that win for one run alone
+ * can lose when many runs share the GPU, which is why the ensemble measures
+ * its own.  choice (may be NULL) gets {warps, threads per cell}. */
+int ccs_ensemble_autotune(ccs_ensemble *e, int rounds, int choice[2]);
 
 /* Internal buffers, for tests and the console checks of index.html:531-556:
  * which = CCS_BUF_* below; bytes must equal the buffer's size. */

@@ -92,3 +92,23 @@ def test_ensemble_round_steps_members_as_alone(ccmod):
     finally:
         for nb in members + lone + [lone2]:
             nb.close()
+
+
+def test_ensemble_autotune_picks_a_shape_and_steps(ccmod):
+    members = [settled(ccmod, N) for N in (16384, 32768)]
+    try:
+        ens = ccmod.Ensemble(members)
+        before = [nb.sim.stepNo for nb in members]
+        choice = ens.autotune(rounds=1)
+        ens.sync()
+        assert choice["warps"] in (4, 8) and choice["cell_split"] in (2, 4, 8)
+        # one capture round and one timed round for each of the six shapes
+        assert [nb.sim.stepNo - b for nb, b in zip(members, before)] == [6 * 2 * 8] * 2
+        ens.steps(8)
+        ens.sync()
+        for nb in members:
+            assert np.isfinite(nb.read_state()["pos"]).all()
+        ens.close()
+    finally:
+        for nb in members:
+            nb.close()
