@@ -31,6 +31,8 @@ struct MeshBuf {
   int *occN = nullptr;         // ... and how many there are
   int *occBlocks = nullptr;    // the occupied coarse blocks (any order) ...
   int *occCount = nullptr;     // ... and how many
+  int *occAsc = nullptr;       // the occupied coarse blocks in ascending order ...
+  int *occAscN = nullptr;      // ... and how many
 };
 
 // Arguments of the contact step (simFS, src/glsl-sim.js:354-512).

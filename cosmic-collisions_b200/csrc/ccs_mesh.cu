@@ -191,53 +191,107 @@ int launch_coarse(const MeshBuf &m, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// far field: src/glsl-sim.js:263-295.  One warp per coarse block; its lanes
-// split the 4096 source blocks (lane, lane + 32, ...) and the warp reduces the
-// ten sums.  Occupancy (mass > 0) and the "more than two away" test are exact.
+// far field: src/glsl-sim.js:263-295.  The occupied blocks are listed once in
+// ascending order (k_occ_list); a persistent grid of warps takes the occupied
+// target blocks, and a warp's lanes split that list of sources (i, i + 32,
+// ...) and reduce the ten sums.  Empty blocks' outputs are cleared before.
+// Occupancy (mass > 0) and the "more than two away" test are exact.
 // ---------------------------------------------------------------------------
 constexpr int kFarWarps = 8;
 
-__global__ void __launch_bounds__(32 * kFarWarps) k_far(const float4 *__restrict__ coarse, float4 *__restrict__ farA,
+__global__ void __launch_bounds__(1024) k_occ_list(const float4 *__restrict__ coarse, int *__restrict__ list,
+                                                   int *__restrict__ count) {
+  __shared__ int warpSum[32];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  bool occ[4];
+  int n = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    occ[k] = __ldg(coarse + 4 * t + k).w > 0.0f;
+    n += occ[k];
+  }
+  int x = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warpSum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int v = warpSum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+      if (lane >= o) v += y;
+    }
+    warpSum[lane] = v;
+  }
+  __syncthreads();
+  int at = x - n + (w > 0 ? warpSum[w - 1] : 0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (occ[k]) list[at++] = 4 * t + k;
+  if (t == 1023) *count = at;
+}
+
+__global__ void __launch_bounds__(32 * kFarWarps) k_far(const float4 *__restrict__ coarse,
+                                                       const int *__restrict__ targets,
+                                                       const int *__restrict__ nTargets,
+                                                       const int *__restrict__ sources,
+                                                       const int *__restrict__ nSources, float4 *__restrict__ farA,
                                                        float4 *__restrict__ farT0, float4 *__restrict__ farT1) {
   const int lane = threadIdx.x & 31;
-  const int b = blockIdx.x * kFarWarps + (threadIdx.x >> 5);
-  const float4 mc = __ldg(coarse + b);
-  if (!(mc.w > 0.0f)) {
-    if (lane == 0) farA[b] = farT0[b] = farT1[b] = make_float4(0, 0, 0, 0);
-    return;
-  }
-  const int cx = b & 15, cy = (b >> 4) & 15, cz = b >> 8;
-  const f3 x = xyz(mc) * fdiv(1.0f, mc.w);
-  float s[10];
+  const int warp = blockIdx.x * kFarWarps + (threadIdx.x >> 5), warps = gridDim.x * kFarWarps;
+  const int nt = *nTargets, ns = *nSources;
+  for (int ti = warp; ti < nt; ti += warps) {
+    const int b = targets[ti];
+    const float4 mc = __ldg(coarse + b);
+    const int cx = b & 15, cy = (b >> 4) & 15, cz = b >> 8;
+    const f3 x = xyz(mc) * fdiv(1.0f, mc.w);
+    float s[10];
 #pragma unroll
-  for (int k = 0; k < 10; ++k) s[k] = 0.0f;
-  for (int k = lane; k < kCoarse; k += 32) {
-    const int kx = k & 15, ky = (k >> 4) & 15, kz = k >> 8;
-    if (max(abs(kx - cx), max(abs(ky - cy), abs(kz - cz))) <= 2) continue;
-    const float4 m = __ldg(coarse + k);
-    if (!(m.w > 0.0f)) continue;
-    const f3 r = xyz(m) * fdiv(1.0f, m.w) - x;
-    const float inv = rsqrtf(dot(r, r)), inv2 = inv * inv, inv3 = inv * inv2, inv5 = inv3 * inv2;
-    const float a3 = m.w * inv3, a5 = 3.0f * m.w * inv5;
-    s[0] += r.x * a3; s[1] += r.y * a3; s[2] += r.z * a3;
-    s[3] -= m.w * inv;
-    s[4] += a5 * r.x * r.x - a3; s[5] += a5 * r.y * r.y - a3; s[6] += a5 * r.z * r.z - a3;
-    s[7] += a5 * r.x * r.y; s[8] += a5 * r.x * r.z; s[9] += a5 * r.y * r.z;
-  }
+    for (int k = 0; k < 10; ++k) s[k] = 0.0f;
+    for (int i = lane; i < ns; i += 32) {
+      const int k = __ldg(sources + i);
+      const int kx = k & 15, ky = (k >> 4) & 15, kz = k >> 8;
+      if (max(abs(kx - cx), max(abs(ky - cy), abs(kz - cz))) <= 2) continue;
+      const float4 m = __ldg(coarse + k);
+      const f3 r = xyz(m) * fdiv(1.0f, m.w) - x;
+      const float inv = rsqrtf(dot(r, r)), inv2 = inv * inv, inv3 = inv * inv2, inv5 = inv3 * inv2;
+      const float a3 = m.w * inv3, a5 = 3.0f * m.w * inv5;
+      s[0] += r.x * a3; s[1] += r.y * a3; s[2] += r.z * a3;
+      s[3] -= m.w * inv;
+      s[4] += a5 * r.x * r.x - a3; s[5] += a5 * r.y * r.y - a3; s[6] += a5 * r.z * r.z - a3;
+      s[7] += a5 * r.x * r.y; s[8] += a5 * r.x * r.z; s[9] += a5 * r.y * r.z;
+    }
 #pragma unroll
-  for (int k = 0; k < 10; ++k)
+    for (int k = 0; k < 10; ++k)
 #pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) s[k] += __shfl_xor_sync(0xFFFFFFFFu, s[k], o);
-  if (lane == 0) {
-    farA[b] = make_float4(s[0], s[1], s[2], s[3]);
-    farT0[b] = make_float4(s[4], s[5], s[6], s[7]);
-    farT1[b] = make_float4(s[8], s[9], 0.0f, 0.0f);
+      for (int o = 16; o >= 1; o >>= 1) s[k] += __shfl_xor_sync(0xFFFFFFFFu, s[k], o);
+    if (lane == 0) {
+      farA[b] = make_float4(s[0], s[1], s[2], s[3]);
+      farT0[b] = make_float4(s[4], s[5], s[6], s[7]);
+      farT1[b] = make_float4(s[8], s[9], 0.0f, 0.0f);
+    }
   }
 }
 
 int launch_far(const MeshBuf &m, cudaStream_t st) {
-  k_far<<<kCoarse / kFarWarps, 32 * kFarWarps, 0, st>>>(m.coarse, m.farA, m.farT0, m.farT1);
-  return 1;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  cudaMemsetAsync(m.farA, 0, sizeof(float4) * kCoarse, st);
+  cudaMemsetAsync(m.farT0, 0, sizeof(float4) * kCoarse, st);
+  cudaMemsetAsync(m.farT1, 0, sizeof(float4) * kCoarse, st);
+  k_occ_list<<<1, 1024, 0, st>>>(m.coarse, m.occAsc, m.occAscN);
+  k_far<<<2 * sms, 32 * kFarWarps, 0, st>>>(m.coarse, m.occBlocks, m.occCount, m.occAsc, m.occAscN, m.farA, m.farT0,
+                                             m.farT1);
+  return 2;
 }
 
 // ---------------------------------------------------------------------------
