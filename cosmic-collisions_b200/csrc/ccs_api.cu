@@ -661,7 +661,7 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
     rc |= dev_alloc(h, &m.fine, kFine + 1); rc |= dev_alloc(h, &m.force, kFine + 1);
     rc |= dev_alloc(h, &m.coarse, kCoarse); rc |= dev_alloc(h, &m.farA, kCoarse);
     rc |= dev_alloc(h, &m.farT0, kCoarse); rc |= dev_alloc(h, &m.farT1, kCoarse);
-    rc |= dev_alloc(h, &m.mono, 1); rc |= dev_alloc(h, &m.partial, 64); rc |= dev_alloc(h, &m.counter, 1);
+    rc |= dev_alloc(h, &m.mono, 1); rc |= dev_alloc(h, &m.partial, kCoarse); rc |= dev_alloc(h, &m.counter, 1);
     rc |= dev_alloc(h, &m.occ, (size_t)kCoarse * 64); rc |= dev_alloc(h, &m.occIdx, (size_t)kCoarse * 64);
     rc |= dev_alloc(h, &m.occN, kCoarse);
     rc |= dev_alloc(h, &m.occBlocks, kCoarse); rc |= dev_alloc(h, &m.occCount, 1);

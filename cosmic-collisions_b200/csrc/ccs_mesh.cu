@@ -19,8 +19,11 @@ inline int blocks_for(long n, int b = kBlock) { return (int)((n + b - 1) / b); }
 // share a base cell (the common case in Morton order) reduce-scatter their 32
 // values (8 corners x 4 components) with 31 shuffles, so the warp issues 32
 // scalar L2 atomics instead of 256 vector ones; mixed warps fall back to
-// per-lane float4 atomics.  The box a particle is in and its base cell are
-// exact; the summation order is unspecified, as the reference's blending is.
+// per-lane float4 atomics.  The warps of a CTA whose particles share a base
+// cell are added in shared memory first, so a CTA issues one set of 32 atomics
+// per base cell rather than per warp.  The box a particle is in and its base
+// cell are exact; the summation order is unspecified, as the reference's
+// blending is.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void reduce_scatter32(float (&v)[32], int lane) {
 #pragma unroll
@@ -38,9 +41,11 @@ __device__ __forceinline__ void reduce_scatter32(float (&v)[32], int lane) {
 __global__ void __launch_bounds__(kBlock) k_deposit(const ccs_uniforms *__restrict__ U, int box,
                                                     const float4 *__restrict__ pos, const float *__restrict__ mat,
                                                     const float4 *__restrict__ monoPrev, float4 *fine) {
+  __shared__ int sKey[kBlock / 32];
+  __shared__ float sVal[kBlock / 32][32];
   const ccs_uniforms &u = *U;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   bool in = false, stray = false;
   int bx = 0, by = 0, bz = 0;
   f3 t = mk(0, 0, 0), p = mk(0, 0, 0);
@@ -80,10 +85,9 @@ __global__ void __launch_bounds__(kBlock) k_deposit(const ccs_uniforms *__restri
     if (lane == 0) atomicAdd(fine + kFine, s);
   }
   const unsigned inMask = __ballot_sync(0xFFFFFFFFu, in);
-  if (inMask == 0u) return;
   const int key = in ? (bz << 16) | (by << 8) | bx : -1 - lane;
-  const int key0 = __shfl_sync(0xFFFFFFFFu, key, __ffs(inMask) - 1);
-  const bool uniform = __all_sync(0xFFFFFFFFu, !in || key == key0) && __popc(inMask) > 1;
+  const int key0 = inMask ? __shfl_sync(0xFFFFFFFFu, key, __ffs(inMask) - 1) : -1;
+  const bool uniform = inMask && __all_sync(0xFFFFFFFFu, !in || key == key0) && __popc(inMask) > 1;
   float v[32];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
@@ -95,18 +99,37 @@ __global__ void __launch_bounds__(kBlock) k_deposit(const ccs_uniforms *__restri
     v[4 * k + 2] = p.z * w;
     v[4 * k + 3] = w;
   }
-  if (uniform) {
+  if (uniform) {   // this lane ends with corner lane >> 2, component lane & 3 of the warp's sum
     reduce_scatter32(v, lane);
-    const int k = lane >> 2, comp = lane & 3;
-    const int cx = (key0 & 0xFF) + (k & 1), cy = ((key0 >> 8) & 0xFF) + ((k >> 1) & 1), cz = (key0 >> 16) + (k >> 2);
-    if (cx <= 63 && cy <= 63 && cz <= 63 && v[0] != 0.0f)
-      atomicAdd(reinterpret_cast<float *>(fine + fine_index(cx, cy, cz)) + comp, v[0]);
+    sVal[wid][lane] = v[0];
   } else if (in) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int cx = bx + (k & 1), cy = by + ((k >> 1) & 1), cz = bz + (k >> 2);
       if (cx > 63 || cy > 63 || cz > 63) continue;
       atomicAdd(fine + fine_index(cx, cy, cz), make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]));
+    }
+  }
+  if (lane == 0) sKey[wid] = uniform ? key0 : -1;
+  __syncthreads();
+  // warp 0 adds runs of warps that share a base cell (Morton order makes them common), then one set of atomics
+  // per run
+  if (wid == 0) {
+    const int k = lane >> 2, comp = lane & 3;
+    int run = -1;
+    float acc = 0.0f;
+    for (int w = 0; w <= kBlock / 32; ++w) {
+      const int kw = w < kBlock / 32 ? sKey[w] : -1;
+      if (kw != run) {
+        if (run >= 0) {
+          const int cx = (run & 0xFF) + (k & 1), cy = ((run >> 8) & 0xFF) + ((k >> 1) & 1), cz = (run >> 16) + (k >> 2);
+          if (cx <= 63 && cy <= 63 && cz <= 63 && acc != 0.0f)
+            atomicAdd(reinterpret_cast<float *>(fine + fine_index(cx, cy, cz)) + comp, acc);
+        }
+        run = kw;
+        acc = 0.0f;
+      }
+      if (kw >= 0) acc += sVal[w][lane];
     }
   }
 }
@@ -118,56 +141,69 @@ int launch_deposit(const ccs_uniforms *u, int N, int box, const float4 *pos, con
 }
 
 // ---------------------------------------------------------------------------
-// coarse and monopole: src/glsl-sim.js:222-251.  One thread per coarse block
-// sums its 4^3 fine cells in the reference's loop order (bit for bit); the
-// monopole is a fixed-shape tree over the 4096 sums finished by the last CTA
-// to arrive (deterministic, unlike the reference's single serial fragment).
+// coarse and monopole: src/glsl-sim.js:222-251.  One warp per coarse block:
+// its lanes load the block's 4^3 fine cells together into shared memory, and
+// lane 0 sums them in the reference's loop order (bit for bit).  The same warp
+// writes the block's occupied fine cells, in that loop order, as (centre of
+// mass, mass) plus their place in the block -- the source list the cell pass
+// walks instead of all 64 cells of every neighbour block -- and appends an
+// occupied block to the list the cell pass visits.  The monopole is a
+// fixed-shape tree over the 4096 sums finished by the last CTA to arrive
+// (deterministic, unlike the reference's single serial fragment).
 // ---------------------------------------------------------------------------
-// The same thread also writes its block's occupied fine cells, in that loop
-// order, as (centre of mass, mass) plus their place in the block: the source
-// list the cell pass walks instead of all 64 cells of every neighbour block.
-__global__ void __launch_bounds__(kBlock) k_coarse(const float4 *__restrict__ fine, float4 *__restrict__ coarse,
-                                                   float4 *partial, unsigned *counter, float4 *mono,
-                                                   float4 *__restrict__ occ, uint8_t *__restrict__ occIdx,
-                                                   int *__restrict__ occN, int *__restrict__ occBlocks,
-                                                   int *__restrict__ occCount) {
-  __shared__ float4 red[kBlock];
+constexpr int kCoarseWarps = 8;
+
+__global__ void __launch_bounds__(32 * kCoarseWarps) k_coarse(const float4 *__restrict__ fine,
+                                                              float4 *__restrict__ coarse, float4 *partial,
+                                                              unsigned *counter, float4 *mono,
+                                                              float4 *__restrict__ occ, uint8_t *__restrict__ occIdx,
+                                                              int *__restrict__ occN, int *__restrict__ occBlocks,
+                                                              int *__restrict__ occCount) {
+  __shared__ float4 cells[kCoarseWarps][64];
+  __shared__ float4 red[kCoarseWarps];
   __shared__ bool last;
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int b = blockIdx.x * kCoarseWarps + wid;
   const int cx = b & 15, cy = (b >> 4) & 15, cz = b >> 8;
-  float4 s = make_float4(0, 0, 0, 0);
   int n = 0;
-  for (int z = 0; z < 4; z++)
-    for (int y = 0; y < 4; y++)
-      for (int x = 0; x < 4; x++) {
-        const float4 f = fine[fine_index(cx * 4 + x, cy * 4 + y, cz * 4 + z)];
-        s.x = xadd(s.x, f.x);
-        s.y = xadd(s.y, f.y);
-        s.z = xadd(s.z, f.z);
-        s.w = xadd(s.w, f.w);
-        if (f.w > 0.0f) {
-          const float iw = fdiv(1.0f, f.w);
-          occ[b * 64 + n] = make_float4(f.x * iw, f.y * iw, f.z * iw, f.w);
-          occIdx[b * 64 + n] = (uint8_t)((z * 4 + y) * 4 + x);
-          ++n;
-        }
-      }
-  occN[b] = n;
-  if (n) occBlocks[atomicAdd(occCount, 1)] = b;   // the cell pass visits these only
-  coarse[b] = s;
-  red[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = kBlock / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) {
-      float4 a = red[threadIdx.x];
-      const float4 c = red[threadIdx.x + o];
-      a.x += c.x; a.y += c.y; a.z += c.z; a.w += c.w;
-      red[threadIdx.x] = a;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {   // cell c = (z * 4 + y) * 4 + x: the reference's loop order
+    const int c = 32 * h + lane;
+    const float4 f = fine[fine_index(cx * 4 + (c & 3), cy * 4 + ((c >> 2) & 3), cz * 4 + (c >> 4))];
+    cells[wid][c] = f;
+    const bool here = f.w > 0.0f;
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, here);
+    if (here) {
+      const int at = n + __popc(bal & ((1u << lane) - 1u));
+      const float iw = fdiv(1.0f, f.w);
+      occ[b * 64 + at] = make_float4(f.x * iw, f.y * iw, f.z * iw, f.w);
+      occIdx[b * 64 + at] = (uint8_t)c;
     }
-    __syncthreads();
+    n += __popc(bal);
   }
+  __syncwarp();
+  float4 s = make_float4(0, 0, 0, 0);
+  if (lane == 0) {
+    for (int c = 0; c < 64; ++c) {
+      const float4 f = cells[wid][c];
+      s.x = xadd(s.x, f.x);
+      s.y = xadd(s.y, f.y);
+      s.z = xadd(s.z, f.z);
+      s.w = xadd(s.w, f.w);
+    }
+    occN[b] = n;
+    if (n) occBlocks[atomicAdd(occCount, 1)] = b;   // the cell pass visits these only
+    coarse[b] = s;
+    red[wid] = s;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    partial[blockIdx.x] = red[0];
+    float4 a = red[0];
+    for (int w = 1; w < kCoarseWarps; ++w) {
+      const float4 c = red[w];
+      a.x += c.x; a.y += c.y; a.z += c.z; a.w += c.w;
+    }
+    partial[blockIdx.x] = a;
     __threadfence();
     last = atomicAdd(counter, 1u) == gridDim.x - 1;
   }
@@ -185,8 +221,8 @@ __global__ void __launch_bounds__(kBlock) k_coarse(const float4 *__restrict__ fi
 }
 
 int launch_coarse(const MeshBuf &m, cudaStream_t st) {
-  k_coarse<<<kCoarse / kBlock, kBlock, 0, st>>>(m.fine, m.coarse, m.partial, m.counter, m.mono, m.occ, m.occIdx,
-                                               m.occN, m.occBlocks, m.occCount);
+  k_coarse<<<kCoarse / kCoarseWarps, 32 * kCoarseWarps, 0, st>>>(m.fine, m.coarse, m.partial, m.counter, m.mono,
+                                                                 m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount);
   return 1;
 }
 
