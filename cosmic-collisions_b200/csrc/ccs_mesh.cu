@@ -19,11 +19,8 @@ inline int blocks_for(long n, int b = kBlock) { return (int)((n + b - 1) / b); }
 // share a base cell (the common case in Morton order) reduce-scatter their 32
 // values (8 corners x 4 components) with 31 shuffles, so the warp issues 32
 // scalar L2 atomics instead of 256 vector ones; mixed warps fall back to
-// per-lane float4 atomics.  The warps of a CTA whose particles share a base
-// cell are added in shared memory first, so a CTA issues one set of 32 atomics
-// per base cell rather than per warp.  The box a particle is in and its base
-// cell are exact; the summation order is unspecified, as the reference's
-// blending is.
+// per-lane float4 atomics.  The box a particle is in and its base cell are
+// exact; the summation order is unspecified, as the reference's blending is.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void reduce_scatter32(float (&v)[32], int lane) {
 #pragma unroll
@@ -41,11 +38,9 @@ __device__ __forceinline__ void reduce_scatter32(float (&v)[32], int lane) {
 __global__ void __launch_bounds__(kBlock) k_deposit(const ccs_uniforms *__restrict__ U, int box,
                                                     const float4 *__restrict__ pos, const float *__restrict__ mat,
                                                     const float4 *__restrict__ monoPrev, float4 *fine) {
-  __shared__ int sKey[kBlock / 32];
-  __shared__ float sVal[kBlock / 32][32];
   const ccs_uniforms &u = *U;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   bool in = false, stray = false;
   int bx = 0, by = 0, bz = 0;
   f3 t = mk(0, 0, 0), p = mk(0, 0, 0);
@@ -85,9 +80,10 @@ __global__ void __launch_bounds__(kBlock) k_deposit(const ccs_uniforms *__restri
     if (lane == 0) atomicAdd(fine + kFine, s);
   }
   const unsigned inMask = __ballot_sync(0xFFFFFFFFu, in);
+  if (inMask == 0u) return;
   const int key = in ? (bz << 16) | (by << 8) | bx : -1 - lane;
-  const int key0 = inMask ? __shfl_sync(0xFFFFFFFFu, key, __ffs(inMask) - 1) : -1;
-  const bool uniform = inMask && __all_sync(0xFFFFFFFFu, !in || key == key0) && __popc(inMask) > 1;
+  const int key0 = __shfl_sync(0xFFFFFFFFu, key, __ffs(inMask) - 1);
+  const bool uniform = __all_sync(0xFFFFFFFFu, !in || key == key0) && __popc(inMask) > 1;
   float v[32];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
@@ -99,37 +95,18 @@ __global__ void __launch_bounds__(kBlock) k_deposit(const ccs_uniforms *__restri
     v[4 * k + 2] = p.z * w;
     v[4 * k + 3] = w;
   }
-  if (uniform) {   // this lane ends with corner lane >> 2, component lane & 3 of the warp's sum
+  if (uniform) {
     reduce_scatter32(v, lane);
-    sVal[wid][lane] = v[0];
+    const int k = lane >> 2, comp = lane & 3;
+    const int cx = (key0 & 0xFF) + (k & 1), cy = ((key0 >> 8) & 0xFF) + ((k >> 1) & 1), cz = (key0 >> 16) + (k >> 2);
+    if (cx <= 63 && cy <= 63 && cz <= 63 && v[0] != 0.0f)
+      atomicAdd(reinterpret_cast<float *>(fine + fine_index(cx, cy, cz)) + comp, v[0]);
   } else if (in) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int cx = bx + (k & 1), cy = by + ((k >> 1) & 1), cz = bz + (k >> 2);
       if (cx > 63 || cy > 63 || cz > 63) continue;
       atomicAdd(fine + fine_index(cx, cy, cz), make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]));
-    }
-  }
-  if (lane == 0) sKey[wid] = uniform ? key0 : -1;
-  __syncthreads();
-  // warp 0 adds runs of warps that share a base cell (Morton order makes them common), then one set of atomics
-  // per run
-  if (wid == 0) {
-    const int k = lane >> 2, comp = lane & 3;
-    int run = -1;
-    float acc = 0.0f;
-    for (int w = 0; w <= kBlock / 32; ++w) {
-      const int kw = w < kBlock / 32 ? sKey[w] : -1;
-      if (kw != run) {
-        if (run >= 0) {
-          const int cx = (run & 0xFF) + (k & 1), cy = ((run >> 8) & 0xFF) + ((k >> 1) & 1), cz = (run >> 16) + (k >> 2);
-          if (cx <= 63 && cy <= 63 && cz <= 63 && acc != 0.0f)
-            atomicAdd(reinterpret_cast<float *>(fine + fine_index(cx, cy, cz)) + comp, acc);
-        }
-        run = kw;
-        acc = 0.0f;
-      }
-      if (kw >= 0) acc += sVal[w][lane];
     }
   }
 }
@@ -208,15 +185,29 @@ __global__ void __launch_bounds__(32 * kCoarseWarps) k_coarse(const float4 *__re
     last = atomicAdd(counter, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
+  if (last) {   // the CTA partials in a fixed tree: each thread a fixed stride of them, then halving
+    __shared__ float4 tree[32 * kCoarseWarps];
     __threadfence();
     float4 m = make_float4(0, 0, 0, 0);
-    for (int k = 0; k < (int)gridDim.x; ++k) {
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
       const float4 c = __ldcg(partial + k);
       m.x += c.x; m.y += c.y; m.z += c.z; m.w += c.w;
     }
-    *mono = m;
-    *counter = 0u;
+    tree[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) {
+        float4 a = tree[threadIdx.x];
+        const float4 c = tree[threadIdx.x + o];
+        a.x += c.x; a.y += c.y; a.z += c.z; a.w += c.w;
+        tree[threadIdx.x] = a;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      *mono = tree[0];
+      *counter = 0u;
+    }
   }
 }
 
