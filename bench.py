@@ -380,6 +380,31 @@ def run_ensemble(args, log):
     return line
 
 
+def analysis_timing(cc, nb, reps=5):
+    """The worker's fof (src/nbody.js:646-893) on the bench's state, with the Morton sort: on the device
+    (ccs_fof_device, wall time of the call: it returns the report on the host) and on one host core
+    (ccs_fof on the read-back state), and whether the two agree."""
+    import numpy as np
+    N, cap = nb.sim.N, cc.NBody.PP_CAP
+    nb.fof_device(True)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        rd, ld, qd = nb.fof_device(True)
+        times.append(time.perf_counter() - t0)
+    D = nb.buffer("diag").reshape(-1, 4)[:N]
+    st = nb.read_state()
+    s = nb.sim
+    t0 = time.perf_counter()
+    rh, lh, qh = cc.fof(s.N, s.m, s.a, st["pos"], st["vel"], st["mat"], D, s.k, 2 * s.a, cap, True)
+    host_s = time.perf_counter() - t0
+    return {"device_ms": 1e3 * statistics.median(times), "host_ms": 1e3 * host_s, "host_cores": 1,
+            "loose": int(rh.ppLoose), "same_loose_list": bool(np.array_equal(ld, lh)),
+            "same_perm": bool(np.array_equal(qd, qh)),
+            "largest_rel_diff": abs(rd.largest - rh.largest) / rh.largest,
+            "L_rel_diff": abs(rd.L - rh.L) / rh.L}
+
+
 def timed_steps(nb, lib, stream, flush, steps, dev, dist):
     """steps direct-launch steps, L2 flushed before each, each bracketed by CUDA events on the library's
     stream; kernel times from the library's own events; clocks sampled meanwhile."""
@@ -508,6 +533,7 @@ def run_ours(args, rank, world, log):
     d2h = N * (16 + 16 + 16 + 4)
 
     ferr = force_error(cc, dev, N) if rank == 0 else None
+    analysis = analysis_timing(cc, nb) if rank == 0 and not args.no_cpu else None
 
     # the learned correction (config 4): train, attach, the same timed steps, the same force sweep
     nn_line = None
@@ -572,6 +598,7 @@ def run_ours(args, rank, world, log):
         "gpu_launches": int(launches),
         "clocks": clk,
         "force_error": ferr,
+        "analysis": analysis,
         "nn_corrected": nn_line,
     }
     nb.close()

@@ -8,6 +8,7 @@
 // blocks whose uniform slots are refreshed by one memcpy node each replay.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -97,6 +98,12 @@ struct ccs_handle {
   bool pending = false;
   // books
   double *booksPartial = nullptr, *booksOut = nullptr;
+  // the analysis on the device (allocated on first use)
+  int *fofParent = nullptr, *fofSize = nullptr, *fofStart = nullptr, *fofEnd = nullptr, *fofCounts = nullptr,
+      *fofOffs = nullptr, *fofNDist = nullptr;
+  int32_t *fofList = nullptr;
+  double *fofPart = nullptr, *fofElastic = nullptr, *fofDist = nullptr;
+  unsigned long long *fofTop = nullptr;
   // graphs
   std::map<GraphKey, GraphSlot> graphs;
   int ping = 0;
@@ -567,6 +574,9 @@ void free_state(ccs_handle *h) {
   dev_free(h->tab); dev_free(h->diag);
   dev_free(h->keys); dev_free(h->keysTmp); dev_free(h->hist); dev_free(h->vals); dev_free(h->valsTmp);
   dev_free(h->into); dev_free(h->permDev);
+  dev_free(h->fofParent); dev_free(h->fofSize); dev_free(h->fofStart); dev_free(h->fofEnd); dev_free(h->fofCounts);
+  dev_free(h->fofOffs); dev_free(h->fofNDist); dev_free(h->fofList); dev_free(h->fofPart); dev_free(h->fofElastic);
+  dev_free(h->fofDist); dev_free(h->fofTop);
   dev_free(h->booksPartial); dev_free(h->booksOut); dev_free(h->status);
   if (h->stageP) cudaFreeHost(h->stageP);
   if (h->stageV) cudaFreeHost(h->stageV);
@@ -1365,6 +1375,19 @@ int ccs_apply_perm(ccs_handle *h, const int32_t *perm) {
   return CCS_OK;
 }
 
+// passDiag, src/nbody.js:488-507
+static int diag_pass(ccs_handle *h) {
+  set_boxes(h);
+  const ccs_uniforms *U;
+  int rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+  if (rc) return rc;
+  pass_slots(h, U);
+  pass_mesh(h, U, h->boxB > 0.5f);
+  pass_pp(h, U, h->ppCount);
+  pass_diag_kernel(h, U);
+  return check_launch(h);
+}
+
 int ccs_sort_morton(ccs_handle *h, const double core[3], int32_t *perm_out, int32_t *into_out) {
   int rc = ensure_built(h);
   if (rc) return rc;
@@ -1383,16 +1406,286 @@ int ccs_sort_morton(ccs_handle *h, const double core[3], int32_t *perm_out, int3
   return CCS_OK;
 }
 
-// passDiag, src/nbody.js:488-507
-static int diag_pass(ccs_handle *h) {
-  set_boxes(h);
-  const ccs_uniforms *U;
-  int rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+}  // extern "C"
+
+// ---- fof of src/nbody.js:646-893 on the device; the report assembled as ccs_fof assembles it ----
+namespace {
+struct DevGroup {
+  int n = 0;
+  double mass = 0, com[3] = {}, core[3] = {}, vel[3] = {}, imp = 0, iron = 0, R = 0, Redge = 0, Tsurf = 0;
+  double hotCom[3] = {}, hotR = 0, impMass = 0, impCom[3] = {}, impRms = 0;
+};
+
+int fof_sum(ccs_handle *h, const FofSumArgs &a, double out[kFofTerms]) {
+  h->launches += launch_fof_sums(a, h->fofPart, h->st);
+  const int nb = fof_blocks(a.N);
+  std::vector<double> part((size_t)nb * kFofTerms);
+  CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->fofPart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  for (int k = 0; k < kFofTerms; ++k) out[k] = 0.0;
+  for (int b = 0; b < nb; ++b)
+    for (int k = 0; k < kFofTerms; ++k) out[k] += part[(size_t)b * kFofTerms + k];
+  return CCS_OK;
+}
+
+int fof_group(ccs_handle *h, FofSumArgs a, int g, DevGroup &G) {
+  double t[kFofTerms];
+  a.g = g;
+  a.pass = kFofGroup;
+  int rc = fof_sum(h, a, t);
   if (rc) return rc;
-  pass_slots(h, U);
-  pass_mesh(h, U, h->boxB > 0.5f);
-  pass_pp(h, U, h->ppCount);
-  pass_diag_kernel(h, U);
+  G.n = (int)t[0];
+  G.mass = t[1];
+  G.impMass = t[8];
+  G.iron = t[12];
+  const double mass = G.mass, imp = G.impMass, Rg = std::cbrt(mass);
+  for (int k = 0; k < 3; ++k) {
+    G.com[k] = t[2 + k] / mass;
+    G.impCom[k] = imp > 0 ? t[9 + k] / imp : 0;
+  }
+  const double tm = mass - imp;
+  double core[3];
+  if (imp > tm) for (int k = 0; k < 3; ++k) core[k] = G.impCom[k];
+  else for (int k = 0; k < 3; ++k) core[k] = (t[2 + k] - t[9 + k]) / tm;
+  a.pass = kFofCore;
+  a.r2 = 0.9 * 0.9 * Rg * Rg;
+  for (int it = 0; it < 3; ++it) {
+    for (int k = 0; k < 3; ++k) a.c[k] = core[k];
+    double c[kFofTerms];
+    rc = fof_sum(h, a, c);
+    if (rc) return rc;
+    if (c[0] > 0) for (int k = 0; k < 3; ++k) core[k] = c[1 + k] / c[0];
+  }
+  std::memcpy(G.core, core, sizeof core);
+  const double shell = 0.64 * Rg * Rg, dr = 3 * Rg / kFofBins;
+  a.pass = kFofShape;
+  a.r2 = shell;
+  for (int k = 0; k < 3; ++k) { a.c[k] = core[k]; a.d[k] = G.impCom[k]; }
+  double sh[kFofTerms];
+  rc = fof_sum(h, a, sh);
+  if (rc) return rc;
+  const double Ts = sh[0], ws = sh[1], irms = sh[2], hs = sh[3], hx = sh[4], hy = sh[5], hz = sh[6], hr2 = sh[7];
+  std::memcpy(G.hotCom, core, sizeof core);
+  G.hotR = Rg;
+  if (hs > 0) {
+    G.hotCom[0] = hx / hs; G.hotCom[1] = hy / hs; G.hotCom[2] = hz / hs;
+    const double ox = G.hotCom[0] - core[0], oy = G.hotCom[1] - core[1], oz = G.hotCom[2] - core[2];
+    G.hotR = std::sqrt(std::max(hr2 / hs - (ox * ox + oy * oy + oz * oz), 0.0));
+  }
+  if (G.n >= 2000) {   // where the body ends: the first shell under a third of the mantle's density
+    h->launches += launch_fof_hist(a, dr, h->fofPart, h->st);
+    const int nb = fof_blocks(a.N);
+    std::vector<double> part((size_t)nb * kFofBins);
+    CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->fofPart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, h->st));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st));
+    double hist[kFofBins] = {};
+    for (int b = 0; b < nb; ++b)
+      for (int k = 0; k < kFofBins; ++k) hist[k] += part[(size_t)b * kFofBins + k];
+    const double Rb = std::cbrt(std::max(imp, tm));
+    double rho[kFofBins], refS = 0;
+    int refN = 0;
+    for (int b = 0; b < kFofBins; ++b) {
+      const double rm = (b + 0.5) * dr;
+      rho[b] = hist[b] / (rm * rm * dr);
+      if (rm > 0.6 * Rb && rm < 0.85 * Rb) { refS += rho[b]; ++refN; }
+    }
+    G.Redge = Rg;
+    for (int b = 0; b < kFofBins; ++b)
+      if ((b + 0.5) * dr > 0.85 * Rb && refN > 0 && rho[b] < 0.35 * refS / refN) { G.Redge = b * dr; break; }
+  }
+  for (int k = 0; k < 3; ++k) G.vel[k] = t[5 + k] / mass;
+  G.imp = imp / mass;
+  G.iron /= mass;
+  G.R = Rg;
+  G.Tsurf = ws > 0 ? Ts / ws : 0;
+  G.impRms = imp > 0 ? std::sqrt(irms / imp) : 0;
+  return CCS_OK;
+}
+
+int ensure_fof_buffers(ccs_handle *h) {
+  if (h->fofParent) return CCS_OK;
+  const int N = h->N, nb = fof_blocks(N);
+  int rc = CCS_OK;
+  rc |= dev_alloc(h, &h->fofParent, N); rc |= dev_alloc(h, &h->fofSize, N);
+  rc |= dev_alloc(h, &h->fofStart, kFofBuckets); rc |= dev_alloc(h, &h->fofEnd, kFofBuckets);
+  rc |= dev_alloc(h, &h->fofCounts, nb); rc |= dev_alloc(h, &h->fofOffs, nb + 1); rc |= dev_alloc(h, &h->fofNDist, 1);
+  rc |= dev_alloc(h, &h->fofList, CCS_PP_CAP); rc |= dev_alloc(h, &h->fofPart, (size_t)nb * kFofBins);
+  rc |= dev_alloc(h, &h->fofElastic, nb); rc |= dev_alloc(h, &h->fofDist, N); rc |= dev_alloc(h, &h->fofTop, 2 * nb);
+  return rc ? CCS_E_NOMEM : CCS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int ccs_fof_device(ccs_handle *h, double spring, double touch, int cap, int sort, ccs_report *rep, int32_t *list,
+                   int32_t *perm) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!rep || cap < 0 || cap > CCS_PP_CAP || (cap > 0 && !list) || (sort && !perm)) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  rc = ensure_fof_buffers(h);
+  if (rc) return rc;
+  rc = diag_pass(h);   // the read-outs the books need, as the reference's analysis reads them
+  if (rc) return rc;
+  const int N = h->N, nb = fof_blocks(N);
+  const double mref = h->sim.m, a = h->sim.a;
+  const float4 *P = h->pos[h->cur], *V = h->vel[h->cur];
+  // groups
+  h->launches += launch_fof_groups(N, P, a, touch, spring, h->keys, h->vals, h->keysTmp, h->valsTmp, h->hist,
+                                   h->fofStart, h->fofEnd, h->fofParent, h->fofSize, h->fofElastic, h->fofTop,
+                                   h->status, h->st);
+  std::vector<unsigned long long> top(2 * (size_t)nb);
+  std::vector<double> el((size_t)nb);
+  CUDA_TRY(h, cudaMemcpyAsync(top.data(), h->fofTop, 8 * top.size(), cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaMemcpyAsync(el.data(), h->fofElastic, 8 * el.size(), cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  rc = check_status(h);
+  if (rc) return rc;
+  unsigned long long t1 = 0, t2 = 0;
+  for (unsigned long long v : top) {
+    if (v > t1) { t2 = t1; t1 = v; }
+    else if (v > t2 && v != t1) t2 = v;
+  }
+  double elastic = 0;
+  for (double v : el) elastic += v;
+  const int g1 = t1 ? (int)(0xFFFFFFFFu - (uint32_t)(t1 & 0xFFFFFFFFu)) : -1;
+  const int g2 = t2 ? (int)(0xFFFFFFFFu - (uint32_t)(t2 & 0xFFFFFFFFu)) : -1;
+  FofSumArgs base{};
+  base.N = N;
+  base.mref = mref;
+  base.pos = P;
+  base.vel = V;
+  base.diag = h->diag;
+  base.mat = h->mat;
+  base.label = h->fofParent;
+  DevGroup A, B;
+  rc = fof_group(h, base, g1, A);
+  if (rc) return rc;
+  const bool hasB = g2 >= 0;
+  if (hasB) {
+    rc = fof_group(h, base, g2, B);
+    if (rc) return rc;
+  }
+  // the planet's spin over the body proper, within 1.15 of its own radius
+  const double rb = 1.15 * std::cbrt(std::max(A.impMass, A.mass - A.impMass)), rb2 = rb * rb;
+  FofSumArgs pa = base;
+  pa.g = g1;
+  pa.r2 = rb2;
+  for (int k = 0; k < 3; ++k) pa.c[k] = A.core[k];
+  double t[kFofTerms];
+  pa.pass = kFofProper1;
+  if ((rc = fof_sum(h, pa, t))) return rc;
+  const double bm = t[0];
+  double bv[3] = {t[1], t[2], t[3]};
+  if (bm > 0) for (int k = 0; k < 3; ++k) bv[k] /= bm;
+  pa.pass = kFofProper2;
+  for (int k = 0; k < 3; ++k) pa.d[k] = bv[k];
+  if ((rc = fof_sum(h, pa, t))) return rc;
+  const double Lx = t[0], Ly = t[1], Lz = t[2];
+  const double Lm = std::sqrt(Lx * Lx + Ly * Ly + Lz * Lz);
+  const double lx = Lx / (Lm + 1e-30), ly = Ly / (Lm + 1e-30), lz = Lz / (Lm + 1e-30);
+  const double tilt = std::acos(std::max(-1.0, std::min(1.0, ly))) * 180 / 3.141592653589793;
+  pa.pass = kFofProper3;
+  pa.d[0] = lx; pa.d[1] = ly; pa.d[2] = lz;
+  if ((rc = fof_sum(h, pa, t))) return rc;
+  const double I = t[0];
+  const double day = Lm > 1e-9 ? 2 * 3.141592653589793 * I / Lm * 805 / 3600 : INFINITY;
+  // the disk: what is bound in orbit about the planet, and the Moon it makes
+  FofSumArgs oa = base;
+  oa.pass = kFofOrbit;
+  oa.g = g1;
+  oa.s0 = A.mass;
+  oa.s1 = A.R;
+  for (int k = 0; k < 3; ++k) { oa.c[k] = A.com[k]; oa.d[k] = A.vel[k]; }
+  if ((rc = fof_sum(h, oa, t))) return rc;
+  const double orbit = t[0], esc = t[1], J[3] = {t[2], t[3], t[4]};
+  const double jD = orbit > 0 ? std::sqrt(J[0] * J[0] + J[1] * J[1] + J[2] * J[2]) / (orbit * std::sqrt(A.mass * 2.9)) : 0;
+  const double moon = std::min(std::max(0.0, orbit * (1.9 * jD - 1.1 - 1.9 * 0.05)), 0.95 * orbit);
+  std::memset(rep, 0, sizeof *rep);
+  auto energy = [&](const double *x, const double *v) {
+    const double r = std::sqrt((x[0] - A.com[0]) * (x[0] - A.com[0]) + (x[1] - A.com[1]) * (x[1] - A.com[1]) +
+                               (x[2] - A.com[2]) * (x[2] - A.com[2]));
+    const double dv2 = (v[0] - A.vel[0]) * (v[0] - A.vel[0]) + (v[1] - A.vel[1]) * (v[1] - A.vel[1]) +
+                       (v[2] - A.vel[2]) * (v[2] - A.vel[2]);
+    return 0.5 * dv2 - A.mass / std::max(r, A.R);
+  };
+  if (hasB && B.n >= std::max(8.0, N / 1000.0)) {
+    const double dAB = std::sqrt((B.com[0] - A.com[0]) * (B.com[0] - A.com[0]) +
+                                 (B.com[1] - A.com[1]) * (B.com[1] - A.com[1]) +
+                                 (B.com[2] - A.com[2]) * (B.com[2] - A.com[2]));
+    if (dAB > A.R + B.R + 2 * a) {
+      rep->hasSecond = 1;
+      rep->secMass = B.mass;
+      rep->secDist = dAB;
+      rep->secBound = energy(B.com, B.vel) < 0;
+      rep->secImp = B.imp;
+      rep->secIron = B.iron;
+      std::memcpy(rep->secCom, B.com, sizeof B.com);
+      std::memcpy(rep->secCore, B.core, sizeof B.core);
+      std::memcpy(rep->secVel, B.vel, sizeof B.vel);
+      rep->secR = B.R;
+    }
+  }
+  // the books
+  FofSumArgs ba = base;
+  ba.pass = kFofBooks;
+  if ((rc = fof_sum(h, ba, t))) return rc;
+  const double Mt = t[0], p[3] = {t[1], t[2], t[3]}, Jx = t[4], Jy = t[5], Jz = t[6];
+  // the loose list: beyond 1.3 radii of the planet (and of a big second body), the farthest first over the cap
+  FofLooseArgs la{};
+  la.N = N;
+  la.pos = P;
+  la.bigB = hasB && B.mass > 0.05;
+  la.RA = A.R;
+  la.RB = B.R;
+  for (int k = 0; k < 3; ++k) { la.comA[k] = A.com[k]; la.comB[k] = B.com[k]; }
+  CUDA_TRY(h, cudaMemsetAsync(h->fofNDist, 0, sizeof(int), h->st));
+  h->launches += launch_fof_loose(la, 0, h->fofCounts, h->fofOffs, h->fofDist, h->fofNDist, nullptr, h->st);
+  std::vector<int> counts((size_t)nb);
+  CUDA_TRY(h, cudaMemcpyAsync(counts.data(), h->fofCounts, 4 * (size_t)nb, cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  int nLoose = 0;
+  for (int c : counts) nLoose += c;
+  double least = 0;
+  if (nLoose > cap) {
+    std::vector<double> ds((size_t)nLoose);
+    CUDA_TRY(h, cudaMemcpyAsync(ds.data(), h->fofDist, 8 * (size_t)nLoose, cudaMemcpyDeviceToHost, h->st));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st));
+    std::nth_element(ds.begin(), ds.begin() + (nLoose - cap), ds.end());
+    least = ds[(size_t)(nLoose - cap)];
+  }
+  const int len = std::min(nLoose, cap);
+  la.len = len;
+  la.least = least;
+  if (len > 0) h->launches += launch_fof_loose(la, 1, h->fofCounts, h->fofOffs, nullptr, nullptr, h->fofList, h->st);
+  if (sort) {   // the spatial order: a Morton key of 7 bits an axis over the largest body's box
+    h->launches += launch_morton_keys(N, P, A.core[0], A.core[1], A.core[2], h->keys, h->vals, h->st);
+    h->launches += launch_radix_sort(N, 21, h->keys, h->vals, h->keysTmp, h->valsTmp, h->hist, h->st);
+    h->launches += launch_invert_perm(N, h->vals, h->into, h->st);
+    h->launches += launch_fof_remap(len, h->into, h->fofList, h->st);
+    CUDA_TRY(h, cudaMemcpyAsync(perm, h->vals, 4 * (size_t)N, cudaMemcpyDeviceToHost, h->st));
+  }
+  if (len > 0) CUDA_TRY(h, cudaMemcpyAsync(list, h->fofList, 4 * (size_t)len, cudaMemcpyDeviceToHost, h->st));
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  rep->largest = A.mass; rep->largestImp = A.imp; rep->largestIron = A.iron; rep->day = day; rep->tilt = tilt;
+  rep->axis[0] = lx; rep->axis[1] = ly; rep->axis[2] = lz;
+  std::memcpy(rep->bodyVel, bv, sizeof bv);
+  rep->orbit = orbit; rep->escape = esc;
+  std::memcpy(rep->com, A.com, sizeof A.com);
+  std::memcpy(rep->core, A.core, sizeof A.core);
+  std::memcpy(rep->vel, A.vel, sizeof A.vel);
+  rep->R = A.R; rep->Redge = A.Redge; rep->Tsurf = A.Tsurf;
+  std::memcpy(rep->hotCom, A.hotCom, sizeof A.hotCom);
+  rep->hotR = A.hotR; rep->impMass = A.impMass;
+  std::memcpy(rep->impCom, A.impCom, sizeof A.impCom);
+  rep->impRms = A.impRms;
+  rep->M = Mt; rep->iron = t[10] / Mt;
+  rep->drift = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) / Mt;
+  rep->L = std::sqrt(Jx * Jx + Jy * Jy + Jz * Jz);
+  rep->KE = t[7]; rep->PE = t[8]; rep->EL = elastic; rep->Q = t[9];
+  rep->unseated = t[11] / N; rep->full = t[12] / N;
+  rep->jD = jD; rep->moon = moon;
+  rep->ppCount = len; rep->ppLoose = nLoose;
   return check_launch(h);
 }
 

@@ -16,6 +16,36 @@ constexpr int kCoarse = 4096;                 // 16^3 blocks
 constexpr int kSeats = CCS_SEATS;
 constexpr unsigned kStatusGrid = 1u;          // a contact-cell insertion gave up (degenerate pile)
 constexpr unsigned kStatusNN = 2u;            // a tensor-core wait of the learned P3M pass gave up
+constexpr unsigned kStatusFof = 4u;           // a union of the device analysis gave up its retries
+
+// the analysis on the device (ccs_fof.cu): src/nbody.js:646-893
+constexpr int kFofBuckets = 1 << 20;          // hashed cells of side 2.4 a, as the host restatement hashes them
+constexpr int kFofTerms = 13;                 // binary64 terms one sum pass adds per particle
+constexpr int kFofBins = 96;                  // shells of the density histogram
+enum FofPass { kFofGroup = 0, kFofCore, kFofShape, kFofProper1, kFofProper2, kFofProper3, kFofOrbit, kFofBooks };
+struct FofSumArgs {
+  int N, pass, g;                             // g: the group label the pass is about
+  double mref, r2, s0, s1;
+  double c[3], d[3];                          // a centre and a second vector, by pass
+  const float4 *pos, *vel, *diag;
+  const float *mat;
+  const int *label;
+};
+struct FofLooseArgs {
+  int N, len, bigB;
+  double RA, RB, least;
+  double comA[3], comB[3];
+  const float4 *pos;
+};
+int fof_blocks(int N);
+int launch_fof_groups(int N, const float4 *pos, double a, double touch, double spring, uint32_t *keys, int32_t *vals,
+                      uint32_t *keysTmp, int32_t *valsTmp, uint32_t *hist, int *start, int *end, int *parent,
+                      int *size, double *elasticPart, unsigned long long *top, unsigned *status, cudaStream_t st);
+int launch_fof_sums(const FofSumArgs &a, double *part, cudaStream_t st);
+int launch_fof_hist(const FofSumArgs &a, double dr, double *part, cudaStream_t st);
+int launch_fof_loose(const FofLooseArgs &a, int pass, int *counts, int *offs, double *dist, int *nDist,
+                     int32_t *list, cudaStream_t st);
+int launch_fof_remap(int n, const int32_t *into, int32_t *list, cudaStream_t st);
 
 // One gravity mesh box: the textures of meshBox(), src/nbody.js:1050-1068,
 // as plain float4 arrays.  fine/force hold 64^3 cells in [z][y][x] order

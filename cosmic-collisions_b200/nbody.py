@@ -54,6 +54,7 @@ class NBody:
         self.analyzed_at = 0
         self.pending = None
         self.async_read = True
+        self.device_fof = False   # True: the analysis runs on the device (ccs_fof_device), synchronously
         self._worker = ThreadPoolExecutor(max_workers=1)
         self._job = None
         self._opt = None
@@ -241,6 +242,10 @@ class NBody:
         if s.phase == 2:   # `sim.phase === 'full' && analyses++ % 8 === 0`
             sort = self.analyses % 8 == 0
             self.analyses += 1
+        if self.device_fof:
+            r, lst, perm = self.fof_device(sort)
+            self._apply_report(r, lst, perm, s.t)
+            return
         self._check(lib().ccs_diag_async(self._h), "ccs_diag_async")
         if not sync and self.async_read:
             self.pending = {"gen": self.gen, "sort": sort, "t": s.t}
@@ -248,6 +253,17 @@ class NBody:
         P, V, D = self._wait_read()
         r, lst, perm = L.fof(s.N, s.m, s.a, P, V, self._mat, D, s.k, 2 * s.a, PP_CAP, sort)
         self._apply_report(r, lst, perm, s.t)
+
+    def fof_device(self, sort=False, cap=PP_CAP):
+        """The worker's fof (src/nbody.js:646-893) on the device over the current state:
+        (report, loose list, Morton permutation or None).  The state is not moved."""
+        s = self.sim
+        rep = L.Report()
+        lst = np.zeros(max(cap, 1), np.int32)
+        perm = np.zeros(s.N, np.int32) if sort else None
+        self._check(lib().ccs_fof_device(self._h, s.k, 2 * s.a, int(cap), 1 if sort else 0, C.byref(rep), ptr(lst),
+                                         ptr(perm)), "ccs_fof_device")
+        return rep, lst[:rep.ppCount].copy(), perm
 
     def _wait_read(self):
         N = self.sim.N

@@ -156,6 +156,16 @@ int ccs_poll(ccs_handle *h, float *P, float *V, float *D);
  * books, loose list (cap entries) and, with sort, the Morton permutation. */
 int ccs_fof(int N, double mref, double a, const float *P, const float *V, const float *R, const float *D,
             double spring, double touch, int cap, int sort, ccs_report *rep, int32_t *list, int32_t *perm);
+/* The same analysis on the device, on the engine's current state (it runs the
+ * diag pass first, as analyze() reads diag): the groups over an exact cell
+ * list with a lock-free union-find, every sum in binary64, the loose list by
+ * an ordered compaction and, with sort, the Morton order of ccs_sort_morton's
+ * key.  Same report, loose list (cap <= CCS_PP_CAP) and permutation as
+ * ccs_fof on the read-back state, the report's sums to rounding (they are
+ * added in another order); a tie between the two largest groups' sizes goes
+ * to the group holding the smaller index. */
+int ccs_fof_device(ccs_handle *h, double spring, double touch, int cap, int sort, ccs_report *rep, int32_t *list,
+                   int32_t *perm);
 /* The mesh's own pair force and potential by distance, meshPairTable of
  * src/nbody.js:56-108 (host, binary64 -> binary32). */
 int ccs_pair_table(int bins, double cut, float *f, float *p);
