@@ -39,7 +39,7 @@ EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_ma
            "ccs_nn_clear", "ccs_nn_pool_size", "ccs_nn_sample_state", "ccs_nn_sample_uniform", "ccs_nn_read_pool",
            "ccs_nn_train", "ccs_nn_forward", "ccs_nn_labels", "ccs_nn_grad", "ccs_set_pp_nn", "ccs_autotune",
            "ccs_ensemble_create", "ccs_ensemble_destroy", "ccs_ensemble_last_error", "ccs_ensemble_steps",
-           "ccs_ensemble_sync", "ccs_ensemble_autotune", "ccs_fof_device"]
+           "ccs_ensemble_sync", "ccs_ensemble_autotune", "ccs_fof_device", "ccs_set_field"]
 NN_PARAMS = 4803
 NN_CUT_CELLS = 2.5
 
@@ -58,6 +58,7 @@ class Uniforms(C.Structure):
                 ("invH", C.c_float), ("eps2Mesh", C.c_float), ("eps2Cell", C.c_float), ("Gm", C.c_float),
                 ("LA", C.c_float * 3), ("LB", C.c_float * 3), ("boxB", C.c_float),
                 ("cut", C.c_float), ("a2", C.c_float),
+                ("field", C.c_float), ("gField", C.c_float * 3), ("frozen", C.c_float),
                 ("ppCount", C.c_int),
                 ("rot0", C.c_float * 9), ("rot1", C.c_float * 9), ("rdt", C.c_float)]
 
@@ -199,6 +200,7 @@ def lib():
         "ccs_ensemble_sync": (I, [H]),
         "ccs_ensemble_autotune": (I, [H, I, P]),
         "ccs_fof_device": (I, [H, D, D, I, I, C.POINTER(Report), P, P]),
+        "ccs_set_field": (I, [H, I, P, D, D, D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

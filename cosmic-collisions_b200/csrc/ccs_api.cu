@@ -34,7 +34,7 @@ constexpr int kMaxBlock = 16;     // largest meshEvery a captured block supports
 constexpr int kTimedKernels = 5;  // simulate, contact grid, deposit, cell, P3M force
 
 struct GraphKey {
-  int boxB, pp, seatCur, cur, meshEvery, ping;
+  int boxB, pp, seatCur, cur, meshEvery, ping, field;
   bool operator<(const GraphKey &o) const {
     return std::memcmp(this, &o, sizeof *this) < 0;
   }
@@ -59,6 +59,9 @@ struct ccs_handle {
   ccs_uniforms stat{};                  // setStaticUniforms
   float LA[3] = {0, 0, 0}, LB[3] = {0, 0, 0}, boxB = 0.0f;   // what boxes() last set
   int N = 0, meshEvery = 8;
+  // the crater page's field-gravity step (ccs_set_field)
+  bool field = false;
+  double gField[3] = {0, 0, 0}, frozen = -1, fieldInvM = 1, fieldCpIron = 1;
   // per-step uniform ring (direct launches)
   ccs_uniforms *uniDev = nullptr, *uniHost = nullptr;
   cudaEvent_t uniEv[kRing] = {};
@@ -219,6 +222,14 @@ void make_static(ccs_handle *h) {
   u.Gm = (float)s.m;
   u.cut = (float)kPPCut;
   u.a2 = (float)(s.a * s.a);
+  u.frozen = -1.0f;
+  if (h->field) {   // the crater page's setStaticUniforms, chicxulub.html:700-710
+    u.field = 1.0f;
+    for (int k = 0; k < 3; ++k) u.gField[k] = (float)h->gField[k];
+    u.frozen = h->frozen < 0 ? -1.0f : (float)h->frozen;
+    u.invM = (float)h->fieldInvM;
+    u.cpIron = (float)h->fieldCpIron;
+  }
 }
 
 // boxes(), src/nbody.js:342-350
@@ -382,7 +393,7 @@ void pass_sim(ccs_handle *h, const ccs_uniforms *U) {
   const SimArgs a = sim_args(h);
   cudaEvent_t b, e;
   time_begin(h, 0, &b, &e);
-  h->launches += launch_simulate(U, h->N, a, h->st, h->tuneWarps);
+  h->launches += launch_simulate(U, h->N, a, h->st, h->tuneWarps, h->field);
   time_end(h, e);
   h->cur ^= 1;
 }
@@ -411,9 +422,16 @@ struct StepPlan {
 };
 StepPlan plan_step(ccs_handle *h, int settle, int kick) {
   ccs_sim &s = h->sim;
+  StepPlan p;
+  if (h->field) {   // chicxulub.html:763-766: the grid every 2nd step, the field every step
+    const int n = s.stepNo++;
+    p.slots = n % 2 == 0;
+    p.mesh = false;
+    p.u = pass_uniforms(h, settle, kick, s.dt);
+    return p;
+  }
   if (!settle && !kick && !s.soft && s.t - s.impactT > 1.5) soften(h);
   const int n = s.stepNo++;
-  StepPlan p;
   p.slots = n % 2 == 0;
   p.mesh = n % h->meshEvery == 0;
   if (p.mesh) set_boxes(h);
@@ -467,7 +485,7 @@ void free_graphs(ccs_handle *h) {
 // replayed from a captured graph
 int graph_block(ccs_handle *h) {
   const int M = h->meshEvery;
-  GraphKey key{(int)(h->boxB > 0.5f), h->ppCount > 0, h->seatCur, h->cur, M, h->ping};
+  GraphKey key{(int)(h->boxB > 0.5f), h->ppCount > 0, h->seatCur, h->cur, M, h->ping, (int)h->field};
   // plan the block's steps on the host (the boxes are set at its first step)
   ccs_uniforms us[kMaxBlock];
   StepPlan plans[kMaxBlock];
@@ -770,6 +788,19 @@ int ccs_set_mesh_every(ccs_handle *h, int n) {
   return CCS_OK;
 }
 
+int ccs_set_field(ccs_handle *h, int on, const double g[3], double frozen, double invM, double cpIron) {
+  if (!h || (on && (!g || !(invM > 0) || !(cpIron > 0)))) return CCS_E_ARG;
+  h->field = on != 0;
+  if (on) {
+    for (int k = 0; k < 3; ++k) h->gField[k] = g[k];
+    h->frozen = frozen;
+    h->fieldInvM = invM;
+    h->fieldCpIron = cpIron;
+  }
+  make_static(h);
+  return CCS_OK;
+}
+
 int ccs_step(ccs_handle *h, int settle, int kick) {
   int rc = ensure_built(h);
   if (rc) return rc;
@@ -859,7 +890,7 @@ int ccs_autotune(ccs_handle *h, int reps, int choice[2]) {
     float best = 1e30f;
     for (int w : {8, 4}) {
       float ms = 0.0f;
-      rc = time_launches(h, reps, [&] { launch_simulate(U, h->N, a, h->st, w); }, &ms);
+      rc = time_launches(h, reps, [&] { launch_simulate(U, h->N, a, h->st, w, h->field); }, &ms);
       if (rc) break;
       if (ms < best) { best = ms; warps = w; }
     }
@@ -950,7 +981,8 @@ int ensemble_block(ccs_ensemble *e, int R) {
       plans[i][k] = plan_step(h, 0, 0);
       h->sim.t += h->sim.dt;   // the frame loop's clock, index.html:372
     }
-    keys[i] = GraphKey{(int)(plans[i][0].u.boxB > 0.5f), h->ppCount > 0, h->seatCur, h->cur, e->M, h->ping};
+    keys[i] = GraphKey{(int)(plans[i][0].u.boxB > 0.5f), h->ppCount > 0, h->seatCur, h->cur, e->M, h->ping,
+                       (int)h->field};
     seat0[i] = h->seatCur;
     cur0[i] = h->cur;
   }

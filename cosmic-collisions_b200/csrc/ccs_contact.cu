@@ -128,8 +128,9 @@ __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const Si
   if (two) push_near(u, a, spc, w, near1, e1, r21, lane, nn);
 }
 
-// W warps per CTA (8 or 4: the autotuner's choice; 4 CTAs of 8 or 8 of 4 share an SM)
-template <int W>
+// W warps per CTA (8 or 4: the autotuner's choice; 4 CTAs of 8 or 8 of 4 share an SM); FIELD: the crater
+// page's constant gravity and frozen material in place of the mesh gather and the pairwise add
+template <int W, bool FIELD>
 __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_uniforms *__restrict__ U,
                                                                  const SimArgs a) {
   constexpr int kThreads = 32 * W;
@@ -227,34 +228,38 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
   if (!live) return;
   const f3 push = mk(w.fx[lane], w.fy[lane], w.fz[lane]);
   const float lost = w.lost[lane], flow = w.flow[lane], nb = (float)w.nb[lane];
-  // SIM_GRAV_MESH, src/glsl-sim.js:469-488
   f3 grav = mk(0.0f, 0.0f, 0.0f), g;
-  const int box = box_of(u, p, g);
-  if (box >= 0) {
-    const float4 *F = box == 0 ? a.forceA : a.forceB;
-    const float fx = floorf(g.x), fy = floorf(g.y), fz = floorf(g.z);
-    const f3 t = mk(g.x - fx, g.y - fy, g.z - fz);
-    const int bx = (int)fx, by = (int)fy, bz = (int)fz;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
-      const float wgt = (ox ? t.x : 1.0f - t.x) * (oy ? t.y : 1.0f - t.y) * (oz ? t.z : 1.0f - t.z);
-      const float4 f = __ldg(F + fine_index(min(bx + ox, 63), min(by + oy, 63), min(bz + oz, 63)));
-      grav = grav + xyz(f) * wgt;
-    }
-    grav = grav - xyz(__ldg(F + kFine)) * u.Gm;   // the strays in neither box pull back
-    if (u.boxB > 0.5f) {
-      const float4 mA = __ldg(a.monoA), mB = __ldg(a.monoB);
-      grav = grav + (box == 0 ? cross_at(u, mB, mA) : cross_at(u, mA, mB));
-    }
+  if (FIELD) {
+    grav = ld3(u.gField);   // SIM_GRAV_FIELD, src/glsl-sim.js:490-492: the whole of gravity
   } else {
-    grav = mass_at(u, p, __ldg(a.monoA));
-    if (u.boxB > 0.5f) grav = grav + mass_at(u, p, __ldg(a.monoB));
-  }
-  const int seat = a.ppSlot[me];
-  if (seat >= 0) {
+    // SIM_GRAV_MESH, src/glsl-sim.js:469-488
+    const int box = box_of(u, p, g);
+    if (box >= 0) {
+      const float4 *F = box == 0 ? a.forceA : a.forceB;
+      const float fx = floorf(g.x), fy = floorf(g.y), fz = floorf(g.z);
+      const f3 t = mk(g.x - fx, g.y - fy, g.z - fz);
+      const int bx = (int)fx, by = (int)fy, bz = (int)fz;
 #pragma unroll
-    for (int s = 0; s < 4; ++s) grav = grav + xyz(__ldg(a.ppForce + (size_t)s * a.cap + seat));
+      for (int k = 0; k < 8; ++k) {
+        const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
+        const float wgt = (ox ? t.x : 1.0f - t.x) * (oy ? t.y : 1.0f - t.y) * (oz ? t.z : 1.0f - t.z);
+        const float4 f = __ldg(F + fine_index(min(bx + ox, 63), min(by + oy, 63), min(bz + oz, 63)));
+        grav = grav + xyz(f) * wgt;
+      }
+      grav = grav - xyz(__ldg(F + kFine)) * u.Gm;   // the strays in neither box pull back
+      if (u.boxB > 0.5f) {
+        const float4 mA = __ldg(a.monoA), mB = __ldg(a.monoB);
+        grav = grav + (box == 0 ? cross_at(u, mB, mA) : cross_at(u, mA, mB));
+      }
+    } else {
+      grav = mass_at(u, p, __ldg(a.monoA));
+      if (u.boxB > 0.5f) grav = grav + mass_at(u, p, __ldg(a.monoB));
+    }
+    const int seat = a.ppSlot[me];
+    if (seat >= 0) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) grav = grav + xyz(__ldg(a.ppForce + (size_t)s * a.cap + seat));
+    }
   }
   // SIM_POST, src/glsl-sim.js:493-511
   const float dt = u.dt;
@@ -268,6 +273,8 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
   }
   if (u.kick > 0.5f) v = (tgt ? ld3(u.bulk0) : ld3(u.bulk1)) + vr;
   const float Q = u.settle > 0.5f ? 0.0f : a.q[me] + (lost + fdiv(flow * u.kappa, u.tK)) * dt;
+  // simFS({frozen: true}), src/glsl-sim.js:523-526: the material that does not move
+  if (FIELD && u.frozen >= 0.0f && fabsf(xsub(body, u.frozen)) < 0.5f) v = mk(0.0f, 0.0f, 0.0f);
   const f3 pn = p + v * dt;
   a.posO[me] = make_float4(pn.x, pn.y, pn.z, body);
   a.velO[me] = make_float4(v.x, v.y, v.z, fdiv(u.tK * Q, ci));
@@ -278,18 +285,23 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
 size_t contact_smem_bytes(int warps) { return sizeof(ContactWarp) * warps; }
 
 cudaError_t init_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(k_contact_step<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)contact_smem_bytes(8));
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_contact_step<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)contact_smem_bytes(4));
+  const cudaFuncAttribute smem = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(k_contact_step<8, false>, smem, (int)contact_smem_bytes(8));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_contact_step<4, false>, smem, (int)contact_smem_bytes(4));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_contact_step<8, true>, smem, (int)contact_smem_bytes(8));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_contact_step<4, true>, smem, (int)contact_smem_bytes(4));
+  return e;
 }
 
-int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st, int warps) {
-  if (warps == 4)
-    k_contact_step<4><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st, int warps, bool field) {
+  if (warps == 4 && field)
+    k_contact_step<4, true><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+  else if (warps == 4)
+    k_contact_step<4, false><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+  else if (field)
+    k_contact_step<8, true><<<blocks_for(N, 256), 256, contact_smem_bytes(8), st>>>(u, a);
   else
-    k_contact_step<8><<<blocks_for(N, 256), 256, contact_smem_bytes(8), st>>>(u, a);
+    k_contact_step<8, false><<<blocks_for(N, 256), 256, contact_smem_bytes(8), st>>>(u, a);
   return 1;
 }
 

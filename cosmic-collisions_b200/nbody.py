@@ -111,6 +111,18 @@ class NBody:
         self.analyzed_at = 0
         self.pp = {"count": 0, "loose": 0}
 
+    def set_field(self, g, frozen=-1.0, invM=1.0, cpIron=1.0):
+        """The crater page's field-gravity step (simFS({gravity: 'field', frozen: true}), chicxulub.html:235,
+        700-710, 763-766): constant gravity g, the material tagged `frozen` held still (negative: none),
+        the contact grid every 2nd step and no mesh.  invM and cpIron are 1 on that page."""
+        gg = np.ascontiguousarray(g, np.float64)
+        self._check(lib().ccs_set_field(self._h, 1, ptr(gg), float(frozen), float(invM), float(cpIron)),
+                    "ccs_set_field")
+
+    def clear_field(self):
+        """Back to the giant impact's mesh step."""
+        self._check(lib().ccs_set_field(self._h, 0, None, -1.0, 1.0, 1.0), "ccs_set_field")
+
     @property
     def sim(self):
         """The live run scalars (a ctypes view: writes go straight to the engine)."""

@@ -51,6 +51,8 @@ typedef struct {
   float invH, eps2Mesh, eps2Cell, Gm;               /* eps2Mesh = FH^2, eps2Cell = FH^2/2 */
   float LA[3], LB[3], boxB;                         /* the two mesh boxes, src/glsl-sim.js:25-37 */
   float cut, a2;                                    /* P3M cut-off and particle radius^2 */
+  float field, gField[3];                           /* 1: constant gravity gField (SIM_GRAV_FIELD) */
+  float frozen;                                     /* the material held still (uFrozen); < 0: none */
   int ppCount;                                      /* loose-list length (pp.count) */
   float rot0[9], rot1[9], rdt;                      /* rigid carry (src/glsl-sim.js:537-570) */
 } ccs_uniforms;
@@ -123,6 +125,17 @@ int ccs_set_static(ccs_handle *h);
 int ccs_get_uniforms(ccs_handle *h, ccs_uniforms *out);
 /* meshEvery setter, src/nbody.js:1115 (default 8) */
 int ccs_set_mesh_every(ccs_handle *h, int n);
+
+/* The field-gravity step of the crater page: simFS({gravity: 'field',
+ * frozen: true}) (src/glsl-sim.js:466-468, 490-492, 517-533) on the page's
+ * schedule (chicxulub.html:763-766: the contact grid on even steps, the
+ * contact step with uGDt = dt on every step, no mesh, no pairwise pass, no
+ * soften).  g is the constant acceleration (uGField); particles whose tag is
+ * within 0.5 of `frozen` are held still (a negative value holds none); invM
+ * and cpIron replace the impact's 1/m and cp_iron/cp_rock (the crater page
+ * sets both to 1: its spring is per unit mass and all its material is rock).
+ * on = 0 returns to the impact's mesh step.  Applies from the next step. */
+int ccs_set_field(ccs_handle *h, int on, const double g[3], double frozen, double invM, double cpIron);
 
 /* ---- the step: src/nbody.js:551-558 step(settle, kick) ---- */
 int ccs_step(ccs_handle *h, int settle, int kick);

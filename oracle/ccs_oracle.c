@@ -520,6 +520,7 @@ void orc_make_uni(const orc_sim *s, orc_uni *u) {
   u->invH = (float)(1 / FH); u->eps2Mesh = (float)(FH * FH); u->eps2Cell = (float)(0.5 * FH * FH);
   u->Gm = (float)s->m;
   u->cut = (float)PP_CUT; u->a2 = (float)(s->a * s->a);
+  u->frozen = -1.0f;   /* simFS without frozen: nothing is held */
   /* uLA, uLB, uBoxB keep GL's initial zeros until boxes() first runs */
 }
 void orc_boxes(const orc_sim *s, orc_uni *u) {
@@ -881,11 +882,13 @@ void orc_sim_pass(const orc_uni *u, const float *pos4, const float *vel4, const 
             }
           }
         }
-    /* SIM_GRAV_MESH */
+    /* SIM_GRAV_FIELD (src/glsl-sim.js:490-492) or SIM_GRAV_MESH */
     v3 grav = V3(0, 0, 0);
     float pp[3] = {p.x, p.y, p.z}, g[3];
-    int box = orc_box_of(u, pp, g);
-    if (box >= 0) {
+    int box = u->field > 0.5f ? -2 : orc_box_of(u, pp, g);
+    if (box == -2) {
+      grav = ld3(u->gField);
+    } else if (box >= 0) {
       const float *F = box == 0 ? forceA : forceB;
       float f[3], t[3];
       int cf[3];
@@ -906,7 +909,7 @@ void orc_sim_pass(const orc_uni *u, const float *pos4, const float *vel4, const 
       grav = mass_at(u, p, monoA);
       if (u->boxB > 0.5f) grav = vadd(grav, mass_at(u, p, monoB));
     }
-    int seat = ppslot[me];
+    int seat = box == -2 ? -1 : ppslot[me];
     if (seat >= 0)
       for (int s = 0; s < 4; s++) grav = vadd(grav, ld3(ppforce + 4 * ((size_t)s * cap + seat)));
     /* SIM_POST */
@@ -922,6 +925,7 @@ void orc_sim_pass(const orc_uni *u, const float *pos4, const float *vel4, const 
     }
     if (u->kick > 0.5f) v = vadd(ld3(body < 3.5f ? u->bulk0 : u->bulk1), vr);
     float Q = u->settle > 0.5f ? 0.0f : qa[me] + (lost + flow * u->kappa / u->tK) * u->dt;
+    if (u->frozen >= 0.0f && fabsf(body - u->frozen) < 0.5f) v = V3(0, 0, 0);   /* src/glsl-sim.js:523-526 */
     p = vadd(p, vmuls(v, u->dt));
     float *po = pos_o + 4 * (size_t)me, *vo = vel_o + 4 * (size_t)me, *ao = aux_o + 4 * (size_t)me;
     po[0] = p.x; po[1] = p.y; po[2] = p.z; po[3] = body;
@@ -1032,6 +1036,8 @@ struct orc_engine {
   orc_sim sim;
   orc_uni u;
   int N, cap, meshEvery, ppCount;
+  int field;
+  double gField[3], frozen, fieldInvM, fieldCpIron;
   float *pos, *vel, *aux, *q, *pos2, *vel2, *aux2, *q2, *mat;
   uint32_t *seats;
   orc_mesh pm[2];
@@ -1095,6 +1101,8 @@ static void refresh_static(orc_engine *e) {
   orc_uni keep = e->u;
   orc_make_uni(&e->sim, &e->u);
   e->u.gdt = keep.gdt; e->u.settle = keep.settle; e->u.kick = keep.kick;
+  e->u.field = keep.field; e->u.frozen = keep.frozen; memcpy(e->u.gField, keep.gField, 12);
+  e->u.invM = keep.invM; e->u.cpIron = keep.cpIron;
   memcpy(e->u.LA, keep.LA, sizeof keep.LA); memcpy(e->u.LB, keep.LB, sizeof keep.LB); e->u.boxB = keep.boxB;
   memcpy(e->u.bulk0, keep.bulk0, 12); memcpy(e->u.bulk1, keep.bulk1, 12);
   memcpy(e->u.cen0, keep.cen0, 12); memcpy(e->u.cen1, keep.cen1, 12);
@@ -1139,8 +1147,27 @@ static void pass_sim(orc_engine *e, int settle, int kick, double gdt) {
   swap_state(e);
 }
 
+void orc_engine_set_field(orc_engine *e, int on, const double g[3], double frozen, double invM, double cpIron) {
+  /* the crater page's setStaticUniforms: uGField, uFrozen, uInvM = 1, uCpIron = 1 (chicxulub.html:700-710) */
+  e->field = on;
+  orc_make_uni(&e->sim, &e->u);
+  if (on) {
+    e->u.field = 1.0f;
+    for (int k = 0; k < 3; k++) e->u.gField[k] = (float)g[k];
+    e->u.frozen = frozen < 0 ? -1.0f : (float)frozen;
+    e->u.invM = (float)invM;
+    e->u.cpIron = (float)cpIron;
+  }
+}
+
 void orc_engine_step(orc_engine *e, int settle, int kick) {
   orc_sim *s = &e->sim;
+  if (e->field) {   /* chicxulub.html:763-766: step(settle) { if (stepNo++ % 2 === 0) passSlots(); passSim(settle, dt) } */
+    int n = s->stepNo++;
+    if (n % 2 == 0) pass_slots(e);
+    pass_sim(e, settle, kick, s->dt);
+    return;
+  }
   if (!settle && !kick && !s->soft && s->t - s->impactT > 1.5) { orc_soften(s); refresh_static(e); }
   int n = s->stepNo++;
   if (n % 2 == 0) pass_slots(e);

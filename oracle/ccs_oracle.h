@@ -48,6 +48,7 @@ typedef struct {
   float invH, eps2Mesh, eps2Cell, Gm;                   /* eps2Mesh: FH^2; eps2Cell: 0.5 FH^2 */
   float LA[3], LB[3], boxB;
   float cut, a2;
+  float field, gField[3], frozen;   /* the crater page's field step: src/glsl-sim.js:466-468, 490-492, 517-533 */
 } orc_uni;
 
 /* The run's scalars (the JS `sim` object), binary64. */
@@ -126,6 +127,8 @@ orc_engine *orc_engine_new(const orc_sim *sim, const float *pos4, const float *v
 void orc_engine_free(orc_engine *e);
 orc_sim *orc_engine_sim(orc_engine *e);
 void orc_engine_step(orc_engine *e, int settle, int kick);
+/* the crater page's field-gravity step and schedule (chicxulub.html:700-710, 763-766); on = 0: the impact's */
+void orc_engine_set_field(orc_engine *e, int on, const double g[3], double frozen, double invM, double cpIron);
 void orc_engine_rigid_step(orc_engine *e, double dtF);
 void orc_engine_set_pp(orc_engine *e, const int *list, int n);
 void orc_engine_prime_mono(orc_engine *e, int box, const float mono[4]);

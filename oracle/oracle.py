@@ -44,7 +44,8 @@ class Uni(C.Structure):
                 ("cen1", C.c_float * 3), ("spin0", C.c_float * 3), ("spin1", C.c_float * 3),
                 ("invH", C.c_float), ("eps2Mesh", C.c_float), ("eps2Cell", C.c_float), ("Gm", C.c_float),
                 ("LA", C.c_float * 3), ("LB", C.c_float * 3), ("boxB", C.c_float),
-                ("cut", C.c_float), ("a2", C.c_float)]
+                ("cut", C.c_float), ("a2", C.c_float),
+                ("field", C.c_float), ("gField", C.c_float * 3), ("frozen", C.c_float)]
 
 
 class Sim(C.Structure):
@@ -151,6 +152,7 @@ def lib():
         L.orc_engine_sim.restype = C.POINTER(Sim)
         L.orc_engine_sim.argtypes = [P]
         L.orc_engine_step.argtypes = [P, C.c_int, C.c_int]
+        L.orc_engine_set_field.argtypes = [P, C.c_int, P, C.c_double, C.c_double, C.c_double]
         L.orc_engine_rigid_step.argtypes = [P, C.c_double]
         L.orc_engine_set_pp.argtypes = [P, P, C.c_int]
         L.orc_engine_prime_mono.argtypes = [P, C.c_int, P]
@@ -317,6 +319,10 @@ class Engine:
 
     def step(self, settle=False, kick=False):
         lib().orc_engine_step(self.h, int(settle), int(kick))
+
+    def set_field(self, g, frozen=-1.0, invM=1.0, cpIron=1.0, on=True):
+        gg = np.ascontiguousarray(g, np.float64)
+        lib().orc_engine_set_field(self.h, int(on), ptr(gg), float(frozen), float(invM), float(cpIron))
 
     def rigid_step(self, dtF):
         lib().orc_engine_rigid_step(self.h, dtF)
