@@ -39,7 +39,8 @@ EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_ma
            "ccs_nn_clear", "ccs_nn_pool_size", "ccs_nn_sample_state", "ccs_nn_sample_uniform", "ccs_nn_read_pool",
            "ccs_nn_train", "ccs_nn_forward", "ccs_nn_labels", "ccs_nn_grad", "ccs_set_pp_nn", "ccs_autotune",
            "ccs_ensemble_create", "ccs_ensemble_destroy", "ccs_ensemble_last_error", "ccs_ensemble_steps",
-           "ccs_ensemble_sync", "ccs_ensemble_autotune", "ccs_fof_device", "ccs_set_field"]
+           "ccs_ensemble_sync", "ccs_ensemble_autotune", "ccs_fof_device", "ccs_set_field",
+           "ccs_checkpoint_size", "ccs_checkpoint_save", "ccs_checkpoint_load"]
 NN_PARAMS = 4803
 NN_CUT_CELLS = 2.5
 
@@ -201,6 +202,9 @@ def lib():
         "ccs_ensemble_autotune": (I, [H, I, P]),
         "ccs_fof_device": (I, [H, D, D, I, I, C.POINTER(Report), P, P]),
         "ccs_set_field": (I, [H, I, P, D, D, D]),
+        "ccs_checkpoint_size": (I, [H, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "ccs_checkpoint_save": (I, [H, P, C.c_size_t, P, C.c_size_t]),
+        "ccs_checkpoint_load": (I, [H, P, C.c_size_t]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -1956,6 +1956,146 @@ int ccs_advance_host(ccs_handle *h, const float *pos4, const float *vel4, const 
   return check_launch(h);
 }
 
+// ---- checkpoint and restore ----
+namespace {
+// CRC-32 (IEEE 802.3: reflected polynomial 0xEDB88320, initial and final 0xFFFFFFFF), byte-table driven
+uint64_t crc32(const unsigned char *p, size_t n) {
+  static uint32_t table[256];
+  static std::once_flag once;
+  std::call_once(once, [] {
+    for (uint32_t i = 0; i < 256; ++i) {
+      uint32_t c = i;
+      for (int k = 0; k < 8; ++k) c = (c & 1u) ? 0xEDB88320u ^ (c >> 1) : c >> 1;
+      table[i] = c;
+    }
+  });
+  uint32_t c = 0xFFFFFFFFu;
+  for (size_t i = 0; i < n; ++i) c = table[(c ^ p[i]) & 0xFFu] ^ (c >> 8);
+  return c ^ 0xFFFFFFFFu;
+}
+size_t ckpt_payload(int N, int pp, size_t extra) {
+  return sizeof(ccs_sim) + (size_t)N * (16 + 16 + 16 + 4 + 4 + 16) + 4 * (size_t)pp + extra;
+}
+bool ckpt_boundary(const ccs_handle *h) {
+  return h->field ? h->sim.stepNo % 2 == 0 : h->sim.stepNo % h->meshEvery == 0;
+}
+}  // namespace
+
+int ccs_checkpoint_size(ccs_handle *h, size_t extraBytes, size_t *bytes) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!bytes) return CCS_E_ARG;
+  *bytes = sizeof(ccs_checkpoint_header) + ckpt_payload(h->N, h->ppCount, extraBytes);
+  return CCS_OK;
+}
+
+int ccs_checkpoint_save(ccs_handle *h, const void *extra, size_t extraBytes, void *buf, size_t cap) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!buf || (extraBytes && !extra)) return CCS_E_ARG;
+  const size_t N = (size_t)h->N, total = sizeof(ccs_checkpoint_header) + ckpt_payload(h->N, h->ppCount, extraBytes);
+  if (cap < total) {
+    h->err = "checkpoint buffer too small (ccs_checkpoint_size)";
+    return CCS_E_ARG;
+  }
+  if (!ckpt_boundary(h)) {
+    h->err = "a checkpoint is taken where the next step rebuilds the grid and the mesh (stepNo % meshEvery == 0)";
+    return CCS_E_STATE;
+  }
+  cudaSetDevice(h->device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  ccs_checkpoint_header hd;
+  std::memset(&hd, 0, sizeof hd);
+  std::memcpy(hd.magic, CCS_CKPT_MAGIC, 8);
+  hd.version = CCS_CKPT_VERSION;
+  hd.headerBytes = sizeof hd;
+  hd.simBytes = sizeof(ccs_sim);
+  hd.flags = h->field ? 2u : 0u;
+  hd.N = h->N;
+  hd.meshEvery = h->meshEvery;
+  hd.ppCount = h->ppCount;
+  hd.ppLoose = h->ppLoose;
+  for (int k = 0; k < 3; ++k) hd.field[k] = h->gField[k];
+  hd.field[3] = h->frozen;
+  hd.field[4] = h->fieldInvM;
+  hd.field[5] = h->fieldCpIron;
+  CUDA_TRY(h, cudaMemcpy(hd.monoA, h->pm[0].mono, 16, cudaMemcpyDeviceToHost));
+  CUDA_TRY(h, cudaMemcpy(hd.monoB, h->pm[1].mono, 16, cudaMemcpyDeviceToHost));
+  hd.extraBytes = extraBytes;
+  hd.payloadBytes = total - sizeof hd;
+  unsigned char *p = static_cast<unsigned char *>(buf) + sizeof hd, *p0 = p;
+  std::memcpy(p, &h->sim, sizeof(ccs_sim));
+  p += sizeof(ccs_sim);
+  const int c = h->cur;
+  CUDA_TRY(h, cudaMemcpy(p, h->pos[c], 16 * N, cudaMemcpyDeviceToHost)); p += 16 * N;
+  CUDA_TRY(h, cudaMemcpy(p, h->vel[c], 16 * N, cudaMemcpyDeviceToHost)); p += 16 * N;
+  CUDA_TRY(h, cudaMemcpy(p, h->aux[c], 16 * N, cudaMemcpyDeviceToHost)); p += 16 * N;
+  CUDA_TRY(h, cudaMemcpy(p, h->q[c], 4 * N, cudaMemcpyDeviceToHost)); p += 4 * N;
+  CUDA_TRY(h, cudaMemcpy(p, h->mat, 4 * N, cudaMemcpyDeviceToHost)); p += 4 * N;
+  CUDA_TRY(h, cudaMemcpy(p, h->home, 16 * N, cudaMemcpyDeviceToHost)); p += 16 * N;
+  if (h->ppCount) CUDA_TRY(h, cudaMemcpy(p, h->ppIndex, 4 * (size_t)h->ppCount, cudaMemcpyDeviceToHost));
+  p += 4 * (size_t)h->ppCount;
+  if (extraBytes) std::memcpy(p, extra, extraBytes);
+  p += extraBytes;
+  hd.checksum = crc32(p0, (size_t)(p - p0));
+  std::memcpy(buf, &hd, sizeof hd);
+  return CCS_OK;
+}
+
+int ccs_checkpoint_load(ccs_handle *h, const void *buf, size_t bytes) {
+  if (!h || !buf) return CCS_E_ARG;
+  ccs_checkpoint_header hd;
+  if (bytes < sizeof hd) {
+    h->err = "checkpoint: shorter than its header";
+    return CCS_E_ARG;
+  }
+  std::memcpy(&hd, buf, sizeof hd);
+  if (std::memcmp(hd.magic, CCS_CKPT_MAGIC, 8) != 0 || hd.version != CCS_CKPT_VERSION ||
+      hd.headerBytes != sizeof hd || hd.simBytes != sizeof(ccs_sim)) {
+    h->err = "checkpoint: not a version-1 checkpoint of this library's layout";
+    return CCS_E_ARG;
+  }
+  if (hd.N <= 0 || hd.N > CCS_MAX_N || hd.ppCount < 0 || hd.ppCount > CCS_PP_CAP || hd.meshEvery < 1 ||
+      hd.meshEvery > kMaxBlock || hd.payloadBytes != ckpt_payload(hd.N, hd.ppCount, hd.extraBytes) ||
+      bytes < sizeof hd + hd.payloadBytes) {
+    h->err = "checkpoint: sizes do not add up";
+    return CCS_E_ARG;
+  }
+  const unsigned char *p = static_cast<const unsigned char *>(buf) + sizeof hd;
+  if (crc32(p, hd.payloadBytes) != hd.checksum) {
+    h->err = "checkpoint: checksum mismatch";
+    return CCS_E_ARG;
+  }
+  ccs_sim sim;
+  std::memcpy(&sim, p, sizeof sim);
+  if (sim.N != hd.N) {
+    h->err = "checkpoint: sizes do not add up";
+    return CCS_E_ARG;
+  }
+  const size_t N = (size_t)hd.N;
+  // the arrays are copied out of the (possibly unaligned) buffer before they are used
+  std::vector<float> pos(4 * N), vel(4 * N), aux(4 * N), q(N), mat(N), home(4 * N);
+  std::vector<int32_t> list((size_t)hd.ppCount);
+  const unsigned char *a = p + sizeof sim;
+  std::memcpy(pos.data(), a, 16 * N); a += 16 * N;
+  std::memcpy(vel.data(), a, 16 * N); a += 16 * N;
+  std::memcpy(aux.data(), a, 16 * N); a += 16 * N;
+  std::memcpy(q.data(), a, 4 * N); a += 4 * N;
+  std::memcpy(mat.data(), a, 4 * N); a += 4 * N;
+  std::memcpy(home.data(), a, 16 * N); a += 16 * N;
+  if (hd.ppCount) std::memcpy(list.data(), a, 4 * (size_t)hd.ppCount);
+  int rc = ccs_build(h, &sim, pos.data(), vel.data(), mat.data(), home.data());
+  if (rc) return rc;
+  rc = ccs_write_state(h, nullptr, nullptr, aux.data(), q.data(), nullptr);
+  if (rc) return rc;
+  h->meshEvery = hd.meshEvery;
+  rc = ccs_set_field(h, (hd.flags & 2u) != 0, hd.field, hd.field[3], hd.field[4] > 0 ? hd.field[4] : 1.0,
+                     hd.field[5] > 0 ? hd.field[5] : 1.0);
+  if (rc) return rc;
+  if ((rc = ccs_prime_mono(h, 0, hd.monoA)) || (rc = ccs_prime_mono(h, 1, hd.monoB))) return rc;
+  return ccs_set_pp(h, list.data(), hd.ppCount, hd.ppLoose);
+}
+
 int ccs_sync(ccs_handle *h) {
   if (!h) return CCS_E_ARG;
   CUDA_TRY(h, cudaStreamSynchronize(h->st));

@@ -12,7 +12,9 @@ Errors: every failing library call raises `CCSError` (the reference throws
 dropped by generation (src/nbody.js:969,1016) exactly as the reference does.
 """
 import ctypes as C
+import json
 import math
+import os
 from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
@@ -122,6 +124,55 @@ class NBody:
     def clear_field(self):
         """Back to the giant impact's mesh step."""
         self._check(lib().ccs_set_field(self._h, 0, None, -1.0, 1.0, 1.0), "ccs_set_field")
+
+    # ---- checkpoint and restore (ccs_checkpoint_*) ---------------------------
+    def save(self, path=None):
+        """Checkpoint the run with this mirror's own analysis state (the energy reference, the cadence,
+        the last report) as the format's extra bytes.  Only where the next step rebuilds the grid and the
+        mesh (stepNo a multiple of meshEvery; even in the field step).  Returns the bytes; writes them to
+        path too when given."""
+        mine = {"ref": self.ref, "analyses": self.analyses, "analyzed_at": self.analyzed_at, "com1": self.com1,
+                "pp": self.pp, "report": bytes(self.report).hex() if self.report is not None else None}
+        extra = json.dumps(mine).encode()
+        n = C.c_size_t()
+        self._check(lib().ccs_checkpoint_size(self._h, len(extra), C.byref(n)), "ccs_checkpoint_size")
+        buf = C.create_string_buffer(n.value)
+        self._check(lib().ccs_checkpoint_save(self._h, extra, len(extra), buf, n.value), "ccs_checkpoint_save")
+        data = buf.raw
+        if path is not None:
+            with open(path, "wb") as f:
+                f.write(data)
+        return data
+
+    def load(self, src):
+        """Restore a checkpoint (bytes or a path) into this engine: the run, and the mirror's analysis
+        state when the checkpoint carries it."""
+        from . import checkpoint
+        if isinstance(src, (str, os.PathLike)):
+            with open(src, "rb") as f:
+                src = f.read()
+        data = bytes(src)
+        self._check(lib().ccs_checkpoint_load(self._h, data, len(data)), "ccs_checkpoint_load")
+        ck = checkpoint.read(data, verify=False)
+        self._mat = ck["mat"]
+        self.gen += 1
+        self.pending = None
+        self._job = None
+        self.report = None
+        self.ref = None
+        self.analyses = self.analyzed_at = 0
+        self.pp = {"count": int(ck["ppCount"]), "loose": int(ck["ppLoose"])}
+        try:
+            mine = json.loads(ck["extra"].decode()) if ck["extra"] else {}
+        except (UnicodeDecodeError, ValueError):
+            mine = {}
+        if mine:
+            self.ref = mine.get("ref")
+            self.analyses = int(mine.get("analyses", 0))
+            self.analyzed_at = int(mine.get("analyzed_at", 0))
+            self.com1 = list(mine.get("com1", self.com1))
+            if mine.get("report"):
+                self.report = L.Report.from_buffer_copy(bytes.fromhex(mine["report"]))
 
     @property
     def sim(self):

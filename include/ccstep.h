@@ -326,6 +326,34 @@ int ccs_pass_diag(ccs_handle *h);
 int ccs_advance_host(ccs_handle *h, const float *pos4, const float *vel4, const float *q, int nsteps,
                      float *pos4_out, float *vel4_out, float *aux4_out, float *q_out);
 
+/* ---- checkpoint and restore (no counterpart in the reference: its runTo
+ * replays a run from the build, index.html:592-600) ----
+ * A run's whole state at a step whose successor rebuilds everything derived
+ * from it -- the contact grid, the mesh and the pairwise pass: stepNo a
+ * multiple of meshEvery for the impact's step, an even stepNo for the field
+ * step; elsewhere ccs_checkpoint_save returns CCS_E_STATE.  Restored into any
+ * handle, the run continues as the saved one would (to the rounding of the
+ * float atomics that sum contacts and deposits).  Layout, little-endian:
+ * this header; the ccs_sim struct (simBytes); pos4, vel4, aux4 (16 B a
+ * particle each), q, mat (4 B each), home4 (16 B); the loose list (4 B x
+ * ppCount); the caller's own bytes (extraBytes, e.g. its analysis state).
+ * checksum = the CRC-32 of zlib (IEEE 802.3 polynomial, reflected, initial
+ * and final value 0xFFFFFFFF) of everything after the header. */
+#define CCS_CKPT_MAGIC "CCSCKPT1"
+#define CCS_CKPT_VERSION 1u
+typedef struct {
+  char magic[8];
+  uint32_t version, headerBytes, simBytes, flags;   /* flags: 2 = the field step is on */
+  int32_t N, meshEvery, ppCount, ppLoose;
+  double field[6];                                  /* ccs_set_field's g[3], frozen, invM, cpIron */
+  float monoA[4], monoB[4];                         /* the boxes' monopoles (the strays' pull, src/glsl-sim.js:196-206) */
+  uint64_t extraBytes, payloadBytes, checksum;      /* payloadBytes: everything after the header */
+} ccs_checkpoint_header;
+int ccs_checkpoint_size(ccs_handle *h, size_t extraBytes, size_t *bytes);
+int ccs_checkpoint_save(ccs_handle *h, const void *extra, size_t extraBytes, void *buf, size_t cap);
+/* rebuilds the handle's run from buf (as ccs_build does) and restores the rest */
+int ccs_checkpoint_load(ccs_handle *h, const void *buf, size_t bytes);
+
 /* ---- timing helpers for the benchmark ---- */
 int ccs_sync(ccs_handle *h);
 /* average device time (ms) of the kernels named by `kernel` launched since the
