@@ -9,14 +9,15 @@
 // leaves most of each warp idle.  So the warp works in three stages that keep
 // its lanes busy:
 //   1. cells: the warp walks the 27 offsets in lockstep; each lane applies its
-//      nearest-point test, loads its cell's seats and appends the occupied
-//      seats to a per-warp queue in shared memory;
+//      nearest-point test, loads its cell's seats, applies the reference's
+//      quantised seat cull to each (where the seat sat at the rebuild, to a
+//      fifteenth of a cell: beyond reach, the reference never fetches it)
+//      and appends the seats that pass to a per-warp queue in shared memory;
 //   2. candidates: 32 queued seats at a time, one per lane: load the
 //      neighbour's position and keep the pairs inside the link radius;
-//   3. neighbours: 32 at a time: the reference's quantised seat cull (which
-//      only ever saves it a fetch, so it is applied where it can matter),
-//      the neighbour count, and for touching pairs the spring-dashpot, its
-//      heat and the conduction, added into the owner's slots.
+//   3. neighbours: 32 at a time: the neighbour count, and for touching pairs
+//      the spring-dashpot, its heat and the conduction, added into the
+//      owner's slots.
 // The pair set and the neighbour counts are decided with exact arithmetic and
 // integer counts; force, dissipation and heat flow are summed in whatever
 // order the shared-memory atomics land, to tolerance.
@@ -38,28 +39,19 @@ struct ContactWarp {
   float ci[32];        // owner heat capacity
   float fx[32], fy[32], fz[32], lost[32], flow[32];   // what the contacts add up, per owner
   int nb[32];
-  uint2 q[kQCap];      // x: seat word; y: owner | offset code << 5
-  uint4 nq[kNCap];     // x: seat word; y: owner | code << 5; z: r^2 bits
+  uint2 q[kQCap];      // x: seat word; y: owner
+  uint4 nq[kNCap];     // x: seat word; y: owner; z: r^2 bits
 };
 
-// offset code: dx | dy << 2 | dz << 4 (each 0..2 for -1..+1)
-__device__ __forceinline__ void drain_neighbours(const ccs_uniforms &u, const SimArgs &a, const float *spc,
-                                                 ContactWarp &w, int base, int n, int lane) {
+__device__ __forceinline__ void drain_neighbours(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, int base,
+                                                 int n, int lane) {
   if (lane < n) {
     const uint4 e = w.nq[base + lane];
     const uint32_t sv = e.x;
     const int o = (int)(e.y & 31u);
-    const int code = (int)(e.y >> 5);
     const float r2 = __uint_as_float(e.z);
     const float4 Po = w.P[o], C0 = w.C0[o];
-    const float cell = u.cell;
-    // where it sat at the rebuild, to a fifteenth of a cell: beyond reach, the reference never fetched it
-    const float lox = xadd(C0.x, xmul((float)((code & 3) - 1), cell));
-    const float loy = xadd(C0.y, xmul((float)(((code >> 2) & 3) - 1), cell));
-    const float loz = xadd(C0.z, xmul((float)((code >> 4) - 1), cell));
-    const f3 dq = mk(xsub(xadd(lox, spc[(sv >> 18) & 15u]), Po.x), xsub(xadd(loy, spc[(sv >> 22) & 15u]), Po.y),
-                     xsub(xadd(loz, spc[(sv >> 26) & 15u]), Po.z));
-    if (!(xdot(dq, dq) > u.reach2)) {
+    {
       atomicAdd(&w.nb[o], 1);
       const float r = __fsqrt_rn(r2);
       if (xsub(u.touch, r) > 0.0f) {
@@ -89,7 +81,7 @@ __device__ __forceinline__ void drain_neighbours(const ccs_uniforms &u, const Si
 
 // stage 2: queued seats, two per lane when there are 64 (two position loads in flight), else one
 // (lanes >= n idle); pairs inside the link radius go on to stage 3
-__device__ __forceinline__ void push_near(const ccs_uniforms &u, const SimArgs &a, const float *spc, ContactWarp &w,
+__device__ __forceinline__ void push_near(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w,
                                           bool near, uint2 e, float r2, int lane, int &nn) {
   const unsigned bal = __ballot_sync(0xFFFFFFFFu, near);
   if (near) w.nq[nn + __popc(bal & ((1u << lane) - 1u))] = make_uint4(e.x, e.y, __float_as_uint(r2), 0u);
@@ -97,12 +89,12 @@ __device__ __forceinline__ void push_near(const ccs_uniforms &u, const SimArgs &
   __syncwarp();
   if (nn >= 32) {
     nn -= 32;
-    drain_neighbours(u, a, spc, w, nn, 32, lane);
+    drain_neighbours(u, a, w, nn, 32, lane);
   }
 }
 
-__device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const SimArgs &a, const float *spc,
-                                                 ContactWarp &w, int base, int n, int lane, int &nn) {
+__device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, int base,
+                                                 int n, int lane, int &nn) {
   const bool two = n == 64;
   bool near0 = false, near1 = false;
   uint2 e0 = make_uint2(0u, 0u), e1 = e0;
@@ -124,8 +116,8 @@ __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const Si
     }
   }
   __syncwarp();   // every lane has read its entries before the queue is written again
-  push_near(u, a, spc, w, near0, e0, r20, lane, nn);
-  if (two) push_near(u, a, spc, w, near1, e1, r21, lane, nn);
+  push_near(u, a, w, near0, e0, r20, lane, nn);
+  if (two) push_near(u, a, w, near1, e1, r21, lane, nn);
 }
 
 // W warps per CTA (8 or 4: the autotuner's choice; 4 CTAs of 8 or 8 of 4 share an SM); FIELD: the crater
@@ -195,7 +187,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
           s0 = __ldg(cp);       // both halves of the cell: one 32-byte sector, one round trip
           s1 = __ldg(cp + 1);
         }
-        const uint32_t tag = (uint32_t)lane | ((uint32_t)(dx | dy << 2 | dz << 4) << 5);
+        const uint32_t tag = (uint32_t)lane;
         const bool more = __any_sync(0xFFFFFFFFu, !(s0.w & 0x80000000u));   // any cell with more than four?
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
@@ -204,7 +196,13 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
           const uint32_t sv[4] = {s.x, s.y, s.z, s.w};
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
-            const bool seat = !(sv[k] & 0x80000000u) && (int)(sv[k] & 0x3FFFFu) != me;
+            bool seat = !(sv[k] & 0x80000000u) && (int)(sv[k] & 0x3FFFFu) != me;
+            if (seat) {   // the quantised cull: where the seat sat at the rebuild, against this particle now
+              const f3 dq = mk(xsub(xadd(lx, spc[(sv[k] >> 18) & 15u]), p.x),
+                               xsub(xadd(ly, spc[(sv[k] >> 22) & 15u]), p.y),
+                               xsub(xadd(lz, spc[(sv[k] >> 26) & 15u]), p.z));
+              seat = !(xdot(dq, dq) > u.reach2);
+            }
             const unsigned bal = __ballot_sync(0xFFFFFFFFu, seat);
             if (seat) w.q[qn + __popc(bal & ((1u << lane) - 1u))] = make_uint2(sv[k], tag);
             qn += __popc(bal);
@@ -213,17 +211,17 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
         __syncwarp();
         while (qn >= 64) {
           qn -= 64;
-          drain_candidates(u, a, spc, w, qn, 64, lane, nn);
+          drain_candidates(u, a, w, qn, 64, lane, nn);
         }
       }
     }
   }
   if (qn >= 32) {
     qn -= 32;
-    drain_candidates(u, a, spc, w, qn, 32, lane, nn);
+    drain_candidates(u, a, w, qn, 32, lane, nn);
   }
-  if (qn > 0) drain_candidates(u, a, spc, w, 0, qn, lane, nn);
-  if (nn > 0) drain_neighbours(u, a, spc, w, 0, nn, lane);
+  if (qn > 0) drain_candidates(u, a, w, 0, qn, lane, nn);
+  if (nn > 0) drain_neighbours(u, a, w, 0, nn, lane);
   __syncwarp();
   if (!live) return;
   const f3 push = mk(w.fx[lane], w.fy[lane], w.fz[lane]);
