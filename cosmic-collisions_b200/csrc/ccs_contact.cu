@@ -39,17 +39,17 @@ struct ContactWarp {
   float ci[32];        // owner heat capacity
   float fx[32], fy[32], fz[32], lost[32], flow[32];   // what the contacts add up, per owner
   int nb[32];
-  uint2 q[kQCap];      // x: seat word; y: owner
-  uint4 nq[kNCap];     // x: seat word; y: owner; z: r^2 bits
+  uint32_t q[kQCap];   // particle index | owner << 18
+  uint2 nq[kNCap];     // x: particle index | owner << 18; y: r^2 bits
 };
 
 __device__ __forceinline__ void drain_neighbours(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, int base,
                                                  int n, int lane) {
   if (lane < n) {
-    const uint4 e = w.nq[base + lane];
+    const uint2 e = w.nq[base + lane];
     const uint32_t sv = e.x;
-    const int o = (int)(e.y & 31u);
-    const float r2 = __uint_as_float(e.z);
+    const int o = (int)(e.x >> 18);
+    const float r2 = __uint_as_float(e.y);
     const float4 Po = w.P[o], C0 = w.C0[o];
     {
       atomicAdd(&w.nb[o], 1);
@@ -82,9 +82,9 @@ __device__ __forceinline__ void drain_neighbours(const ccs_uniforms &u, const Si
 // stage 2: queued seats, two per lane when there are 64 (two position loads in flight), else one
 // (lanes >= n idle); pairs inside the link radius go on to stage 3
 __device__ __forceinline__ void push_near(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w,
-                                          bool near, uint2 e, float r2, int lane, int &nn) {
+                                          bool near, uint32_t e, float r2, int lane, int &nn) {
   const unsigned bal = __ballot_sync(0xFFFFFFFFu, near);
-  if (near) w.nq[nn + __popc(bal & ((1u << lane) - 1u))] = make_uint4(e.x, e.y, __float_as_uint(r2), 0u);
+  if (near) w.nq[nn + __popc(bal & ((1u << lane) - 1u))] = make_uint2(e, __float_as_uint(r2));
   nn += __popc(bal);
   __syncwarp();
   if (nn >= 32) {
@@ -97,19 +97,19 @@ __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const Si
                                                  int n, int lane, int &nn) {
   const bool two = n == 64;
   bool near0 = false, near1 = false;
-  uint2 e0 = make_uint2(0u, 0u), e1 = e0;
+  uint32_t e0 = 0u, e1 = 0u;
   float r20 = 0.0f, r21 = 0.0f;
   if (lane < n) {
     e0 = w.q[base + lane];
     if (two) e1 = w.q[base + 32 + lane];
-    const float4 Pj0 = __ldg(a.pos + (e0.x & 0x3FFFFu));
-    const float4 Pj1 = two ? __ldg(a.pos + (e1.x & 0x3FFFFu)) : Pj0;
-    const float4 Po0 = w.P[e0.y & 31u];
+    const float4 Pj0 = __ldg(a.pos + (e0 & 0x3FFFFu));
+    const float4 Pj1 = two ? __ldg(a.pos + (e1 & 0x3FFFFu)) : Pj0;
+    const float4 Po0 = w.P[e0 >> 18];
     const f3 d0 = xsub3(xyz(Pj0), xyz(Po0));
     r20 = xdot(d0, d0);
     near0 = r20 < u.link2;
     if (two) {
-      const float4 Po1 = w.P[e1.y & 31u];
+      const float4 Po1 = w.P[e1 >> 18];
       const f3 d1 = xsub3(xyz(Pj1), xyz(Po1));
       r21 = xdot(d1, d1);
       near1 = r21 < u.link2;
@@ -187,7 +187,6 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
           s0 = __ldg(cp);       // both halves of the cell: one 32-byte sector, one round trip
           s1 = __ldg(cp + 1);
         }
-        const uint32_t tag = (uint32_t)lane;
         const bool more = __any_sync(0xFFFFFFFFu, !(s0.w & 0x80000000u));   // any cell with more than four?
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
@@ -204,7 +203,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
               seat = !(xdot(dq, dq) > u.reach2);
             }
             const unsigned bal = __ballot_sync(0xFFFFFFFFu, seat);
-            if (seat) w.q[qn + __popc(bal & ((1u << lane) - 1u))] = make_uint2(sv[k], tag);
+            if (seat) w.q[qn + __popc(bal & ((1u << lane) - 1u))] = (sv[k] & 0x3FFFFu) | ((uint32_t)lane << 18);
             qn += __popc(bal);
           }
         }
