@@ -63,9 +63,7 @@ struct ccs_handle {
   bool field = false;
   double gField[3] = {0, 0, 0}, frozen = -1, fieldInvM = 1, fieldCpIron = 1;
   // per-step uniform ring (direct launches)
-  ccs_uniforms *uniDev = nullptr, *uniHost = nullptr;
-  cudaEvent_t uniEv[kRing] = {};
-  bool uniUsed[kRing] = {};
+  ccs_uniforms *uniDev = nullptr;
   int uniNext = 0;
   // particle state, double-buffered (sim.src / sim.dst)
   float4 *pos[2] = {}, *vel[2] = {}, *aux[2] = {};
@@ -114,7 +112,7 @@ struct ccs_handle {
   // launch shapes chosen by ccs_autotune: contact-step warps per CTA, cell-gravity threads per cell
   int tuneWarps = 8, tuneSplit = 4;
   // timing of chosen kernels with events on the stream
-  bool timing = false;
+  int timing = 0;                       // ccs_timing's mask of kernel ids
   std::vector<cudaEvent_t> evPool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> evRecs;
   size_t evNext = 0;
@@ -274,15 +272,20 @@ void soften(ccs_handle *h) {
 }
 
 // a ring slot holding u on the device (direct path)
+// a pass's uniforms into the next ring slot, as a kernel's by-value argument: in stream order with the
+// kernels that read them, with no copy engine, pinned staging or host wait in between
+__global__ void k_put_uniforms(const ccs_uniforms u, ccs_uniforms *dst) {
+  static_assert(sizeof(ccs_uniforms) % 4 == 0, "uniforms are whole words");
+  const uint32_t *s = reinterpret_cast<const uint32_t *>(&u);
+  uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(ccs_uniforms) / 4); i += blockDim.x) d[i] = s[i];
+}
+
 int push_uniforms(ccs_handle *h, const ccs_uniforms &u, const ccs_uniforms **dev) {
   const int slot = h->uniNext;
   h->uniNext = (h->uniNext + 1) % kRing;
-  if (h->uniUsed[slot]) CUDA_TRY(h, cudaEventSynchronize(h->uniEv[slot]));
-  h->uniHost[slot] = u;
-  CUDA_TRY(h, cudaMemcpyAsync(h->uniDev + slot, h->uniHost + slot, sizeof(ccs_uniforms), cudaMemcpyHostToDevice,
-                              h->st));
-  CUDA_TRY(h, cudaEventRecord(h->uniEv[slot], h->st));
-  h->uniUsed[slot] = true;
+  k_put_uniforms<<<1, 128, 0, h->st>>>(u, h->uniDev + slot);
+  h->launches += 1;
   *dev = h->uniDev + slot;
   return CCS_OK;
 }
@@ -290,7 +293,7 @@ int push_uniforms(ccs_handle *h, const ccs_uniforms &u, const ccs_uniforms **dev
 // timing brackets around chosen kernels
 void time_begin(ccs_handle *h, int kernel, cudaEvent_t *b, cudaEvent_t *e) {
   *b = *e = nullptr;
-  if (!h->timing) return;
+  if (!((h->timing >> kernel) & 1)) return;
   if (h->evNext + 2 > h->evPool.size()) {
     for (int k = 0; k < 256; ++k) {
       cudaEvent_t ev;
@@ -439,7 +442,7 @@ StepPlan plan_step(ccs_handle *h, int settle, int kick) {
   return p;
 }
 
-// a block's launches counted as the direct path would count them
+// the kernels a captured block launches (its uniforms come by one memcpy node, not a kernel)
 int block_launches(const ccs_handle *h, const StepPlan *plans, int M) {
   int per = 0;
   for (int k = 0; k < M; ++k) {
@@ -503,8 +506,8 @@ int graph_block(ccs_handle *h) {
     CUDA_TRY(h, cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
     std::memcpy(g.host, us, sizeof(ccs_uniforms) * M);
     cudaGraph_t graph;
-    const bool timing = h->timing;
-    h->timing = false;
+    const int timing = h->timing;
+    h->timing = 0;
     const int64_t l0 = h->launches;
     CUDA_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
     cudaMemcpyAsync(g.dev, g.host, sizeof(ccs_uniforms) * M, cudaMemcpyHostToDevice, h->st);
@@ -625,13 +628,11 @@ int ccs_create(int device, ccs_handle **out) {
     delete h;
     return CCS_E_CUDA;
   }
-  if (cudaMalloc(&h->uniDev, sizeof(ccs_uniforms) * kRing) != cudaSuccess ||
-      cudaMallocHost(&h->uniHost, sizeof(ccs_uniforms) * kRing) != cudaSuccess) {
+  if (cudaMalloc(&h->uniDev, sizeof(ccs_uniforms) * kRing) != cudaSuccess) {
     cudaStreamDestroy(h->st);
     delete h;
     return CCS_E_NOMEM;
   }
-  for (int k = 0; k < kRing; ++k) cudaEventCreateWithFlags(&h->uniEv[k], cudaEventDisableTiming);
   if (init_kernels() != cudaSuccess) {
     h->err = "kernel attributes could not be set";
   }
@@ -645,12 +646,9 @@ int ccs_destroy(ccs_handle *h) {
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->st);
   free_state(h);
-  for (int k = 0; k < kRing; ++k)
-    if (h->uniEv[k]) cudaEventDestroy(h->uniEv[k]);
   for (auto ev : h->evPool) cudaEventDestroy(ev);
   if (h->readEv) cudaEventDestroy(h->readEv);
   if (h->uniDev) cudaFree(h->uniDev);
-  if (h->uniHost) cudaFreeHost(h->uniHost);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
   return CCS_OK;
@@ -882,8 +880,8 @@ int ccs_autotune(ccs_handle *h, int reps, int choice[2]) {
     const ccs_uniforms *U;
     rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
     if (rc) return rc;
-    const bool timing = h->timing;
-    h->timing = false;
+    const int timing = h->timing;
+    h->timing = 0;
     const int64_t l0 = h->launches;
     // the contact step into the spare buffers (no state changes), at each CTA width
     const SimArgs a = sim_args(h);
@@ -1000,9 +998,9 @@ int ensemble_block(ccs_ensemble *e, int R) {
     cudaEventRecord(e->fork, e->st);
     for (int i = 0; i < n; ++i) {   // every member's block on its own stream: parallel branches
       ccs_handle *h = e->m[i];
-      const bool timing = h->timing;
+      const int timing = h->timing;
       const int64_t l0 = h->launches;
-      h->timing = false;
+      h->timing = 0;
       cudaStreamWaitEvent(h->st, e->fork, 0);
       cudaMemcpyAsync(g.dev[i], g.host[i], sizeof(ccs_uniforms) * M, cudaMemcpyHostToDevice, h->st);
       for (int k = 0; k < M; ++k) enqueue_step(h, plans[i][k], g.dev[i] + k);
@@ -2106,7 +2104,7 @@ int ccs_sync(ccs_handle *h) {
 int ccs_timing(ccs_handle *h, int enable) {
   if (!h) return CCS_E_ARG;
   time_collect(h);
-  h->timing = enable != 0;
+  h->timing = enable & ((1 << kTimedKernels) - 1);
   for (int k = 0; k < kTimedKernels; ++k) {
     h->tAcc[k] = 0;
     h->tCount[k] = 0;

@@ -358,7 +358,11 @@ int ccs_checkpoint_load(ccs_handle *h, const void *buf, size_t bytes);
 int ccs_sync(ccs_handle *h);
 /* average device time (ms) of the kernels named by `kernel` launched since the
  * last reset, measured with CUDA events on the handle's stream; kernel ids:
- * 0 contact step (simulate), 1 contact grid, 2 deposit, 3 cell, 4 P3M force */
+ * 0 contact step (simulate), 1 contact grid, 2 deposit, 3 cell, 4 P3M force.
+ * `enable` is a mask of the ids to time (bit k for id k; CCS_TIME_ALL for all,
+ * 0 for none): each timed launch records two events, which widen the gap
+ * before and after it by a microsecond or two. */
+#define CCS_TIME_ALL 0x1F
 int ccs_timing(ccs_handle *h, int enable);
 int ccs_timing_read(ccs_handle *h, int kernel, double *total_ms, int *launches);
 /* kernels launched by this handle since creation (the benchmark's gpu_launches) */
