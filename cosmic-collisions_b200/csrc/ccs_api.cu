@@ -585,7 +585,7 @@ void free_state(ccs_handle *h) {
     dev_free(m.fine); dev_free(m.force); dev_free(m.coarse); dev_free(m.farA); dev_free(m.farT0);
     dev_free(m.farT1); dev_free(m.mono); dev_free(m.partial); dev_free(m.counter);
     dev_free(m.occ); dev_free(m.occIdx); dev_free(m.occN); dev_free(m.occBlocks); dev_free(m.occCount);
-    dev_free(m.occAsc); dev_free(m.occAscN);
+    dev_free(m.occAsc); dev_free(m.occAscN); dev_free(m.cellPart); dev_free(m.cellDone);
   }
   dev_free(h->mat); dev_free(h->matTmp); dev_free(h->home); dev_free(h->homeTmp);
   dev_free(h->ppIndex); dev_free(h->ppSlot); dev_free(h->ppList); dev_free(h->ppForce); dev_free(h->ppBox);
@@ -692,6 +692,7 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
     rc |= dev_alloc(h, &m.occN, kCoarse);
     rc |= dev_alloc(h, &m.occBlocks, kCoarse); rc |= dev_alloc(h, &m.occCount, 1);
     rc |= dev_alloc(h, &m.occAsc, kCoarse); rc |= dev_alloc(h, &m.occAscN, 1);
+    rc |= dev_alloc(h, &m.cellPart, (size_t)kCoarse * kCellChunks * 64); rc |= dev_alloc(h, &m.cellDone, kCoarse);
   }
   rc |= dev_alloc(h, &h->ppIndex, CCS_PP_CAP); rc |= dev_alloc(h, &h->ppSlot, N);
   rc |= dev_alloc(h, &h->ppList, CCS_PP_CAP); rc |= dev_alloc(h, &h->ppForce, 4 * CCS_PP_CAP);
@@ -738,6 +739,7 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
     CUDA_TRY(h, cudaMemsetAsync(m.occN, 0, sizeof(int) * kCoarse, st));
     CUDA_TRY(h, cudaMemsetAsync(m.occCount, 0, sizeof(int), st));
     CUDA_TRY(h, cudaMemsetAsync(m.occAscN, 0, sizeof(int), st));
+    CUDA_TRY(h, cudaMemsetAsync(m.cellDone, 0, sizeof(int) * kCoarse, st));
     CUDA_TRY(h, cudaMemsetAsync(m.force, 0, sizeof(float4) * (kFine + 1), st));
   }
   h->launches += launch_fill_u32((uint32_t *)h->ppIndex, CCS_PP_CAP, 0xFFFFFFFFu, st);

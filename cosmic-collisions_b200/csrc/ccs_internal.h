@@ -13,6 +13,7 @@ constexpr uint32_t kEmpty = CCS_SEAT_EMPTY;   // -1.0f bit pattern: an empty sea
 constexpr uint32_t kNoCell = 0xFFFFFFFFu;     // no cell recorded for this particle
 constexpr int kFine = 64 * 64 * 64;           // 64^3 mesh; index kFine is the scratch texel
 constexpr int kCoarse = 4096;                 // 16^3 blocks
+constexpr int kCellChunks = 8;                // CTAs of the cell pass per occupied block, each a source chunk
 constexpr int kSeats = CCS_SEATS;
 constexpr unsigned kStatusGrid = 1u;          // a contact-cell insertion gave up (degenerate pile)
 constexpr unsigned kStatusNN = 2u;            // a tensor-core wait of the learned P3M pass gave up
@@ -63,6 +64,8 @@ struct MeshBuf {
   int *occCount = nullptr;     // ... and how many
   int *occAsc = nullptr;       // the occupied coarse blocks in ascending order ...
   int *occAscN = nullptr;      // ... and how many
+  float4 *cellPart = nullptr;  // the cell pass's partial sums: [listed block][source chunk][cell]
+  int *cellDone = nullptr;     // per listed block: the chunks done (the last one adds them up)
 };
 
 // Arguments of the contact step (simFS, src/glsl-sim.js:354-512).

@@ -322,21 +322,25 @@ int launch_far(const MeshBuf &m, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// cell gravity: src/glsl-sim.js:303-352.  A persistent grid walks the
-// occupied coarse blocks the coarse pass listed (the force mesh is cleared
-// before, so empty blocks and empty cells read zero); a CTA takes one block
-// at a time and gives each of its 64 fine cells SPLIT threads.  It reads how
-// many occupied cells each of the 5^3 blocks around it holds, then copies the
-// occupied cells of all of them -- centre of mass and mass, as the coarse pass
-// listed them, block by block in the reference's order -- into shared memory
-// in one pass of independent loads (in batches of kCellBatch when the
-// neighbourhood holds more).  A block in the bodies sees thousands of
-// sources, so each occupied cell's sum is split over its SPLIT threads (every
-// SPLIT-th source; 2, 4 or 8, the autotuner's choice), and the partial sums
-// are added in a fixed order: the result is deterministic for a given SPLIT.
-// A cell skips itself.  Then the block's far field is carried to the cell by
-// the tidal tensor.  Cell-on-cell pulls are fast arithmetic (rsqrt, FMA).
+// cell gravity: src/glsl-sim.js:303-352.  Every occupied coarse block the
+// coarse pass listed is split into kCellChunks work items, one CTA each: the
+// item reads how many occupied cells each of the 5^3 blocks around its block
+// holds (a warp scan gives where each one's cells start in the
+// neighbourhood's list), takes its share of that list -- centre of mass and
+// mass, as the coarse pass listed them, block by block in the reference's
+// order -- into shared memory, and sums it onto each of the block's occupied
+// cells with SPLIT threads a cell (every SPLIT-th source; 2, 4 or 8, the
+// autotuner's choice).  The partial sums of a chunk are added in a fixed
+// order and written out; the last of the block's CTAs to finish adds the
+// chunks in chunk order, carries the block's far field to each cell by the
+// tidal tensor and writes the force (the force mesh is cleared before, so
+// empty cells read zero).  The result is deterministic for a given SPLIT.
+// A block near the bodies sees about 1,500 occupied cells while only some 60
+// blocks are occupied at all, so splitting a block's sources over CTAs is
+// what keeps the SMs busy.  A cell skips itself.  Cell-on-cell pulls are fast
+// arithmetic (rsqrt, FMA).
 // ---------------------------------------------------------------------------
+namespace {
 constexpr int kCellBatch = 1024;
 
 template <int SPLIT>
@@ -350,26 +354,47 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restr
                                                      const int *__restrict__ occCount,
                                                      const float4 *__restrict__ farA,
                                                      const float4 *__restrict__ farT0,
-                                                     const float4 *__restrict__ farT1, float4 *__restrict__ force) {
+                                                     const float4 *__restrict__ farT1, float4 *__restrict__ force,
+                                                     float4 *__restrict__ cellPart, int *__restrict__ cellDone) {
   constexpr int kCellThreads = 64 * SPLIT;
-  __shared__ int nbK[125], nbOff[126];
+  __shared__ int nbK[128], nbOff[129];
   __shared__ float4 src[kCellBatch];
   __shared__ uint8_t sidx[kCellBatch];   // a source's place in its block; 255 for another block's cells
   __shared__ float4 part[SPLIT][64];
-  const int t = threadIdx.x, cellT = t & 63, q = t >> 6;
+  __shared__ int last;
+  const int t = threadIdx.x, cellT = t & 63, q = t >> 6, lane = t & 31;
   if (blockIdx.x == 0 && t == 0) force[kFine] = fine[kFine];   // the scratch texel, carried through
   const float eps2 = U->eps2Cell, Gm = U->Gm;
-  const int nBlocks = *occCount;
-  for (int bi = blockIdx.x; bi < nBlocks; bi += gridDim.x) {
+  const int items = *occCount * kCellChunks;
+  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+    const int bi = it / kCellChunks, chunk = it % kCellChunks;
     const int blk = occBlocks[bi];
     const int ccx = blk & 15, ccy = (blk >> 4) & 15, ccz = blk >> 8;
-    const float4 mb = coarse[blk];
-    for (int o = t; o < 125; o += kCellThreads) {   // o = kx + 5 ky + 25 kz: the reference's loop order
-      const int kx = ccx + o % 5 - 2, ky = ccy + (o / 5) % 5 - 2, kz = ccz + o / 25 - 2;
-      const bool in = kx >= 0 && ky >= 0 && kz >= 0 && kx <= 15 && ky <= 15 && kz <= 15;
-      const int k = in ? coarse_index(kx, ky, kz) : 0;
-      nbK[o] = k;
-      nbOff[o + 1] = in ? __ldg(occN + k) : 0;
+    if (t < 32) {   // the 125 neighbour blocks (o = kx + 5 ky + 25 kz: the reference's loop order), 4 a lane
+      int n[4], run = 0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int o = lane * 4 + r;
+        const int kx = ccx + o % 5 - 2, ky = ccy + (o / 5) % 5 - 2, kz = ccz + o / 25 - 2;
+        const bool in = o < 125 && kx >= 0 && ky >= 0 && kz >= 0 && kx <= 15 && ky <= 15 && kz <= 15;
+        const int k = in ? coarse_index(kx, ky, kz) : 0;
+        nbK[o] = k;
+        n[r] = in ? __ldg(occN + k) : 0;
+        run += n[r];
+      }
+      int incl = run;   // where each lane's four start: an exclusive scan over the lanes
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) incl += y;
+      }
+      int at = incl - run;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        nbOff[lane * 4 + r] = at;
+        at += n[r];
+      }
+      if (lane == 31) nbOff[128] = at;
     }
     // the cellT-th occupied cell of the block, so the busy lanes sit together
     const int nOwn = __ldg(occN + blk);
@@ -380,15 +405,12 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restr
     f3 acc = mk(0, 0, 0);
     float pot = 0.0f;
     __syncthreads();
-    if (t == 0) {   // where each neighbour block's cells start in the neighbourhood's list
-      nbOff[0] = 0;
-      for (int o = 0; o < 125; ++o) nbOff[o + 1] += nbOff[o];
-    }
-    __syncthreads();
     const int total = nbOff[125];
-    for (int b0 = 0; b0 < total; b0 += kCellBatch) {
-      const int b1 = min(b0 + kCellBatch, total);
-      // the neighbour blocks' cells in [b0, b1): every load independent of the others
+    const int c0 = (int)((long long)total * chunk / kCellChunks);
+    const int c1 = (int)((long long)total * (chunk + 1) / kCellChunks);
+    for (int b0 = c0; b0 < c1; b0 += kCellBatch) {
+      const int b1 = min(b0 + kCellBatch, c1);
+      // this chunk's sources in [b0, b1): every load independent of the others
       for (int o = 0; o < 125; ++o) {
         const int lo = max(nbOff[o], b0), hi = min(nbOff[o + 1], b1);
         if (lo >= hi) continue;
@@ -416,6 +438,7 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restr
     }
     part[q][cellT] = make_float4(acc.x, acc.y, acc.z, pot);
     __syncthreads();
+    float4 *out = cellPart + ((size_t)bi * kCellChunks + chunk) * 64;
     if (mine && q == 0) {
 #pragma unroll
       for (int k = 1; k < SPLIT; ++k) {
@@ -423,18 +446,43 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restr
         acc = acc + mk(p.x, p.y, p.z);
         pot += p.w;
       }
-      const float4 fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
-      const f3 d = x - xyz(mb) * fdiv(1.0f, mb.w);
-      const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
-                       t1.x * d.x + t1.y * d.y + t0.z * d.z);
-      acc = acc + (xyz(fa) + Td);
-      pot += fa.w - dot(xyz(fa), d) - 0.5f * dot(d, Td);
-      force[fine_index(ccx * 4 + (tl & 3), ccy * 4 + ((tl >> 2) & 3), ccz * 4 + (tl >> 4))] =
-          make_float4(acc.x * Gm, acc.y * Gm, acc.z * Gm, pot * Gm);
+      __stcg(out + cellT, make_float4(acc.x, acc.y, acc.z, pot));
     }
-    __syncthreads();   // the shared arrays are the next block's
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(cellDone + bi, 1) == kCellChunks - 1;
+    __syncthreads();
+    if (last) {   // every chunk of this block is in: add them in chunk order, then the far field
+      __threadfence();
+      if (mine && q == 0) {
+        const float4 *pb = cellPart + (size_t)bi * kCellChunks * 64;
+        float4 s = __ldcg(pb + cellT);
+#pragma unroll
+        for (int c = 1; c < kCellChunks; ++c) {
+          const float4 p = __ldcg(pb + (size_t)c * 64 + cellT);
+          s.x += p.x;
+          s.y += p.y;
+          s.z += p.z;
+          s.w += p.w;
+        }
+        f3 a3 = mk(s.x, s.y, s.z);
+        float pt = s.w;
+        const float4 mb = coarse[blk];
+        const float4 fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
+        const f3 d = x - xyz(mb) * fdiv(1.0f, mb.w);
+        const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
+                         t1.x * d.x + t1.y * d.y + t0.z * d.z);
+        a3 = a3 + (xyz(fa) + Td);
+        pt += fa.w - dot(xyz(fa), d) - 0.5f * dot(d, Td);
+        force[fine_index(ccx * 4 + (tl & 3), ccy * 4 + ((tl >> 2) & 3), ccz * 4 + (tl >> 4))] =
+            make_float4(a3.x * Gm, a3.y * Gm, a3.z * Gm, pt * Gm);
+      }
+      if (t == 0) cellDone[bi] = 0;   // ready for the next pass
+    }
+    __syncthreads();   // the shared arrays are the next item's
   }
 }
+}  // namespace
 
 int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int split) {
   static int sms = 0;
@@ -444,18 +492,18 @@ int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int sp
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (sms <= 0) sms = 148;
   }
-  // a persistent grid: four CTAs of 512 threads fill an SM, proportionally more of smaller ones
+  // a persistent grid over (block, chunk) items: four CTAs of 512 threads fill an SM, more of smaller ones
   const int grid = sms * (split == 2 ? 16 : split == 4 ? 8 : 4);
   cudaMemsetAsync(m.force, 0, sizeof(float4) * kFine, st);
   if (split == 2)
     k_cell<2><<<grid, 128, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount, m.farA,
-                                    m.farT0, m.farT1, m.force);
+                                    m.farT0, m.farT1, m.force, m.cellPart, m.cellDone);
   else if (split == 8)
     k_cell<8><<<grid, 512, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount, m.farA,
-                                    m.farT0, m.farT1, m.force);
+                                    m.farT0, m.farT1, m.force, m.cellPart, m.cellDone);
   else
     k_cell<4><<<grid, 256, 0, st>>>(u, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount, m.farA,
-                                    m.farT0, m.farT1, m.force);
+                                    m.farT0, m.farT1, m.force, m.cellPart, m.cellDone);
   return 1;
 }
 
