@@ -15,11 +15,12 @@ inline int blocks_for(long n, int b = kBlock) { return (int)((n + b - 1) / b); }
 // deposit: src/glsl-sim.js:168-211 (DEP_VS) with src/nbody.js:402-416.
 // Each particle's eight cloud-in-cell corners carry (w m x, w m); particles in
 // the other box are left out; a stray (in neither) adds its pull toward last
-// time's monopole into the scratch texel.  Lanes of a warp whose particles
-// share a base cell (the common case in Morton order) reduce-scatter their 32
-// values (8 corners x 4 components) with 31 shuffles, so the warp issues 32
-// scalar L2 atomics instead of 256 vector ones; mixed warps fall back to
-// per-lane float4 atomics.  The box a particle is in and its base cell are
+// time's monopole into the scratch texel.  The lanes of a warp are grouped by
+// base cell (Morton order keeps a warp's particles in one or a few): a group
+// reduce-scatters its 32 values (8 corners x 4 components) over the warp with
+// 31 shuffles and issues 32 scalar L2 atomics instead of 8 vector ones a lane;
+// lone lanes, and lanes past the fourth group, add their own corners with
+// float4 atomics.  The box a particle is in and its base cell are
 // exact; the summation order is unspecified, as the reference's blending is.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void reduce_scatter32(float (&v)[32], int lane) {
@@ -82,31 +83,46 @@ __global__ void __launch_bounds__(kBlock) k_deposit(const ccs_uniforms *__restri
   const unsigned inMask = __ballot_sync(0xFFFFFFFFu, in);
   if (inMask == 0u) return;
   const int key = in ? (bz << 16) | (by << 8) | bx : -1 - lane;
-  const int key0 = __shfl_sync(0xFFFFFFFFu, key, __ffs(inMask) - 1);
-  const bool uniform = __all_sync(0xFFFFFFFFu, !in || key == key0) && __popc(inMask) > 1;
-  float v[32];
+  // the warp's lanes grouped by base cell (Morton order keeps a warp's particles in a few): each group of
+  // two or more reduce-scatters its 8 corners x 4 components over the warp (the others adding zeros) and
+  // issues 32 scalar atomics; a lone lane, and what is left after kDepGroups groups, adds its own corners
+  constexpr int kDepGroups = 4;
+  unsigned todo = inMask, lone = 0u;
+#pragma unroll 1
+  for (int g = 0; g < kDepGroups && todo; ++g) {
+    const int key0 = __shfl_sync(0xFFFFFFFFu, key, __ffs(todo) - 1);
+    const bool member = in && key == key0;
+    const unsigned gm = __ballot_sync(0xFFFFFFFFu, member);
+    todo &= ~gm;
+    if (__popc(gm) == 1) {   // a lone lane: its own atomics below
+      lone |= gm;
+      continue;
+    }
+    float v[32];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
-    const bool ok = in && bx + ox <= 63 && by + oy <= 63 && bz + oz <= 63;
-    const float w = ok ? (ox ? t.x : 1.0f - t.x) * (oy ? t.y : 1.0f - t.y) * (oz ? t.z : 1.0f - t.z) * mr : 0.0f;
-    v[4 * k + 0] = p.x * w;
-    v[4 * k + 1] = p.y * w;
-    v[4 * k + 2] = p.z * w;
-    v[4 * k + 3] = w;
-  }
-  if (uniform) {
+    for (int k = 0; k < 8; ++k) {
+      const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
+      const bool ok = member && bx + ox <= 63 && by + oy <= 63 && bz + oz <= 63;
+      const float w = ok ? (ox ? t.x : 1.0f - t.x) * (oy ? t.y : 1.0f - t.y) * (oz ? t.z : 1.0f - t.z) * mr : 0.0f;
+      v[4 * k + 0] = p.x * w;
+      v[4 * k + 1] = p.y * w;
+      v[4 * k + 2] = p.z * w;
+      v[4 * k + 3] = w;
+    }
     reduce_scatter32(v, lane);
     const int k = lane >> 2, comp = lane & 3;
     const int cx = (key0 & 0xFF) + (k & 1), cy = ((key0 >> 8) & 0xFF) + ((k >> 1) & 1), cz = (key0 >> 16) + (k >> 2);
     if (cx <= 63 && cy <= 63 && cz <= 63 && v[0] != 0.0f)
       atomicAdd(reinterpret_cast<float *>(fine + fine_index(cx, cy, cz)) + comp, v[0]);
-  } else if (in) {
+  }
+  if (((todo | lone) >> lane) & 1u) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const int cx = bx + (k & 1), cy = by + ((k >> 1) & 1), cz = bz + (k >> 2);
+      const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
+      const int cx = bx + ox, cy = by + oy, cz = bz + oz;
       if (cx > 63 || cy > 63 || cz > 63) continue;
-      atomicAdd(fine + fine_index(cx, cy, cz), make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]));
+      const float w = (ox ? t.x : 1.0f - t.x) * (oy ? t.y : 1.0f - t.y) * (oz ? t.z : 1.0f - t.z) * mr;
+      atomicAdd(fine + fine_index(cx, cy, cz), make_float4(p.x * w, p.y * w, p.z * w, w));
     }
   }
 }
