@@ -48,6 +48,14 @@ struct GraphSlot {
   bool used = false;
 };
 
+// one step's launches captured as a graph (ccs_step): its schedule, the buffers it reads and writes
+struct StepKey {
+  int slots, mesh, boxB, pp, nn, seatCur, cur, ping, field, timed;
+  bool operator<(const StepKey &o) const {
+    return std::memcmp(this, &o, sizeof *this) < 0;
+  }
+};
+
 }  // namespace
 
 struct ccs_handle {
@@ -107,6 +115,7 @@ struct ccs_handle {
   unsigned long long *fofTop = nullptr;
   // graphs
   std::map<GraphKey, GraphSlot> graphs;
+  std::map<StepKey, GraphSlot> stepGraphs;
   int ping = 0;
   bool useGraphs = true;
   // launch shapes chosen by ccs_autotune: contact-step warps per CTA, cell-gravity threads per cell
@@ -456,17 +465,81 @@ int block_launches(const ccs_handle *h, const StepPlan *plans, int M) {
   return per;
 }
 
-void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
+// what a step runs before its contact step: the grid, and the mesh and the pairwise pass on mesh steps
+void enqueue_pre(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
   if (p.slots) pass_slots(h, U);
   if (p.mesh) {
     pass_mesh(h, U, p.u.boxB > 0.5f);
     pass_pp(h, U, p.u.ppCount);
   }
+}
+
+void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
+  enqueue_pre(h, p, U);
   pass_sim(h, U);
+}
+
+// one step replayed from a captured graph: the step's uniforms by one memcpy node from pinned memory, then
+// its launches, so a step costs one cudaGraphLaunch.  Graphs are keyed by what the step runs and by the
+// buffers it touches; the uniform ping-pong lets the host run a step ahead.  When the contact step is being
+// timed (ccs_timing bit 0), the graph stops before it and the contact step is launched directly between
+// its two events (events recorded by a graph's nodes do not time).
+int step_graph(ccs_handle *h, const StepPlan &p) {
+  const bool timed = (h->timing & 1) != 0;
+  const StepKey key{(int)p.slots, (int)p.mesh, (int)(p.u.boxB > 0.5f), h->ppCount > 0, h->nn != nullptr,
+                    h->seatCur, h->cur, h->ping, (int)h->field, (int)timed};
+  GraphSlot &g = h->stepGraphs[key];
+  const int seatCur0 = h->seatCur, cur0 = h->cur;
+  if (!g.exec) {
+    CUDA_TRY(h, cudaMalloc(&g.dev, sizeof(ccs_uniforms)));
+    CUDA_TRY(h, cudaMallocHost(&g.host, sizeof(ccs_uniforms)));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+    *g.host = p.u;
+    const int timing = h->timing;
+    const int64_t l0 = h->launches;
+    h->timing = 0;
+    cudaGraph_t graph;
+    CUDA_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(g.dev, g.host, sizeof(ccs_uniforms), cudaMemcpyHostToDevice, h->st);
+    if (timed) enqueue_pre(h, p, g.dev);
+    else enqueue_step(h, p, g.dev);
+    cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
+    h->timing = timing;
+    h->launches = l0;
+    h->seatCur = seatCur0;
+    h->cur = cur0;
+    if (ce != cudaSuccess) {
+      h->err = std::string("step graph capture: ") + cudaGetErrorString(ce);
+      return CCS_E_CUDA;
+    }
+    ce = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) {
+      h->err = std::string("step graph instantiate: ") + cudaGetErrorString(ce);
+      g.exec = nullptr;
+      return CCS_E_CUDA;
+    }
+  }
+  if (g.used) CUDA_TRY(h, cudaEventSynchronize(g.done));
+  *g.host = p.u;
+  CUDA_TRY(h, cudaGraphLaunch(g.exec, h->st));
+  h->seatCur = seatCur0 ^ (p.slots ? 1 : 0);
+  h->launches += block_launches(h, &p, 1);
+  if (timed) {
+    --h->launches;            // pass_sim counts its own
+    pass_sim(h, g.dev);       // reads the uniforms the graph's memcpy node wrote
+  } else {
+    h->cur = cur0 ^ 1;
+  }
+  CUDA_TRY(h, cudaEventRecord(g.done, h->st));
+  g.used = true;
+  h->ping ^= 1;
+  return check_launch(h);
 }
 
 int do_step(ccs_handle *h, int settle, int kick) {
   StepPlan p = plan_step(h, settle, kick);
+  if (h->useGraphs && (h->timing & ~1) == 0) return step_graph(h, p);   // timing beyond the contact step: direct
   const ccs_uniforms *U;
   int rc = push_uniforms(h, p.u, &U);
   if (rc) return rc;
@@ -474,14 +547,18 @@ int do_step(ccs_handle *h, int settle, int kick) {
   return check_launch(h);
 }
 
+void free_graph_slot(GraphSlot &g) {
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.dev) cudaFree(g.dev);
+  if (g.host) cudaFreeHost(g.host);
+  if (g.done) cudaEventDestroy(g.done);
+}
+
 void free_graphs(ccs_handle *h) {
-  for (auto &kv : h->graphs) {
-    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    if (kv.second.dev) cudaFree(kv.second.dev);
-    if (kv.second.host) cudaFreeHost(kv.second.host);
-    if (kv.second.done) cudaEventDestroy(kv.second.done);
-  }
+  for (auto &kv : h->graphs) free_graph_slot(kv.second);
   h->graphs.clear();
+  for (auto &kv : h->stepGraphs) free_graph_slot(kv.second);
+  h->stepGraphs.clear();
 }
 
 // one block of meshEvery frame-loop steps, starting at stepNo % meshEvery == 0,
