@@ -3,13 +3,18 @@
 //
 // The reference gathers the list into a 128x64 texture and runs 4 x 8192
 // fragments, each walking a quarter of the list.  Here the list is tiled two
-// ways: a CTA takes 128 seats (i) against one 128-wide chunk (j) of one
-// quarter, with the chunk staged in shared memory, so a list of 8192 keeps
-// 4096 CTAs busy instead of 32K threads walking 2048 pairs each.  A second
+// ways: a work item is 128 seats (i) against one chunk (j) of one quarter,
+// with the chunk staged in shared memory; chunks are 128 entries wide for a
+// full list (4096 items instead of 32K threads walking 2048 pairs each) and
+// narrower for a short one (down to 16), so the few hundred entries a
+// mid-impact list holds still spread over dozens of CTAs.  A persistent grid
+// takes the items, counted from the list's length on the device.  A second
 // kernel sums each quarter's chunks in a fixed order: the four slices the
 // contact step adds are the reference's four slices, and the result is
 // deterministic.  The cut-off test and the box comparison are exact; the
 // force arithmetic is fast (FMA, rsqrt).
+#include <algorithm>
+
 #include "ccs_device.cuh"
 #include "ccs_internal.h"
 
@@ -49,6 +54,15 @@ int launch_pp_gather(const ccs_uniforms *u, const float4 *pos, const float *mat,
   return 1;
 }
 
+// a quarter's chunk width: eight chunks or so a quarter, 16 to kPPJ entries wide, so that a short list
+// spreads over many CTAs and a long one keeps kPPJ (at most kMaxChunks chunks either way)
+__device__ __forceinline__ int pp_chunk_width(int share) {
+  const int w = ((share + 7) / 8 + 15) / 16 * 16;
+  return min(max(w, 16), kPPJ);
+}
+
+// a persistent grid over (seat tile, quarter, chunk) work items, counted from the list's length on the
+// device, so a captured launch serves any length
 __global__ void __launch_bounds__(kPPI) k_pp_pairs(const ccs_uniforms *__restrict__ U,
                                                    const float4 *__restrict__ list, const float *__restrict__ box,
                                                    int cap, const float2 *__restrict__ tab,
@@ -58,53 +72,59 @@ __global__ void __launch_bounds__(kPPI) k_pp_pairs(const ccs_uniforms *__restric
   __shared__ float2 stab[CCS_PP_BINS];
   const ccs_uniforms &u = *U;
   const int count = u.ppCount;
-  const int slice = blockIdx.y / kMaxChunks, chunk = blockIdx.y % kMaxChunks;
   const int share = (count + 3) >> 2;
-  const int s0 = slice * share, s1 = min(s0 + share, count);
-  const int j0 = s0 + chunk * kPPJ, j1 = min(j0 + kPPJ, s1);
-  const int i0 = blockIdx.x * kPPI;
-  if (i0 >= count || j0 >= j1) return;   // never read by the reduction
-  const int me = i0 + threadIdx.x;
+  const int jw = pp_chunk_width(share);
+  const int nCh = share > 0 ? (share + jw - 1) / jw : 0;
+  const int items = (count + kPPI - 1) / kPPI * 4 * nCh;
   if (threadIdx.x < CCS_PP_BINS) stab[threadIdx.x] = tab[threadIdx.x];
-  if (j0 + (int)threadIdx.x < j1) {
-    sq[threadIdx.x] = list[j0 + threadIdx.x];
-    sb[threadIdx.x] = box[j0 + threadIdx.x];
-  }
-  __syncthreads();
-  const float4 P = me < cap ? list[me] : make_float4(0, 0, 0, 0);
-  const bool active = me < count && P.w != 0.0f;
-  const float myBox = me < cap ? box[me] : -1.0f;
   const float cut = u.cut, a2 = u.a2, cut2 = xmul(cut, cut), a = fsqrt(a2);
   const float binScale = fdiv(64.0f, cut), taperScale = fdiv(1.0f, 0.8f * cut - cut);
-  f3 acc = mk(0, 0, 0);
-  float pot = 0.0f;
-  if (active) {
-    const int n = j1 - j0;
-#pragma unroll 4
-    for (int jj = 0; jj < n; ++jj) {
-      if (j0 + jj == me) continue;
-      const float4 Q = sq[jj];
-      const f3 d = xsub3(xyz(Q), xyz(P));
-      const float r2 = xdot(d, d);
-      if (r2 >= cut2) continue;
-      const float r = fsqrt(r2);
-      const float xx = clampf(r * binScale - 0.5f, 0.0f, 63.0f);
-      const int k = (int)xx, k1 = min(k + 1, 63);
-      const float tt = xx - (float)k;
-      const float invN = rsqrtf(r2 + a2);
-      const float ts = clampf((r - cut) * taperScale, 0.0f, 1.0f);
-      const float taper = ts * ts * (3.0f - 2.0f * ts);
-      const float same = (myBox >= 0.0f && sb[jj] == myBox) ? 1.0f : 0.0f;
-      const float2 ta = stab[k], tb = stab[k1];
-      const float Tx = (ta.x + (tb.x - ta.x) * tt) * same;
-      const float Ty = (ta.y + (tb.y - ta.y) * tt) * same;
-      const float fn = invN * invN * invN * r - fdiv(Tx, fmaxf(r2, a2));
-      const float mj = Q.w;
-      acc = acc + d * (fdiv(1.0f, fmaxf(r, 1e-6f)) * mj * fn * taper);
-      pot += mj * (-invN - fdiv(Ty, fmaxf(r, a))) * taper;
+  for (int item = blockIdx.x; item < items; item += gridDim.x) {
+    const int tile = item / (4 * nCh), rest = item % (4 * nCh);
+    const int slice = rest / nCh, chunk = rest % nCh;
+    const int s0 = slice * share, s1 = min(s0 + share, count);
+    const int j0 = s0 + chunk * jw, j1 = min(j0 + jw, s1);
+    if (j0 >= j1) continue;   // past the end of a short last quarter: never read by the reduction
+    const int me = tile * kPPI + threadIdx.x;
+    __syncthreads();   // the previous item's reads of the chunk are done
+    if (j0 + (int)threadIdx.x < j1) {
+      sq[threadIdx.x] = list[j0 + threadIdx.x];
+      sb[threadIdx.x] = box[j0 + threadIdx.x];
     }
+    __syncthreads();
+    const float4 P = me < count ? list[me] : make_float4(0, 0, 0, 0);
+    const bool active = me < count && P.w != 0.0f;
+    const float myBox = me < count ? box[me] : -1.0f;
+    f3 acc = mk(0, 0, 0);
+    float pot = 0.0f;
+    if (active) {
+      const int n = j1 - j0;
+#pragma unroll 4
+      for (int jj = 0; jj < n; ++jj) {
+        if (j0 + jj == me) continue;
+        const float4 Q = sq[jj];
+        const f3 d = xsub3(xyz(Q), xyz(P));
+        const float r2 = xdot(d, d);
+        if (r2 >= cut2) continue;
+        const float r = fsqrt(r2);
+        const float xx = clampf(r * binScale - 0.5f, 0.0f, 63.0f);
+        const int k = (int)xx, k1 = min(k + 1, 63);
+        const float tt = xx - (float)k;
+        const float invN = rsqrtf(r2 + a2);
+        const float ts = clampf((r - cut) * taperScale, 0.0f, 1.0f);
+        const float taper = ts * ts * (3.0f - 2.0f * ts);
+        const float same = (myBox >= 0.0f && sb[jj] == myBox) ? 1.0f : 0.0f;
+        const float2 ta = stab[k], tb = stab[k1];
+        const float Tx = (ta.x + (tb.x - ta.x) * tt) * same;
+        const float Ty = (ta.y + (tb.y - ta.y) * tt) * same;
+        const float fn = invN * invN * invN * r - fdiv(Tx, fmaxf(r2, a2));
+        const float mj = Q.w;
+        acc = acc + d * (fdiv(1.0f, fmaxf(r, 1e-6f)) * mj * fn * taper);
+        pot += mj * (-invN - fdiv(Ty, fmaxf(r, a))) * taper;
+      }
+    }
+    if (me < count) part[((size_t)slice * kMaxChunks + chunk) * cap + me] = make_float4(acc.x, acc.y, acc.z, pot);
   }
-  part[((size_t)slice * kMaxChunks + chunk) * cap + me] = make_float4(acc.x, acc.y, acc.z, pot);
 }
 
 __global__ void __launch_bounds__(kBlock) k_pp_reduce(const ccs_uniforms *__restrict__ U,
@@ -113,14 +133,15 @@ __global__ void __launch_bounds__(kBlock) k_pp_reduce(const ccs_uniforms *__rest
                                                       float4 *__restrict__ force) {
   const int me = blockIdx.x * blockDim.x + threadIdx.x;
   const int slice = blockIdx.y;
-  if (me >= cap) return;
   const ccs_uniforms &u = *U;
   const int count = u.ppCount;
+  if (me >= count) return;   // only the list's seats are ever read
   float4 o = make_float4(0, 0, 0, 0);
-  if (me < count && list[me].w != 0.0f) {
+  if (list[me].w != 0.0f) {
     const int share = (count + 3) >> 2;
+    const int jw = pp_chunk_width(share);
     const int s0 = slice * share, s1 = min(s0 + share, count);
-    const int nChunks = s1 > s0 ? (s1 - s0 + kPPJ - 1) / kPPJ : 0;
+    const int nChunks = s1 > s0 ? (s1 - s0 + jw - 1) / jw : 0;
     for (int c = 0; c < nChunks; ++c) {
       const float4 v = part[((size_t)slice * kMaxChunks + c) * cap + me];
       o.x += v.x; o.y += v.y; o.z += v.z; o.w += v.w;
@@ -132,8 +153,16 @@ __global__ void __launch_bounds__(kBlock) k_pp_reduce(const ccs_uniforms *__rest
 
 int launch_pp_force(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,
                     float4 *part, float4 *force, cudaStream_t st) {
-  dim3 g1((cap + kPPI - 1) / kPPI, 4 * kMaxChunks);
-  k_pp_pairs<<<g1, kPPI, 0, st>>>(u, list, box, cap, tab, part);
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  // enough CTAs for a full list's items to take a few rounds; a short list's take one
+  const int full = (cap + kPPI - 1) / kPPI * 4 * kMaxChunks;
+  k_pp_pairs<<<std::min(full, sms * 8), kPPI, 0, st>>>(u, list, box, cap, tab, part);
   dim3 g2(blocks_for(cap), 4);
   k_pp_reduce<<<g2, kBlock, 0, st>>>(u, list, part, cap, force);
   return 2;
