@@ -28,7 +28,8 @@ BUF = {"seats": 5, "fineA": 6, "forceA": 7, "monoA": 8, "coarseA": 9, "farA": 10
        "monoB": 13, "pplist": 14, "ppforce": 15, "ppbox": 16, "ppslot": 17, "diag": 18, "cellof": 19}
 
 # every symbol include/ccstep.h declares
-EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_make_bodies", "ccs_build",
+EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_make_bodies", "ccs_make_bodies_device",
+           "ccs_build",
            "ccs_sim_ptr", "ccs_set_static", "ccs_get_uniforms", "ccs_set_mesh_every", "ccs_step", "ccs_steps",
            "ccs_settle_some", "ccs_rigid_step", "ccs_set_pp", "ccs_prime_mono", "ccs_apply_perm",
            "ccs_sort_morton", "ccs_diag_async", "ccs_poll", "ccs_fof", "ccs_pair_table", "ccs_read_state",
@@ -144,6 +145,7 @@ def lib():
         "ccs_create": (I, [I, C.POINTER(C.c_void_p)]),
         "ccs_destroy": (I, [H]),
         "ccs_make_bodies": (I, [C.POINTER(BuildOpt), C.POINTER(Sim), P, P, P, P]),
+        "ccs_make_bodies_device": (I, [I, C.POINTER(BuildOpt), C.POINTER(Sim), P, P, P, P]),
         "ccs_build": (I, [H, C.POINTER(Sim), P, P, P, P]),
         "ccs_sim_ptr": (C.POINTER(Sim), [H]),
         "ccs_set_static": (I, [H]),
@@ -236,16 +238,21 @@ def make_opt(N, q=0.1, dens=0.75, core=0.325, coreImp=None, spin0=0.18, spin1=0.
                     rest, int(n2), mImp, mTarget, rhoR, rhoCrust, crustFrac)
 
 
-def make_bodies(opt):
-    """Host builder (src/nbody.js:114-250): (sim, pos4, vel4, mat, home4)."""
+def make_bodies(opt, device=None):
+    """Host builder (src/nbody.js:114-250): (sim, pos4, vel4, mat, home4).  With a device index the
+    overlap relaxation runs on that GPU (ccs_make_bodies_device)."""
     N = opt.N
     sim = Sim()
     pos = np.zeros((N, 4), np.float32)
     vel = np.zeros((N, 4), np.float32)
     mat = np.zeros(N, np.float32)
     home = np.zeros((N, 4), np.float32)
-    check(lib().ccs_make_bodies(C.byref(opt), C.byref(sim), ptr(pos), ptr(vel), ptr(mat), ptr(home)),
-          what="ccs_make_bodies")
+    if device is None:
+        check(lib().ccs_make_bodies(C.byref(opt), C.byref(sim), ptr(pos), ptr(vel), ptr(mat), ptr(home)),
+              what="ccs_make_bodies")
+    else:
+        check(lib().ccs_make_bodies_device(int(device), C.byref(opt), C.byref(sim), ptr(pos), ptr(vel), ptr(mat),
+                                           ptr(home)), what="ccs_make_bodies_device")
     return sim, pos, vel, mat, home
 
 

@@ -17,9 +17,15 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/ccstep.h"
+
+namespace ccs {
+// the same relaxation on a GPU (ccs_build.cu)
+int relax_device(int device, float *p, int n, double a, double A, double C, std::string *err);
+}  // namespace ccs
 
 namespace {
 
@@ -128,7 +134,8 @@ void relax(std::vector<float> &p, int n, double a, double A, double C) {
 
 // the onion of Fibonacci shells, src/bodies.js:23-76; returns the shell
 // bounds (ascending, 0 .. n)
-std::vector<int> ball(int n, double s, double a, Mulberry &rng, double e, std::vector<float> &out) {
+std::vector<int> ball(int n, double s, double a, Mulberry &rng, double e, std::vector<float> &out, int device,
+                      int *rc) {
   constexpr int NB = 256;
   const double R = std::cbrt(3 * n * s * s * s / (16 * kPi));
   const double ae = R / std::pow(1 - e * e, 1.0 / 6), ce = ae * std::sqrt(1 - e * e);
@@ -200,7 +207,8 @@ std::vector<int> ball(int n, double s, double a, Mulberry &rng, double e, std::v
   }
   bounds.push_back(0);
   std::reverse(bounds.begin(), bounds.end());
-  relax(out, n, a, ae - h * 0.5, ce - h * 0.5);
+  if (device < 0) relax(out, n, a, ae - h * 0.5, ce - h * 0.5);
+  else *rc = ccs::relax_device(device, out.data(), n, a, ae - h * 0.5, ce - h * 0.5, nullptr);
   return bounds;
 }
 
@@ -232,8 +240,8 @@ int closest_bound(const std::vector<int> &bounds, double target) {
 
 }  // namespace
 
-extern "C" int ccs_make_bodies(const ccs_build_opt *opt, ccs_sim *sim, float *pos, float *vel, float *matR,
-                               float *home) {
+static int make_bodies(const ccs_build_opt *opt, ccs_sim *sim, float *pos, float *vel, float *matR, float *home,
+                       int device) {
   if (!opt || !sim || !pos || !vel || !matR) return CCS_E_ARG;
   const int N = opt->N;
   if (N < 64 || N > CCS_MAX_N) return CCS_E_RANGE;
@@ -257,8 +265,11 @@ extern "C" int ccs_make_bodies(const ccs_build_opt *opt, ccs_sim *sim, float *po
   const double e1 = maclaurin(std::fabs(opt->spin0)), e2 = maclaurin(std::fabs(opt->spin1));
   Mulberry rng(1234567u);
   std::vector<float> b1, b2;
-  const std::vector<int> bd1 = ball(n1, s, a, rng, e1, b1);
-  const std::vector<int> bd2 = ball(n2, s, a, rng, e2, b2);
+  int rc = CCS_OK;
+  const std::vector<int> bd1 = ball(n1, s, a, rng, e1, b1, device, &rc);
+  if (rc) return rc;
+  const std::vector<int> bd2 = ball(n2, s, a, rng, e2, b2, device, &rc);
+  if (rc) return rc;
   std::vector<unsigned char> lay((size_t)N);
   auto layers = [&](int off, int n, const std::vector<int> &bounds, double densB, double cv) {
     const int nCore = closest_bound(bounds, cv * n);
@@ -337,6 +348,17 @@ extern "C" int ccs_make_bodies(const ccs_build_opt *opt, ccs_sim *sim, float *po
   sim->tK = 0.5 * kEkg / kCpRock / mref;
   sim->kappa = 0.3;
   return CCS_OK;
+}
+
+extern "C" int ccs_make_bodies(const ccs_build_opt *opt, ccs_sim *sim, float *pos, float *vel, float *matR,
+                               float *home) {
+  return make_bodies(opt, sim, pos, vel, matR, home, -1);
+}
+
+extern "C" int ccs_make_bodies_device(int device, const ccs_build_opt *opt, ccs_sim *sim, float *pos, float *vel,
+                                      float *matR, float *home) {
+  if (device < 0) return CCS_E_ARG;
+  return make_bodies(opt, sim, pos, vel, matR, home, device);
 }
 
 // ---------------------------------------------------------------------------

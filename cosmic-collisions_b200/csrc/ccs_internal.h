@@ -142,6 +142,8 @@ int launch_morton_keys(int N, const float4 *pos, double cx, double cy, double cz
 // stable LSD radix sort of (key, value) pairs on `bits` key bits; tmp buffers
 // hold N entries each, hist holds radix_hist_words(N) words
 size_t radix_hist_words(int N);
+// the builder's overlap relaxation of n points (x, y, z binary32) on the device: ccs_build.cu
+int relax_device(int device, float *p, int n, double a, double A, double C, std::string *err);
 int launch_radix_sort(int N, int bits, uint32_t *keys, int32_t *vals, uint32_t *keysTmp, int32_t *valsTmp,
                       uint32_t *hist, cudaStream_t st);
 int launch_invert_perm(int N, const int32_t *perm, int32_t *into, cudaStream_t st);

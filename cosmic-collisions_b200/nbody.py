@@ -85,14 +85,15 @@ class NBody:
         return self._h
 
     # ---- build(opt): src/nbody.js:114-250 -----------------------------------
-    def build(self, opt=None, **kw):
-        """Build a run from options (a BuildOpt or keywords of make_opt) and upload it."""
+    def build(self, opt=None, relax_on_device=False, **kw):
+        """Build a run from options (a BuildOpt or keywords of make_opt) and upload it.  relax_on_device:
+        the builder's overlap relaxation on this engine's GPU (equivalent to the host's, not identical)."""
         if opt is None:
             opt = L.make_opt(**kw)
         elif isinstance(opt, dict):
             opt = L.make_opt(**opt)
         self._opt = opt
-        sim, pos, vel, mat, home = L.make_bodies(opt)
+        sim, pos, vel, mat, home = L.make_bodies(opt, self.device if relax_on_device else None)
         self.upload(sim, pos, vel, mat, home)
         return self.sim
 

@@ -113,6 +113,15 @@ int ccs_version(void);
  * of src/bodies.js:23-160 and mulberry of src/math.js:8-15.  Fills sim and the
  * particle arrays (pos4, vel4, home4: N*4 floats; mat: N floats). */
 int ccs_make_bodies(const ccs_build_opt *opt, ccs_sim *sim, float *pos4, float *vel4, float *mat, float *home4);
+/* The same builder with relax() (src/bodies.js:97-146) on GPU `device`: the
+ * shells, layers, masses, encounter and every other output are the host
+ * builder's; the ten sweeps run as 27 race-free phases of cells a sweep, each
+ * cell's particles walked in index order, so the relaxed pile is equivalent
+ * to the host's (the same overlap statistics, each particle within a small
+ * fraction of a radius) but not bit-identical.  Allocates device memory for
+ * the call's duration. */
+int ccs_make_bodies_device(int device, const ccs_build_opt *opt, ccs_sim *sim, float *pos4, float *vel4, float *mat,
+                           float *home4);
 /* Upload a run: the texture uploads and setStaticUniforms of src/nbody.js:208-249.
  * home4 may be NULL. */
 int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float *vel4, const float *mat,
