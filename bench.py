@@ -48,6 +48,7 @@ sys.path.insert(0, ROOT)
 
 ALG_BYTES_SIM = 92          # bytes per particle per contact-step launch
 L2_FLUSH_BYTES = 256 << 20
+TIME_EVERY = 8                 # inside the timed region the contact step is timed on every 8th launch
 
 
 def impact_opt(N):
@@ -408,8 +409,9 @@ def analysis_timing(cc, nb, reps=5):
 def timed_steps(nb, lib, stream, flush, steps, dev, dist):
     """steps direct-launch steps, L2 flushed before each, each bracketed by CUDA events on the library's
     stream; clocks sampled meanwhile.  Inside the timed region the library times the contact step alone
-    with its own pair of events per launch (the roofline's kernel); the other kernels are timed in a pass
-    of their own after it, since every timed launch widens the step by its events."""
+    (the roofline's kernel) with its own pair of events on every 8th launch, a sample spread over the whole
+    region; the other kernels are timed in a pass of their own after it, since every timed launch widens
+    its step by its events (and leaves the step's captured graph for a direct launch)."""
     import ctypes as C
     import torch
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
@@ -418,6 +420,7 @@ def timed_steps(nb, lib, stream, flush, steps, dev, dist):
         import torch.distributed as td
         td.barrier()
     torch.cuda.synchronize()
+    lib.ccs_timing_every(nb.handle, TIME_EVERY)
     lib.ccs_timing(nb.handle, 1)            # kernel id 0, the contact step
     l0 = lib.ccs_launch_count(nb.handle)
     clocks.start()
@@ -446,6 +449,7 @@ def timed_steps(nb, lib, stream, flush, steps, dev, dist):
             kt[names[kid]] = {"launches": cnt.value, "total_ms": tot.value,
                               "mean_us": 1e3 * tot.value / cnt.value if cnt.value else None}
     read([0])
+    lib.ccs_timing_every(nb.handle, 1)
     # the other kernels: a pass of their own after the timed region, L2 flushed before each step as above
     lib.ccs_timing(nb.handle, 0x1E)
     for k in range(max(16, min(steps, 64))):
@@ -609,7 +613,10 @@ def run_ours(args, rank, world, log):
                      "frac": achieved / peak if achieved else None, "peak_kind": peak_kind + " hbm_gbs",
                      "kernel": "k_contact_step (contacts + gather + kick/drift)",
                      "traffic": tpp * N if tpp else None,
-                     "algorithmic_bytes_per_launch": ALG_BYTES_SIM * N},
+                     "algorithmic_bytes_per_launch": ALG_BYTES_SIM * N,
+                     "timed_launches": kt["simulate"]["launches"],
+                     "timing": "CUDA events on the library's stream around every %dth contact step of the timed "
+                               "region" % TIME_EVERY},
         "gpu_launches": int(launches),
         "clocks": clk,
         "force_error": ferr,

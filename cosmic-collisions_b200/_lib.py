@@ -41,7 +41,7 @@ EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_ma
            "ccs_nn_train", "ccs_nn_forward", "ccs_nn_labels", "ccs_nn_grad", "ccs_set_pp_nn", "ccs_autotune",
            "ccs_ensemble_create", "ccs_ensemble_destroy", "ccs_ensemble_last_error", "ccs_ensemble_steps",
            "ccs_ensemble_sync", "ccs_ensemble_autotune", "ccs_fof_device", "ccs_set_field",
-           "ccs_checkpoint_size", "ccs_checkpoint_save", "ccs_checkpoint_load"]
+           "ccs_checkpoint_size", "ccs_checkpoint_save", "ccs_checkpoint_load", "ccs_timing_every"]
 NN_PARAMS = 4803
 NN_CUT_CELLS = 2.5
 
@@ -207,6 +207,7 @@ def lib():
         "ccs_checkpoint_size": (I, [H, C.c_size_t, C.POINTER(C.c_size_t)]),
         "ccs_checkpoint_save": (I, [H, P, C.c_size_t, P, C.c_size_t]),
         "ccs_checkpoint_load": (I, [H, P, C.c_size_t]),
+        "ccs_timing_every": (I, [H, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -122,6 +122,8 @@ struct ccs_handle {
   int tuneWarps = 8, tuneSplit = 4;
   // timing of chosen kernels with events on the stream
   int timing = 0;                       // ccs_timing's mask of kernel ids
+  int timingEvery = 1;                  // ccs_timing_every: the contact step timed on every n-th launch
+  int64_t timingSeq = 0;                // contact-step launches while it is being timed
   std::vector<cudaEvent_t> evPool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> evRecs;
   size_t evNext = 0;
@@ -300,9 +302,15 @@ int push_uniforms(ccs_handle *h, const ccs_uniforms &u, const ccs_uniforms **dev
 }
 
 // timing brackets around chosen kernels
+// whether this launch of `kernel` is timed: its mask bit, and for the contact step every timingEvery-th launch
+bool time_this(const ccs_handle *h, int kernel) {
+  if (!((h->timing >> kernel) & 1)) return false;
+  return kernel != 0 || h->timingEvery <= 1 || h->timingSeq % h->timingEvery == 0;
+}
+
 void time_begin(ccs_handle *h, int kernel, cudaEvent_t *b, cudaEvent_t *e) {
   *b = *e = nullptr;
-  if (!((h->timing >> kernel) & 1)) return;
+  if (!time_this(h, kernel)) return;
   if (h->evNext + 2 > h->evPool.size()) {
     for (int k = 0; k < 256; ++k) {
       cudaEvent_t ev;
@@ -407,6 +415,7 @@ void pass_sim(ccs_handle *h, const ccs_uniforms *U) {
   time_begin(h, 0, &b, &e);
   h->launches += launch_simulate(U, h->N, a, h->st, h->tuneWarps, h->field);
   time_end(h, e);
+  if (h->timing & 1) ++h->timingSeq;
   h->cur ^= 1;
 }
 
@@ -485,7 +494,7 @@ void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
 // timed (ccs_timing bit 0), the graph stops before it and the contact step is launched directly between
 // its two events (events recorded by a graph's nodes do not time).
 int step_graph(ccs_handle *h, const StepPlan &p) {
-  const bool timed = (h->timing & 1) != 0;
+  const bool timed = time_this(h, 0);
   const StepKey key{(int)p.slots, (int)p.mesh, (int)(p.u.boxB > 0.5f), h->ppCount > 0, h->nn != nullptr,
                     h->seatCur, h->cur, h->ping, (int)h->field, (int)timed};
   GraphSlot &g = h->stepGraphs[key];
@@ -530,6 +539,7 @@ int step_graph(ccs_handle *h, const StepPlan &p) {
     pass_sim(h, g.dev);       // reads the uniforms the graph's memcpy node wrote
   } else {
     h->cur = cur0 ^ 1;
+    if (h->timing & 1) ++h->timingSeq;   // a contact step that was not this sample's
   }
   CUDA_TRY(h, cudaEventRecord(g.done, h->st));
   g.used = true;
@@ -2180,10 +2190,18 @@ int ccs_sync(ccs_handle *h) {
   return rc ? rc : (h->built ? check_status(h) : CCS_OK);
 }
 
+int ccs_timing_every(ccs_handle *h, int every) {
+  if (!h || every < 1) return CCS_E_ARG;
+  h->timingEvery = every;
+  h->timingSeq = 0;
+  return CCS_OK;
+}
+
 int ccs_timing(ccs_handle *h, int enable) {
   if (!h) return CCS_E_ARG;
   time_collect(h);
   h->timing = enable & ((1 << kTimedKernels) - 1);
+  h->timingSeq = 0;
   for (int k = 0; k < kTimedKernels; ++k) {
     h->tAcc[k] = 0;
     h->tCount[k] = 0;

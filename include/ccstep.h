@@ -373,6 +373,9 @@ int ccs_sync(ccs_handle *h);
  * before and after it by a microsecond or two. */
 #define CCS_TIME_ALL 0x1F
 int ccs_timing(ccs_handle *h, int enable);
+/* time the contact step on every `every`-th launch only (1, the default: on
+ * every launch), so that a long run carries its events on a sample */
+int ccs_timing_every(ccs_handle *h, int every);
 int ccs_timing_read(ccs_handle *h, int kernel, double *total_ms, int *launches);
 /* kernels launched by this handle since creation (the benchmark's gpu_launches) */
 int64_t ccs_launch_count(ccs_handle *h);
