@@ -43,12 +43,14 @@ int launch_fill_u32(uint32_t *p, size_t n, uint32_t v, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 constexpr int kMaxRetries = 1 << 20;
 
+// Each seat is first tried as if it were empty: the swap checks the guess and, when it fails, returns the
+// seat's word -- one round trip a seat where a read and then a swap would take two.
 __device__ __forceinline__ void seat_insert(uint32_t *cell, uint32_t w, unsigned *status) {
   uint32_t wi = w & 0x3FFFFu;
   int retries = 0;
 #pragma unroll 1
   for (int k = 0; k < kSeats; ++k) {
-    uint32_t cur = __ldcg(cell + k);
+    uint32_t cur = kEmpty;
     while (true) {
       if ((cur & 0x80000000u) != 0u || (cur & 0x3FFFFu) > wi) {
         const uint32_t prev = atomicCAS(cell + k, cur, w);
