@@ -426,16 +426,18 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restr
     const int c1 = (int)((long long)total * (chunk + 1) / kCellChunks);
     for (int b0 = c0; b0 < c1; b0 += kCellBatch) {
       const int b1 = min(b0 + kCellBatch, c1);
-      // this chunk's sources in [b0, b1): every load independent of the others
-      for (int o = 0; o < 125; ++o) {
-        const int lo = max(nbOff[o], b0), hi = min(nbOff[o + 1], b1);
-        if (lo >= hi) continue;
-        const int k = nbK[o];
-        for (int e = lo + t; e < hi; e += kCellThreads) {
-          const int i = e - nbOff[o];
-          src[e - b0] = __ldg(occ + (size_t)k * 64 + i);
-          sidx[e - b0] = k == blk ? __ldg(occIdx + (size_t)k * 64 + i) : (uint8_t)255;
+      // this chunk's sources in [b0, b1), a thread an entry: the neighbour block holding entry e is the
+      // last o with nbOff[o] <= e (a binary search over the 126 starts); every load independent
+      for (int e = b0 + t; e < b1; e += kCellThreads) {
+        int lo = 0, hi = 125;   // nbOff[lo] <= e < nbOff[hi]
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (nbOff[mid] <= e) lo = mid;
+          else hi = mid;
         }
+        const int k = nbK[lo], i = e - nbOff[lo];
+        src[e - b0] = __ldg(occ + (size_t)k * 64 + i);
+        sidx[e - b0] = k == blk ? __ldg(occIdx + (size_t)k * 64 + i) : (uint8_t)255;
       }
       __syncthreads();
       if (mine) {
