@@ -58,6 +58,30 @@ def impact_opt(N):
                 rest=0.3, mImp=0.1, mTarget=0.9, rhoR=7.8 / 3.3, rhoCrust=2.7 / 3.3, crustFrac=0.05)
 
 
+def sum_over_ranks(x):
+    """The sum of x over the ranks of the process group (x itself without one)."""
+    import torch
+    import torch.distributed as td
+    if not (td.is_available() and td.is_initialized()) or td.get_world_size() == 1:
+        return x
+    dev = "cuda" if td.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    td.all_reduce(t, op=td.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier():
+    import torch.distributed as td
+    if td.is_available() and td.is_initialized() and td.get_world_size() > 1:
+        td.barrier()
+
+
+def ensemble_share(count, rank, world):
+    """The impacts rank `rank` of `world` runs: every world-th from its own index, so each GPU gets a
+    mix of sizes (whole impacts per GPU, no exchange during the run)."""
+    return list(range(rank, count, world))
+
+
 def max_over_ranks(x):
     """The largest of x over the ranks of the process group (x itself without one): the job's time is
     its slowest rank's."""
@@ -297,21 +321,26 @@ def learned_correction(cc, dev, N, log, pairs=9_000_000, epochs=8, snaps=(0, 100
     return net, info
 
 
-def run_ensemble(args, log):
+def run_ensemble(args, log, rank=0, world=1):
     """The batched ensemble: `args.ensemble` impacts of uneven size (seeded: N over the page's counts,
     impactor 0.02-1 M_earth, 0-75 degrees, 1.0-2.6 v_esc), each prepared to first touch, then advanced
     `args.ens_steps` steps each.  Every instance is a handle on its own stream; the host interleaves one
     captured 8-step graph per instance per round, so the instances run concurrently on the GPU.
-    Reports the aggregate particle-steps/s and the p50/p99 of the per-instance step time."""
+    Reports the aggregate particle-steps/s and the p50/p99 of the per-instance step time.  Under torchrun
+    the impacts are shared out by instance (ensemble_share): each rank runs its own on its own GPU, and only
+    the totals cross ranks at the end (the slowest rank's wall time, the sum of particle-steps)."""
     import numpy as np
     import torch
     import cosmic_collisions_b200 as cc
     from cosmic_collisions_b200 import configs
-    opts = configs.ensemble_opts(args.ensemble)
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    allopts = configs.ensemble_opts(args.ensemble)
+    opts = [allopts[k] for k in ensemble_share(len(allopts), rank, world)]
     runs = []
     t0 = time.perf_counter()
     for opt in opts:
-        nb = cc.NBody(0)
+        nb = cc.NBody(dev)
         nb.build(cc.make_opt(**opt))
         while nb.sim.phase == 0:
             nb.settle_some(256)
@@ -342,6 +371,7 @@ def run_ensemble(args, log):
     streams = [torch.cuda.ExternalStream(nb.device_buffers().stream) for nb in runs]
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in runs]
     torch.cuda.synchronize()
+    barrier()
     w0 = time.perf_counter()
     for k, (nb, s) in enumerate(zip(runs, streams)):
         with torch.cuda.stream(s):
@@ -353,26 +383,31 @@ def run_ensemble(args, log):
         with torch.cuda.stream(s):
             ev[k][1].record(s)
     torch.cuda.synchronize()
-    wall = time.perf_counter() - w0
+    wall = max_over_ranks(time.perf_counter() - w0)
     per_step_ms = np.array([a.elapsed_time(b) / (8 * blocks) for a, b in ev])
-    total = sum(nb.sim.N for nb in runs) * 8 * blocks
+    total = sum_over_ranks(sum(nb.sim.N for nb in runs) * 8 * blocks)
     # the same number of steps again, every round one graph holding all instances' blocks (ccs_ensemble)
     ens = cc.Ensemble(runs)
     ens.steps(8)                                          # capture the round's graphs
     ens.sync()
     torch.cuda.synchronize()
+    barrier()
     w1 = time.perf_counter()
     ens.steps(8 * blocks)
     ens.sync()
-    wall_graph = time.perf_counter() - w1
+    wall_graph = max_over_ranks(time.perf_counter() - w1)
     ens.close()
+    p50 = max_over_ranks(float(np.percentile(per_step_ms, 50)))
+    p99 = max_over_ranks(float(np.percentile(per_step_ms, 99)))
     line = {"metric": "ensemble aggregate particle-steps/s", "value": total / wall_graph, "unit": "particle-steps/s",
-            "instances": len(runs), "steps_each": 8 * blocks, "particles": int(sum(nb.sim.N for nb in runs)),
+            "instances": int(sum_over_ranks(len(runs))), "n_gpus": world, "steps_each": 8 * blocks,
+            "particles": int(sum_over_ranks(sum(nb.sim.N for nb in runs))),
+            "sharding": "whole impacts per GPU (every world-th instance), no exchange during the run; the "
+                        "slowest rank's wall time and the summed particle-steps",
             "mode": "one CUDA graph per four 8-step rounds holding every instance's steps as a parallel branch "
                     "(ccs_ensemble); wall clock over the rounds",
             "per_handle_streams": {"value": total / wall, "wall_s": wall,
-                                   "per_instance_step_ms": {"p50": float(np.percentile(per_step_ms, 50)),
-                                                            "p99": float(np.percentile(per_step_ms, 99))},
+                                   "per_instance_step_ms": {"p50": p50, "p99": p99},
                                    "mode": "one handle and stream per impact, captured 8-step graphs interleaved"},
             "wall_s": wall_graph,
             "autotuned": tuned}
@@ -668,17 +703,21 @@ def main():
         print(json.dumps(line), flush=True)
         return
 
-    if args.ensemble:
-        if rank == 0:
-            print(json.dumps(run_ensemble(args, log)), flush=True)
-        return
-
     if world > 1:
         import datetime
         import torch
         import torch.distributed as td
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.ensemble:
+        line = run_ensemble(args, log, rank, world)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as td
+            td.barrier()
+            td.destroy_process_group()
+        return
     line = run_ours(args, rank, world, log)
     if rank == 0:
         if world == 1 and not args.no_cpu and not args.profile:
