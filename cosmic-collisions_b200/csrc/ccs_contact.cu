@@ -13,14 +13,18 @@
 //      quantised seat cull to each (where the seat sat at the rebuild, to a
 //      fifteenth of a cell: beyond reach, the reference never fetches it)
 //      and appends the seats that pass to a per-warp queue in shared memory;
-//   2. candidates: 32 queued seats at a time, one per lane: load the
-//      neighbour's position and keep the pairs inside the link radius;
-//   3. neighbours: 32 at a time: the neighbour count, and for touching pairs
-//      the spring-dashpot, its heat and the conduction, added into the
-//      owner's slots.
+//   2. candidates: 32 or 64 queued seats at a time, one or two per lane: load
+//      the neighbour's position; a pair inside the link radius adds to its
+//      owner's count (a shared-memory integer atomic), and a touching one goes
+//      on its owner's list;
+//   3. contacts: each owner, in its own lane, walks its list of touching
+//      neighbours -- the spring-dashpot, its heat and the conduction -- with
+//      the sums in registers, so no floating-point atomics are needed (a list
+//      holds kTCap; the rare contact past that is worked out in stage 2 and
+//      added to the owner's shared slots atomically).
 // The pair set and the neighbour counts are decided with exact arithmetic and
-// integer counts; force, dissipation and heat flow are summed in whatever
-// order the shared-memory atomics land, to tolerance.
+// integer counts; force, dissipation and heat flow are summed in the order the
+// list was filled, to tolerance.
 #include "ccs_device.cuh"
 #include "ccs_internal.h"
 
@@ -28,7 +32,7 @@ namespace ccs {
 
 namespace {
 constexpr int kQCap = 32 * kSeats + 64;      // seat candidates: one stage-1 round plus what is left
-constexpr int kNCap = 64;                    // neighbours: one stage-2 round plus what is left
+constexpr int kTCap = 16;                    // touching neighbours listed per owner
 inline int blocks_for(long n, int b) { return (int)((n + b - 1) / b); }
 }  // namespace
 
@@ -37,87 +41,81 @@ struct ContactWarp {
   float4 V[32];        // owner velocity, temperature
   float4 C0[32];       // lower corner of the owner's cell (exact), mass ratio
   float ci[32];        // owner heat capacity
-  float fx[32], fy[32], fz[32], lost[32], flow[32];   // what the contacts add up, per owner
-  int nb[32];
+  float fx[32], fy[32], fz[32], lost[32], flow[32];   // contacts past an owner's list, added here
+  int nb[32];          // neighbours inside the link radius, per owner
+  int tn[32];          // touching neighbours listed, per owner
+  uint32_t tl[kTCap][32];   // the touching neighbours of owner o: tl[k][o]
   uint32_t q[kQCap];   // particle index | owner << 18
-  uint2 nq[kNCap];     // x: particle index | owner << 18; y: r^2 bits
 };
 
-__device__ __forceinline__ void drain_neighbours(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, int base,
-                                                 int n, int lane) {
-  if (lane < n) {
-    const uint2 e = w.nq[base + lane];
-    const uint32_t sv = e.x;
-    const int o = (int)(e.x >> 18);
-    const float r2 = __uint_as_float(e.y);
-    const float4 Po = w.P[o], C0 = w.C0[o];
-    {
-      atomicAdd(&w.nb[o], 1);
-      const float r = __fsqrt_rn(r2);
-      if (xsub(u.touch, r) > 0.0f) {
-        const uint32_t j = sv & 0x3FFFFu;
-        const float4 Pj = __ldg(a.pos + j);
-        const float4 Vj = __ldg(a.vel + j);
-        const float rj = __ldg(a.mat + j);
-        const float4 Vo = w.V[o];
-        const float ri = C0.w, ci = w.ci[o];
-        const f3 nrm = (xyz(Pj) - xyz(Po)) * fdiv(1.0f, fmaxf(r, 1e-6f));
-        const float ov = u.touch - r;
-        const float cij = u.C * fsqrt(fdiv(2.0f * ri * rj, ri + rj));   // the dashpot for this pair's reduced mass
-        const float vn = dot(xyz(Vj) - xyz(Vo), nrm);
-        const float fs = u.K * ov - cij * vn;
-        const float fn = fmaxf(fs, 0.0f);                                // no tension
-        atomicAdd(&w.fx[o], -nrm.x * fn);
-        atomicAdd(&w.fy[o], -nrm.y * fn);
-        atomicAdd(&w.fz[o], -nrm.z * fn);
-        atomicAdd(&w.lost[o], fs >= 0.0f ? cij * vn * vn : u.K * ov * vn);
-        const float cj = rj * (is_iron(Pj.w) ? u.cpIron : 1.0f);
-        atomicAdd(&w.flow[o], (Vj.w - Vo.w) * fdiv(2.0f * ci * cj, ci + cj));   // heat crosses the contact
-      }
+// one touching pair's spring-dashpot, dissipation and conduction (src/glsl-sim.js:433-446)
+struct Contact {
+  f3 push;
+  float lost, flow;
+};
+__device__ __forceinline__ Contact contact_of(const ccs_uniforms &u, const SimArgs &a, float4 Po, float4 Vo, float ri,
+                                              float ci, uint32_t j, float r) {
+  const float4 Pj = __ldg(a.pos + j);
+  const float4 Vj = __ldg(a.vel + j);
+  const float rj = __ldg(a.mat + j);
+  const f3 nrm = (xyz(Pj) - xyz(Po)) * fdiv(1.0f, fmaxf(r, 1e-6f));
+  const float ov = u.touch - r;
+  const float cij = u.C * fsqrt(fdiv(2.0f * ri * rj, ri + rj));   // the dashpot for this pair's reduced mass
+  const float vn = dot(xyz(Vj) - xyz(Vo), nrm);
+  const float fs = u.K * ov - cij * vn;
+  const float fn = fmaxf(fs, 0.0f);                                // no tension
+  const float cj = rj * (is_iron(Pj.w) ? u.cpIron : 1.0f);
+  Contact c;
+  c.push = nrm * (-fn);
+  c.lost = fs >= 0.0f ? cij * vn * vn : u.K * ov * vn;
+  c.flow = (Vj.w - Vo.w) * fdiv(2.0f * ci * cj, ci + cj);         // heat crosses the contact
+  return c;
+}
+
+// a pair inside the link radius: its owner's count; a touching one onto its owner's list (past the list's
+// end, rarely, its contact is worked out here and added to the owner's shared slots)
+__device__ __forceinline__ void take_near(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, uint32_t e,
+                                          float r2) {
+  const int o = (int)(e >> 18);
+  atomicAdd(&w.nb[o], 1);
+  const float r = __fsqrt_rn(r2);
+  if (xsub(u.touch, r) > 0.0f) {
+    const int k = atomicAdd(&w.tn[o], 1);
+    if (k < kTCap) {
+      w.tl[k][o] = e & 0x3FFFFu;
+    } else {
+      const Contact c = contact_of(u, a, w.P[o], w.V[o], w.C0[o].w, w.ci[o], e & 0x3FFFFu, r);
+      atomicAdd(&w.fx[o], c.push.x);
+      atomicAdd(&w.fy[o], c.push.y);
+      atomicAdd(&w.fz[o], c.push.z);
+      atomicAdd(&w.lost[o], c.lost);
+      atomicAdd(&w.flow[o], c.flow);
     }
   }
-  __syncwarp();
 }
 
 // stage 2: queued seats, two per lane when there are 64 (two position loads in flight), else one
-// (lanes >= n idle); pairs inside the link radius go on to stage 3
-__device__ __forceinline__ void push_near(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w,
-                                          bool near, uint32_t e, float r2, int lane, int &nn) {
-  const unsigned bal = __ballot_sync(0xFFFFFFFFu, near);
-  if (near) w.nq[nn + __popc(bal & ((1u << lane) - 1u))] = make_uint2(e, __float_as_uint(r2));
-  nn += __popc(bal);
-  __syncwarp();
-  if (nn >= 32) {
-    nn -= 32;
-    drain_neighbours(u, a, w, nn, 32, lane);
-  }
-}
-
+// (lanes >= n idle); pairs inside the link radius are counted, touching ones listed for their owner
 __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, int base,
-                                                 int n, int lane, int &nn) {
-  const bool two = n == 64;
-  bool near0 = false, near1 = false;
-  uint32_t e0 = 0u, e1 = 0u;
-  float r20 = 0.0f, r21 = 0.0f;
+                                                 int n, int lane) {
   if (lane < n) {
-    e0 = w.q[base + lane];
-    if (two) e1 = w.q[base + 32 + lane];
+    const bool two = n == 64;
+    const uint32_t e0 = w.q[base + lane];
+    const uint32_t e1 = two ? w.q[base + 32 + lane] : 0u;
     const float4 Pj0 = __ldg(a.pos + (e0 & 0x3FFFFu));
     const float4 Pj1 = two ? __ldg(a.pos + (e1 & 0x3FFFFu)) : Pj0;
     const float4 Po0 = w.P[e0 >> 18];
     const f3 d0 = xsub3(xyz(Pj0), xyz(Po0));
-    r20 = xdot(d0, d0);
-    near0 = r20 < u.link2;
+    const float r20 = xdot(d0, d0);
+    if (r20 < u.link2) take_near(u, a, w, e0, r20);
     if (two) {
       const float4 Po1 = w.P[e1 >> 18];
       const f3 d1 = xsub3(xyz(Pj1), xyz(Po1));
-      r21 = xdot(d1, d1);
-      near1 = r21 < u.link2;
+      const float r21 = xdot(d1, d1);
+      if (r21 < u.link2) take_near(u, a, w, e1, r21);
     }
   }
   __syncwarp();   // every lane has read its entries before the queue is written again
-  push_near(u, a, w, near0, e0, r20, lane, nn);
-  if (two) push_near(u, a, w, near1, e1, r21, lane, nn);
 }
 
 // W warps per CTA (8 or 4: the autotuner's choice; 4 CTAs of 8 or 8 of 4 share an SM); FIELD: the crater
@@ -155,11 +153,12 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
   w.ci[lane] = ci;
   w.fx[lane] = w.fy[lane] = w.fz[lane] = w.lost[lane] = w.flow[lane] = 0.0f;
   w.nb[lane] = 0;
+  w.tn[lane] = 0;
   __syncthreads();   // spc, and every owner slot
   const int sh = u.GShift;
   const uint32_t gm = (uint32_t)u.GMask;
   const uint4 *seats = reinterpret_cast<const uint4 *>(a.seats);
-  int qn = 0, nn = 0;   // queue fills (warp-uniform)
+  int qn = 0;   // queue fill (warp-uniform)
   // stage 1: the 27 neighbour cells in the reference's order, the warp in lockstep
 #pragma unroll 1
   for (int dz = 0; dz < 3; ++dz) {
@@ -210,21 +209,32 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
         __syncwarp();
         while (qn >= 64) {
           qn -= 64;
-          drain_candidates(u, a, w, qn, 64, lane, nn);
+          drain_candidates(u, a, w, qn, 64, lane);
         }
       }
     }
   }
   if (qn >= 32) {
     qn -= 32;
-    drain_candidates(u, a, w, qn, 32, lane, nn);
+    drain_candidates(u, a, w, qn, 32, lane);
   }
-  if (qn > 0) drain_candidates(u, a, w, 0, qn, lane, nn);
-  if (nn > 0) drain_neighbours(u, a, w, 0, nn, lane);
+  if (qn > 0) drain_candidates(u, a, w, 0, qn, lane);
   __syncwarp();
   if (!live) return;
-  const f3 push = mk(w.fx[lane], w.fy[lane], w.fz[lane]);
-  const float lost = w.lost[lane], flow = w.flow[lane], nb = (float)w.nb[lane];
+  // stage 3: each owner's touching neighbours in its own lane, the sums in registers
+  f3 push = mk(w.fx[lane], w.fy[lane], w.fz[lane]);
+  float lost = w.lost[lane], flow = w.flow[lane];
+  const float nb = (float)w.nb[lane];
+  const int nt = min(w.tn[lane], kTCap);
+  for (int k = 0; k < nt; ++k) {
+    const uint32_t j = w.tl[k][lane];
+    const float4 Pj = __ldg(a.pos + j);
+    const f3 d = xsub3(xyz(Pj), p);
+    const Contact c = contact_of(u, a, P, V, ri, ci, j, __fsqrt_rn(xdot(d, d)));
+    push = push + c.push;
+    lost += c.lost;
+    flow += c.flow;
+  }
   f3 grav = mk(0.0f, 0.0f, 0.0f), g;
   if (FIELD) {
     grav = ld3(u.gField);   // SIM_GRAV_FIELD, src/glsl-sim.js:490-492: the whole of gravity
