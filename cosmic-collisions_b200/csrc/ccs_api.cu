@@ -119,7 +119,7 @@ struct ccs_handle {
   int ping = 0;
   bool useGraphs = true;
   // launch shapes chosen by ccs_autotune: contact-step warps per CTA, cell-gravity threads per cell
-  int tuneWarps = 8, tuneSplit = 4;
+  int tuneWarps = 4, tuneSplit = 4;
   // timing of chosen kernels with events on the stream
   int timing = 0;                       // ccs_timing's mask of kernel ids
   int timingEvery = 1;                  // ccs_timing_every: the contact step timed on every n-th launch

@@ -226,7 +226,8 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
   float lost = w.lost[lane], flow = w.flow[lane];
   const float nb = (float)w.nb[lane];
   const int nt = min(w.tn[lane], kTCap);
-  for (int k = 0; k < nt; ++k) {
+#pragma unroll 4
+  for (int k = 0; k < nt; ++k) {   // unrolled: the next contacts' loads are in flight with this one's math
     const uint32_t j = w.tl[k][lane];
     const float4 Pj = __ldg(a.pos + j);
     const f3 d = xsub3(xyz(Pj), p);
