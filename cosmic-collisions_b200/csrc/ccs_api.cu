@@ -116,6 +116,9 @@ struct ccs_handle {
   // graphs
   std::map<GraphKey, GraphSlot> graphs;
   std::map<StepKey, GraphSlot> stepGraphs;
+  // ccs_advance_host's read-back of its last step's first half, overlapping the second half's contact step
+  cudaStream_t cst = nullptr;
+  cudaEvent_t halfEv = nullptr, copyEv = nullptr;
   int ping = 0;
   bool useGraphs = true;
   // launch shapes chosen by ccs_autotune: contact-step warps per CTA, cell-gravity threads per cell
@@ -493,8 +496,8 @@ void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
 // buffers it touches; the uniform ping-pong lets the host run a step ahead.  When the contact step is being
 // timed (ccs_timing bit 0), the graph stops before it and the contact step is launched directly between
 // its two events (events recorded by a graph's nodes do not time).
-int step_graph(ccs_handle *h, const StepPlan &p) {
-  const bool timed = time_this(h, 0);
+int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false, const ccs_uniforms **Uout = nullptr) {
+  const bool timed = time_this(h, 0) || simOutside;
   const StepKey key{(int)p.slots, (int)p.mesh, (int)(p.u.boxB > 0.5f), h->ppCount > 0, h->nn != nullptr,
                     h->seatCur, h->cur, h->ping, (int)h->field, (int)timed};
   GraphSlot &g = h->stepGraphs[key];
@@ -534,7 +537,10 @@ int step_graph(ccs_handle *h, const StepPlan &p) {
   CUDA_TRY(h, cudaGraphLaunch(g.exec, h->st));
   h->seatCur = seatCur0 ^ (p.slots ? 1 : 0);
   h->launches += block_launches(h, &p, 1);
-  if (timed) {
+  if (simOutside) {
+    --h->launches;            // the caller launches the contact step
+    *Uout = g.dev;
+  } else if (timed) {
     --h->launches;            // pass_sim counts its own
     pass_sim(h, g.dev);       // reads the uniforms the graph's memcpy node wrote
   } else {
@@ -735,6 +741,9 @@ int ccs_destroy(ccs_handle *h) {
   free_state(h);
   for (auto ev : h->evPool) cudaEventDestroy(ev);
   if (h->readEv) cudaEventDestroy(h->readEv);
+  if (h->halfEv) cudaEventDestroy(h->halfEv);
+  if (h->copyEv) cudaEventDestroy(h->copyEv);
+  if (h->cst) cudaStreamDestroy(h->cst);
   if (h->uniDev) cudaFree(h->uniDev);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
@@ -2023,6 +2032,42 @@ int ccs_pass_diag(ccs_handle *h) {
   return diag_pass(h);
 }
 
+// the last step of a host-buffer call: its contact step in two halves, the first half's outputs read back on
+// a second stream while the second half runs (the copies over PCIe are most of such a call's time)
+static int last_step_overlapped(ccs_handle *h, float *pos4_out, float *vel4_out, float *aux4_out, float *q_out) {
+  if (!h->cst) {
+    CUDA_TRY(h, cudaStreamCreateWithFlags(&h->cst, cudaStreamNonBlocking));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->halfEv, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->copyEv, cudaEventDisableTiming));
+  }
+  StepPlan p = plan_step(h, 0, 0);
+  const ccs_uniforms *U = nullptr;
+  int rc = step_graph(h, p, true, &U);   // the grid, the mesh and the pairwise pass
+  if (rc) return rc;
+  const SimArgs a = sim_args(h);
+  const int N = h->N, half = std::min(N, (N / 2 + 255) / 256 * 256), d = h->cur ^ 1;
+  h->launches += launch_simulate_range(U, N, a, h->st, h->tuneWarps, h->field, 0, half);
+  CUDA_TRY(h, cudaEventRecord(h->halfEv, h->st));
+  h->launches += launch_simulate_range(U, N, a, h->st, h->tuneWarps, h->field, half, N - half);
+  CUDA_TRY(h, cudaStreamWaitEvent(h->cst, h->halfEv, 0));
+  auto read = [&](cudaStream_t st, int i0, int n) -> int {
+    if (n <= 0) return CCS_OK;
+    const size_t o4 = 4 * (size_t)i0, b4 = 16 * (size_t)n;
+    if (pos4_out) CUDA_TRY(h, cudaMemcpyAsync(pos4_out + o4, h->pos[d] + i0, b4, cudaMemcpyDeviceToHost, st));
+    if (vel4_out) CUDA_TRY(h, cudaMemcpyAsync(vel4_out + o4, h->vel[d] + i0, b4, cudaMemcpyDeviceToHost, st));
+    if (aux4_out) CUDA_TRY(h, cudaMemcpyAsync(aux4_out + o4, h->aux[d] + i0, b4, cudaMemcpyDeviceToHost, st));
+    if (q_out) CUDA_TRY(h, cudaMemcpyAsync(q_out + i0, h->q[d] + i0, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+    return CCS_OK;
+  };
+  if ((rc = read(h->cst, 0, half))) return rc;
+  if ((rc = read(h->st, half, N - half))) return rc;
+  CUDA_TRY(h, cudaEventRecord(h->copyEv, h->cst));
+  CUDA_TRY(h, cudaStreamWaitEvent(h->st, h->copyEv, 0));
+  h->cur = d;
+  h->sim.t += h->sim.dt;   // the frame loop's clock, as ccs_steps keeps it
+  return CCS_OK;
+}
+
 int ccs_advance_host(ccs_handle *h, const float *pos4, const float *vel4, const float *q, int nsteps, float *pos4_out,
                      float *vel4_out, float *aux4_out, float *q_out) {
   int rc = ensure_built(h);
@@ -2033,6 +2078,15 @@ int ccs_advance_host(ccs_handle *h, const float *pos4, const float *vel4, const 
   if (pos4) CUDA_TRY(h, cudaMemcpyAsync(h->pos[h->cur], pos4, 16 * N, cudaMemcpyHostToDevice, h->st));
   if (vel4) CUDA_TRY(h, cudaMemcpyAsync(h->vel[h->cur], vel4, 16 * N, cudaMemcpyHostToDevice, h->st));
   if (q) CUDA_TRY(h, cudaMemcpyAsync(h->q[h->cur], q, 4 * N, cudaMemcpyHostToDevice, h->st));
+  const bool reads = pos4_out || vel4_out || aux4_out || q_out;
+  if (nsteps > 0 && reads && h->useGraphs && h->timing == 0) {
+    rc = ccs_steps(h, nsteps - 1);
+    if (rc) return rc;
+    rc = last_step_overlapped(h, pos4_out, vel4_out, aux4_out, q_out);
+    if (rc) return rc;
+    CUDA_TRY(h, cudaStreamSynchronize(h->st));
+    return check_launch(h);
+  }
   rc = ccs_steps(h, nsteps);
   if (rc) return rc;
   if (pos4_out) CUDA_TRY(h, cudaMemcpyAsync(pos4_out, h->pos[h->cur], 16 * N, cudaMemcpyDeviceToHost, h->st));

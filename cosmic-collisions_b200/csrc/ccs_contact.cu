@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
   if (threadIdx.x < 16) spc[threadIdx.x] = xmul(__fdiv_rn((float)threadIdx.x + 0.5f, 15.0f), u.cell);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   ContactWarp &w = reinterpret_cast<ContactWarp *>(smem_raw)[wid];
-  const int me = blockIdx.x * kThreads + threadIdx.x;
+  const int me = a.first + blockIdx.x * kThreads + threadIdx.x;
   const bool live = me < u.N;
   const float cell = u.cell;
   float4 P = make_float4(0, 0, 0, 0), V = make_float4(0, 0, 0, 0);
@@ -301,16 +301,24 @@ cudaError_t init_kernels() {
   return e;
 }
 
-int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st, int warps, bool field) {
+int launch_simulate_range(const ccs_uniforms *u, int N, SimArgs a, cudaStream_t st, int warps, bool field, int first,
+                          int count) {
+  (void)N;
+  a.first = first;
+  if (count <= 0) return 0;
   if (warps == 4 && field)
-    k_contact_step<4, true><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+    k_contact_step<4, true><<<blocks_for(count, 128), 128, contact_smem_bytes(4), st>>>(u, a);
   else if (warps == 4)
-    k_contact_step<4, false><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+    k_contact_step<4, false><<<blocks_for(count, 128), 128, contact_smem_bytes(4), st>>>(u, a);
   else if (field)
-    k_contact_step<8, true><<<blocks_for(N, 256), 256, contact_smem_bytes(8), st>>>(u, a);
+    k_contact_step<8, true><<<blocks_for(count, 256), 256, contact_smem_bytes(8), st>>>(u, a);
   else
-    k_contact_step<8, false><<<blocks_for(N, 256), 256, contact_smem_bytes(8), st>>>(u, a);
+    k_contact_step<8, false><<<blocks_for(count, 256), 256, contact_smem_bytes(8), st>>>(u, a);
   return 1;
+}
+
+int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st, int warps, bool field) {
+  return launch_simulate_range(u, N, a, st, warps, field, 0, N);
 }
 
 }  // namespace ccs

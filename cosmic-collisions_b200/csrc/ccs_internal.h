@@ -79,6 +79,7 @@ struct SimArgs {
   int cap;
   float4 *posO, *velO, *auxO;
   float *qO;
+  int first = 0;   // the launch's first particle (a launch over a range of them)
 };
 
 struct DiagArgs {
@@ -104,6 +105,9 @@ int launch_contact_grid(const ccs_uniforms *u, int N, const float4 *pos, uint32_
 // warps: CTA width of the contact step, 8 or 4
 int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st, int warps = 8,
                     bool field = false);
+// the contact step for particles [first, first + count) only; first a multiple of 256
+int launch_simulate_range(const ccs_uniforms *u, int N, SimArgs a, cudaStream_t st, int warps, bool field, int first,
+                          int count);
 int launch_deposit(const ccs_uniforms *u, int N, int box, const float4 *pos, const float *mat, const float4 *monoPrev,
                    float4 *fine, cudaStream_t st);
 int launch_coarse(const MeshBuf &m, cudaStream_t st);
