@@ -118,7 +118,7 @@ struct ccs_handle {
   std::map<StepKey, GraphSlot> stepGraphs;
   // ccs_advance_host's read-back of its last step's first half, overlapping the second half's contact step
   cudaStream_t cst = nullptr;
-  cudaEvent_t halfEv = nullptr, copyEv = nullptr;
+  cudaEvent_t halfEv = nullptr, copyEv = nullptr, inEv = nullptr;
   int ping = 0;
   bool useGraphs = true;
   // launch shapes chosen by ccs_autotune: contact-step warps per CTA, cell-gravity threads per cell
@@ -743,6 +743,7 @@ int ccs_destroy(ccs_handle *h) {
   if (h->readEv) cudaEventDestroy(h->readEv);
   if (h->halfEv) cudaEventDestroy(h->halfEv);
   if (h->copyEv) cudaEventDestroy(h->copyEv);
+  if (h->inEv) cudaEventDestroy(h->inEv);
   if (h->cst) cudaStreamDestroy(h->cst);
   if (h->uniDev) cudaFree(h->uniDev);
   if (h->st) cudaStreamDestroy(h->st);
@@ -2034,16 +2035,27 @@ int ccs_pass_diag(ccs_handle *h) {
 
 // the last step of a host-buffer call: its contact step in two halves, the first half's outputs read back on
 // a second stream while the second half runs (the copies over PCIe are most of such a call's time)
-static int last_step_overlapped(ccs_handle *h, float *pos4_out, float *vel4_out, float *aux4_out, float *q_out) {
+static int ensure_copy_stream(ccs_handle *h) {
   if (!h->cst) {
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->cst, cudaStreamNonBlocking));
     CUDA_TRY(h, cudaEventCreateWithFlags(&h->halfEv, cudaEventDisableTiming));
     CUDA_TRY(h, cudaEventCreateWithFlags(&h->copyEv, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->inEv, cudaEventDisableTiming));
   }
+  return CCS_OK;
+}
+
+// inputsOnCopyStream: vel and q are still arriving on the copy stream (the grid, the mesh and the pairwise pass
+// need only the positions), and the contact step waits for them
+static int last_step_overlapped(ccs_handle *h, float *pos4_out, float *vel4_out, float *aux4_out, float *q_out,
+                                bool inputsOnCopyStream) {
+  int rc = ensure_copy_stream(h);
+  if (rc) return rc;
   StepPlan p = plan_step(h, 0, 0);
   const ccs_uniforms *U = nullptr;
-  int rc = step_graph(h, p, true, &U);   // the grid, the mesh and the pairwise pass
+  rc = step_graph(h, p, true, &U);   // the grid, the mesh and the pairwise pass
   if (rc) return rc;
+  if (inputsOnCopyStream) CUDA_TRY(h, cudaStreamWaitEvent(h->st, h->inEv, 0));
   const SimArgs a = sim_args(h);
   const int N = h->N, half = std::min(N, (N / 2 + 255) / 256 * 256), d = h->cur ^ 1;
   h->launches += launch_simulate_range(U, N, a, h->st, h->tuneWarps, h->field, 0, half);
@@ -2075,14 +2087,22 @@ int ccs_advance_host(ccs_handle *h, const float *pos4, const float *vel4, const 
   if (nsteps < 0) return CCS_E_ARG;
   cudaSetDevice(h->device);
   const size_t N = (size_t)h->N;
-  if (pos4) CUDA_TRY(h, cudaMemcpyAsync(h->pos[h->cur], pos4, 16 * N, cudaMemcpyHostToDevice, h->st));
-  if (vel4) CUDA_TRY(h, cudaMemcpyAsync(h->vel[h->cur], vel4, 16 * N, cudaMemcpyHostToDevice, h->st));
-  if (q) CUDA_TRY(h, cudaMemcpyAsync(h->q[h->cur], q, 4 * N, cudaMemcpyHostToDevice, h->st));
   const bool reads = pos4_out || vel4_out || aux4_out || q_out;
-  if (nsteps > 0 && reads && h->useGraphs && h->timing == 0) {
+  const bool overlapped = nsteps > 0 && reads && h->useGraphs && h->timing == 0;
+  // a one-step call: velocities and heat come over on the copy stream while the step's grid and mesh run
+  const bool split = overlapped && nsteps == 1;
+  if (split && (rc = ensure_copy_stream(h))) return rc;
+  if (split) CUDA_TRY(h, cudaEventRecord(h->inEv, h->st));   // the copy stream starts after what came before
+  if (split) CUDA_TRY(h, cudaStreamWaitEvent(h->cst, h->inEv, 0));
+  cudaStream_t vs = split ? h->cst : h->st;
+  if (pos4) CUDA_TRY(h, cudaMemcpyAsync(h->pos[h->cur], pos4, 16 * N, cudaMemcpyHostToDevice, h->st));
+  if (vel4) CUDA_TRY(h, cudaMemcpyAsync(h->vel[h->cur], vel4, 16 * N, cudaMemcpyHostToDevice, vs));
+  if (q) CUDA_TRY(h, cudaMemcpyAsync(h->q[h->cur], q, 4 * N, cudaMemcpyHostToDevice, vs));
+  if (split) CUDA_TRY(h, cudaEventRecord(h->inEv, h->cst));
+  if (overlapped) {
     rc = ccs_steps(h, nsteps - 1);
     if (rc) return rc;
-    rc = last_step_overlapped(h, pos4_out, vel4_out, aux4_out, q_out);
+    rc = last_step_overlapped(h, pos4_out, vel4_out, aux4_out, q_out, split);
     if (rc) return rc;
     CUDA_TRY(h, cudaStreamSynchronize(h->st));
     return check_launch(h);
