@@ -5,8 +5,8 @@ order; the device runs each sweep as 27 race-free phases of cells, so the
 same pushes happen in another order and the pile comes out equivalent, not
 bit-identical.  Everything else the builder makes -- the run's scalars, the
 layers and masses, the tags, the velocities, the home positions -- must be
-identical.  The relaxed piles are compared as the relaxation is meant to be
-judged: each particle ends within a small fraction of a radius of where the
+identical.  The relaxed piles are compared as a relaxation is meant to be
+assessed: each particle ends within a small fraction of a radius of where the
 host puts it, and the overlaps left (pairs closer than 0.96 diameters) have
 the same count, mean and worst case to within a few tens of per cent.
 """
