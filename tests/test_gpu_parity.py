@@ -138,6 +138,52 @@ def test_contact_step(nb, ccmod, orc, settle, kick):
     assert np.abs(qo).max() > 0 or settle
 
 
+def test_contact_step_crowded_particle(nb, ccmod, orc):
+    """A particle touching more neighbours than the kernel lists per owner (16): twenty on a sphere of 1.5
+    radii around it, away from the bodies (those past a cell's eight seats unseated, as always).  The contacts past the list are worked out as they are found and
+    added atomically; counts exact, state to tolerance, as for every other particle."""
+    osim, pos, vel, mat, q = oracle_state(orc, settle_steps=4)
+    vel = with_motion(pos, vel, scale=0.05)
+    a = osim.a
+    c = np.array([3.0, 3.0, 3.0])
+    k = np.arange(20) + 0.5
+    z = 1 - 2 * k / 20
+    phi = np.pi * (3 - np.sqrt(5)) * k
+    ring = np.stack([np.sqrt(1 - z * z) * np.cos(phi), np.sqrt(1 - z * z) * np.sin(phi), z], 1) * 1.5 * a
+    pos = pos.copy()
+    pos[0, :3] = c
+    pos[1:21, :3] = c + ring            # the lowest indices, so every one of them holds a seat
+    nb.upload(to_lib_sim(ccmod, osim), pos, vel, mat)
+    nb.write_state(q=q)
+    nb.pass_slots()
+    nb.pass_sim(0, 0, 0.0)
+    got = nb.read_state()
+    u = uni_for(orc, osim)
+    u.settle, u.kick, u.gdt = 0.0, 0.0, 0.0
+    for kk in range(3):
+        u.bulk0[kk], u.bulk1[kk] = osim.bulk0[kk], osim.bulk1[kk]
+        u.cen0[kk], u.cen1[kk] = osim.cen0[kk], osim.cen1[kk]
+    seats = orc.slots(u, pos)
+    N = osim.N
+    zf = np.zeros(((orc.FINE + 1), 4), np.float32)
+    z4 = np.zeros(4, np.float32)
+    slot = np.full(N, -1, np.int32)
+    ppf = np.zeros((4 * orc.PP_CAP, 4), np.float32)
+    po, vo, ao, qo = (np.zeros((N, 4), np.float32), np.zeros((N, 4), np.float32), np.zeros((N, 4), np.float32),
+                      np.zeros(N, np.float32))
+    P = orc.ptr
+    orc.lib().orc_sim_pass(C.byref(u), P(pos), P(vel), P(mat), P(q), P(seats), P(zf), P(z4), P(zf), P(z4), P(slot),
+                           P(ppf), orc.PP_CAP, P(po), P(vo), P(ao), P(qo))
+    assert ao[0, 3] > 16          # more touching neighbours than a list holds (a cell's ninth is unseated)
+    assert np.array_equal(got["aux"][:, 3], ao[:, 3])
+    for name, x, y in (("pos", got["pos"][:, :3], po[:, :3]), ("vel", got["vel"][:, :3], vo[:, :3]),
+                       ("q", got["q"], qo)):
+        assert scaled_err(x, y) < TOL, name
+    dv1 = got["vel"][0, :3].astype(np.float64) - vel[0, :3]
+    dv2 = vo[0, :3].astype(np.float64) - vel[0, :3]
+    assert np.abs(dv1 - dv2).max() <= 1e-4 * np.abs(dv2).max()   # the crowded particle's own kick
+
+
 def set_box(sim, cen, vel=(0.0, 0.0, 0.0), on_b=False, cen_b=(0.0, 0.0, 0.0)):
     sim.boxOn[0] = 1
     sim.boxOn[1] = 1 if on_b else 0
