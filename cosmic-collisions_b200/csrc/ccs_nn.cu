@@ -36,6 +36,8 @@
 //
 // The input goes in as a high and a low BF16 part (both multiplied by the
 // same BF16 weights), so the offset keeps about 16 bits through layer 1.
+#include <algorithm>
+
 #include "ccs_device.cuh"
 #include "ccs_internal.h"
 #include "ccs_umma.cuh"
@@ -331,6 +333,8 @@ __global__ void __launch_bounds__(kRows, 1) k_nn_forward(Rows rows, const uint8_
   uint64_t *bar = reinterpret_cast<uint64_t *>(sm + fMisc);
   uint32_t *slot = reinterpret_cast<uint32_t *>(sm + fMisc + 8);
   const float *b1 = reinterpret_cast<const float *>(sm + fBias), *b2 = b1 + 64, *b3 = b2 + 64;
+  const long n = rows.count(), tiles = (n + kRows - 1) / kRows;
+  if (blockIdx.x >= tiles) return;   // no tile for this CTA: nothing loaded, nothing allocated
   load_image(img, sm + fW, sm + fBias);
   if (t == 0) mbar_init(bar, 1);
   if (warp == 0) tmem_alloc(slot, 128);
@@ -339,7 +343,6 @@ __global__ void __launch_bounds__(kRows, 1) k_nn_forward(Rows rows, const uint8_
   fence_after();
   const uint32_t tm = *slot, lane = tm + ((uint32_t)(warp * 32) << 16);
   const uint32_t base = smem_u32(sm);
-  const long n = rows.count(), tiles = (n + kRows - 1) / kRows;
   uint32_t phase = 0;
   bool ok = true;
   for (long tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
@@ -708,13 +711,14 @@ __global__ void __launch_bounds__(256) k_nn_pp_pairs(const ccs_uniforms *__restr
                                                      const float4 *__restrict__ list, int cap,
                                                      const int *__restrict__ offs, int *__restrict__ counts,
                                                      int2 *__restrict__ pairs) {
-  const int me = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warps = (gridDim.x * blockDim.x) >> 5;
   const ccs_uniforms &u = *U;
   const int count = u.ppCount;
-  if (me >= count || me >= cap) return;   // whole warps
+  const float cutN = xmul(0.5f, u.cut), cut2 = xmul(cutN, cutN);
+  // a warp per target, the grid striding over the list's length (read on the device)
+  for (int me = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; me < min(count, cap); me += warps) {
   const float4 P = list[me];
   const bool active = P.w != 0.0f;
-  const float cutN = xmul(0.5f, u.cut), cut2 = xmul(cutN, cutN);
   int n = 0;
   const int at = pairs ? offs[me] : 0;
   if (active) {
@@ -731,6 +735,7 @@ __global__ void __launch_bounds__(256) k_nn_pp_pairs(const ccs_uniforms *__restr
     }
   }
   if (!pairs && lane == 0) counts[me] = n;
+  }
 }
 
 // exclusive scan of the targets' pair counts: offs[0..count], total = offs[count]
@@ -779,13 +784,14 @@ __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__rest
                                                       int cap, const float2 *__restrict__ tab,
                                                       const int2 *__restrict__ pairs, const int *__restrict__ offs,
                                                       const float4 *__restrict__ mesh, float4 *__restrict__ force) {
-  const int me = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (me >= cap) return;   // whole warps
+  const int lane = threadIdx.x & 31, warps = (gridDim.x * blockDim.x) >> 5;
   const ccs_uniforms &u = *U;
   const int count = u.ppCount;
+  // a warp per target, the grid striding over the list's length; only the list's seats are ever read
+  for (int me = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; me < min(count, cap); me += warps) {
   float4 o = make_float4(0, 0, 0, 0);
   const float4 P = list[me];
-  if (me < count && P.w != 0.0f) {
+  if (P.w != 0.0f) {
     const float myBox = box[me];
     const float cutN = xmul(0.5f, u.cut), a2 = u.a2, a = fsqrt(a2);
     const float binScale = fdiv(64.0f, u.cut), taperScale = fdiv(1.0f, 0.8f * cutN - cutN);
@@ -826,6 +832,7 @@ __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__rest
     o = make_float4(acc.x * u.Gm, acc.y * u.Gm, acc.z * u.Gm, pot * u.Gm);
   }
   if (lane < 4) force[(size_t)lane * cap + me] = lane == 0 ? o : make_float4(0, 0, 0, 0);
+  }
 }
 
 int forward_grid() {
@@ -849,13 +856,14 @@ size_t nn_pp_count_ints() { return (size_t)CCS_PP_CAP + 1; }
 int launch_pp_nn(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,
                  const uint8_t *img, int *counts, int *offs, int *total, int2 *pairs, float4 *mesh, float4 *force,
                  unsigned *status, cudaStream_t st) {
-  const int g = (cap * 32 + 255) / 256;   // a warp per list entry
+  // grids striding over the list's length on the device, so a captured launch serves any length
+  const int g = std::min((cap * 32 + 255) / 256, 8 * (nn::forward_grid() / 3));
   nn::k_nn_pp_pairs<<<g, 256, 0, st>>>(u, list, cap, nullptr, counts, nullptr);
   nn::k_nn_pp_scan<<<1, 1024, 0, st>>>(u, counts, offs, total);
   nn::k_nn_pp_pairs<<<g, 256, 0, st>>>(u, list, cap, offs, counts, pairs);
   nn::LoosePairs rows{u, list, pairs, total};
   nn::k_nn_forward<nn::LoosePairs><<<nn::forward_grid(), nn::kRows, nn::kFwdSmem, st>>>(rows, img, mesh, status);
-  nn::k_nn_pp_reduce<<<(cap * 32 + 255) / 256, 256, 0, st>>>(u, list, box, cap, tab, pairs, offs, mesh, force);
+  nn::k_nn_pp_reduce<<<g, 256, 0, st>>>(u, list, box, cap, tab, pairs, offs, mesh, force);
   return 5;
 }
 
