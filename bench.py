@@ -17,7 +17,9 @@ A step is one full-phase step of the reference schedule (contact grid every
            the library's stream, with L2 flushed (a 256 MiB write) before every
            step, so each step starts from HBM.  Max over ranks.
   e2e      the same metric through the host-buffer C-ABI call
-           (ccs_advance_host: pinned host state in, one step, state out).
+           (ccs_advance_host: pinned host state in, one step, state out);
+           pcie_floor: the same bytes as plain pinned copies, in then out,
+           which bound that call from below.
   roofline the contact step kernel (k_contact_step): algorithmic bytes (92 B per
            particle: pos, vel, mat, q in; pos, vel, aux, q out) over its mean
            event-timed duration, against the measured HBM copy bandwidth.
@@ -104,6 +106,36 @@ def measured_peaks():
         except Exception:
             pass
     return 6650.0, "fallback"
+
+
+def pcie_floor(hp, hv, hq, ha, dev, reps=20):
+    """The copies of one host-buffer call as plain pinned copies on this box: the inputs (positions,
+    velocities, heat) in, then the outputs (positions, velocities, aux, heat) out.  Their sum bounds a
+    one-step call from below, since no output exists before the inputs have arrived."""
+    import torch
+    N = hp.shape[0]
+    d = torch.empty(13 * N, dtype=torch.float32, device=dev)
+    ins = ((d[:4 * N], hp), (d[4 * N:8 * N], hv), (d[8 * N:9 * N], hq))
+    outs = ((hp, d[:4 * N]), (hv, d[4 * N:8 * N]), (ha, d[8 * N:12 * N]), (hq, d[12 * N:]))
+
+    def us(pairs):
+        for dst, src in pairs:
+            dst.view(-1).copy_(src.view(-1), non_blocking=True)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(reps):
+            for dst, src in pairs:
+                dst.view(-1).copy_(src.view(-1), non_blocking=True)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) / reps * 1e6
+
+    # the outputs' copy overwrites the host inputs with device scratch: put the inputs back afterwards
+    keep = [t.clone() for t in (hp, hv, hq)]
+    h2d_us, d2h_us = us(ins), us(outs)
+    for t, k in zip((hp, hv, hq), keep):
+        t.copy_(k)
+    return {"h2d_us": h2d_us, "d2h_us": d2h_us, "bound_us_per_call": h2d_us + d2h_us,
+            "how": "the same bytes as plain pinned cudaMemcpyAsync copies, in then out, on this box"}
 
 
 def committed_traffic():
@@ -585,6 +617,7 @@ def run_ours(args, rank, world, log):
     e2e_s = max_over_ranks(time.perf_counter() - e0)
     h2d = N * (16 + 16 + 4)
     d2h = N * (16 + 16 + 16 + 4)
+    copy_floor = pcie_floor(hp, hv, hq, ha, dev)
 
     ferr = force_error(cc, dev, N) if rank == 0 else None
     analysis = analysis_timing(cc, nb) if rank == 0 and not args.no_cpu else None
@@ -643,7 +676,9 @@ def run_ours(args, rank, world, log):
             "kernels_us": {k: v["mean_us"] for k, v in kt.items()},
         },
         "e2e": {"value": world * N * e2e_steps / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "api": "ccs_advance_host, one step per call, pinned host buffers"},
+                "d2h_bytes_per_step": d2h, "api": "ccs_advance_host, one step per call, pinned host buffers",
+                "us_per_call": e2e_s / e2e_steps * 1e6, "pcie_floor": copy_floor,
+                "floor_frac": copy_floor["bound_us_per_call"] / (e2e_s / e2e_steps * 1e6)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "peak_kind": peak_kind + " hbm_gbs",
                      "kernel": "k_contact_step (contacts + gather + kick/drift)",

@@ -12,7 +12,9 @@
 //      nearest-point test, loads its cell's seats, applies the reference's
 //      quantised seat cull to each (where the seat sat at the rebuild, to a
 //      fifteenth of a cell: beyond reach, the reference never fetches it)
-//      and appends the seats that pass to a per-warp queue in shared memory;
+//      and appends the seats that pass to a per-warp queue in shared memory
+//      (a cell's seats fill from the front, so the walk over them stops at
+//      the first seat that is empty in every lane's cell);
 //   2. candidates: 32 or 64 queued seats at a time, one or two per lane: load
 //      the neighbour's position; a pair inside the link radius adds to its
 //      owner's count (a shared-memory integer atomic), and a touching one goes
@@ -186,14 +188,12 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
           s0 = __ldg(cp);       // both halves of the cell: one 32-byte sector, one round trip
           s1 = __ldg(cp + 1);
         }
-        const bool more = __any_sync(0xFFFFFFFFu, !(s0.w & 0x80000000u));   // any cell with more than four?
+        {
+          const uint32_t sv[kSeats] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-          if (half && !more) break;
-          const uint4 s = half ? s1 : s0;
-          const uint32_t sv[4] = {s.x, s.y, s.z, s.w};
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
+          for (int k = 0; k < kSeats; ++k) {
+            // a cell's seats fill from the front: the walk ends at the first seat empty in every lane's cell
+            if (!__any_sync(0xFFFFFFFFu, !(sv[k] & 0x80000000u))) break;
             bool seat = !(sv[k] & 0x80000000u) && (int)(sv[k] & 0x3FFFFu) != me;
             if (seat) {   // the quantised cull: where the seat sat at the rebuild, against this particle now
               const f3 dq = mk(xsub(xadd(lx, spc[(sv[k] >> 18) & 15u]), p.x),
