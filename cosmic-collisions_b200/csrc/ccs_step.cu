@@ -32,7 +32,11 @@ int launch_fill_u32(uint32_t *p, size_t n, uint32_t v, cudaStream_t st) {
 // compare-and-swap, carrying any displaced word further down; a word that
 // falls off the end is unseated.  Each seat only ever decreases, so the final
 // cell holds exactly the eight lowest indices in ascending order -- the depth
-// peel's result -- whatever order the threads arrive in.  The same launch
+// peel's result -- whatever order the threads arrive in.  A particle whose
+// warp holds r lower indices in the same cell starts at seat r: those r end
+// in the seats before its own whenever it is seated, and one with r >= 8 is
+// unseated at once.  In Morton order most cell-mates share a warp, so most
+// inserts take their seat at the first swap.  The same launch
 // retires the previous table by clearing the cells it touched, so the next
 // rebuild finds it empty without a memset of the 2 x G^3 x 32-byte tables.
 //
@@ -45,11 +49,11 @@ constexpr int kMaxRetries = 1 << 20;
 
 // Each seat is first tried as if it were empty: the swap checks the guess and, when it fails, returns the
 // seat's word -- one round trip a seat where a read and then a swap would take two.
-__device__ __forceinline__ void seat_insert(uint32_t *cell, uint32_t w, unsigned *status) {
+__device__ __forceinline__ void seat_insert(uint32_t *cell, uint32_t w, unsigned *status, int start) {
   uint32_t wi = w & 0x3FFFFu;
   int retries = 0;
 #pragma unroll 1
-  for (int k = 0; k < kSeats; ++k) {
+  for (int k = start; k < kSeats; ++k) {
     uint32_t cur = kEmpty;
     while (true) {
       if ((cur & 0x80000000u) != 0u || (cur & 0x3FFFFu) > wi) {
@@ -77,7 +81,17 @@ __global__ void __launch_bounds__(kBlock) k_contact_grid(const ccs_uniforms *__r
                                                          const uint32_t *__restrict__ hkOld, unsigned *status) {
   const ccs_uniforms &u = *U;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= u.N) return;
+  const bool live = i < u.N;
+  float4 P = make_float4(0, 0, 0, 0);
+  if (live) P = pos[i];
+  float gx, gy, gz;
+  int cx, cy, cz;
+  cell_of(u, xyz(P), gx, gy, gz, cx, cy, cz);
+  const uint32_t h = live ? hash_cell(u, cx, cy, cz) : 0xFFFFFFFFu;
+  // the lanes that share this cell hold ascending indices: the lower ones end in the seats before this one's
+  const unsigned mates = __match_any_sync(0xFFFFFFFFu, h);
+  if (!live) return;
+  const int start = __popc(mates & ((1u << (threadIdx.x & 31)) - 1u));
   const uint32_t old = hkOld[i];
   if (old != kNoCell) {
     uint4 *c = reinterpret_cast<uint4 *>(seatsOld + (size_t)old * kSeats);
@@ -85,17 +99,12 @@ __global__ void __launch_bounds__(kBlock) k_contact_grid(const ccs_uniforms *__r
     c[0] = e;
     c[1] = e;
   }
-  const float4 P = pos[i];
-  float gx, gy, gz;
-  int cx, cy, cz;
-  cell_of(u, xyz(P), gx, gy, gz, cx, cy, cz);
   const uint32_t qx = (uint32_t)clampf(xmul(xsub(gx, (float)cx), 15.0f), 0.0f, 14.0f);
   const uint32_t qy = (uint32_t)clampf(xmul(xsub(gy, (float)cy), 15.0f), 0.0f, 14.0f);
   const uint32_t qz = (uint32_t)clampf(xmul(xsub(gz, (float)cz), 15.0f), 0.0f, 14.0f);
   const uint32_t w = (uint32_t)i | (qx << 18) | (qy << 22) | (qz << 26) | 0x40000000u;
-  const uint32_t h = hash_cell(u, cx, cy, cz);
   hk[i] = h;
-  seat_insert(seats + (size_t)h * kSeats, w, status);
+  if (start < kSeats) seat_insert(seats + (size_t)h * kSeats, w, status, start);
 }
 
 int launch_contact_grid(const ccs_uniforms *u, int N, const float4 *pos, uint32_t *seats, uint32_t *hk,

@@ -5,6 +5,13 @@ stream while the second half's contact step runs.  Its outputs must be the
 step's own: the same run advanced through the device-resident path (write
 the state, ccs_steps, read it back) agrees to 1e-5 of each field's scale,
 with the neighbour counts exact, and the two runs keep the same clock.
+
+The device path itself varies from run to run in the last bits: the mesh
+deposit adds with float atomics, in no fixed order.  Over several steps the
+contact springs carry that variation to about 1e-5 of the velocities' scale
+(two device-path runs of three settling steps differ by 1.15e-5).  So a
+call of more than one step is held to 1e-5 or four times the spread between
+two device-path runs, whichever is larger; the counts stay exact.
 """
 import ctypes as C
 
@@ -25,9 +32,9 @@ def scaled_err(a, b):
 def test_host_call_matches_device_path(ccmod, nsteps):
     from cosmic_collisions_b200 import configs
     opt = configs.small_impact_opt(16384)
-    a, b = ccmod.NBody(0), ccmod.NBody(0)
+    a, b, c = ccmod.NBody(0), ccmod.NBody(0), ccmod.NBody(0)
     try:
-        for nb in (a, b):
+        for nb in (a, b, c):
             nb.build(opt)
             nb.settle_some(40)
             nb.sync()
@@ -39,15 +46,25 @@ def test_host_call_matches_device_path(ccmod, nsteps):
         rc = lib.ccs_advance_host(a.handle, P(pos), P(vel), P(q), nsteps, P(out["pos"]), P(out["vel"]),
                                   P(out["aux"]), P(out["q"]))
         assert rc == 0
-        b.write_state(pos=pos, vel=vel, q=q)
-        b.steps(nsteps)
-        ref = b.read_state()
+        refs = []
+        for nb in (b, c):
+            nb.write_state(pos=pos, vel=vel, q=q)
+            nb.steps(nsteps)
+            refs.append(nb.read_state())
+        ref = refs[0]
         assert (a.sim.stepNo, a.sim.t) == (b.sim.stepNo, b.sim.t)
         assert np.array_equal(out["aux"][:, 3], ref["aux"][:, 3])
+
+        def tol(k, cols=slice(0, 3)):
+            if nsteps == 1:
+                return 1e-5
+            return max(1e-5, 4 * scaled_err(refs[1][k][..., cols], ref[k][..., cols]))
+
         for k in ("pos", "vel", "aux"):
-            assert scaled_err(out[k][:, :3], ref[k][:, :3]) < 1e-5, k
-        assert scaled_err(out["q"], ref["q"]) < 1e-5
+            assert scaled_err(out[k][:, :3], ref[k][:, :3]) < tol(k), k
+        assert scaled_err(out["q"], ref["q"]) < tol("q", slice(None))
         assert np.array_equal(out["pos"], a.read_state()["pos"])   # what came back is the engine's state
     finally:
         a.close()
         b.close()
+        c.close()

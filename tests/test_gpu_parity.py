@@ -82,12 +82,18 @@ def test_contact_grid_is_exact(nb, ccmod, orc, N):
     assert np.array_equal(nb.buffer("seats"), orc.slots(u, pos2))
 
 
-def test_contact_grid_overfull_cells(nb, ccmod, orc):
-    # a dense blob overfills cells: the eight lowest indices keep the seats
+@pytest.mark.parametrize("order", ["scattered", "by_cell"])
+def test_contact_grid_overfull_cells(nb, ccmod, orc, order):
+    # a dense blob overfills cells: the eight lowest indices keep the seats.  "by_cell" numbers each cell's
+    # particles consecutively, so a warp holds up to 32 of one cell's particles and most start past seat 0
+    # or are unseated at once
     sim, pos, vel, mat, home = orc.build_run(orc.make_opt(16384))
     rng = np.random.default_rng(4)
     pos = pos.copy()
     pos[:, :3] = rng.normal(scale=0.1, size=(len(pos), 3)).astype(np.float32)
+    if order == "by_cell":
+        key = np.floor(pos[:, :3] / np.float32(uni_for(orc, sim).cell)).astype(np.int64)
+        pos = pos[np.lexsort((key[:, 0], key[:, 1], key[:, 2]))]
     nb.upload(to_lib_sim(ccmod, sim), pos, vel, mat)
     nb.pass_slots()
     want = orc.slots(uni_for(orc, sim), pos)
