@@ -5,7 +5,8 @@
 // mesh + P3M every 8th, gravity as one impulse), the phases (settle, rigid
 // approach, kick) and the analysis hand-off.  Per-step uniforms live in
 // device memory; `ccs_steps` replays captured CUDA graphs of whole 8-step
-// blocks whose uniform slots are refreshed by one memcpy node each replay.
+// blocks whose uniform slots are refreshed by one memcpy node each replay,
+// and `ccs_step` one step's graph whose root kernel writes its uniforms.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,6 +47,8 @@ struct GraphSlot {
   ccs_uniforms *host = nullptr;  // pinned staging the memcpy node reads at replay
   cudaEvent_t done = nullptr;    // recorded after the last replay
   bool used = false;
+  cudaGraph_t graph = nullptr;   // a step graph's template, kept for its uniforms node
+  cudaGraphNode_t put = nullptr; // a step graph's k_put_uniforms node, given each replay's uniforms
 };
 
 // one step's launches captured as a graph (ccs_step): its schedule, the buffers it reads and writes
@@ -491,9 +494,10 @@ void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
   pass_sim(h, U);
 }
 
-// one step replayed from a captured graph: the step's uniforms by one memcpy node from pinned memory, then
+// one step replayed from a captured graph: the step's uniforms by its root node, k_put_uniforms, whose
+// by-value argument is set before each replay (no copy engine or pinned staging on the step's path), then
 // its launches, so a step costs one cudaGraphLaunch.  Graphs are keyed by what the step runs and by the
-// buffers it touches; the uniform ping-pong lets the host run a step ahead.  When the contact step is being
+// buffers it touches.  When the contact step is being
 // timed (ccs_timing bit 0), the graph stops before it and the contact step is launched directly between
 // its two events (events recorded by a graph's nodes do not time).
 int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false, const ccs_uniforms **Uout = nullptr) {
@@ -504,15 +508,13 @@ int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false, const 
   const int seatCur0 = h->seatCur, cur0 = h->cur;
   if (!g.exec) {
     CUDA_TRY(h, cudaMalloc(&g.dev, sizeof(ccs_uniforms)));
-    CUDA_TRY(h, cudaMallocHost(&g.host, sizeof(ccs_uniforms)));
     CUDA_TRY(h, cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
-    *g.host = p.u;
     const int timing = h->timing;
     const int64_t l0 = h->launches;
     h->timing = 0;
     cudaGraph_t graph;
     CUDA_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-    cudaMemcpyAsync(g.dev, g.host, sizeof(ccs_uniforms), cudaMemcpyHostToDevice, h->st);
+    k_put_uniforms<<<1, 128, 0, h->st>>>(p.u, g.dev);   // the graph's root: each replay's uniforms, by value
     if (timed) enqueue_pre(h, p, g.dev);
     else enqueue_step(h, p, g.dev);
     cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
@@ -524,25 +526,38 @@ int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false, const 
       h->err = std::string("step graph capture: ") + cudaGetErrorString(ce);
       return CCS_E_CUDA;
     }
-    ce = cudaGraphInstantiate(&g.exec, graph, 0);
-    cudaGraphDestroy(graph);
+    size_t roots = 1;
+    ce = cudaGraphGetRootNodes(graph, &g.put, &roots);
+    if (ce == cudaSuccess && roots != 1) ce = cudaErrorInvalidValue;
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&g.exec, graph, 0);
     if (ce != cudaSuccess) {
+      cudaGraphDestroy(graph);
       h->err = std::string("step graph instantiate: ") + cudaGetErrorString(ce);
       g.exec = nullptr;
       return CCS_E_CUDA;
     }
+    g.graph = graph;
+  } else {
+    // this replay's uniforms into the root node's argument (launches already enqueued keep theirs)
+    ccs_uniforms u = p.u;
+    ccs_uniforms *dst = g.dev;
+    void *args[] = {&u, &dst};
+    cudaKernelNodeParams kp = {};
+    kp.func = reinterpret_cast<void *>(k_put_uniforms);
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(128);
+    kp.kernelParams = args;
+    CUDA_TRY(h, cudaGraphExecKernelNodeSetParams(g.exec, g.put, &kp));
   }
-  if (g.used) CUDA_TRY(h, cudaEventSynchronize(g.done));
-  *g.host = p.u;
   CUDA_TRY(h, cudaGraphLaunch(g.exec, h->st));
   h->seatCur = seatCur0 ^ (p.slots ? 1 : 0);
-  h->launches += block_launches(h, &p, 1);
+  h->launches += block_launches(h, &p, 1) + 1;   // and the uniforms node
   if (simOutside) {
     --h->launches;            // the caller launches the contact step
     *Uout = g.dev;
   } else if (timed) {
     --h->launches;            // pass_sim counts its own
-    pass_sim(h, g.dev);       // reads the uniforms the graph's memcpy node wrote
+    pass_sim(h, g.dev);       // reads the uniforms the graph's root node wrote
   } else {
     h->cur = cur0 ^ 1;
     if (h->timing & 1) ++h->timingSeq;   // a contact step that was not this sample's
@@ -565,6 +580,7 @@ int do_step(ccs_handle *h, int settle, int kick) {
 
 void free_graph_slot(GraphSlot &g) {
   if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.graph) cudaGraphDestroy(g.graph);
   if (g.dev) cudaFree(g.dev);
   if (g.host) cudaFreeHost(g.host);
   if (g.done) cudaEventDestroy(g.done);
