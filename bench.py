@@ -138,20 +138,35 @@ def pcie_floor(hp, hv, hq, ha, dev, reps=20):
             "how": "the same bytes as plain pinned cudaMemcpyAsync copies, in then out, on this box"}
 
 
-def committed_traffic():
-    """dram bytes per k_contact_step launch from the committed ncu summary, scaled to a launch of N particles."""
+def committed_profile():
+    """The k_contact_step figures of the committed ncu summary (profiles/contact_step_traffic.txt)."""
     p = os.path.join(ROOT, "profiles", "contact_step_traffic.txt")
-    if not os.path.exists(p):
-        return None
     vals = {}
-    for line in open(p):
-        if ":" in line and not line.startswith("#"):
-            k, v = line.split(":", 1)
-            vals[k.strip()] = v.strip()
-    try:
-        return float(vals["dram_bytes_per_particle"])
-    except Exception:
+    if os.path.exists(p):
+        for line in open(p):
+            if ":" in line and not line.startswith("#"):
+                k, v = line.split(":", 1)
+                try:
+                    vals[k.strip()] = float(v.strip())
+                except ValueError:
+                    pass
+    return vals
+
+
+def limiter_note():
+    """What bounds the roofline's kernel, from the committed ncu summary: it issues, it does not stream."""
+    v = committed_profile()
+    if "issue_active_pct" not in v:
         return None
+    return {"issue_active_pct": v["issue_active_pct"], "warp_instructions_per_particle":
+            v.get("warp_instructions_per_particle"), "dram_busy_pct": v.get("dram_busy_pct"),
+            "source": "the committed ncu --set full capture of the same workload; the state stays in L2, so the "
+                      "kernel is bound by instruction issue, not by HBM"}
+
+
+def committed_traffic():
+    """dram bytes per particle of a k_contact_step launch, from the committed ncu summary."""
+    return committed_profile().get("dram_bytes_per_particle")
 
 
 class Clocks:
@@ -686,7 +701,8 @@ def run_ours(args, rank, world, log):
                      "algorithmic_bytes_per_launch": ALG_BYTES_SIM * N,
                      "timed_launches": kt["simulate"]["launches"],
                      "timing": "CUDA events on the library's stream around every %dth contact step of the timed "
-                               "region" % TIME_EVERY},
+                               "region" % TIME_EVERY,
+                     "limiter": limiter_note()},
         "gpu_launches": int(launches),
         "clocks": clk,
         "force_error": ferr,

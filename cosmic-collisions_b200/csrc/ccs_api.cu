@@ -41,14 +41,22 @@ struct GraphKey {
   }
 };
 
+// a captured contact-step node: its uniforms are its first, by-value argument, so every replay sets them
+// (the other argument, the buffers, stays as captured: the template graph owns its storage)
+struct SimNode {
+  cudaGraphNode_t node = nullptr;
+  cudaKernelNodeParams kp = {};
+};
+
 struct GraphSlot {
   cudaGraphExec_t exec = nullptr;
   ccs_uniforms *dev = nullptr;   // meshEvery slots on the device
   ccs_uniforms *host = nullptr;  // pinned staging the memcpy node reads at replay
   cudaEvent_t done = nullptr;    // recorded after the last replay
   bool used = false;
-  cudaGraph_t graph = nullptr;   // a step graph's template, kept for its uniforms node
+  cudaGraph_t graph = nullptr;   // the template, kept for its nodes' arguments
   cudaGraphNode_t put = nullptr; // a step graph's k_put_uniforms node, given each replay's uniforms
+  std::vector<SimNode> sim;      // the contact-step nodes, in step order
 };
 
 // one step's launches captured as a graph (ccs_step): its schedule, the buffers it reads and writes
@@ -119,6 +127,8 @@ struct ccs_handle {
   // graphs
   std::map<GraphKey, GraphSlot> graphs;
   std::map<StepKey, GraphSlot> stepGraphs;
+  std::vector<cudaGraphNode_t> *simCapture = nullptr;   // while capturing: where pass_sim records its node
+  bool simCaptureLost = false;                          // a node it could not identify
   // ccs_advance_host's read-back of its last step's first half, overlapping the second half's contact step
   cudaStream_t cst = nullptr;
   cudaEvent_t halfEv = nullptr, copyEv = nullptr, inEv = nullptr;
@@ -415,11 +425,21 @@ SimArgs sim_args(const ccs_handle *h) {
   return a;
 }
 
-void pass_sim(ccs_handle *h, const ccs_uniforms *U) {
+void pass_sim(ccs_handle *h, const ccs_uniforms &u) {
   const SimArgs a = sim_args(h);
   cudaEvent_t b, e;
   time_begin(h, 0, &b, &e);
-  h->launches += launch_simulate(U, h->N, a, h->st, h->tuneWarps, h->field);
+  h->launches += launch_simulate(u, h->N, a, h->st, h->tuneWarps, h->field);
+  if (h->simCapture) {   // the node just captured is the capture's one sink
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    if (cudaStreamGetCaptureInfo(h->st, &cs, nullptr, nullptr, &deps, &nd) == cudaSuccess &&
+        cs == cudaStreamCaptureStatusActive && nd == 1)
+      h->simCapture->push_back(deps[0]);
+    else
+      h->simCaptureLost = true;
+  }
   time_end(h, e);
   if (h->timing & 1) ++h->timingSeq;
   h->cur ^= 1;
@@ -491,73 +511,126 @@ void enqueue_pre(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
 
 void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
   enqueue_pre(h, p, U);
-  pass_sim(h, U);
+  pass_sim(h, p.u);
 }
 
-// one step replayed from a captured graph: the step's uniforms by its root node, k_put_uniforms, whose
-// by-value argument is set before each replay (no copy engine or pinned staging on the step's path), then
-// its launches, so a step costs one cudaGraphLaunch.  Graphs are keyed by what the step runs and by the
-// buffers it touches.  When the contact step is being
-// timed (ccs_timing bit 0), the graph stops before it and the contact step is launched directly between
-// its two events (events recorded by a graph's nodes do not time).
-int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false, const ccs_uniforms **Uout = nullptr) {
+// after a capture: the contact-step nodes it recorded, with their captured arguments
+int resolve_sim_nodes(ccs_handle *h, const std::vector<cudaGraphNode_t> &nodes, std::vector<SimNode> &out) {
+  if (h->simCaptureLost) {
+    h->simCaptureLost = false;
+    h->err = "graph capture: a contact-step node was not identified";
+    return CCS_E_CUDA;
+  }
+  out.resize(nodes.size());
+  for (size_t i = 0; i < nodes.size(); ++i) {
+    out[i].node = nodes[i];
+    CUDA_TRY(h, cudaGraphKernelNodeGetParams(nodes[i], &out[i].kp));
+  }
+  return CCS_OK;
+}
+
+// a contact-step node of an instantiated graph given this replay's uniforms (replays already enqueued keep theirs)
+int set_sim_uniforms(ccs_handle *h, cudaGraphExec_t exec, const SimNode &n, const ccs_uniforms &u) {
+  ccs_uniforms v = u;
+  void *args[2] = {&v, n.kp.kernelParams[1]};
+  cudaKernelNodeParams kp = n.kp;
+  kp.kernelParams = args;
+  kp.extra = nullptr;
+  CUDA_TRY(h, cudaGraphExecKernelNodeSetParams(exec, n.node, &kp));
+  return CCS_OK;
+}
+
+void free_graph_slot(GraphSlot &g);
+
+// one step replayed from a captured graph, so a step costs one cudaGraphLaunch.  The contact step takes the
+// step's uniforms as its by-value argument, set in its node before each replay; the grid and mesh kernels
+// read them from device memory, written by the graph's root node, k_put_uniforms, whose by-value argument
+// is set the same way (no copy engine or pinned staging on the step's path).  Graphs are keyed by what
+// the step runs and by the buffers it touches.  When the contact step is being timed (ccs_timing bit 0),
+// or its caller launches it (simOutside), the graph stops before it and the contact step is launched
+// directly, between its two events when timed (events recorded by a graph's nodes do not time).
+int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false) {
   const bool timed = time_this(h, 0) || simOutside;
+  const bool pre = p.slots || p.mesh;   // kernels that read the uniforms from device memory
+  if (timed && !pre) {                  // nothing to replay: the contact step alone, launched directly
+    if (!simOutside) pass_sim(h, p.u);
+    return check_launch(h);
+  }
   const StepKey key{(int)p.slots, (int)p.mesh, (int)(p.u.boxB > 0.5f), h->ppCount > 0, h->nn != nullptr,
                     h->seatCur, h->cur, h->ping, (int)h->field, (int)timed};
   GraphSlot &g = h->stepGraphs[key];
   const int seatCur0 = h->seatCur, cur0 = h->cur;
   if (!g.exec) {
-    CUDA_TRY(h, cudaMalloc(&g.dev, sizeof(ccs_uniforms)));
-    CUDA_TRY(h, cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+    if (pre && !g.dev) CUDA_TRY(h, cudaMalloc(&g.dev, sizeof(ccs_uniforms)));
+    if (!g.done) CUDA_TRY(h, cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
     const int timing = h->timing;
     const int64_t l0 = h->launches;
-    h->timing = 0;
     cudaGraph_t graph;
+    std::vector<cudaGraphNode_t> simNodes;
     CUDA_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-    k_put_uniforms<<<1, 128, 0, h->st>>>(p.u, g.dev);   // the graph's root: each replay's uniforms, by value
+    h->timing = 0;
+    h->simCapture = &simNodes;
+    if (pre) k_put_uniforms<<<1, 128, 0, h->st>>>(p.u, g.dev);   // the graph's root
     if (timed) enqueue_pre(h, p, g.dev);
     else enqueue_step(h, p, g.dev);
+    h->simCapture = nullptr;
     cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
     h->timing = timing;
     h->launches = l0;
     h->seatCur = seatCur0;
     h->cur = cur0;
     if (ce != cudaSuccess) {
+      h->simCaptureLost = false;
       h->err = std::string("step graph capture: ") + cudaGetErrorString(ce);
       return CCS_E_CUDA;
     }
-    size_t roots = 1;
-    ce = cudaGraphGetRootNodes(graph, &g.put, &roots);
-    if (ce == cudaSuccess && roots != 1) ce = cudaErrorInvalidValue;
+    g.put = nullptr;
+    if (pre) {
+      size_t roots = 1;
+      ce = cudaGraphGetRootNodes(graph, &g.put, &roots);
+      if (ce == cudaSuccess && roots != 1) ce = cudaErrorInvalidValue;
+    }
     if (ce == cudaSuccess) ce = cudaGraphInstantiate(&g.exec, graph, 0);
     if (ce != cudaSuccess) {
       cudaGraphDestroy(graph);
+      h->simCaptureLost = false;
       h->err = std::string("step graph instantiate: ") + cudaGetErrorString(ce);
       g.exec = nullptr;
       return CCS_E_CUDA;
     }
     g.graph = graph;
+    int rc = resolve_sim_nodes(h, simNodes, g.sim);
+    if (rc) {
+      free_graph_slot(g);
+      h->stepGraphs.erase(key);
+      return rc;
+    }
   } else {
-    // this replay's uniforms into the root node's argument (launches already enqueued keep theirs)
-    ccs_uniforms u = p.u;
-    ccs_uniforms *dst = g.dev;
-    void *args[] = {&u, &dst};
-    cudaKernelNodeParams kp = {};
-    kp.func = reinterpret_cast<void *>(k_put_uniforms);
-    kp.gridDim = dim3(1);
-    kp.blockDim = dim3(128);
-    kp.kernelParams = args;
-    CUDA_TRY(h, cudaGraphExecKernelNodeSetParams(g.exec, g.put, &kp));
+    // this replay's uniforms into the root node's argument and the contact step's
+    if (g.put) {
+      ccs_uniforms u = p.u;
+      ccs_uniforms *dst = g.dev;
+      void *args[] = {&u, &dst};
+      cudaKernelNodeParams kp = {};
+      kp.func = reinterpret_cast<void *>(k_put_uniforms);
+      kp.gridDim = dim3(1);
+      kp.blockDim = dim3(128);
+      kp.kernelParams = args;
+      CUDA_TRY(h, cudaGraphExecKernelNodeSetParams(g.exec, g.put, &kp));
+    }
+    for (const SimNode &n : g.sim) {
+      const int rc = set_sim_uniforms(h, g.exec, n, p.u);
+      if (rc) return rc;
+    }
   }
   CUDA_TRY(h, cudaGraphLaunch(g.exec, h->st));
   h->seatCur = seatCur0 ^ (p.slots ? 1 : 0);
-  h->launches += block_launches(h, &p, 1) + 1;   // and the uniforms node
+  h->launches += block_launches(h, &p, 1) + (pre ? 1 : 0);   // and the uniforms node
   if (simOutside) {
     --h->launches;            // the caller launches the contact step
-    *Uout = g.dev;
   } else if (timed) {
     --h->launches;            // pass_sim counts its own
-    pass_sim(h, g.dev);       // reads the uniforms the graph's root node wrote
+    pass_sim(h, p.u);
   } else {
     h->cur = cur0 ^ 1;
     if (h->timing & 1) ++h->timingSeq;   // a contact step that was not this sample's
@@ -616,28 +689,49 @@ int graph_block(ccs_handle *h) {
     std::memcpy(g.host, us, sizeof(ccs_uniforms) * M);
     cudaGraph_t graph;
     const int timing = h->timing;
-    h->timing = 0;
     const int64_t l0 = h->launches;
+    std::vector<cudaGraphNode_t> simNodes;
     CUDA_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    h->timing = 0;
+    h->simCapture = &simNodes;
     cudaMemcpyAsync(g.dev, g.host, sizeof(ccs_uniforms) * M, cudaMemcpyHostToDevice, h->st);
     for (int k = 0; k < M; ++k) enqueue_step(h, plans[k], g.dev + k);
+    h->simCapture = nullptr;
     cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
     h->timing = timing;
     h->launches = l0;
+    // capture ran the buffer rotation once on the host; restore it for the replay
+    h->seatCur = seatCur0;
+    h->cur = cur0;
     if (ce != cudaSuccess) {
+      h->simCaptureLost = false;
       h->err = std::string("graph capture: ") + cudaGetErrorString(ce);
       return CCS_E_CUDA;
     }
     ce = cudaGraphInstantiate(&g.exec, graph, 0);
-    cudaGraphDestroy(graph);
     if (ce != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      h->simCaptureLost = false;
       h->err = std::string("graph instantiate: ") + cudaGetErrorString(ce);
       g.exec = nullptr;
       return CCS_E_CUDA;
     }
-    // capture ran the buffer rotation once on the host; restore it for the replay
-    h->seatCur = seatCur0;
-    h->cur = cur0;
+    g.graph = graph;
+    int rc = resolve_sim_nodes(h, simNodes, g.sim);
+    if (rc == CCS_OK && (int)g.sim.size() != M) {
+      h->err = "graph capture: one contact-step node per step expected";
+      rc = CCS_E_CUDA;
+    }
+    if (rc) {
+      free_graph_slot(g);
+      h->graphs.erase(key);
+      return rc;
+    }
+  } else {
+    for (int k = 0; k < M; ++k) {   // each step's uniforms into its contact step's argument
+      const int rc = set_sim_uniforms(h, g.exec, g.sim[k], us[k]);
+      if (rc) return rc;
+    }
   }
   if (g.used) CUDA_TRY(h, cudaEventSynchronize(g.done));
   std::memcpy(g.host, us, sizeof(ccs_uniforms) * M);
@@ -992,8 +1086,9 @@ int ccs_autotune(ccs_handle *h, int reps, int choice[2]) {
     }
   } else {
     CUDA_TRY(h, cudaStreamSynchronize(h->st));
+    const ccs_uniforms tu = pass_uniforms(h, 0, 0, 0.0);
     const ccs_uniforms *U;
-    rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+    rc = push_uniforms(h, tu, &U);
     if (rc) return rc;
     const int timing = h->timing;
     h->timing = 0;
@@ -1003,7 +1098,7 @@ int ccs_autotune(ccs_handle *h, int reps, int choice[2]) {
     float best = 1e30f;
     for (int w : {8, 4}) {
       float ms = 0.0f;
-      rc = time_launches(h, reps, [&] { launch_simulate(U, h->N, a, h->st, w, h->field); }, &ms);
+      rc = time_launches(h, reps, [&] { launch_simulate(tu, h->N, a, h->st, w, h->field); }, &ms);
       if (rc) break;
       if (ms < best) { best = ms; warps = w; }
     }
@@ -1043,7 +1138,9 @@ int ccs_autotune(ccs_handle *h, int reps, int choice[2]) {
 namespace {
 struct EnsembleGraph {
   cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;             // the template, kept for its contact-step nodes' arguments
   std::vector<ccs_uniforms *> dev, host;   // per member: meshEvery uniform slots, and their pinned staging
+  std::vector<SimNode> sim;                // every member's contact-step nodes, member by member, in step order
   cudaEvent_t done = nullptr;
   bool used = false;
 };
@@ -1066,6 +1163,7 @@ void free_ensemble_graphs(ccs_ensemble *e) {
   for (auto &kv : e->graphs) {
     EnsembleGraph &g = kv.second;
     if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
     for (auto p : g.dev) cudaFree(p);
     for (auto p : g.host) cudaFreeHost(p);
     if (g.done) cudaEventDestroy(g.done);
@@ -1109,6 +1207,8 @@ int ensemble_block(ccs_ensemble *e, int R) {
     }
     ENS_TRY(e, cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
     cudaGraph_t graph;
+    std::vector<cudaGraphNode_t> simNodes;
+    bool lost = false;
     ENS_TRY(e, cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
     cudaEventRecord(e->fork, e->st);
     for (int i = 0; i < n; ++i) {   // every member's block on its own stream: parallel branches
@@ -1118,7 +1218,11 @@ int ensemble_block(ccs_ensemble *e, int R) {
       h->timing = 0;
       cudaStreamWaitEvent(h->st, e->fork, 0);
       cudaMemcpyAsync(g.dev[i], g.host[i], sizeof(ccs_uniforms) * M, cudaMemcpyHostToDevice, h->st);
+      h->simCapture = &simNodes;
       for (int k = 0; k < M; ++k) enqueue_step(h, plans[i][k], g.dev[i] + k);
+      h->simCapture = nullptr;
+      lost = lost || h->simCaptureLost;
+      h->simCaptureLost = false;
       cudaEventRecord(e->join[i], h->st);
       cudaStreamWaitEvent(e->st, e->join[i], 0);
       h->timing = timing;
@@ -1132,12 +1236,30 @@ int ensemble_block(ccs_ensemble *e, int R) {
       return CCS_E_CUDA;
     }
     ce = cudaGraphInstantiate(&g.exec, graph, 0);
-    cudaGraphDestroy(graph);
     if (ce != cudaSuccess) {
+      cudaGraphDestroy(graph);
       e->err = std::string("ensemble instantiate: ") + cudaGetErrorString(ce);
       g.exec = nullptr;
       return CCS_E_CUDA;
     }
+    g.graph = graph;
+    int rc = lost ? CCS_E_CUDA : resolve_sim_nodes(e->m[0], simNodes, g.sim);
+    if (rc == CCS_OK && g.sim.size() != (size_t)n * M) rc = CCS_E_CUDA;
+    if (rc) {
+      e->err = "ensemble capture: one contact-step node per member step expected";
+      cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+      return rc;
+    }
+  } else {
+    for (int i = 0; i < n; ++i)   // each member step's uniforms into its contact step's argument
+      for (int k = 0; k < M; ++k) {
+        const int rc = set_sim_uniforms(e->m[i], g.exec, g.sim[(size_t)i * M + k], plans[i][k].u);
+        if (rc) {
+          e->err = e->m[i]->err;
+          return rc;
+        }
+      }
   }
   if (g.used) ENS_TRY(e, cudaEventSynchronize(g.done));
   for (int i = 0; i < n; ++i)
@@ -2036,10 +2158,7 @@ int ccs_pass_pp(ccs_handle *h) {
 int ccs_pass_sim(ccs_handle *h, int settle, int kick, double gdt) {
   int rc = ensure_built(h);
   if (rc) return rc;
-  const ccs_uniforms *U;
-  rc = push_uniforms(h, pass_uniforms(h, settle, kick, gdt), &U);
-  if (rc) return rc;
-  pass_sim(h, U);
+  pass_sim(h, pass_uniforms(h, settle, kick, gdt));
   return check_launch(h);
 }
 
@@ -2068,15 +2187,14 @@ static int last_step_overlapped(ccs_handle *h, float *pos4_out, float *vel4_out,
   int rc = ensure_copy_stream(h);
   if (rc) return rc;
   StepPlan p = plan_step(h, 0, 0);
-  const ccs_uniforms *U = nullptr;
-  rc = step_graph(h, p, true, &U);   // the grid, the mesh and the pairwise pass
+  rc = step_graph(h, p, true);   // the grid, the mesh and the pairwise pass
   if (rc) return rc;
   if (inputsOnCopyStream) CUDA_TRY(h, cudaStreamWaitEvent(h->st, h->inEv, 0));
   const SimArgs a = sim_args(h);
   const int N = h->N, half = std::min(N, (N / 2 + 255) / 256 * 256), d = h->cur ^ 1;
-  h->launches += launch_simulate_range(U, N, a, h->st, h->tuneWarps, h->field, 0, half);
+  h->launches += launch_simulate_range(p.u, N, a, h->st, h->tuneWarps, h->field, 0, half);
   CUDA_TRY(h, cudaEventRecord(h->halfEv, h->st));
-  h->launches += launch_simulate_range(U, N, a, h->st, h->tuneWarps, h->field, half, N - half);
+  h->launches += launch_simulate_range(p.u, N, a, h->st, h->tuneWarps, h->field, half, N - half);
   CUDA_TRY(h, cudaStreamWaitEvent(h->cst, h->halfEv, 0));
   auto read = [&](cudaStream_t st, int i0, int n) -> int {
     if (n <= 0) return CCS_OK;

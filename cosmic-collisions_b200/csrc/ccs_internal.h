@@ -102,11 +102,11 @@ cudaError_t init_kernels();
 int launch_fill_u32(uint32_t *p, size_t n, uint32_t v, cudaStream_t st);
 int launch_contact_grid(const ccs_uniforms *u, int N, const float4 *pos, uint32_t *seats, uint32_t *hk,
                         uint32_t *seatsOld, const uint32_t *hkOld, unsigned *status, cudaStream_t st);
-// warps: CTA width of the contact step, 8 or 4
-int launch_simulate(const ccs_uniforms *u, int N, const SimArgs &a, cudaStream_t st, int warps = 8,
+// warps: CTA width of the contact step, 8 or 4; u by value (the kernel's first argument)
+int launch_simulate(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps = 8,
                     bool field = false);
 // the contact step for particles [first, first + count) only; first a multiple of 256
-int launch_simulate_range(const ccs_uniforms *u, int N, SimArgs a, cudaStream_t st, int warps, bool field, int first,
+int launch_simulate_range(const ccs_uniforms &u, int N, SimArgs a, cudaStream_t st, int warps, bool field, int first,
                           int count);
 int launch_deposit(const ccs_uniforms *u, int N, int box, const float4 *pos, const float *mat, const float4 *monoPrev,
                    float4 *fine, cudaStream_t st);
