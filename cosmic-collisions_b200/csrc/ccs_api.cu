@@ -41,10 +41,14 @@ struct GraphKey {
   }
 };
 
-// a captured contact-step node: its uniforms are its first, by-value argument, so every replay sets them
-// (the other argument, the buffers, stays as captured: the template graph owns its storage)
-struct SimNode {
+// a captured node of a kernel whose first argument is the uniforms by value (the contact step, the contact
+// grid): every replay sets them; its other arguments stay as captured (the template graph owns their storage)
+struct CapturedNode {
   cudaGraphNode_t node = nullptr;
+  int nargs = 0, step = 0;   // the kernel's argument count; the step of the graph it belongs to
+};
+struct UniNode {
+  CapturedNode c;
   cudaKernelNodeParams kp = {};
 };
 
@@ -56,7 +60,7 @@ struct GraphSlot {
   bool used = false;
   cudaGraph_t graph = nullptr;   // the template, kept for its nodes' arguments
   cudaGraphNode_t put = nullptr; // a step graph's k_put_uniforms node, given each replay's uniforms
-  std::vector<SimNode> sim;      // the contact-step nodes, in step order
+  std::vector<UniNode> uni;      // the nodes that take the uniforms by value, in capture order
 };
 
 // one step's launches captured as a graph (ccs_step): its schedule, the buffers it reads and writes
@@ -127,8 +131,9 @@ struct ccs_handle {
   // graphs
   std::map<GraphKey, GraphSlot> graphs;
   std::map<StepKey, GraphSlot> stepGraphs;
-  std::vector<cudaGraphNode_t> *simCapture = nullptr;   // while capturing: where pass_sim records its node
-  bool simCaptureLost = false;                          // a node it could not identify
+  std::vector<CapturedNode> *uniCapture = nullptr;   // while capturing: where by-value launches record their node
+  int captureStep = 0;                               // the step of the graph being captured
+  bool uniCaptureLost = false;                       // a node that could not be identified
   // ccs_advance_host's read-back of its last step's first half, overlapping the second half's contact step
   cudaStream_t cst = nullptr;
   cudaEvent_t halfEv = nullptr, copyEv = nullptr, inEv = nullptr;
@@ -358,12 +363,26 @@ void time_collect(ccs_handle *h) {
 
 // ---- the passes, each enqueued on h->st reading uniforms at U ----
 
-void pass_slots(ccs_handle *h, const ccs_uniforms *U) {
+// while a graph is being captured: the node just added (the capture's one sink) takes the uniforms by value
+void record_uniform_node(ccs_handle *h, int nargs) {
+  if (!h->uniCapture) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  if (cudaStreamGetCaptureInfo(h->st, &cs, nullptr, nullptr, &deps, &nd) == cudaSuccess &&
+      cs == cudaStreamCaptureStatusActive && nd == 1)
+    h->uniCapture->push_back(CapturedNode{deps[0], nargs, h->captureStep});
+  else
+    h->uniCaptureLost = true;
+}
+
+void pass_slots(ccs_handle *h, const ccs_uniforms &u) {
   const int nxt = h->seatCur ^ 1;
   cudaEvent_t b, e;
   time_begin(h, 1, &b, &e);
-  h->launches += launch_contact_grid(U, h->N, h->pos[h->cur], h->seats[nxt], h->hk[nxt], h->seats[h->seatCur],
+  h->launches += launch_contact_grid(u, h->N, h->pos[h->cur], h->seats[nxt], h->hk[nxt], h->seats[h->seatCur],
                                      h->hk[h->seatCur], h->status, h->st);
+  record_uniform_node(h, 7);
   time_end(h, e);
   h->seatCur = nxt;
 }
@@ -430,16 +449,7 @@ void pass_sim(ccs_handle *h, const ccs_uniforms &u) {
   cudaEvent_t b, e;
   time_begin(h, 0, &b, &e);
   h->launches += launch_simulate(u, h->N, a, h->st, h->tuneWarps, h->field);
-  if (h->simCapture) {   // the node just captured is the capture's one sink
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t nd = 0;
-    if (cudaStreamGetCaptureInfo(h->st, &cs, nullptr, nullptr, &deps, &nd) == cudaSuccess &&
-        cs == cudaStreamCaptureStatusActive && nd == 1)
-      h->simCapture->push_back(deps[0]);
-    else
-      h->simCaptureLost = true;
-  }
+  record_uniform_node(h, 2);
   time_end(h, e);
   if (h->timing & 1) ++h->timingSeq;
   h->cur ^= 1;
@@ -502,7 +512,7 @@ int block_launches(const ccs_handle *h, const StepPlan *plans, int M) {
 
 // what a step runs before its contact step: the grid, and the mesh and the pairwise pass on mesh steps
 void enqueue_pre(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
-  if (p.slots) pass_slots(h, U);
+  if (p.slots) pass_slots(h, p.u);
   if (p.mesh) {
     pass_mesh(h, U, p.u.boxB > 0.5f);
     pass_pp(h, U, p.u.ppCount);
@@ -515,44 +525,49 @@ void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
 }
 
 // after a capture: the contact-step nodes it recorded, with their captured arguments
-int resolve_sim_nodes(ccs_handle *h, const std::vector<cudaGraphNode_t> &nodes, std::vector<SimNode> &out) {
-  if (h->simCaptureLost) {
-    h->simCaptureLost = false;
-    h->err = "graph capture: a contact-step node was not identified";
+int resolve_uniform_nodes(ccs_handle *h, const std::vector<CapturedNode> &nodes, std::vector<UniNode> &out) {
+  if (h->uniCaptureLost) {
+    h->uniCaptureLost = false;
+    h->err = "graph capture: a node taking the uniforms was not identified";
     return CCS_E_CUDA;
   }
   out.resize(nodes.size());
   for (size_t i = 0; i < nodes.size(); ++i) {
-    out[i].node = nodes[i];
-    CUDA_TRY(h, cudaGraphKernelNodeGetParams(nodes[i], &out[i].kp));
+    out[i].c = nodes[i];
+    CUDA_TRY(h, cudaGraphKernelNodeGetParams(nodes[i].node, &out[i].kp));
   }
   return CCS_OK;
 }
 
-// a contact-step node of an instantiated graph given this replay's uniforms (replays already enqueued keep theirs)
-int set_sim_uniforms(ccs_handle *h, cudaGraphExec_t exec, const SimNode &n, const ccs_uniforms &u) {
+// a node of an instantiated graph given this replay's uniforms (replays already enqueued keep theirs)
+int set_node_uniforms(ccs_handle *h, cudaGraphExec_t exec, const UniNode &n, const ccs_uniforms &u) {
+  constexpr int kMaxArgs = 8;
+  if (n.c.nargs < 1 || n.c.nargs > kMaxArgs) return CCS_E_STATE;
   ccs_uniforms v = u;
-  void *args[2] = {&v, n.kp.kernelParams[1]};
+  void *args[kMaxArgs];
+  args[0] = &v;
+  for (int i = 1; i < n.c.nargs; ++i) args[i] = n.kp.kernelParams[i];
   cudaKernelNodeParams kp = n.kp;
   kp.kernelParams = args;
   kp.extra = nullptr;
-  CUDA_TRY(h, cudaGraphExecKernelNodeSetParams(exec, n.node, &kp));
+  CUDA_TRY(h, cudaGraphExecKernelNodeSetParams(exec, n.c.node, &kp));
   return CCS_OK;
 }
 
 void free_graph_slot(GraphSlot &g);
 
-// one step replayed from a captured graph, so a step costs one cudaGraphLaunch.  The contact step takes the
-// step's uniforms as its by-value argument, set in its node before each replay; the grid and mesh kernels
-// read them from device memory, written by the graph's root node, k_put_uniforms, whose by-value argument
-// is set the same way (no copy engine or pinned staging on the step's path).  Graphs are keyed by what
-// the step runs and by the buffers it touches.  When the contact step is being timed (ccs_timing bit 0),
-// or its caller launches it (simOutside), the graph stops before it and the contact step is launched
-// directly, between its two events when timed (events recorded by a graph's nodes do not time).
+// one step replayed from a captured graph, so a step costs one cudaGraphLaunch.  The contact step and the
+// contact grid take the step's uniforms as their by-value first argument, set in their nodes before each
+// replay; the mesh and pairwise kernels read them from device memory, written on a mesh step by the
+// graph's root node, k_put_uniforms, whose by-value argument is set the same way (no copy engine or
+// pinned staging on the step's path).  Graphs are keyed by what the step runs and by the buffers it
+// touches.  When the contact step is being timed (ccs_timing bit 0), or its caller launches it
+// (simOutside), the graph stops before it and the contact step is launched directly, between its two
+// events when timed (events recorded by a graph's nodes do not time).
 int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false) {
   const bool timed = time_this(h, 0) || simOutside;
-  const bool pre = p.slots || p.mesh;   // kernels that read the uniforms from device memory
-  if (timed && !pre) {                  // nothing to replay: the contact step alone, launched directly
+  const bool pre = p.mesh;   // kernels that read the uniforms from device memory (the mesh and pairwise passes)
+  if (timed && !p.slots && !p.mesh) {   // nothing to replay: the contact step alone, launched directly
     if (!simOutside) pass_sim(h, p.u);
     return check_launch(h);
   }
@@ -566,21 +581,22 @@ int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false) {
     const int timing = h->timing;
     const int64_t l0 = h->launches;
     cudaGraph_t graph;
-    std::vector<cudaGraphNode_t> simNodes;
+    std::vector<CapturedNode> uniNodes;
     CUDA_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
     h->timing = 0;
-    h->simCapture = &simNodes;
+    h->uniCapture = &uniNodes;
+    h->captureStep = 0;
     if (pre) k_put_uniforms<<<1, 128, 0, h->st>>>(p.u, g.dev);   // the graph's root
     if (timed) enqueue_pre(h, p, g.dev);
     else enqueue_step(h, p, g.dev);
-    h->simCapture = nullptr;
+    h->uniCapture = nullptr;
     cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
     h->timing = timing;
     h->launches = l0;
     h->seatCur = seatCur0;
     h->cur = cur0;
     if (ce != cudaSuccess) {
-      h->simCaptureLost = false;
+      h->uniCaptureLost = false;
       h->err = std::string("step graph capture: ") + cudaGetErrorString(ce);
       return CCS_E_CUDA;
     }
@@ -593,20 +609,20 @@ int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false) {
     if (ce == cudaSuccess) ce = cudaGraphInstantiate(&g.exec, graph, 0);
     if (ce != cudaSuccess) {
       cudaGraphDestroy(graph);
-      h->simCaptureLost = false;
+      h->uniCaptureLost = false;
       h->err = std::string("step graph instantiate: ") + cudaGetErrorString(ce);
       g.exec = nullptr;
       return CCS_E_CUDA;
     }
     g.graph = graph;
-    int rc = resolve_sim_nodes(h, simNodes, g.sim);
+    int rc = resolve_uniform_nodes(h, uniNodes, g.uni);
     if (rc) {
       free_graph_slot(g);
       h->stepGraphs.erase(key);
       return rc;
     }
   } else {
-    // this replay's uniforms into the root node's argument and the contact step's
+    // this replay's uniforms into the root node's argument, the grid's and the contact step's
     if (g.put) {
       ccs_uniforms u = p.u;
       ccs_uniforms *dst = g.dev;
@@ -618,8 +634,8 @@ int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false) {
       kp.kernelParams = args;
       CUDA_TRY(h, cudaGraphExecKernelNodeSetParams(g.exec, g.put, &kp));
     }
-    for (const SimNode &n : g.sim) {
-      const int rc = set_sim_uniforms(h, g.exec, n, p.u);
+    for (const UniNode &n : g.uni) {
+      const int rc = set_node_uniforms(h, g.exec, n, p.u);
       if (rc) return rc;
     }
   }
@@ -690,13 +706,16 @@ int graph_block(ccs_handle *h) {
     cudaGraph_t graph;
     const int timing = h->timing;
     const int64_t l0 = h->launches;
-    std::vector<cudaGraphNode_t> simNodes;
+    std::vector<CapturedNode> uniNodes;
     CUDA_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
     h->timing = 0;
-    h->simCapture = &simNodes;
+    h->uniCapture = &uniNodes;
     cudaMemcpyAsync(g.dev, g.host, sizeof(ccs_uniforms) * M, cudaMemcpyHostToDevice, h->st);
-    for (int k = 0; k < M; ++k) enqueue_step(h, plans[k], g.dev + k);
-    h->simCapture = nullptr;
+    for (int k = 0; k < M; ++k) {
+      h->captureStep = k;
+      enqueue_step(h, plans[k], g.dev + k);
+    }
+    h->uniCapture = nullptr;
     cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
     h->timing = timing;
     h->launches = l0;
@@ -704,22 +723,24 @@ int graph_block(ccs_handle *h) {
     h->seatCur = seatCur0;
     h->cur = cur0;
     if (ce != cudaSuccess) {
-      h->simCaptureLost = false;
+      h->uniCaptureLost = false;
       h->err = std::string("graph capture: ") + cudaGetErrorString(ce);
       return CCS_E_CUDA;
     }
     ce = cudaGraphInstantiate(&g.exec, graph, 0);
     if (ce != cudaSuccess) {
       cudaGraphDestroy(graph);
-      h->simCaptureLost = false;
+      h->uniCaptureLost = false;
       h->err = std::string("graph instantiate: ") + cudaGetErrorString(ce);
       g.exec = nullptr;
       return CCS_E_CUDA;
     }
     g.graph = graph;
-    int rc = resolve_sim_nodes(h, simNodes, g.sim);
-    if (rc == CCS_OK && (int)g.sim.size() != M) {
-      h->err = "graph capture: one contact-step node per step expected";
+    int rc = resolve_uniform_nodes(h, uniNodes, g.uni);
+    int want = M;
+    for (int k = 0; k < M; ++k) want += plans[k].slots ? 1 : 0;
+    if (rc == CCS_OK && (int)g.uni.size() != want) {
+      h->err = "graph capture: a contact-step node per step and a grid node per even step expected";
       rc = CCS_E_CUDA;
     }
     if (rc) {
@@ -728,8 +749,8 @@ int graph_block(ccs_handle *h) {
       return rc;
     }
   } else {
-    for (int k = 0; k < M; ++k) {   // each step's uniforms into its contact step's argument
-      const int rc = set_sim_uniforms(h, g.exec, g.sim[k], us[k]);
+    for (const UniNode &n : g.uni) {   // each step's uniforms into its grid's and contact step's argument
+      const int rc = set_node_uniforms(h, g.exec, n, us[n.c.step]);
       if (rc) return rc;
     }
   }
@@ -1140,7 +1161,8 @@ struct EnsembleGraph {
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;             // the template, kept for its contact-step nodes' arguments
   std::vector<ccs_uniforms *> dev, host;   // per member: meshEvery uniform slots, and their pinned staging
-  std::vector<SimNode> sim;                // every member's contact-step nodes, member by member, in step order
+  std::vector<UniNode> uni;                // every member's by-value nodes, member by member, in capture order
+  std::vector<int> member;                 // the member each of them belongs to
   cudaEvent_t done = nullptr;
   bool used = false;
 };
@@ -1207,7 +1229,8 @@ int ensemble_block(ccs_ensemble *e, int R) {
     }
     ENS_TRY(e, cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
     cudaGraph_t graph;
-    std::vector<cudaGraphNode_t> simNodes;
+    std::vector<CapturedNode> uniNodes;
+    std::vector<int> member;
     bool lost = false;
     ENS_TRY(e, cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
     cudaEventRecord(e->fork, e->st);
@@ -1218,11 +1241,15 @@ int ensemble_block(ccs_ensemble *e, int R) {
       h->timing = 0;
       cudaStreamWaitEvent(h->st, e->fork, 0);
       cudaMemcpyAsync(g.dev[i], g.host[i], sizeof(ccs_uniforms) * M, cudaMemcpyHostToDevice, h->st);
-      h->simCapture = &simNodes;
-      for (int k = 0; k < M; ++k) enqueue_step(h, plans[i][k], g.dev[i] + k);
-      h->simCapture = nullptr;
-      lost = lost || h->simCaptureLost;
-      h->simCaptureLost = false;
+      h->uniCapture = &uniNodes;
+      for (int k = 0; k < M; ++k) {
+        h->captureStep = k;
+        enqueue_step(h, plans[i][k], g.dev[i] + k);
+      }
+      h->uniCapture = nullptr;
+      member.resize(uniNodes.size(), i);
+      lost = lost || h->uniCaptureLost;
+      h->uniCaptureLost = false;
       cudaEventRecord(e->join[i], h->st);
       cudaStreamWaitEvent(e->st, e->join[i], 0);
       h->timing = timing;
@@ -1243,23 +1270,27 @@ int ensemble_block(ccs_ensemble *e, int R) {
       return CCS_E_CUDA;
     }
     g.graph = graph;
-    int rc = lost ? CCS_E_CUDA : resolve_sim_nodes(e->m[0], simNodes, g.sim);
-    if (rc == CCS_OK && g.sim.size() != (size_t)n * M) rc = CCS_E_CUDA;
+    int rc = lost ? CCS_E_CUDA : resolve_uniform_nodes(e->m[0], uniNodes, g.uni);
+    g.member = member;
+    size_t want = 0;
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < M; ++k) want += plans[i][k].slots ? 2 : 1;
+    if (rc == CCS_OK && g.uni.size() != want) rc = CCS_E_CUDA;
     if (rc) {
-      e->err = "ensemble capture: one contact-step node per member step expected";
+      e->err = "ensemble capture: a contact-step node per member step and a grid node per even step expected";
       cudaGraphExecDestroy(g.exec);
       g.exec = nullptr;
       return rc;
     }
   } else {
-    for (int i = 0; i < n; ++i)   // each member step's uniforms into its contact step's argument
-      for (int k = 0; k < M; ++k) {
-        const int rc = set_sim_uniforms(e->m[i], g.exec, g.sim[(size_t)i * M + k], plans[i][k].u);
-        if (rc) {
-          e->err = e->m[i]->err;
-          return rc;
-        }
+    for (size_t j = 0; j < g.uni.size(); ++j) {   // each member step's uniforms into its by-value nodes
+      const int i = g.member[j];
+      const int rc = set_node_uniforms(e->m[i], g.exec, g.uni[j], plans[i][g.uni[j].c.step].u);
+      if (rc) {
+        e->err = e->m[i]->err;
+        return rc;
       }
+    }
   }
   if (g.used) ENS_TRY(e, cudaEventSynchronize(g.done));
   for (int i = 0; i < n; ++i)
@@ -1615,10 +1646,7 @@ static int apply_perm_device(ccs_handle *h, const int32_t *permDev) {
   std::swap(h->home, h->homeTmp);
   h->cur = d;
   // the old cells name particles by their old places: fresh ones
-  const ccs_uniforms *U;
-  int rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
-  if (rc) return rc;
-  pass_slots(h, U);
+  pass_slots(h, pass_uniforms(h, 0, 0, 0.0));
   return check_launch(h);
 }
 
@@ -1645,10 +1673,11 @@ int ccs_apply_perm(ccs_handle *h, const int32_t *perm) {
 // passDiag, src/nbody.js:488-507
 static int diag_pass(ccs_handle *h) {
   set_boxes(h);
+  const ccs_uniforms du = pass_uniforms(h, 0, 0, 0.0);
   const ccs_uniforms *U;
-  int rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
+  int rc = push_uniforms(h, du, &U);
   if (rc) return rc;
-  pass_slots(h, U);
+  pass_slots(h, du);
   pass_mesh(h, U, h->boxB > 0.5f);
   pass_pp(h, U, h->ppCount);
   pass_diag_kernel(h, U);
@@ -2127,10 +2156,7 @@ int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes) {
 int ccs_pass_slots(ccs_handle *h) {
   int rc = ensure_built(h);
   if (rc) return rc;
-  const ccs_uniforms *U;
-  rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
-  if (rc) return rc;
-  pass_slots(h, U);
+  pass_slots(h, pass_uniforms(h, 0, 0, 0.0));
   return check_launch(h);
 }
 

@@ -100,7 +100,8 @@ cudaError_t init_kernels();
 // kernel launchers (ccs_kernels.cu); all enqueue on `st` and return the
 // number of kernels launched.
 int launch_fill_u32(uint32_t *p, size_t n, uint32_t v, cudaStream_t st);
-int launch_contact_grid(const ccs_uniforms *u, int N, const float4 *pos, uint32_t *seats, uint32_t *hk,
+// u by value (the kernel's first argument, as for the contact step)
+int launch_contact_grid(const ccs_uniforms &u, int N, const float4 *pos, uint32_t *seats, uint32_t *hk,
                         uint32_t *seatsOld, const uint32_t *hkOld, unsigned *status, cudaStream_t st);
 // warps: CTA width of the contact step, 8 or 4; u by value (the kernel's first argument)
 int launch_simulate(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps = 8,

@@ -75,11 +75,11 @@ __device__ __forceinline__ void seat_insert(uint32_t *cell, uint32_t w, unsigned
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_contact_grid(const ccs_uniforms *__restrict__ U,
-                                                         const float4 *__restrict__ pos, uint32_t *seats,
-                                                         uint32_t *__restrict__ hk, uint32_t *seatsOld,
-                                                         const uint32_t *__restrict__ hkOld, unsigned *status) {
-  const ccs_uniforms &u = *U;
+// the uniforms by value: constant-bank operands, no load at the head of each warp's chain
+__global__ void __launch_bounds__(kBlock) k_contact_grid(const ccs_uniforms u, const float4 *__restrict__ pos,
+                                                         uint32_t *seats, uint32_t *__restrict__ hk,
+                                                         uint32_t *seatsOld, const uint32_t *__restrict__ hkOld,
+                                                         unsigned *status) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < u.N;
   float4 P = make_float4(0, 0, 0, 0);
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kBlock) k_contact_grid(const ccs_uniforms *__r
   if (start < kSeats) seat_insert(seats + (size_t)h * kSeats, w, status, start);
 }
 
-int launch_contact_grid(const ccs_uniforms *u, int N, const float4 *pos, uint32_t *seats, uint32_t *hk,
+int launch_contact_grid(const ccs_uniforms &u, int N, const float4 *pos, uint32_t *seats, uint32_t *hk,
                         uint32_t *seatsOld, const uint32_t *hkOld, unsigned *status, cudaStream_t st) {
   k_contact_grid<<<blocks_for(N), kBlock, 0, st>>>(u, pos, seats, hk, seatsOld, hkOld, status);
   return 1;
