@@ -3,10 +3,13 @@
 // The handle owns the device state (the reference's textures as flat arrays),
 // runs the step schedule of src/nbody.js:551-558 (contact grid every 2nd step,
 // mesh + P3M every 8th, gravity as one impulse), the phases (settle, rigid
-// approach, kick) and the analysis hand-off.  Per-step uniforms live in
-// device memory; `ccs_steps` replays captured CUDA graphs of whole 8-step
-// blocks whose uniform slots are refreshed by one memcpy node each replay,
-// and `ccs_step` one step's graph whose root kernel writes its uniforms.
+// approach, kick) and the analysis hand-off.  The contact step and the
+// contact grid take a step's uniforms by value, set in their captured graph
+// nodes before each replay; the mesh and pairwise kernels read them from
+// device memory.  `ccs_steps` replays captured CUDA graphs of whole 8-step
+// blocks, whose device uniform slots one memcpy node refreshes each replay,
+// and `ccs_step` one step's graph, whose root kernel writes its uniforms on
+// a mesh step.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -496,7 +499,8 @@ StepPlan plan_step(ccs_handle *h, int settle, int kick) {
   return p;
 }
 
-// the kernels a captured block launches (its uniforms come by one memcpy node, not a kernel)
+// the kernels a captured block launches (a block's device uniforms come by one memcpy node, not a kernel;
+// a single step's graph adds its uniforms kernel on a mesh step)
 int block_launches(const ccs_handle *h, const StepPlan *plans, int M) {
   int per = 0;
   for (int k = 0; k < M; ++k) {
