@@ -729,6 +729,8 @@ int graph_block(ccs_handle *h) {
     if (ce != cudaSuccess) {
       h->uniCaptureLost = false;
       h->err = std::string("graph capture: ") + cudaGetErrorString(ce);
+      free_graph_slot(g);
+      h->graphs.erase(key);
       return CCS_E_CUDA;
     }
     ce = cudaGraphInstantiate(&g.exec, graph, 0);
@@ -737,6 +739,8 @@ int graph_block(ccs_handle *h) {
       h->uniCaptureLost = false;
       h->err = std::string("graph instantiate: ") + cudaGetErrorString(ce);
       g.exec = nullptr;
+      free_graph_slot(g);
+      h->graphs.erase(key);
       return CCS_E_CUDA;
     }
     g.graph = graph;
@@ -1185,15 +1189,17 @@ struct ccs_ensemble {
 constexpr int kEnsRounds = 4;   // rounds of meshEvery steps one ensemble graph holds
 
 namespace {
+void free_ensemble_graph(EnsembleGraph &g) {
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.graph) cudaGraphDestroy(g.graph);
+  for (auto p : g.dev) cudaFree(p);
+  for (auto p : g.host) cudaFreeHost(p);
+  if (g.done) cudaEventDestroy(g.done);
+  g = EnsembleGraph();
+}
+
 void free_ensemble_graphs(ccs_ensemble *e) {
-  for (auto &kv : e->graphs) {
-    EnsembleGraph &g = kv.second;
-    if (g.exec) cudaGraphExecDestroy(g.exec);
-    if (g.graph) cudaGraphDestroy(g.graph);
-    for (auto p : g.dev) cudaFree(p);
-    for (auto p : g.host) cudaFreeHost(p);
-    if (g.done) cudaEventDestroy(g.done);
-  }
+  for (auto &kv : e->graphs) free_ensemble_graph(kv.second);
   e->graphs.clear();
 }
 
@@ -1264,6 +1270,8 @@ int ensemble_block(ccs_ensemble *e, int R) {
     cudaError_t ce = cudaStreamEndCapture(e->st, &graph);
     if (ce != cudaSuccess) {
       e->err = std::string("ensemble capture: ") + cudaGetErrorString(ce);
+      free_ensemble_graph(g);
+      e->graphs.erase(std::make_pair(R, keys));
       return CCS_E_CUDA;
     }
     ce = cudaGraphInstantiate(&g.exec, graph, 0);
@@ -1271,6 +1279,8 @@ int ensemble_block(ccs_ensemble *e, int R) {
       cudaGraphDestroy(graph);
       e->err = std::string("ensemble instantiate: ") + cudaGetErrorString(ce);
       g.exec = nullptr;
+      free_ensemble_graph(g);
+      e->graphs.erase(std::make_pair(R, keys));
       return CCS_E_CUDA;
     }
     g.graph = graph;
@@ -1282,8 +1292,8 @@ int ensemble_block(ccs_ensemble *e, int R) {
     if (rc == CCS_OK && g.uni.size() != want) rc = CCS_E_CUDA;
     if (rc) {
       e->err = "ensemble capture: a contact-step node per member step and a grid node per even step expected";
-      cudaGraphExecDestroy(g.exec);
-      g.exec = nullptr;
+      free_ensemble_graph(g);
+      e->graphs.erase(std::make_pair(R, keys));
       return rc;
     }
   } else {
