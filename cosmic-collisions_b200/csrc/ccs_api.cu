@@ -139,6 +139,10 @@ struct ccs_handle {
   bool uniCaptureLost = false;                       // a node that could not be identified
   // ccs_advance_host's read-back of its last step's first half, overlapping the second half's contact step
   cudaStream_t cst = nullptr;
+  // a mesh step's grid and pairwise passes, beside its mesh passes (forked from st and joined back)
+  cudaStream_t side = nullptr;
+  cudaEvent_t forkEv = nullptr, joinEv = nullptr;
+  bool inEnsemble = false;   // captured as an ensemble member: its steps are already a parallel branch
   cudaEvent_t halfEv = nullptr, copyEv = nullptr, inEv = nullptr;
   int ping = 0;
   bool useGraphs = true;
@@ -514,13 +518,30 @@ int block_launches(const ccs_handle *h, const StepPlan *plans, int M) {
   return per;
 }
 
-// what a step runs before its contact step: the grid, and the mesh and the pairwise pass on mesh steps
+// what a step runs before its contact step: the grid, and the mesh and the pairwise pass on mesh steps.
+// The three read the positions and write disjoint buffers, so on a mesh step the grid and the pairwise pass
+// run on the side stream beside the mesh chain (deposit, coarse, far, cell), and the contact step waits for
+// both.  While kernels are being timed one by one, or when the step is an ensemble member's (the members'
+// steps are parallel branches already), they run in order on st.
 void enqueue_pre(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
-  if (p.slots) pass_slots(h, p.u);
-  if (p.mesh) {
-    pass_mesh(h, U, p.u.boxB > 0.5f);
-    pass_pp(h, U, p.u.ppCount);
+  if (!p.mesh || !h->side || h->timing || h->inEnsemble) {
+    if (p.slots) pass_slots(h, p.u);
+    if (p.mesh) {
+      pass_mesh(h, U, p.u.boxB > 0.5f);
+      pass_pp(h, U, p.u.ppCount);
+    }
+    return;
   }
+  cudaEventRecord(h->forkEv, h->st);
+  cudaStreamWaitEvent(h->side, h->forkEv, 0);
+  const cudaStream_t main = h->st;
+  h->st = h->side;
+  if (p.slots) pass_slots(h, p.u);
+  pass_pp(h, U, p.u.ppCount);
+  h->st = main;
+  pass_mesh(h, U, p.u.boxB > 0.5f);
+  cudaEventRecord(h->joinEv, h->side);
+  cudaStreamWaitEvent(h->st, h->joinEv, 0);
 }
 
 void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
@@ -869,6 +890,17 @@ int ccs_create(int device, ccs_handle **out) {
     h->err = "kernel attributes could not be set";
   }
   cudaEventCreateWithFlags(&h->readEv, cudaEventDisableTiming);
+  // without them a mesh step's passes run one after another on st
+  if (cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->forkEv, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->joinEv, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->forkEv) cudaEventDestroy(h->forkEv);
+    h->side = nullptr;
+    h->forkEv = nullptr;
+    h->joinEv = nullptr;
+  }
   *out = h;
   return CCS_OK;
 }
@@ -884,6 +916,9 @@ int ccs_destroy(ccs_handle *h) {
   if (h->copyEv) cudaEventDestroy(h->copyEv);
   if (h->inEv) cudaEventDestroy(h->inEv);
   if (h->cst) cudaStreamDestroy(h->cst);
+  if (h->forkEv) cudaEventDestroy(h->forkEv);
+  if (h->joinEv) cudaEventDestroy(h->joinEv);
+  if (h->side) cudaStreamDestroy(h->side);
   if (h->uniDev) cudaFree(h->uniDev);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
@@ -1252,10 +1287,12 @@ int ensemble_block(ccs_ensemble *e, int R) {
       cudaStreamWaitEvent(h->st, e->fork, 0);
       cudaMemcpyAsync(g.dev[i], g.host[i], sizeof(ccs_uniforms) * M, cudaMemcpyHostToDevice, h->st);
       h->uniCapture = &uniNodes;
+      h->inEnsemble = true;
       for (int k = 0; k < M; ++k) {
         h->captureStep = k;
         enqueue_step(h, plans[i][k], g.dev[i] + k);
       }
+      h->inEnsemble = false;
       h->uniCapture = nullptr;
       member.resize(uniNodes.size(), i);
       lost = lost || h->uniCaptureLost;
