@@ -50,7 +50,8 @@ sys.path.insert(0, ROOT)
 
 ALG_BYTES_SIM = 92          # bytes per particle per contact-step launch
 L2_FLUSH_BYTES = 256 << 20
-TIME_EVERY = 8                 # inside the timed region the contact step is timed on every 8th launch
+TIME_EVERY = 9                 # inside the timed region the contact step is timed on every 9th launch: a stride
+                               # coprime with the 8-step cycle, so the samples cover every step of it
 
 
 def impact_opt(N):
@@ -491,7 +492,7 @@ def analysis_timing(cc, nb, reps=5):
 def timed_steps(nb, lib, stream, flush, steps, dev, dist):
     """steps direct-launch steps, L2 flushed before each, each bracketed by CUDA events on the library's
     stream; clocks sampled meanwhile.  Inside the timed region the library times the contact step alone
-    (the roofline's kernel) with its own pair of events on every 8th launch, a sample spread over the whole
+    (the roofline's kernel) with its own pair of events on every 9th launch, a sample spread over the whole
     region; the other kernels are timed in a pass of their own after it, since every timed launch widens
     its step by its events (and leaves the step's captured graph for a direct launch)."""
     import ctypes as C

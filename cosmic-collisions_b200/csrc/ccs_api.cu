@@ -97,6 +97,8 @@ struct ccs_handle {
   int cur = 0;
   float *mat = nullptr, *matTmp = nullptr;
   float4 *home = nullptr, *homeTmp = nullptr;
+  float4 *part = nullptr;   // a split mesh step's contact sums (SimArgs::part, part2)
+  float2 *part2 = nullptr;
   // contact grid: two seat tables used in turn, and the cell each particle went to
   uint32_t *seats[2] = {}, *hk[2] = {};
   int seatCur = 0;
@@ -448,6 +450,8 @@ SimArgs sim_args(const ccs_handle *h) {
   a.velO = h->vel[d];
   a.auxO = h->aux[d];
   a.qO = h->q[d];
+  a.part = h->part;
+  a.part2 = h->part2;
   return a;
 }
 
@@ -505,7 +509,7 @@ StepPlan plan_step(ccs_handle *h, int settle, int kick) {
 
 // the kernels a captured block launches (a block's device uniforms come by one memcpy node, not a kernel;
 // a single step's graph adds its uniforms kernel on a mesh step)
-int block_launches(const ccs_handle *h, const StepPlan *plans, int M) {
+int block_launches(const ccs_handle *h, const StepPlan *plans, int M, bool split = false) {
   int per = 0;
   for (int k = 0; k < M; ++k) {
     per += 1;                                       // contact step
@@ -513,10 +517,15 @@ int block_launches(const ccs_handle *h, const StepPlan *plans, int M) {
     if (plans[k].mesh) {
       per += 5 * (1 + (plans[k].u.boxB > 0.5f));    // deposit, coarse, occupied list, far, cell per box
       if (plans[k].u.ppCount) per += h->nn ? 6 : 3; // gather, then pairs + reduce (or the learned pass's five)
+      if (split) per += 1;                          // the contact step as its walk and its tail
     }
   }
   return per;
 }
+
+// whether a captured mesh step splits its contact step (needs the side stream and the sums buffers; the
+// field step has no mesh)
+bool can_split(const ccs_handle *h) { return h->side && h->part && h->part2 && !h->field; }
 
 // what a step runs before its contact step: the grid, and the mesh and the pairwise pass on mesh steps.
 // The three read the positions and write disjoint buffers, so on a mesh step the grid and the pairwise pass
@@ -544,9 +553,32 @@ void enqueue_pre(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
   cudaStreamWaitEvent(h->st, h->joinEv, 0);
 }
 
+// one step's launches.  A mesh step splits its contact step: the grid and then the contact walk run on the
+// side stream beside the mesh chain and the pairwise pass, which the walk does not read; the particles'
+// gravity, settle/kick, heat and kick/drift (the tail) run after both.  Steps whose kernels are timed one
+// by one, and ensemble members' steps (parallel branches already), run the contact step whole.
 void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
-  enqueue_pre(h, p, U);
-  pass_sim(h, p.u);
+  if (!p.mesh || !can_split(h) || h->timing || h->inEnsemble) {
+    enqueue_pre(h, p, U);
+    pass_sim(h, p.u);
+    return;
+  }
+  cudaEventRecord(h->forkEv, h->st);
+  cudaStreamWaitEvent(h->side, h->forkEv, 0);
+  const cudaStream_t main = h->st;
+  h->st = h->side;
+  if (p.slots) pass_slots(h, p.u);
+  const SimArgs a = sim_args(h);   // the table the grid has just filled
+  h->launches += launch_contacts_only(p.u, h->N, a, h->st, h->tuneWarps);
+  record_uniform_node(h, 2);
+  h->st = main;
+  pass_mesh(h, U, p.u.boxB > 0.5f);
+  pass_pp(h, U, p.u.ppCount);
+  cudaEventRecord(h->joinEv, h->side);
+  cudaStreamWaitEvent(h->st, h->joinEv, 0);
+  h->launches += launch_contact_tail(p.u, h->N, a, h->st);
+  record_uniform_node(h, 2);
+  h->cur ^= 1;
 }
 
 // after a capture: the contact-step nodes it recorded, with their captured arguments
@@ -666,7 +698,7 @@ int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false) {
   }
   CUDA_TRY(h, cudaGraphLaunch(g.exec, h->st));
   h->seatCur = seatCur0 ^ (p.slots ? 1 : 0);
-  h->launches += block_launches(h, &p, 1) + (pre ? 1 : 0);   // and the uniforms node
+  h->launches += block_launches(h, &p, 1, !timed && can_split(h)) + (pre ? 1 : 0);   // and the uniforms node
   if (simOutside) {
     --h->launches;            // the caller launches the contact step
   } else if (timed) {
@@ -767,7 +799,7 @@ int graph_block(ccs_handle *h) {
     g.graph = graph;
     int rc = resolve_uniform_nodes(h, uniNodes, g.uni);
     int want = M;
-    for (int k = 0; k < M; ++k) want += plans[k].slots ? 1 : 0;
+    for (int k = 0; k < M; ++k) want += (plans[k].slots ? 1 : 0) + (plans[k].mesh && can_split(h) ? 1 : 0);
     if (rc == CCS_OK && (int)g.uni.size() != want) {
       h->err = "graph capture: a contact-step node per step and a grid node per even step expected";
       rc = CCS_E_CUDA;
@@ -792,7 +824,7 @@ int graph_block(ccs_handle *h) {
   // a block does 4 grid rebuilds (the table parity returns) and M swaps
   h->cur = cur0 ^ (M & 1);
   h->seatCur = seatCur0 ^ (((M + 1) / 2) & 1);
-  h->launches += block_launches(h, plans, M);
+  h->launches += block_launches(h, plans, M, can_split(h));
   return CCS_OK;
 }
 
@@ -841,6 +873,7 @@ void free_state(ccs_handle *h) {
     dev_free(m.occAsc); dev_free(m.occAscN); dev_free(m.cellPart); dev_free(m.cellDone);
   }
   dev_free(h->mat); dev_free(h->matTmp); dev_free(h->home); dev_free(h->homeTmp);
+  dev_free(h->part); dev_free(h->part2);
   dev_free(h->ppIndex); dev_free(h->ppSlot); dev_free(h->ppList); dev_free(h->ppForce); dev_free(h->ppBox);
   dev_free(h->ppPart);
   dev_free(h->nnCounts); dev_free(h->nnOffs); dev_free(h->nnTotal); dev_free(h->nnPairs); dev_free(h->nnMesh);
@@ -949,6 +982,7 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
   }
   rc |= dev_alloc(h, &h->mat, N); rc |= dev_alloc(h, &h->matTmp, N);
   rc |= dev_alloc(h, &h->home, N); rc |= dev_alloc(h, &h->homeTmp, N);
+  rc |= dev_alloc(h, &h->part, N); rc |= dev_alloc(h, &h->part2, N);
   make_static(h);
   h->ncell = (size_t)h->stat.AW * (size_t)h->stat.AH;
   for (int b = 0; b < 2; ++b) {

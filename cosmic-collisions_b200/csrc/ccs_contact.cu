@@ -120,11 +120,73 @@ __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const Si
   __syncwarp();   // every lane has read its entries before the queue is written again
 }
 
+// a particle's gravity (the mesh gather and the pairwise add, or the field), settle/kick, heat and kick/drift
+// from its contact sums: the end of the contact step, and all of a split mesh step's tail
+template <bool FIELD>
+__device__ __forceinline__ void finish_particle(const ccs_uniforms &u, const SimArgs &a, int me, float4 P, float4 V,
+                                                float ri, float ci, f3 push, float lost, float flow, float nb) {
+  const f3 p = xyz(P);
+  const float body = P.w;
+  f3 grav = mk(0.0f, 0.0f, 0.0f), g;
+  if (FIELD) {
+    grav = ld3(u.gField);   // SIM_GRAV_FIELD, src/glsl-sim.js:490-492: the whole of gravity
+  } else {
+    // SIM_GRAV_MESH, src/glsl-sim.js:469-488
+    const int box = box_of(u, p, g);
+    if (box >= 0) {
+      const float4 *F = box == 0 ? a.forceA : a.forceB;
+      const float fx = floorf(g.x), fy = floorf(g.y), fz = floorf(g.z);
+      const f3 t = mk(g.x - fx, g.y - fy, g.z - fz);
+      const int bx = (int)fx, by = (int)fy, bz = (int)fz;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
+        const float wgt = (ox ? t.x : 1.0f - t.x) * (oy ? t.y : 1.0f - t.y) * (oz ? t.z : 1.0f - t.z);
+        const float4 f = __ldg(F + fine_index(min(bx + ox, 63), min(by + oy, 63), min(bz + oz, 63)));
+        grav = grav + xyz(f) * wgt;
+      }
+      grav = grav - xyz(__ldg(F + kFine)) * u.Gm;   // the strays in neither box pull back
+      if (u.boxB > 0.5f) {
+        const float4 mA = __ldg(a.monoA), mB = __ldg(a.monoB);
+        grav = grav + (box == 0 ? cross_at(u, mB, mA) : cross_at(u, mA, mB));
+      }
+    } else {
+      grav = mass_at(u, p, __ldg(a.monoA));
+      if (u.boxB > 0.5f) grav = grav + mass_at(u, p, __ldg(a.monoB));
+    }
+    const int seat = a.ppSlot[me];
+    if (seat >= 0) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) grav = grav + xyz(__ldg(a.ppForce + (size_t)s * a.cap + seat));
+    }
+  }
+  // SIM_POST, src/glsl-sim.js:493-511
+  const float dt = u.dt;
+  f3 v = xyz(V) + push * (fdiv(u.invM, ri) * dt) + grav * u.gdt;
+  const bool tgt = body < 3.5f;
+  const f3 vr = cross(tgt ? ld3(u.spin0) : ld3(u.spin1), p - (tgt ? ld3(u.cen0) : ld3(u.cen1)));
+  if (u.settle > 0.5f) {   // damp everything but the spin, and let nothing run
+    const f3 dv = (v - vr) * u.damp;
+    const float sp = fsqrt(dot(dv, dv));
+    v = vr + dv * fminf(1.0f, fdiv(u.creep, fmaxf(sp, 1e-9f)));
+  }
+  if (u.kick > 0.5f) v = (tgt ? ld3(u.bulk0) : ld3(u.bulk1)) + vr;
+  const float Q = u.settle > 0.5f ? 0.0f : a.q[me] + (lost + fdiv(flow * u.kappa, u.tK)) * dt;
+  // simFS({frozen: true}), src/glsl-sim.js:523-526: the material that does not move
+  if (FIELD && u.frozen >= 0.0f && fabsf(xsub(body, u.frozen)) < 0.5f) v = mk(0.0f, 0.0f, 0.0f);
+  const f3 pn = p + v * dt;
+  a.posO[me] = make_float4(pn.x, pn.y, pn.z, body);
+  a.velO[me] = make_float4(v.x, v.y, v.z, fdiv(u.tK * Q, ci));
+  a.auxO[me] = make_float4(grav.x, grav.y, grav.z, nb);
+  a.qO[me] = Q;
+}
+
 // W warps per CTA (8 or 4: the autotuner's choice; 4 CTAs of 8 or 8 of 4 share an SM); FIELD: the crater
 // page's constant gravity and frozen material in place of the mesh gather and the pairwise add.
 // The uniforms come by value: every field is then an operand from the constant bank, where through a pointer
 // each was a load and a register held across the walk (5.7 % of the launch's time at 262k).
-template <int W, bool FIELD>
+// SPLIT: stop at the contact sums (a mesh step whose mesh runs beside the contact walk; k_contact_tail ends it).
+template <int W, bool FIELD, bool SPLIT = false>
 __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_uniforms u, const SimArgs a) {
   constexpr int kThreads = 32 * W;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -236,58 +298,25 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
     lost += c.lost;
     flow += c.flow;
   }
-  f3 grav = mk(0.0f, 0.0f, 0.0f), g;
-  if (FIELD) {
-    grav = ld3(u.gField);   // SIM_GRAV_FIELD, src/glsl-sim.js:490-492: the whole of gravity
-  } else {
-    // SIM_GRAV_MESH, src/glsl-sim.js:469-488
-    const int box = box_of(u, p, g);
-    if (box >= 0) {
-      const float4 *F = box == 0 ? a.forceA : a.forceB;
-      const float fx = floorf(g.x), fy = floorf(g.y), fz = floorf(g.z);
-      const f3 t = mk(g.x - fx, g.y - fy, g.z - fz);
-      const int bx = (int)fx, by = (int)fy, bz = (int)fz;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
-        const float wgt = (ox ? t.x : 1.0f - t.x) * (oy ? t.y : 1.0f - t.y) * (oz ? t.z : 1.0f - t.z);
-        const float4 f = __ldg(F + fine_index(min(bx + ox, 63), min(by + oy, 63), min(bz + oz, 63)));
-        grav = grav + xyz(f) * wgt;
-      }
-      grav = grav - xyz(__ldg(F + kFine)) * u.Gm;   // the strays in neither box pull back
-      if (u.boxB > 0.5f) {
-        const float4 mA = __ldg(a.monoA), mB = __ldg(a.monoB);
-        grav = grav + (box == 0 ? cross_at(u, mB, mA) : cross_at(u, mA, mB));
-      }
-    } else {
-      grav = mass_at(u, p, __ldg(a.monoA));
-      if (u.boxB > 0.5f) grav = grav + mass_at(u, p, __ldg(a.monoB));
-    }
-    const int seat = a.ppSlot[me];
-    if (seat >= 0) {
-#pragma unroll
-      for (int s = 0; s < 4; ++s) grav = grav + xyz(__ldg(a.ppForce + (size_t)s * a.cap + seat));
-    }
+  if (SPLIT) {   // a split mesh step: the sums wait in part for the tail, which runs after the mesh
+    a.part[me] = make_float4(push.x, push.y, push.z, nb);
+    a.part2[me] = make_float2(lost, flow);
+    return;
   }
-  // SIM_POST, src/glsl-sim.js:493-511
-  const float dt = u.dt;
-  f3 v = xyz(V) + push * (fdiv(u.invM, ri) * dt) + grav * u.gdt;
-  const bool tgt = body < 3.5f;
-  const f3 vr = cross(tgt ? ld3(u.spin0) : ld3(u.spin1), p - (tgt ? ld3(u.cen0) : ld3(u.cen1)));
-  if (u.settle > 0.5f) {   // damp everything but the spin, and let nothing run
-    const f3 dv = (v - vr) * u.damp;
-    const float sp = fsqrt(dot(dv, dv));
-    v = vr + dv * fminf(1.0f, fdiv(u.creep, fmaxf(sp, 1e-9f)));
-  }
-  if (u.kick > 0.5f) v = (tgt ? ld3(u.bulk0) : ld3(u.bulk1)) + vr;
-  const float Q = u.settle > 0.5f ? 0.0f : a.q[me] + (lost + fdiv(flow * u.kappa, u.tK)) * dt;
-  // simFS({frozen: true}), src/glsl-sim.js:523-526: the material that does not move
-  if (FIELD && u.frozen >= 0.0f && fabsf(xsub(body, u.frozen)) < 0.5f) v = mk(0.0f, 0.0f, 0.0f);
-  const f3 pn = p + v * dt;
-  a.posO[me] = make_float4(pn.x, pn.y, pn.z, body);
-  a.velO[me] = make_float4(v.x, v.y, v.z, fdiv(u.tK * Q, ci));
-  a.auxO[me] = make_float4(grav.x, grav.y, grav.z, nb);
-  a.qO[me] = Q;
+  finish_particle<FIELD>(u, a, me, P, V, ri, ci, push, lost, flow, nb);
+}
+
+// the tail of a split mesh step, one thread a particle: the contact sums the contact walk left in part, then
+// the same gravity, settle/kick, heat and kick/drift as the whole step's
+__global__ void __launch_bounds__(256) k_contact_tail(const ccs_uniforms u, const SimArgs a) {
+  const int me = a.first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (me >= u.N) return;
+  const float4 P = a.pos[me], V = a.vel[me];
+  const float ri = a.mat[me];
+  const float ci = ri * (is_iron(P.w) ? u.cpIron : 1.0f);
+  const float4 s = a.part[me];
+  const float2 s2 = a.part2[me];
+  finish_particle<false>(u, a, me, P, V, ri, ci, mk(s.x, s.y, s.z), s2.x, s2.y, s.w);
 }
 
 size_t contact_smem_bytes(int warps) { return sizeof(ContactWarp) * warps; }
@@ -298,6 +327,10 @@ cudaError_t init_kernels() {
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_contact_step<4, false>, smem, (int)contact_smem_bytes(4));
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_contact_step<8, true>, smem, (int)contact_smem_bytes(8));
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_contact_step<4, true>, smem, (int)contact_smem_bytes(4));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_contact_step<8, false, true>, smem, (int)contact_smem_bytes(8));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_contact_step<4, false, true>, smem, (int)contact_smem_bytes(4));
   return e;
 }
 
@@ -319,6 +352,21 @@ int launch_simulate_range(const ccs_uniforms &u, int N, SimArgs a, cudaStream_t 
 
 int launch_simulate(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps, bool field) {
   return launch_simulate_range(u, N, a, st, warps, field, 0, N);
+}
+
+int launch_contacts_only(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps) {
+  if (N <= 0) return 0;
+  if (warps == 4)
+    k_contact_step<4, false, true><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+  else
+    k_contact_step<8, false, true><<<blocks_for(N, 256), 256, contact_smem_bytes(8), st>>>(u, a);
+  return 1;
+}
+
+int launch_contact_tail(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st) {
+  if (N <= 0) return 0;
+  k_contact_tail<<<blocks_for(N, 256), 256, 0, st>>>(u, a);
+  return 1;
 }
 
 }  // namespace ccs

@@ -80,6 +80,8 @@ struct SimArgs {
   float4 *posO, *velO, *auxO;
   float *qO;
   int first = 0;   // the launch's first particle (a launch over a range of them)
+  float4 *part = nullptr;   // a split mesh step's contact sums: push, neighbour count
+  float2 *part2 = nullptr;  // and dissipation, heat flow
 };
 
 struct DiagArgs {
@@ -106,6 +108,10 @@ int launch_contact_grid(const ccs_uniforms &u, int N, const float4 *pos, uint32_
 // warps: CTA width of the contact step, 8 or 4; u by value (the kernel's first argument)
 int launch_simulate(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps = 8,
                     bool field = false);
+// a split mesh step: the contact walk alone (its sums into a.part, a.part2), then, after the mesh and the
+// pairwise pass, the tail that turns them and the gravity into the step's outputs
+int launch_contacts_only(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps);
+int launch_contact_tail(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st);
 // the contact step for particles [first, first + count) only; first a multiple of 256
 int launch_simulate_range(const ccs_uniforms &u, int N, SimArgs a, cudaStream_t st, int warps, bool field, int first,
                           int count);
