@@ -17,14 +17,15 @@ A step is one full-phase step of the reference schedule (contact grid every
            the library's stream, with L2 flushed (a 256 MiB write) before every
            step, so each step starts from HBM.  Max over ranks.
   e2e      the same metric through the host-buffer C-ABI call
-           (ccs_advance_host: pinned host state in, one step, state out);
-           pcie_floor: the same bytes as plain pinned copies, in then out,
-           which bound that call from below.
+           (ccs_advance_host: pinned host state in, one step, state out).
   roofline the contact step kernel (k_contact_step): algorithmic bytes (92 B per
            particle: pos, vel, mat, q in; pos, vel, aux, q out) over its mean
            event-timed duration, against the measured HBM copy bandwidth.
   cpu_baseline / --impl reference: the CPU oracle (a C restatement of the
-           reference's step, all host cores, OpenMP) on a bounded sample.
+           reference's step, all host cores, OpenMP) on a bounded sample of
+           the same workload: full-phase steps from the same saved mid-impact
+           state (the run prepared by the library, untimed, then handed over
+           as a checkpoint).
   nn_corrected  the same timed steps with the learned pairwise correction
            attached (BF16 network on the tensor cores, half the plain cut),
            after training it on the device on pairs drawn from the same impact
@@ -50,8 +51,19 @@ sys.path.insert(0, ROOT)
 
 ALG_BYTES_SIM = 92          # bytes per particle per contact-step launch
 L2_FLUSH_BYTES = 256 << 20
-TIME_EVERY = 9                 # inside the timed region the contact step is timed on every 9th launch: a stride
-                               # coprime with the 8-step cycle, so the samples cover every step of it
+MIN_SAMPLES = 8                # contact-step launches timed inside the timed region, at least
+# the metric both arms report under (the driver divides their values only when the strings agree)
+METRIC = "particle-steps/s @262k, plain vs NN-corrected P\u00b3M at \u22641e-3 force error"
+
+
+def sample_every(steps):
+    """The stride of the contact-step sample inside the timed region: odd, so coprime with the 8-step cycle
+    and the samples cover every step of it; 9 when that still gives MIN_SAMPLES samples, else the largest
+    odd stride that does (1: every launch)."""
+    for every in (9, 7, 5, 3):
+        if steps // every >= MIN_SAMPLES:
+            return every
+    return 1
 
 
 def impact_opt(N):
@@ -107,36 +119,6 @@ def measured_peaks():
         except Exception:
             pass
     return 6650.0, "fallback"
-
-
-def pcie_floor(hp, hv, hq, ha, dev, reps=20):
-    """The copies of one host-buffer call as plain pinned copies on this box: the inputs (positions,
-    velocities, heat) in, then the outputs (positions, velocities, aux, heat) out.  Their sum bounds a
-    one-step call from below, since no output exists before the inputs have arrived."""
-    import torch
-    N = hp.shape[0]
-    d = torch.empty(13 * N, dtype=torch.float32, device=dev)
-    ins = ((d[:4 * N], hp), (d[4 * N:8 * N], hv), (d[8 * N:9 * N], hq))
-    outs = ((hp, d[:4 * N]), (hv, d[4 * N:8 * N]), (ha, d[8 * N:12 * N]), (hq, d[12 * N:]))
-
-    def us(pairs):
-        for dst, src in pairs:
-            dst.view(-1).copy_(src.view(-1), non_blocking=True)
-        torch.cuda.synchronize()
-        t = time.perf_counter()
-        for _ in range(reps):
-            for dst, src in pairs:
-                dst.view(-1).copy_(src.view(-1), non_blocking=True)
-        torch.cuda.synchronize()
-        return (time.perf_counter() - t) / reps * 1e6
-
-    # the outputs' copy overwrites the host inputs with device scratch: put the inputs back afterwards
-    keep = [t.clone() for t in (hp, hv, hq)]
-    h2d_us, d2h_us = us(ins), us(outs)
-    for t, k in zip((hp, hv, hq), keep):
-        t.copy_(k)
-    return {"h2d_us": h2d_us, "d2h_us": d2h_us, "bound_us_per_call": h2d_us + d2h_us,
-            "how": "the same bytes as plain pinned cudaMemcpyAsync copies, in then out, on this box"}
 
 
 def committed_profile():
@@ -222,20 +204,54 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_reference(N, min_seconds=10.0, min_steps=8, threads=None):
+def prepared_checkpoint(N, prep_steps, log, dev=0):
+    """The mid-impact state both arms time: the run built, settled, brought in and advanced prep_steps
+    full-phase steps by the library (untimed), then saved at a block boundary as a checkpoint (bytes)."""
+    import cosmic_collisions_b200 as cc
+    nb = cc.NBody(dev)
+    try:
+        prepare(nb, cc, N, prep_steps, log)
+        if nb.sim.stepNo % 8:
+            nb.steps(8 - nb.sim.stepNo % 8)
+        nb.sync()
+        return nb.save()
+    finally:
+        nb.close()
+
+
+def cpu_reference(ckpt, min_seconds=10.0, min_steps=8, threads=None, N=None):
     """The CPU oracle's step (the reference's algorithm restated in C, OpenMP over all host cores) on a
-    bounded sample: the freshly built impact, boxes on the target, full-phase steps."""
+    bounded sample of the bench's workload: full-phase steps from the saved mid-impact state `ckpt` (a
+    checkpoint: state, run scalars, boxes, loose list and the boxes' monopoles), with runTo's cadence held
+    fixed (no analysis inside the sample, as the GPU arm's timed steps have none).  Without a checkpoint
+    (a host with no GPU to prepare one) it steps the freshly built N-particle impact instead, and says so."""
+    import numpy as np
+    from cosmic_collisions_b200 import checkpoint
     from oracle import oracle as O
     O.build()
     cores = threads or os.cpu_count()
     O.set_threads(cores)
-    sim, pos, vel, mat, home = O.build_run(O.make_opt(**impact_opt(N)))
-    sim.phase, sim.impactT = 2, sim.t
-    for k in range(3):
-        sim.boxCen[0][k] = sim.cen0[k]
-    sim.boxT[0] = sim.t
-    e = O.Engine(sim, pos, vel, mat)
+    if ckpt is not None:
+        ck = checkpoint.read(ckpt)
+        sim = O.Sim.from_buffer_copy(bytes(ck["sim"]))
+        e = O.Engine(sim, ck["pos"], ck["vel"], ck["mat"])
+        e.prime_mono(0, ck["monoA"])
+        e.prime_mono(1, ck["monoB"])
+        if len(ck["pp_list"]):
+            e.set_pp(np.asarray(ck["pp_list"], np.int32))
+        what = "the GPU arm's saved mid-impact state (step %d, loose list %d)" % (int(ck["sim"].stepNo),
+                                                                                  len(ck["pp_list"]))
+    else:
+        sim, pos, vel, mat, home = O.build_run(O.make_opt(**impact_opt(N)))
+        sim.phase, sim.impactT = 2, sim.t
+        for k in range(3):
+            sim.boxCen[0][k] = sim.cen0[k]
+        sim.boxT[0] = sim.t
+        e = O.Engine(sim, pos, vel, mat)
+        what = "the freshly built impact (no GPU on this host to prepare the mid-impact state)"
+    N = int(e.sim.N)
     e.step(False, False)           # warm: the pair table, first touches of the arrays
+    e.sim.t += e.sim.dt
     steps = 0
     t0 = time.perf_counter()
     while True:
@@ -246,8 +262,8 @@ def cpu_reference(N, min_seconds=10.0, min_steps=8, threads=None):
         if steps >= min_steps and el >= min_seconds:
             break
     return {"value": N * steps / el, "unit": "particle-steps/s", "cores": cores, "kind": "port",
-            "sample": "%d full-phase steps of the freshly built %d-particle impact (%.1f s, %d OpenMP threads)"
-                      % (steps, N, el, cores)}
+            "sample": "%d full-phase steps of the %d-particle impact from %s (%.1f s, %d OpenMP threads)"
+                      % (steps, N, what, el, cores)}
 
 
 def force_error(cc, dev, N, sample=2048, seed=3, net=None):
@@ -489,21 +505,39 @@ def analysis_timing(cc, nb, reps=5):
             "L_rel_diff": abs(rd.L - rh.L) / rh.L}
 
 
+def warm_step_graphs(nb, lib, every):
+    """Capture, before anything is timed, every step graph the timed loop replays: the loop times the contact
+    step on every `every`-th launch (a graph that stops before it) and replays whole-step graphs otherwise,
+    keyed by the step's place in the 8-step cycle and the buffers it touches, so 2 x 8 x every steps of the
+    same loop visit every key."""
+    lib.ccs_timing_every(nb.handle, every)
+    lib.ccs_timing(nb.handle, 1)
+    for _ in range(2 * 8 * every):
+        nb.step(False, False)
+        nb.sim.t += nb.sim.dt
+    nb.sync()
+    lib.ccs_timing(nb.handle, 0)
+    lib.ccs_timing_every(nb.handle, 1)
+
+
 def timed_steps(nb, lib, stream, flush, steps, dev, dist):
-    """steps direct-launch steps, L2 flushed before each, each bracketed by CUDA events on the library's
-    stream; clocks sampled meanwhile.  Inside the timed region the library times the contact step alone
-    (the roofline's kernel) with its own pair of events on every 9th launch, a sample spread over the whole
-    region; the other kernels are timed in a pass of their own after it, since every timed launch widens
-    its step by its events (and leaves the step's captured graph for a direct launch)."""
+    """steps step graphs, L2 flushed before each, each bracketed by CUDA events on the library's stream;
+    clocks sampled meanwhile.  Inside the timed region the library times the contact step alone (the
+    roofline's kernel) with its own pair of events on every n-th launch (sample_every), a sample spread over
+    the whole region.  The other kernels are timed in passes of their own after it, since every timed launch
+    widens its step by its events: the grid, deposit, cell and pairwise kernels on steps launched one kernel
+    at a time, then the two halves of the split mesh step (the contact walk and the tail)."""
     import ctypes as C
     import torch
+    every = sample_every(steps)
+    warm_step_graphs(nb, lib, every)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     clocks = Clocks(dev)
     if dist:
         import torch.distributed as td
         td.barrier()
     torch.cuda.synchronize()
-    lib.ccs_timing_every(nb.handle, TIME_EVERY)
+    lib.ccs_timing_every(nb.handle, every)
     lib.ccs_timing(nb.handle, 1)            # kernel id 0, the contact step
     l0 = lib.ccs_launch_count(nb.handle)
     clocks.start()
@@ -522,7 +556,7 @@ def timed_steps(nb, lib, stream, flush, steps, dev, dist):
     clk = clocks.stop()
     launches = lib.ccs_launch_count(nb.handle) - l0
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    names = ["simulate", "contact_grid", "deposit", "cell", "pp_force"]
+    names = ["simulate", "contact_grid", "deposit", "cell", "pp_force", "contact_walk", "contact_tail"]
     kt = {}
 
     def read(kids):
@@ -532,16 +566,18 @@ def timed_steps(nb, lib, stream, flush, steps, dev, dist):
             kt[names[kid]] = {"launches": cnt.value, "total_ms": tot.value,
                               "mean_us": 1e3 * tot.value / cnt.value if cnt.value else None}
     read([0])
+    kt["simulate"]["every"] = every
     lib.ccs_timing_every(nb.handle, 1)
-    # the other kernels: a pass of their own after the timed region, L2 flushed before each step as above
-    lib.ccs_timing(nb.handle, 0x1E)
-    for k in range(max(16, min(steps, 64))):
-        with torch.cuda.stream(stream):
-            flush.fill_(float(k))
-        nb.step(False, False)
-        nb.sim.t += nb.sim.dt
-    nb.sync()
-    read([1, 2, 3, 4])
+    # the other kernels: passes of their own after the timed region, L2 flushed before each step as above
+    for mask, kids, n in ((0x1E, [1, 2, 3, 4], max(16, min(steps, 64))), (0x60, [5, 6], 32)):
+        lib.ccs_timing(nb.handle, mask)
+        for k in range(n):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+            nb.step(False, False)
+            nb.sim.t += nb.sim.dt
+        nb.sync()
+        read(kids)
     lib.ccs_timing(nb.handle, 0)
     return step_ms, kt, launches, wall, clk
 
@@ -582,7 +618,7 @@ def run_ours(args, rank, world, log):
         nb.close()
         if net is not None:
             net.close()
-        return out
+        return out, None
     import ctypes as C
     buf = nb.device_buffers()
     stream = torch.cuda.ExternalStream(buf.stream, device=dev)
@@ -595,7 +631,7 @@ def run_ours(args, rank, world, log):
     if nb.sim.stepNo % 8:
         nb.steps(8 - nb.sim.stepNo % 8)
     nb.sync()
-    snap_state, snap_sim = nb.read_state(), bytes(nb.sim)
+    snapshot = nb.save()                   # the state the CPU baseline and the learned leg start from
     step_ms, kt, launches, wall, clk = timed_steps(nb, lib, stream, flush, args.steps, dev, dist)
     total_ms = max_over_ranks(sum(step_ms))
     value = world * N * args.steps / (total_ms / 1e3)
@@ -605,6 +641,8 @@ def run_ours(args, rank, world, log):
     ksteps = max(8, args.steps // 8 * 8)
     if nb.sim.stepNo % 8:
         nb.steps(8 - nb.sim.stepNo % 8)
+    nb.steps(ksteps)                       # captures the block graphs (both buffer parities) untimed
+    nb.steps(ksteps)
     nb.sync()
     with torch.cuda.stream(stream):
         g0.record(stream)
@@ -622,6 +660,14 @@ def run_ours(args, rank, world, log):
     ha = torch.empty((N, 4), dtype=torch.float32).pin_memory()
     P = lambda t: C.c_void_p(t.data_ptr())
     e2e_steps = max(8, min(args.steps, 256))
+    for _ in range(16):                    # capture the call's step graphs (every place in the cycle) untimed
+        rc = lib.ccs_advance_host(nb.handle, P(hp), P(hv), P(hq), 1, P(hp), P(hv), P(ha), P(hq))
+        if rc:
+            raise RuntimeError("ccs_advance_host: %d" % rc)
+    for _ in range(2):
+        rc = lib.ccs_advance_host(nb.handle, P(hp), P(hv), P(hq), 8, P(hp), P(hv), P(ha), P(hq))
+        if rc:
+            raise RuntimeError("ccs_advance_host: %d" % rc)
     if dist:
         td.barrier()
     torch.cuda.synchronize()
@@ -644,7 +690,6 @@ def run_ours(args, rank, world, log):
     e2e8_s = max_over_ranks(time.perf_counter() - e0)
     h2d = N * (16 + 16 + 4)
     d2h = N * (16 + 16 + 16 + 4)
-    copy_floor = pcie_floor(hp, hv, hq, ha, dev)
 
     ferr = force_error(cc, dev, N) if rank == 0 else None
     analysis = analysis_timing(cc, nb) if rank == 0 and not args.no_cpu else None
@@ -653,17 +698,8 @@ def run_ours(args, rank, world, log):
     nn_line = None
     if not args.no_nn:
         net, info = learned_correction(cc, dev, N, log, pairs=args.nn_pairs, epochs=args.nn_epochs)
-        C.memmove(C.addressof(nb.sim), snap_sim, len(snap_sim))   # back to the plain leg's starting state
-        nb.set_static()
-        nb.write_state(pos=snap_state["pos"], vel=snap_state["vel"], aux=snap_state["aux"], q=snap_state["q"])
+        nb.load(snapshot)                  # back to the plain leg's starting state
         nb.set_pp_nn(net)
-        for _ in range(args.warmup // 8 * 8):   # whole blocks: the timed steps start where the plain ones did
-            nb.step(False, False)
-            nb.sim.t += nb.sim.dt
-        nb.sync()
-        C.memmove(C.addressof(nb.sim), snap_sim, len(snap_sim))
-        nb.set_static()
-        nb.write_state(pos=snap_state["pos"], vel=snap_state["vel"], aux=snap_state["aux"], q=snap_state["q"])
         nn_ms, nn_kt, nn_launches, nn_wall, nn_clk = timed_steps(nb, lib, stream, flush, args.steps, dev, dist)
         nn_total = max_over_ranks(sum(nn_ms))
         nn_err = force_error(cc, dev, N, net=net) if rank == 0 else None
@@ -679,7 +715,7 @@ def run_ours(args, rank, world, log):
     achieved = ALG_BYTES_SIM * N / (sim_mean_us * 1e-6) / 1e9 if sim_mean_us else None
     tpp = committed_traffic()
     line = {
-        "metric": "particle-steps/s @262k, plain P3M step (value) and the NN-corrected P3M step (nn_corrected)",
+        "metric": METRIC,
         "value": value,
         "unit": "particle-steps/s",
         "n_gpus": world,
@@ -704,8 +740,7 @@ def run_ours(args, rank, world, log):
         },
         "e2e": {"value": world * N * e2e_steps / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "api": "ccs_advance_host, one step per call, pinned host buffers",
-                "us_per_call": e2e_s / e2e_steps * 1e6, "pcie_floor": copy_floor,
-                "floor_frac": copy_floor["bound_us_per_call"] / (e2e_s / e2e_steps * 1e6),
+                "us_per_call": e2e_s / e2e_steps * 1e6,
                 "eight_steps_per_call": {"value": world * N * 8 * calls8 / e2e8_s, "unit": "particle-steps/s",
                                          "calls": calls8, "us_per_call": e2e8_s / calls8 * 1e6,
                                          "what": "the same call with nsteps = 8 (a mesh cycle between the "
@@ -716,8 +751,8 @@ def run_ours(args, rank, world, log):
                      "traffic": tpp * N if tpp else None,
                      "algorithmic_bytes_per_launch": ALG_BYTES_SIM * N,
                      "timed_launches": kt["simulate"]["launches"],
-                     "timing": "CUDA events on the library's stream around every %dth contact step of the timed "
-                               "region" % TIME_EVERY,
+                     "timing": "CUDA events on the library's stream around every %d-th contact step of the timed "
+                               "region" % kt["simulate"]["every"],
                      "limiter": limiter_note()},
         "gpu_launches": int(launches),
         "clocks": clk,
@@ -726,7 +761,7 @@ def run_ours(args, rank, world, log):
         "nn_corrected": nn_line,
     }
     nb.close()
-    return line
+    return line, snapshot
 
 
 def main():
@@ -759,8 +794,14 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        ref = cpu_reference(args.particles, min_seconds=args.cpu_seconds)
-        line = {"impl": "reference", "metric": "particle-steps/s @262k, plain P3M step", "value": ref["value"],
+        import torch
+        log = lambda s: print("[bench] " + s, file=sys.stderr, flush=True)
+        ckpt = None
+        if torch.cuda.is_available():
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+            ckpt = prepared_checkpoint(args.particles, args.prep, log, int(os.environ.get("LOCAL_RANK", "0")))
+        ref = cpu_reference(ckpt, min_seconds=args.cpu_seconds, N=args.particles)
+        line = {"impl": "reference", "metric": METRIC, "value": ref["value"],
                 "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": {"workload": "full plain giant impact, %d particles" % args.particles},
@@ -785,10 +826,10 @@ def main():
             td.barrier()
             td.destroy_process_group()
         return
-    line = run_ours(args, rank, world, log)
+    line, snapshot = run_ours(args, rank, world, log)
     if rank == 0:
         if world == 1 and not args.no_cpu and not args.profile:
-            line["cpu_baseline"] = cpu_reference(args.particles, min_seconds=args.cpu_seconds)
+            line["cpu_baseline"] = cpu_reference(snapshot, min_seconds=args.cpu_seconds)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as td

@@ -41,7 +41,8 @@ EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_ma
            "ccs_nn_train", "ccs_nn_forward", "ccs_nn_labels", "ccs_nn_grad", "ccs_set_pp_nn", "ccs_autotune",
            "ccs_ensemble_create", "ccs_ensemble_destroy", "ccs_ensemble_last_error", "ccs_ensemble_steps",
            "ccs_ensemble_sync", "ccs_ensemble_autotune", "ccs_fof_device", "ccs_set_field",
-           "ccs_checkpoint_size", "ccs_checkpoint_save", "ccs_checkpoint_load", "ccs_timing_every"]
+           "ccs_checkpoint_size", "ccs_checkpoint_save", "ccs_checkpoint_load", "ccs_timing_every",
+           "ccs_set_boxes", "ccs_set_graphs"]
 NN_PARAMS = 4803
 NN_CUT_CELLS = 2.5
 
@@ -113,6 +114,12 @@ class Report(C.Structure):
                 ("ppCount", C.c_int), ("ppLoose", C.c_int)]
 
 
+class Box(C.Structure):
+    """One mesh box as placeBoxes leaves it (sim.boxes[b], src/nbody.js:361-374)."""
+    _fields_ = [("on", C.c_int), ("cen", C.c_double * 3), ("vel", C.c_double * 3), ("t", C.c_double),
+                ("primeMono", C.c_int), ("mono", C.c_float * 4)]
+
+
 class DeviceBuffers(C.Structure):
     _fields_ = [("pos4", C.c_void_p), ("vel4", C.c_void_p), ("aux4", C.c_void_p), ("q", C.c_void_p),
                 ("mat", C.c_void_p), ("home4", C.c_void_p), ("force", C.c_void_p * 2), ("mono", C.c_void_p * 2),
@@ -157,6 +164,7 @@ def lib():
         "ccs_rigid_step": (I, [H, D]),
         "ccs_set_pp": (I, [H, P, I, I]),
         "ccs_prime_mono": (I, [H, I, P]),
+        "ccs_set_boxes": (I, [H, C.POINTER(Box)]),
         "ccs_apply_perm": (I, [H, P]),
         "ccs_sort_morton": (I, [H, P, P, P]),
         "ccs_diag_async": (I, [H]),
@@ -208,6 +216,7 @@ def lib():
         "ccs_checkpoint_save": (I, [H, P, C.c_size_t, P, C.c_size_t]),
         "ccs_checkpoint_load": (I, [H, P, C.c_size_t]),
         "ccs_timing_every": (I, [H, I]),
+        "ccs_set_graphs": (I, [H, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

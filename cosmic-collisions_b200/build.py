@@ -22,8 +22,8 @@ NVCC_FLAGS = [
     "-lineinfo",
     "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
-    "-shared",
 ]
+OBJ = os.path.join(HERE, "_build")
 
 
 def _nvcc():
@@ -31,6 +31,19 @@ def _nvcc():
         if cand and (os.path.sep not in cand or os.path.exists(cand)):
             return cand
     return "nvcc"
+
+
+def _newest_header():
+    return max(os.path.getmtime(os.path.join(CSRC, h)) for h in HEADERS if os.path.exists(os.path.join(CSRC, h)))
+
+
+def _obj(src):
+    return os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
+
+
+def _obj_stale(src, hdr_t):
+    o = _obj(src)
+    return not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(os.path.join(CSRC, src)), hdr_t)
 
 
 def stale():
@@ -42,10 +55,31 @@ def stale():
 
 
 def build(force=False, verbose=False):
-    """Compile the library if any source is newer than it (or force)."""
+    """Compile the library if any source is newer than it (or force): one object per source, compiled in
+    parallel (only the stale ones), then linked into libccstep.so."""
     if not force and not stale():
         return LIB
-    cmd = [_nvcc()] + NVCC_FLAGS + [os.path.join(CSRC, s) for s in SOURCES] + ["-o", LIB + ".tmp"]
+    from concurrent.futures import ThreadPoolExecutor
+    os.makedirs(OBJ, exist_ok=True)
+    hdr_t = _newest_header()
+    todo = [s for s in SOURCES if force or _obj_stale(s, hdr_t)]
+
+    def compile_one(src):
+        cmd = [_nvcc()] + NVCC_FLAGS + ["-c", os.path.join(CSRC, src), "-o", _obj(src) + ".tmp"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError("nvcc failed on %s:\n%s%s" % (src, r.stdout, r.stderr))
+        if r.stderr.strip() and verbose:
+            print(r.stderr, file=sys.stderr)
+        os.replace(_obj(src) + ".tmp", _obj(src))
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 4))) as ex:
+        for f in [ex.submit(compile_one, s) for s in todo]:
+            f.result()
+    cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a"] + [_obj(s) for s in SOURCES] + \
+        ["-o", LIB + ".tmp"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True, cwd=CSRC)

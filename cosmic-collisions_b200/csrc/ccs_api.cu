@@ -35,7 +35,7 @@ constexpr double kSeatSlack = 0.6;
 constexpr double kCpIron = 450.0, kCpRock = 1200.0;
 constexpr int kRing = 256;        // per-step uniform slots of the direct path
 constexpr int kMaxBlock = 16;     // largest meshEvery a captured block supports
-constexpr int kTimedKernels = 5;  // simulate, contact grid, deposit, cell, P3M force
+constexpr int kTimedKernels = 7;  // simulate, contact grid, deposit, cell, P3M force, contact walk, contact tail
 
 struct GraphKey {
   int boxB, pp, seatCur, cur, meshEvery, ping, field;
@@ -558,6 +558,23 @@ void enqueue_pre(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
 // gravity, settle/kick, heat and kick/drift (the tail) run after both.  Steps whose kernels are timed one
 // by one, and ensemble members' steps (parallel branches already), run the contact step whole.
 void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
+  if (p.mesh && can_split(h) && !h->inEnsemble && (h->timing & (3 << 5))) {
+    // the split mesh step with its two halves timed (kernel ids 5 and 6): everything in order on st, so
+    // each half sits alone between its events
+    if (p.slots) pass_slots(h, p.u);
+    const SimArgs a = sim_args(h);
+    cudaEvent_t b, e;
+    time_begin(h, 5, &b, &e);
+    h->launches += launch_contacts_only(p.u, h->N, a, h->st, h->tuneWarps);
+    time_end(h, e);
+    pass_mesh(h, U, p.u.boxB > 0.5f);
+    pass_pp(h, U, p.u.ppCount);
+    time_begin(h, 6, &b, &e);
+    h->launches += launch_contact_tail(p.u, h->N, a, h->st);
+    time_end(h, e);
+    h->cur ^= 1;
+    return;
+  }
   if (!p.mesh || !can_split(h) || h->timing || h->inEnsemble) {
     enqueue_pre(h, p, U);
     pass_sim(h, p.u);
@@ -1723,6 +1740,38 @@ int ccs_prime_mono(ccs_handle *h, int box, const float mono[4]) {
   return CCS_OK;
 }
 
+int ccs_set_boxes(ccs_handle *h, const ccs_box boxes[2]) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!boxes) return CCS_E_ARG;
+  for (int b = 0; b < 2; ++b) {   // everything checked before anything changes
+    const ccs_box &x = boxes[b];
+    bool ok = (x.on == 0 || x.on == 1) && (x.primeMono == 0 || x.primeMono == 1) && std::isfinite(x.t);
+    for (int k = 0; k < 3; ++k)
+      ok = ok && std::isfinite(x.cen[k]) && std::isfinite(x.vel[k]) && std::fabs(x.cen[k]) < 1e6;
+    if (x.primeMono)
+      for (int k = 0; k < 4; ++k) ok = ok && std::isfinite(x.mono[k]);
+    if (!ok) {
+      h->err = "ccs_set_boxes: box " + std::to_string(b) + " has a flag other than 0/1 or a non-finite value";
+      return CCS_E_ARG;
+    }
+  }
+  for (int b = 0; b < 2; ++b) {
+    const ccs_box &x = boxes[b];
+    h->sim.boxOn[b] = x.on;
+    for (int k = 0; k < 3; ++k) {
+      h->sim.boxCen[b][k] = x.cen[k];
+      h->sim.boxVel[b][k] = x.vel[k];
+    }
+    h->sim.boxT[b] = x.t;
+    if (x.primeMono) {
+      rc = ccs_prime_mono(h, b, x.mono);
+      if (rc) return rc;
+    }
+  }
+  return CCS_OK;
+}
+
 static int apply_perm_device(ccs_handle *h, const int32_t *permDev) {
   const int s = h->cur, d = h->cur ^ 1;
   h->launches += launch_permute(h->N, permDev, h->pos[s], h->vel[s], h->aux[s], h->q[s], h->mat, h->home, h->pos[d],
@@ -2507,6 +2556,12 @@ int ccs_sync(ccs_handle *h) {
   CUDA_TRY(h, cudaStreamSynchronize(h->st));
   int rc = check_launch(h);
   return rc ? rc : (h->built ? check_status(h) : CCS_OK);
+}
+
+int ccs_set_graphs(ccs_handle *h, int on) {
+  if (!h || (on != 0 && on != 1)) return CCS_E_ARG;
+  h->useGraphs = on != 0;
+  return CCS_OK;
 }
 
 int ccs_timing_every(ccs_handle *h, int every) {

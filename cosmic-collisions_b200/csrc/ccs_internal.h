@@ -98,6 +98,8 @@ struct DiagArgs {
 // per-device kernel attributes (dynamic shared memory limits); call once per
 // device before the first launch and never during a stream capture
 cudaError_t init_kernels();
+// the current device's multiprocessor count, looked up once per device (safe from any thread)
+int sm_count();
 
 // kernel launchers (ccs_kernels.cu); all enqueue on `st` and return the
 // number of kernels launched.

@@ -321,13 +321,7 @@ __global__ void __launch_bounds__(32 * kFarWarps) k_far(const float4 *__restrict
 }
 
 int launch_far(const MeshBuf &m, cudaStream_t st) {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
+  const int sms = sm_count();
   cudaMemsetAsync(m.farA, 0, sizeof(float4) * kCoarse, st);
   cudaMemsetAsync(m.farT0, 0, sizeof(float4) * kCoarse, st);
   cudaMemsetAsync(m.farT1, 0, sizeof(float4) * kCoarse, st);
@@ -503,13 +497,7 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restr
 }  // namespace
 
 int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int split) {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
+  const int sms = sm_count();
   // a persistent grid over (block, chunk) items: four CTAs of 512 threads fill an SM, more of smaller ones
   const int grid = sms * (split == 2 ? 16 : split == 4 ? 8 : 4);
   cudaMemsetAsync(m.force, 0, sizeof(float4) * kFine, st);

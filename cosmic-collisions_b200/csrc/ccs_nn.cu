@@ -835,16 +835,7 @@ __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__rest
   }
 }
 
-int forward_grid() {
-  static int grid = 0;
-  if (!grid) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    grid = 3 * sms;
-  }
-  return grid;
-}
+int forward_grid() { return 3 * sm_count(); }
 
 }  // namespace nn
 

@@ -153,13 +153,7 @@ __global__ void __launch_bounds__(kBlock) k_pp_reduce(const ccs_uniforms *__rest
 
 int launch_pp_force(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,
                     float4 *part, float4 *force, cudaStream_t st) {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
+  const int sms = sm_count();
   // enough CTAs for a full list's items to take a few rounds; a short list's take one
   const int full = (cap + kPPI - 1) / kPPI * 4 * kMaxChunks;
   k_pp_pairs<<<std::min(full, sms * 8), kPPI, 0, st>>>(u, list, box, cap, tab, part);
@@ -183,11 +177,12 @@ int launch_pp_force(const ccs_uniforms *u, const float4 *list, const float *box,
 // sums of the 2-D tiling -- lives here, in a file-scope device array sized for
 // lists of up to CCS_PP_STATIC_MAX entries (2 MiB, held by every GPU that
 // loads the library until the process exits).  Its uniforms live in a second
-// static device struct, filled by an asynchronous copy on the caller's stream.
-// Every call shares both: two calls that overlap on the GPU (different
-// streams, or another thread) race and must be ordered by the caller.
-// Nothing in the scratch has to start at zero -- every partial the reduction
-// reads is written earlier in the same call.
+// static device struct, written on the caller's stream by a one-thread kernel
+// that takes them by value (no host staging buffer, pageable or pinned, is
+// read by the GPU).  Every call shares both: two calls that overlap on the GPU
+// (different streams, or another thread) race and must be ordered by the
+// caller.  Nothing in the scratch has to start at zero -- every partial the
+// reduction reads is written earlier in the same call.
 // ---------------------------------------------------------------------------
 #include <mutex>
 
@@ -200,6 +195,10 @@ static __device__ __align__(256) float4 g_pp_scratch[kStaticScratch];
 static __device__ __align__(256) ccs_uniforms g_pp_uniforms;
 
 namespace {
+// the call's uniforms into the static struct, in stream order before the pass that reads them (device code
+// names the array itself; only host code needs its looked-up address)
+__global__ void k_pp_static_uniforms(const ccs_uniforms u) { g_pp_uniforms = u; }
+
 std::mutex g_pp_static_mutex;
 float4 *g_pp_scratch_at[kStaticMaxDevices] = {};
 ccs_uniforms *g_pp_uniforms_at[kStaticMaxDevices] = {};
@@ -230,8 +229,7 @@ extern "C" int ccs_pp_force_static(const float *list4, const float *box, int n, 
   u.a2 = a2;
   u.Gm = gm;
   u.ppCount = n;
-  if (cudaMemcpyAsync(g_pp_uniforms_at[dev], &u, sizeof u, cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return CCS_E_CUDA;
+  k_pp_static_uniforms<<<1, 1, 0, st>>>(u);
   ccs::launch_pp_force(g_pp_uniforms_at[dev], reinterpret_cast<const float4 *>(list4), box, n,
                        reinterpret_cast<const float2 *>(tab2), g_pp_scratch_at[dev],
                        reinterpret_cast<float4 *>(force4), st);

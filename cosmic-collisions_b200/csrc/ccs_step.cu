@@ -1,10 +1,24 @@
 // ccs_step.cu -- the per-particle kernels around the contact step: the contact
 // grid (seat tables), the books' read-outs (diag) and the rigid carry of the
 // approach.
+#include <atomic>
+
 #include "ccs_device.cuh"
 #include "ccs_internal.h"
 
 namespace ccs {
+
+int sm_count() {
+  constexpr int kDevices = 64;
+  static std::atomic<int> cache[kDevices];   // zero until the device's first lookup
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices) return 148;
+  int v = cache[dev].load(std::memory_order_relaxed);
+  if (v > 0) return v;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+  cache[dev].store(v, std::memory_order_relaxed);
+  return v;
+}
 
 namespace {
 constexpr int kBlock = 256;
@@ -19,7 +33,8 @@ __global__ void k_fill_u32(uint32_t *p, size_t n, uint32_t v) {
 int launch_fill_u32(uint32_t *p, size_t n, uint32_t v, cudaStream_t st) {
   if (n == 0) return 0;
   int g = (int)((n + kBlock - 1) / kBlock);
-  if (g > 148 * 16) g = 148 * 16;
+  const int cap = sm_count() * 16;
+  if (g > cap) g = cap;
   k_fill_u32<<<g, kBlock, 0, st>>>(p, n, v);
   return 1;
 }

@@ -389,29 +389,51 @@ class NBody:
         self.set_pp(lst, r.ppLoose)
 
     def _place_boxes(self, r, t):
-        """placeBoxes, src/nbody.js:361-374."""
+        """placeBoxes, src/nbody.js:361-374: the two boxes from a look, handed over in one ccs_set_boxes."""
         s = self.sim
-        s.boxOn[0] = 1
+        boxes = (L.Box * 2)()
+        a, b = boxes[0], boxes[1]
+        a.on, a.t = 1, t
         for k in range(3):
-            s.boxCen[0][k] = r.core[k]
-            s.boxVel[0][k] = r.bodyVel[k]
-        s.boxT[0] = t
+            a.cen[k], a.vel[k] = r.core[k], r.bodyVel[k]
+        b.on = s.boxOn[1]
+        b.t = s.boxT[1]
+        for k in range(3):
+            b.cen[k], b.vel[k] = s.boxCen[1][k], s.boxVel[1][k]
         if r.hasSecond and r.secMass > 0.05:
             d = max(abs(r.secCore[k] - r.core[k]) for k in range(3))
             far = FL - 1.3 * math.pow(r.secMass, 1.0 / 3.0)
             if not s.boxOn[1] and d > far:
-                s.boxOn[1] = 1
+                b.on = 1
                 w = r.secMass / s.m
                 c = r.secCore
-                self.prime_mono(1, np.array([c[0] * w, c[1] * w, c[2] * w, w], np.float32))
+                b.primeMono = 1
+                for k, v in enumerate((c[0] * w, c[1] * w, c[2] * w, w)):
+                    b.mono[k] = v
             elif s.boxOn[1] and d < far - 0.5:
-                s.boxOn[1] = 0
+                b.on = 0
             for k in range(3):
-                s.boxCen[1][k] = r.secCore[k]
-                s.boxVel[1][k] = r.secVel[k]
-            s.boxT[1] = t
+                b.cen[k], b.vel[k] = r.secCore[k], r.secVel[k]
+            b.t = t
         else:
-            s.boxOn[1] = 0
+            b.on = 0
+        self._check(lib().ccs_set_boxes(self._h, boxes), "ccs_set_boxes")
+
+    def set_boxes(self, boxes):
+        """Both mesh boxes at once: a sequence of two dicts with on, cen, vel, t and optionally mono (the
+        first monopole of a box that has just gone up)."""
+        arr = (L.Box * 2)()
+        for b, d in zip(arr, boxes):
+            b.on = int(d["on"])
+            b.t = float(d.get("t", self.sim.t))
+            for k in range(3):
+                b.cen[k] = float(d["cen"][k])
+                b.vel[k] = float(d.get("vel", (0.0, 0.0, 0.0))[k])
+            if d.get("mono") is not None:
+                b.primeMono = 1
+                for k in range(4):
+                    b.mono[k] = float(d["mono"][k])
+        self._check(lib().ccs_set_boxes(self._h, arr), "ccs_set_boxes")
 
     def prime_mono(self, box, mono):
         m = np.ascontiguousarray(mono, np.float32)

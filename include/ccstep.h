@@ -162,6 +162,18 @@ int ccs_rigid_step(ccs_handle *h, double dtF);
 int ccs_set_pp(ccs_handle *h, const int32_t *list, int n, int loose);
 /* placeBoxes' priming of a box's mono texel (src/nbody.js:368-370) */
 int ccs_prime_mono(ccs_handle *h, int box, const float mono[4]);
+/* One mesh box as placeBoxes leaves it (sim.boxes[b], src/nbody.js:361-374). */
+typedef struct {
+  int on;            /* the box is up: box 0 rides the largest body, box 1 a separating second body */
+  double cen[3];     /* the body's core at the look (r.core / r.second.core) */
+  double vel[3];     /* the body's velocity: boxes() carries the centre on at it (src/nbody.js:342-344) */
+  double t;          /* the time of the look */
+  int primeMono;     /* 1: the box has just gone up; mono is its first monopole (src/nbody.js:366-370) */
+  float mono[4];     /* sum of m x and of m, in particle masses (read when primeMono is 1) */
+} ccs_box;
+/* placeBoxes(r): both boxes at once, validated (on is 0 or 1; every value finite; |cen| within 1e6 R_earth)
+ * before anything changes; CCS_E_ARG otherwise.  Takes effect at the next mesh step. */
+int ccs_set_boxes(ccs_handle *h, const ccs_box boxes[2]);
 /* applyPerm(perm): state, mat and home gathered by perm, then fresh contact cells */
 int ccs_apply_perm(ccs_handle *h, const int32_t *perm);
 /* The Morton order of src/nbody.js:871-887 computed on the device (keys in
@@ -365,13 +377,20 @@ int ccs_checkpoint_load(ccs_handle *h, const void *buf, size_t bytes);
 
 /* ---- timing helpers for the benchmark ---- */
 int ccs_sync(ccs_handle *h);
+/* CUDA-graph replay of steps on (1, the default) or off (0: every kernel
+ * launched directly), for comparing the two paths and for debugging */
+int ccs_set_graphs(ccs_handle *h, int on);
 /* average device time (ms) of the kernels named by `kernel` launched since the
  * last reset, measured with CUDA events on the handle's stream; kernel ids:
- * 0 contact step (simulate), 1 contact grid, 2 deposit, 3 cell, 4 P3M force.
+ * 0 contact step (simulate), 1 contact grid, 2 deposit, 3 cell, 4 P3M force,
+ * 5 and 6 the two halves of a split mesh step (the contact walk, which stops
+ * at the contact sums, and the tail: gravity, settle/kick, heat, kick/drift).
  * `enable` is a mask of the ids to time (bit k for id k; CCS_TIME_ALL for all,
  * 0 for none): each timed launch records two events, which widen the gap
- * before and after it by a microsecond or two. */
-#define CCS_TIME_ALL 0x1F
+ * before and after it by a microsecond or two.  Timing ids 5 or 6 runs mesh
+ * steps split and in order on the handle's stream; timing any of ids 1-4
+ * runs them whole. */
+#define CCS_TIME_ALL 0x7F
 int ccs_timing(ccs_handle *h, int enable);
 /* time the contact step on every `every`-th launch only (1, the default: on
  * every launch), so that a long run carries its events on a sample */
