@@ -42,7 +42,7 @@ EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_ma
            "ccs_ensemble_create", "ccs_ensemble_destroy", "ccs_ensemble_last_error", "ccs_ensemble_steps",
            "ccs_ensemble_sync", "ccs_ensemble_autotune", "ccs_fof_device", "ccs_set_field",
            "ccs_checkpoint_size", "ccs_checkpoint_save", "ccs_checkpoint_load", "ccs_timing_every",
-           "ccs_set_boxes", "ccs_set_graphs"]
+           "ccs_set_boxes", "ccs_set_graphs", "ccs_contact_pairs"]
 NN_PARAMS = 4803
 NN_CUT_CELLS = 2.5
 
@@ -217,6 +217,7 @@ def lib():
         "ccs_checkpoint_load": (I, [H, P, C.c_size_t]),
         "ccs_timing_every": (I, [H, I]),
         "ccs_set_graphs": (I, [H, I]),
+        "ccs_contact_pairs": (I, [H, I, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

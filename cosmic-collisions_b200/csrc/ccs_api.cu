@@ -2558,6 +2558,33 @@ int ccs_sync(ccs_handle *h) {
   return rc ? rc : (h->built ? check_status(h) : CCS_OK);
 }
 
+int ccs_contact_pairs(ccs_handle *h, int cap, int32_t *counts, uint32_t *pairs) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (cap < 1 || cap > 1024 || !counts || !pairs) return CCS_E_ARG;
+  cudaSetDevice(h->device);
+  const size_t N = (size_t)h->N;
+  uint32_t *dp = nullptr;
+  rc = dev_alloc(h, &dp, N * (size_t)cap);
+  if (rc) return rc;
+  SimArgs a = sim_args(h);   // the current state in, the spare buffers out (the run does not advance)
+  a.pairs = dp;
+  a.pairCap = cap;
+  CUDA_TRY(h, cudaMemsetAsync(dp, 0xFF, sizeof(uint32_t) * N * (size_t)cap, h->st));
+  h->launches += launch_contact_pairs(pass_uniforms(h, 0, 0, 0.0), h->N, a, h->st);
+  std::vector<float4> aux(N);
+  cudaError_t e = cudaMemcpyAsync(pairs, dp, sizeof(uint32_t) * N * (size_t)cap, cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(aux.data(), a.auxO, sizeof(float4) * N, cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(dp);
+  if (e != cudaSuccess) {
+    h->err = std::string("ccs_contact_pairs: ") + cudaGetErrorString(e);
+    return CCS_E_CUDA;
+  }
+  for (size_t i = 0; i < N; ++i) counts[i] = (int32_t)aux[i].w;
+  return check_launch(h);
+}
+
 int ccs_set_graphs(ccs_handle *h, int on) {
   if (!h || (on != 0 && on != 1)) return CCS_E_ARG;
   h->useGraphs = on != 0;

@@ -75,13 +75,18 @@ __device__ __forceinline__ Contact contact_of(const ccs_uniforms &u, const SimAr
 }
 
 // a pair inside the link radius: its owner's count; a touching one onto its owner's list (past the list's
-// end, rarely, its contact is worked out here and added to the owner's shared slots)
+// end, rarely, its contact is worked out here and added to the owner's shared slots).  PAIRS: the pair is
+// also written to its owner's row of the pair read-out (the warp's first particle is `base`)
+template <bool PAIRS>
 __device__ __forceinline__ void take_near(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, uint32_t e,
-                                          float r2) {
+                                          float r2, int base) {
   const int o = (int)(e >> 18);
-  atomicAdd(&w.nb[o], 1);
+  const int slot = atomicAdd(&w.nb[o], 1);
   const float r = __fsqrt_rn(r2);
-  if (xsub(u.touch, r) > 0.0f) {
+  const bool touch = xsub(u.touch, r) > 0.0f;
+  if (PAIRS && slot < a.pairCap)
+    a.pairs[(size_t)(base + o) * a.pairCap + slot] = (e & 0x3FFFFu) | (touch ? 0x80000000u : 0u);
+  if (touch) {
     const int k = atomicAdd(&w.tn[o], 1);
     if (k < kTCap) {
       w.tl[k][o] = e & 0x3FFFFu;
@@ -98,8 +103,9 @@ __device__ __forceinline__ void take_near(const ccs_uniforms &u, const SimArgs &
 
 // stage 2: queued seats, two per lane when there are 64 (two position loads in flight), else one
 // (lanes >= n idle); pairs inside the link radius are counted, touching ones listed for their owner
+template <bool PAIRS>
 __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, int base,
-                                                 int n, int lane) {
+                                                 int n, int lane, int first) {
   if (lane < n) {
     const bool two = n == 64;
     const uint32_t e0 = w.q[base + lane];
@@ -109,12 +115,12 @@ __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const Si
     const float4 Po0 = w.P[e0 >> 18];
     const f3 d0 = xsub3(xyz(Pj0), xyz(Po0));
     const float r20 = xdot(d0, d0);
-    if (r20 < u.link2) take_near(u, a, w, e0, r20);
+    if (r20 < u.link2) take_near<PAIRS>(u, a, w, e0, r20, first);
     if (two) {
       const float4 Po1 = w.P[e1 >> 18];
       const f3 d1 = xsub3(xyz(Pj1), xyz(Po1));
       const float r21 = xdot(d1, d1);
-      if (r21 < u.link2) take_near(u, a, w, e1, r21);
+      if (r21 < u.link2) take_near<PAIRS>(u, a, w, e1, r21, first);
     }
   }
   __syncwarp();   // every lane has read its entries before the queue is written again
@@ -186,7 +192,7 @@ __device__ __forceinline__ void finish_particle(const ccs_uniforms &u, const Sim
 // The uniforms come by value: every field is then an operand from the constant bank, where through a pointer
 // each was a load and a register held across the walk (5.7 % of the launch's time at 262k).
 // SPLIT: stop at the contact sums (a mesh step whose mesh runs beside the contact walk; k_contact_tail ends it).
-template <int W, bool FIELD, bool SPLIT = false>
+template <int W, bool FIELD, bool SPLIT = false, bool PAIRS = false>
 __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_uniforms u, const SimArgs a) {
   constexpr int kThreads = 32 * W;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -195,6 +201,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   ContactWarp &w = reinterpret_cast<ContactWarp *>(smem_raw)[wid];
   const int me = a.first + blockIdx.x * kThreads + threadIdx.x;
+  const int first = me - lane;   // the warp's first particle (the pair read-out's rows)
   const bool live = me < u.N;
   const float cell = u.cell;
   float4 P = make_float4(0, 0, 0, 0), V = make_float4(0, 0, 0, 0);
@@ -271,16 +278,16 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
         __syncwarp();
         while (qn >= 64) {
           qn -= 64;
-          drain_candidates(u, a, w, qn, 64, lane);
+          drain_candidates<PAIRS>(u, a, w, qn, 64, lane, first);
         }
       }
     }
   }
   if (qn >= 32) {
     qn -= 32;
-    drain_candidates(u, a, w, qn, 32, lane);
+    drain_candidates<PAIRS>(u, a, w, qn, 32, lane, first);
   }
-  if (qn > 0) drain_candidates(u, a, w, 0, qn, lane);
+  if (qn > 0) drain_candidates<PAIRS>(u, a, w, 0, qn, lane, first);
   __syncwarp();
   if (!live) return;
   // stage 3: each owner's touching neighbours in its own lane, the sums in registers
@@ -331,6 +338,8 @@ cudaError_t init_kernels() {
     e = cudaFuncSetAttribute(k_contact_step<8, false, true>, smem, (int)contact_smem_bytes(8));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_contact_step<4, false, true>, smem, (int)contact_smem_bytes(4));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_contact_step<4, false, false, true>, smem, (int)contact_smem_bytes(4));
   return e;
 }
 
@@ -360,6 +369,12 @@ int launch_contacts_only(const ccs_uniforms &u, int N, const SimArgs &a, cudaStr
     k_contact_step<4, false, true><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
   else
     k_contact_step<8, false, true><<<blocks_for(N, 256), 256, contact_smem_bytes(8), st>>>(u, a);
+  return 1;
+}
+
+int launch_contact_pairs(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st) {
+  if (N <= 0) return 0;
+  k_contact_step<4, false, false, true><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
   return 1;
 }
 

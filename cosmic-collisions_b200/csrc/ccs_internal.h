@@ -82,6 +82,8 @@ struct SimArgs {
   int first = 0;   // the launch's first particle (a launch over a range of them)
   float4 *part = nullptr;   // a split mesh step's contact sums: push, neighbour count
   float2 *part2 = nullptr;  // and dissipation, heat flow
+  uint32_t *pairs = nullptr;  // the contact-pair read-out: per owner pairCap words, neighbour | touching << 31
+  int pairCap = 0;
 };
 
 struct DiagArgs {
@@ -114,6 +116,8 @@ int launch_simulate(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t
 // pairwise pass, the tail that turns them and the gravity into the step's outputs
 int launch_contacts_only(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps);
 int launch_contact_tail(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st);
+// the contact step with its pair sets written out (a.pairs, a.pairCap): the same walk, outputs to a's buffers
+int launch_contact_pairs(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st);
 // the contact step for particles [first, first + count) only; first a multiple of 256
 int launch_simulate_range(const ccs_uniforms &u, int N, SimArgs a, cudaStream_t st, int warps, bool field, int first,
                           int count);

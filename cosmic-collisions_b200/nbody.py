@@ -435,6 +435,15 @@ class NBody:
                     b.mono[k] = float(d["mono"][k])
         self._check(lib().ccs_set_boxes(self._h, arr), "ccs_set_boxes")
 
+    def contact_pairs(self, cap=64):
+        """The contact-pair sets of the current state (ccs_contact_pairs): (counts, pairs), pairs an N x cap
+        array of neighbour indices with bit 31 set for touching pairs, unused slots 0xFFFFFFFF."""
+        N = self.sim.N
+        counts = np.zeros(N, np.int32)
+        pairs = np.zeros((N, cap), np.uint32)
+        self._check(lib().ccs_contact_pairs(self._h, int(cap), ptr(counts), ptr(pairs)), "ccs_contact_pairs")
+        return counts, pairs
+
     def prime_mono(self, box, mono):
         m = np.ascontiguousarray(mono, np.float32)
         self._check(lib().ccs_prime_mono(self._h, int(box), ptr(m)), "ccs_prime_mono")

@@ -325,6 +325,17 @@ int ccs_ensemble_sync(ccs_ensemble *e);   /* waits for the rounds; reports any m
  * its own.  choice (may be NULL) gets {warps, threads per cell}. */
 int ccs_ensemble_autotune(ccs_ensemble *e, int rounds, int choice[2]);
 
+/* The contact-pair sets of the current state, read out for checking: the
+ * contact step's own walk over the current seat table (the 27 cells, the
+ * seat cull, the link test, src/glsl-sim.js:415-450), with each pair inside
+ * the link radius written to its owner's row as the neighbour's index, bit 31
+ * set when the two touch (2a - r > 0).  counts (N) gets each owner's
+ * neighbour count; pairs (N x cap) its first min(count, cap) pairs in no
+ * particular order, the rest 0xFFFFFFFF.  The run does not advance.  No
+ * counterpart in the reference, whose pairs live only inside simFS's loop.
+ * Allocates device memory for the call's duration. */
+int ccs_contact_pairs(ccs_handle *h, int cap, int32_t *counts, uint32_t *pairs);
+
 /* Internal buffers, for tests and the console checks of index.html:531-556:
  * which = CCS_BUF_* below; bytes must equal the buffer's size. */
 enum {

@@ -935,6 +935,51 @@ void orc_sim_pass(const orc_uni *u, const float *pos4, const float *vel4, const 
   }
 }
 
+/* src/glsl-sim.js:415-450: the same 27-cell walk, seat cull and link test as orc_sim_pass, recording the
+ * pairs instead of summing their forces */
+void orc_contact_pairs(const orc_uni *u, const float *pos4, const uint32_t *seats, int cap, int32_t *counts,
+                       uint32_t *pairs) {
+#pragma omp parallel for schedule(static)
+  for (int me = 0; me < u->N; me++) {
+    const float *P = pos4 + 4 * (size_t)me;
+    v3 p = ld3(P);
+    int n = 0;
+    uint32_t *row = pairs + (size_t)me * cap;
+    for (int k = 0; k < cap; k++) row[k] = 0xFFFFFFFFu;
+    int c[3] = {(int)floorf(p.x * u->invCell), (int)floorf(p.y * u->invCell), (int)floorf(p.z * u->invCell)};
+    v3 c0 = V3((float)c[0] * u->cell, (float)c[1] * u->cell, (float)c[2] * u->cell);
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          v3 lo = V3(c0.x + (float)dx * u->cell, c0.y + (float)dy * u->cell, c0.z + (float)dz * u->cell);
+          v3 hi = V3(lo.x + u->cell, lo.y + u->cell, lo.z + u->cell);
+          v3 q = vsub(V3(fclampf(p.x, lo.x, hi.x), fclampf(p.y, lo.y, hi.y), fclampf(p.z, lo.z, hi.z)), p);
+          if (vdot(q, q) > u->link2) continue;
+          int ax, ay;
+          orc_hash(u, c[0] + dx, c[1] + dy, c[2] + dz, &ax, &ay);
+          const uint32_t *s = seats + ((size_t)ay * u->AW + ax) * ORC_SEATS;
+          for (int k = 0; k < ORC_SEATS; k++) {
+            uint32_t sv = s[k];
+            if (sv & 0x80000000u) break;
+            int j = (int)(sv & 0x3FFFFu);
+            if (j == me) continue;
+            v3 sp = V3(((float)((sv >> 18) & 15u) + 0.5f) / 15.0f, ((float)((sv >> 22) & 15u) + 0.5f) / 15.0f,
+                       ((float)((sv >> 26) & 15u) + 0.5f) / 15.0f);
+            v3 dq = vsub(vadd(lo, vmuls(sp, u->cell)), p);
+            if (vdot(dq, dq) > u->reach2) continue;
+            v3 d = vsub(ld3(pos4 + 4 * (size_t)j), p);
+            float r2 = vdot(d, d);
+            if (r2 < u->link2) {
+              float r = sqrtf(r2);
+              if (n < cap) row[n] = (uint32_t)j | (u->touch - r > 0.0f ? 0x80000000u : 0u);
+              n++;
+            }
+          }
+        }
+    counts[me] = n;
+  }
+}
+
 /* src/glsl-sim.js:608-667 DIAG_FS */
 void orc_diag(const orc_uni *u, const float *pos4, const float *qa, const uint32_t *seats,
               const float *forceA, const float *monoA, const float *forceB, const float *monoB,

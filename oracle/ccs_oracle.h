@@ -113,6 +113,11 @@ void orc_sim_pass(const orc_uni *u, const float *pos4, const float *vel4, const 
                   const uint32_t *seats, const float *forceA, const float *monoA, const float *forceB,
                   const float *monoB, const int *ppslot, const float *ppforce, int cap,
                   float *pos_o, float *vel_o, float *aux_o, float *q_o);
+/* the contact-pair sets of simFS's loop (src/glsl-sim.js:415-450), walked as orc_sim_pass walks them: per
+ * owner, every neighbour inside the link radius as its index with bit 31 set when the two touch; counts (N)
+ * the owner's neighbours, pairs (N x cap) the first cap of them in walk order, the rest 0xFFFFFFFF */
+void orc_contact_pairs(const orc_uni *u, const float *pos4, const uint32_t *seats, int cap, int32_t *counts,
+                       uint32_t *pairs);
 void orc_diag(const orc_uni *u, const float *pos4, const float *q, const uint32_t *seats,
               const float *forceA, const float *monoA, const float *forceB, const float *monoB,
               const int *ppslot, const float *ppforce, int cap, float *diag4);

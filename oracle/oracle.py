@@ -144,6 +144,7 @@ def lib():
         L.orc_pp_force.argtypes = [C.POINTER(Uni), P, P, C.c_int, C.c_int, P, P]
         L.orc_sim_pass.argtypes = [C.POINTER(Uni)] + [P] * 11 + [C.c_int] + [P] * 4
         L.orc_diag.argtypes = [C.POINTER(Uni)] + [P] * 9 + [C.c_int, P]
+        L.orc_contact_pairs.argtypes = [C.POINTER(Uni), P, P, C.c_int, P, P]
         L.orc_rigid.argtypes = [C.c_int] + [P] * 10 + [C.c_float, P, P]
         L.orc_morton.argtypes = [C.c_int, P, P, P, P, P]
         L.orc_engine_new.restype = P
@@ -263,6 +264,17 @@ def nn_labels(rec):
         lib().orc_nn_label(ptr(d), ptr(s), ptr(o))
         out[k] = o
     return out
+
+
+def contact_pairs(u, pos4, seats, cap=64):
+    """The contact-pair sets of simFS's loop: (counts, pairs N x cap; index | touching << 31)."""
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    seats = np.ascontiguousarray(seats, np.uint32)
+    N = pos4.shape[0]
+    counts = np.zeros(N, np.int32)
+    pairs = np.zeros((N, cap), np.uint32)
+    lib().orc_contact_pairs(C.byref(u), ptr(pos4), ptr(seats), int(cap), ptr(counts), ptr(pairs))
+    return counts, pairs
 
 
 def box_of(u, p):

@@ -133,6 +133,12 @@ def test_contact_step(nb, ccmod, orc, settle, kick):
     # the pair set: every particle counts the same neighbours
     assert np.array_equal(got["aux"][:, 3], ao[:, 3])
     assert ao[:, 3].mean() > 5          # the contact loop found neighbours
+    # ... and the same ones: every owner's neighbours and which of them touch, as sets
+    gc, gp = nb.contact_pairs(64)
+    oc, op = orc.contact_pairs(u, pos, seats, 64)
+    assert np.array_equal(gc, oc) and gc.max() <= 64
+    assert np.array_equal(np.sort(gp, axis=1), np.sort(op, axis=1))
+    assert (op[op != 0xFFFFFFFF] >> 31).sum() > 0          # touching pairs among them
     assert np.array_equal(got["pos"][:, 3], po[:, 3])
     for name, a, b in (("pos", got["pos"][:, :3], po[:, :3]), ("vel", got["vel"][:, :3], vo[:, :3]),
                        ("T", got["vel"][:, 3], vo[:, 3]), ("q", got["q"], qo)):

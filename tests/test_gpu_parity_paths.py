@@ -204,6 +204,7 @@ def test_contact_step_at_262k_mid_impact(ccmod, orc, mid_impact):
     try:
         nb.load(mid_impact)
         nb.pass_slots()
+        gcount, gpairs = nb.contact_pairs(64)
         nb.pass_sim(False, False, 0.0)
         got = nb.read_state()
     finally:
@@ -227,6 +228,10 @@ def test_contact_step_at_262k_mid_impact(ccmod, orc, mid_impact):
     orc.lib().orc_sim_pass(C.byref(u), P(pos), P(vel), P(mat), P(q), P(seats), P(zf), P(z4), P(zf), P(z4), P(slot),
                            P(ppf), orc.PP_CAP, P(po), P(vo), P(ao), P(qo))
     assert np.array_equal(got["aux"][:, 3], ao[:, 3])
+    # the contact-pair sets themselves, owner by owner (neighbour index and whether the two touch)
+    ocount, opairs = orc.contact_pairs(u, pos, seats, 64)
+    assert np.array_equal(gcount, ocount) and ocount.max() <= 64
+    assert np.array_equal(np.sort(gpairs, axis=1), np.sort(opairs, axis=1))
     dv_g = got["vel"][:, :3].astype(np.float64) - vel[:, :3]
     dv_o = vo[:, :3].astype(np.float64) - vel[:, :3]
     rms = np.sqrt((dv_o ** 2).sum(1).mean())

@@ -196,3 +196,34 @@ def test_morton_order(orc):
     assert np.array_equal(keys, want)
     assert np.array_equal(perm, np.lexsort((np.arange(N), keys)))
     assert np.array_equal(into[perm], np.arange(N))
+
+
+def test_contact_pair_sets_match_the_step_counts(orc):
+    """The oracle's pair read-out walks simFS's loop as its step does: every owner's pair count is the
+    step's neighbour count, the touching pairs lie inside the contact distance, and no particle pairs with
+    itself."""
+    import ctypes as C
+    N = 16384
+    sim, pos, vel, mat, home = orc.build_run(orc.make_opt(N))
+    u = orc.make_uni(sim)
+    seats = orc.slots(u, pos)
+    counts, pairs = orc.contact_pairs(u, pos, seats, 64)
+    zf = np.zeros(((orc.FINE + 1), 4), np.float32)
+    z4 = np.zeros(4, np.float32)
+    slot = np.full(N, -1, np.int32)
+    ppf = np.zeros((4 * orc.PP_CAP, 4), np.float32)
+    q = np.zeros(N, np.float32)
+    po, vo, ao, qo = (np.zeros((N, 4), np.float32), np.zeros((N, 4), np.float32), np.zeros((N, 4), np.float32),
+                      np.zeros(N, np.float32))
+    P = orc.ptr
+    orc.lib().orc_sim_pass(C.byref(u), P(pos), P(vel), P(mat), P(q), P(seats), P(zf), P(z4), P(zf), P(z4), P(slot),
+                           P(ppf), orc.PP_CAP, P(po), P(vo), P(ao), P(qo))
+    assert np.array_equal(counts, ao[:, 3].astype(np.int32))
+    assert counts.max() <= 64 and counts.mean() > 5
+    own = np.repeat(np.arange(N), 64).reshape(N, 64)
+    live = pairs != 0xFFFFFFFF
+    j = (pairs & 0x3FFFF).astype(np.int64)
+    assert not np.any(live & (j == own))
+    d = np.linalg.norm(pos[j[live], :3].astype(np.float64) - pos[own[live], :3], axis=1)
+    touch = (pairs[live] >> 31) == 1
+    assert touch.any() and np.all(d[touch] < 2 * sim.a * (1 + 1e-6)) and np.all(d[~touch] >= 2 * sim.a * (1 - 1e-6))
