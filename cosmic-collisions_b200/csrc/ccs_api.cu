@@ -110,6 +110,11 @@ struct ccs_handle {
   float *ppBox = nullptr;
   float2 *tab = nullptr;
   int ppCount = 0, ppLoose = 0;
+  // the stencil-split P3M (ccs_set_pp_split): the stencil S (0: the reference's loose-list pass), the pair
+  // pass's sorted sources, start offsets and occupied target nodes, and every particle's pair sum
+  int ppSplit = 0;
+  int *splitStart = nullptr, *splitCells = nullptr, *splitNCells = nullptr;
+  float4 *splitSrc = nullptr, *splitSrcT = nullptr, *ppAll = nullptr;
   // the learned form of the P3M pass (borrowed network; pair buffers sized for the list)
   ccs_nn *nn = nullptr;
   int *nnCounts = nullptr, *nnOffs = nullptr, *nnTotal = nullptr;
@@ -298,6 +303,7 @@ ccs_uniforms pass_uniforms(const ccs_handle *h, int settle, int kick, double gdt
     u.cen1[k] = (float)h->sim.cen1[k];
   }
   u.ppCount = h->ppCount;
+  u.ppSplit = h->field ? 0 : h->ppSplit;
   return u;
 }
 
@@ -407,7 +413,10 @@ void pass_mesh_box(ccs_handle *h, const ccs_uniforms *U, int b) {
   h->launches += launch_coarse(m, h->st);
   h->launches += launch_far(m, h->st);
   time_begin(h, 3, &eb, &ee);
-  h->launches += launch_cell(U, m, h->st, h->tuneSplit);
+  if (h->ppSplit)
+    h->launches += launch_cell_tide(U, h->ppSplit, m, h->st);
+  else
+    h->launches += launch_cell(U, m, h->st, h->tuneSplit);
   time_end(h, ee);
 }
 
@@ -417,6 +426,15 @@ void pass_mesh(ccs_handle *h, const ccs_uniforms *U, int boxB) {
 }
 
 void pass_pp(ccs_handle *h, const ccs_uniforms *U, int count) {
+  if (h->ppSplit) {   // the stencil-split P3M: every particle's pairs inside the stencil
+    cudaEvent_t b, e;
+    time_begin(h, 4, &b, &e);
+    h->launches += launch_pp_split(U, h->N, h->ppSplit, h->pos[h->cur], h->mat, h->keys, h->vals, h->keysTmp,
+                                   h->valsTmp, h->hist, h->splitStart, h->splitSrc, h->splitSrcT, h->splitCells,
+                                   h->splitNCells, h->ppAll, h->st);
+    time_end(h, e);
+    return;
+  }
   if (!count) return;
   h->launches += launch_pp_gather(U, h->pos[h->cur], h->mat, h->ppIndex, CCS_PP_CAP, h->ppList, h->ppBox, h->st);
   cudaEvent_t b, e;
@@ -452,11 +470,24 @@ SimArgs sim_args(const ccs_handle *h) {
   a.qO = h->q[d];
   a.part = h->part;
   a.part2 = h->part2;
+  a.tideA0 = h->pm[0].tide0;
+  a.tideA1 = h->pm[0].tide1;
+  a.tideB0 = h->pm[1].tide0;
+  a.tideB1 = h->pm[1].tide1;
+  a.fineA = h->pm[0].fine;
+  a.fineB = h->pm[1].fine;
+  a.ppAll = h->ppAll;
   return a;
 }
 
 void pass_sim(ccs_handle *h, const ccs_uniforms &u) {
   const SimArgs a = sim_args(h);
+  if (h->ppSplit && !h->field && h->part && h->part2) {   // the stencil-split P3M's contact step: walk + tail
+    h->launches += launch_contacts_only(u, h->N, a, h->st, h->tuneWarps);
+    h->launches += launch_contact_tail(u, h->N, a, h->st, true);
+    h->cur ^= 1;
+    return;
+  }
   cudaEvent_t b, e;
   time_begin(h, 0, &b, &e);
   h->launches += launch_simulate(u, h->N, a, h->st, h->tuneWarps, h->field);
@@ -479,6 +510,7 @@ void pass_diag_kernel(ccs_handle *h, const ccs_uniforms *U) {
   a.ppForce = h->ppForce;
   a.cap = CCS_PP_CAP;
   a.diag = h->diag;
+  a.ppAll = h->ppAll;
   h->launches += launch_diag(U, h->N, a, h->st);
 }
 
@@ -512,6 +544,11 @@ StepPlan plan_step(ccs_handle *h, int settle, int kick) {
 int block_launches(const ccs_handle *h, const StepPlan *plans, int M, bool split = false) {
   int per = 0;
   for (int k = 0; k < M; ++k) {
+    if (h->ppSplit && !h->field) {                  // the stencil-split P3M: walk + tail every step
+      per += 2 + (plans[k].slots ? 1 : 0);
+      if (plans[k].mesh) per += 5 * (1 + (plans[k].u.boxB > 0.5f)) + pp_split_launches();
+      continue;
+    }
     per += 1;                                       // contact step
     if (plans[k].slots) per += 1;                   // contact grid
     if (plans[k].mesh) {
@@ -558,6 +595,41 @@ void enqueue_pre(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
 // gravity, settle/kick, heat and kick/drift (the tail) run after both.  Steps whose kernels are timed one
 // by one, and ensemble members' steps (parallel branches already), run the contact step whole.
 void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
+  if (h->ppSplit && !h->field && h->part && h->part2) {
+    // the stencil-split P3M: every step's contact step as its walk and its tail, whose gravity is the
+    // first-order gather plus the particle's own pair sum.  On a mesh step the grid and the walk run on the
+    // side stream beside the mesh chain and the pair pass (unless kernels are timed or the step is an
+    // ensemble member's), as in the reference form's split mesh step.
+    const bool fork = p.mesh && h->side && !h->inEnsemble && !h->timing;
+    const cudaStream_t main = h->st;
+    if (fork) {
+      cudaEventRecord(h->forkEv, h->st);
+      cudaStreamWaitEvent(h->side, h->forkEv, 0);
+      h->st = h->side;
+    }
+    if (p.slots) pass_slots(h, p.u);
+    const SimArgs a = sim_args(h);
+    cudaEvent_t b, e;
+    time_begin(h, 5, &b, &e);
+    h->launches += launch_contacts_only(p.u, h->N, a, h->st, h->tuneWarps);
+    record_uniform_node(h, 2);
+    time_end(h, e);
+    h->st = main;
+    if (p.mesh) {
+      pass_mesh(h, U, p.u.boxB > 0.5f);
+      pass_pp(h, U, p.u.ppCount);
+    }
+    if (fork) {
+      cudaEventRecord(h->joinEv, h->side);
+      cudaStreamWaitEvent(h->st, h->joinEv, 0);
+    }
+    time_begin(h, 6, &b, &e);
+    h->launches += launch_contact_tail(p.u, h->N, a, h->st, true);
+    record_uniform_node(h, 2);
+    time_end(h, e);
+    h->cur ^= 1;
+    return;
+  }
   if (p.mesh && can_split(h) && !h->inEnsemble && (h->timing & (3 << 5))) {
     // the split mesh step with its two halves timed (kernel ids 5 and 6): everything in order on st, so
     // each half sits alone between its events
@@ -639,7 +711,7 @@ void free_graph_slot(GraphSlot &g);
 // (simOutside), the graph stops before it and the contact step is launched directly, between its two
 // events when timed (events recorded by a graph's nodes do not time).
 int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false) {
-  const bool timed = time_this(h, 0) || simOutside;
+  const bool timed = (time_this(h, 0) && !h->ppSplit) || simOutside;
   const bool pre = p.mesh;   // kernels that read the uniforms from device memory (the mesh and pairwise passes)
   if (timed && !p.slots && !p.mesh) {   // nothing to replay: the contact step alone, launched directly
     if (!simOutside) pass_sim(h, p.u);
@@ -816,7 +888,9 @@ int graph_block(ccs_handle *h) {
     g.graph = graph;
     int rc = resolve_uniform_nodes(h, uniNodes, g.uni);
     int want = M;
-    for (int k = 0; k < M; ++k) want += (plans[k].slots ? 1 : 0) + (plans[k].mesh && can_split(h) ? 1 : 0);
+    for (int k = 0; k < M; ++k)
+      want += (plans[k].slots ? 1 : 0) +
+              (h->ppSplit && !h->field ? 1 : (plans[k].mesh && can_split(h) ? 1 : 0));
     if (rc == CCS_OK && (int)g.uni.size() != want) {
       h->err = "graph capture: a contact-step node per step and a grid node per even step expected";
       rc = CCS_E_CUDA;
@@ -878,6 +952,39 @@ int ensure_nn_buffers(ccs_handle *h, int n) {
   return CCS_OK;
 }
 
+// the stencil-split P3M's buffers: each box's tides and tide partials, the pair pass's sort and sums
+int ensure_split_buffers(ccs_handle *h) {
+  if (h->ppAll) return CCS_OK;
+  const size_t N = (size_t)h->N;
+  int rc = 0;
+  for (int b = 0; b < 2; ++b) {
+    MeshBuf &m = h->pm[b];
+    rc |= dev_alloc(h, &m.tide0, kFine + 1);
+    rc |= dev_alloc(h, &m.tide1, kFine + 1);
+    rc |= dev_alloc(h, &m.cellPartT, (size_t)kCoarse * kCellChunks * 64 * 3);
+  }
+  rc |= dev_alloc(h, &h->splitStart, split_start_ints());
+  rc |= dev_alloc(h, &h->splitCells, N);
+  rc |= dev_alloc(h, &h->splitNCells, 1);
+  rc |= dev_alloc(h, &h->splitSrc, N);
+  rc |= dev_alloc(h, &h->splitSrcT, N);
+  rc |= dev_alloc(h, &h->ppAll, N);
+  if (rc) {
+    for (int b = 0; b < 2; ++b) {
+      dev_free(h->pm[b].tide0); dev_free(h->pm[b].tide1); dev_free(h->pm[b].cellPartT);
+    }
+    dev_free(h->splitStart); dev_free(h->splitCells); dev_free(h->splitNCells); dev_free(h->splitSrc);
+    dev_free(h->splitSrcT); dev_free(h->ppAll);
+    return CCS_E_NOMEM;
+  }
+  for (int b = 0; b < 2; ++b) {
+    CUDA_TRY(h, cudaMemsetAsync(h->pm[b].tide0, 0, sizeof(float4) * (kFine + 1), h->st));
+    CUDA_TRY(h, cudaMemsetAsync(h->pm[b].tide1, 0, sizeof(float4) * (kFine + 1), h->st));
+  }
+  CUDA_TRY(h, cudaMemsetAsync(h->ppAll, 0, sizeof(float4) * N, h->st));
+  return CCS_OK;
+}
+
 void free_state(ccs_handle *h) {
   free_graphs(h);
   for (int b = 0; b < 2; ++b) {
@@ -888,7 +995,10 @@ void free_state(ccs_handle *h) {
     dev_free(m.farT1); dev_free(m.mono); dev_free(m.partial); dev_free(m.counter);
     dev_free(m.occ); dev_free(m.occIdx); dev_free(m.occN); dev_free(m.occBlocks); dev_free(m.occCount);
     dev_free(m.occAsc); dev_free(m.occAscN); dev_free(m.cellPart); dev_free(m.cellDone);
+    dev_free(m.tide0); dev_free(m.tide1); dev_free(m.cellPartT);
   }
+  dev_free(h->splitStart); dev_free(h->splitCells); dev_free(h->splitNCells); dev_free(h->splitSrc);
+  dev_free(h->splitSrcT); dev_free(h->ppAll);
   dev_free(h->mat); dev_free(h->matTmp); dev_free(h->home); dev_free(h->homeTmp);
   dev_free(h->part); dev_free(h->part2);
   dev_free(h->ppIndex); dev_free(h->ppSlot); dev_free(h->ppList); dev_free(h->ppForce); dev_free(h->ppBox);
@@ -1084,6 +1194,11 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
   h->LB[0] = h->LB[1] = h->LB[2] = 0;
   h->boxB = 0;
   h->built = true;
+  if (h->ppSplit) {
+    rc = ensure_split_buffers(h);
+    if (rc) return rc;
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+  }
   return check_launch(h);
 }
 
@@ -2276,7 +2391,14 @@ int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes) {
     case CCS_BUF_PP_SLOT: src = h->ppSlot; n = 4 * N; break;
     case CCS_BUF_DIAG: src = h->diag; n = 16 * N; break;
     case CCS_BUF_CELL_OF: src = h->hk[h->seatCur]; n = 4 * N; break;
+    case CCS_BUF_TIDE0_A: src = h->pm[0].tide0; n = 16 * (size_t)(kFine + 1); break;
+    case CCS_BUF_TIDE1_A: src = h->pm[0].tide1; n = 16 * (size_t)(kFine + 1); break;
+    case CCS_BUF_PP_ALL: src = h->ppAll; n = 16 * N; break;
     default: h->err = "unknown buffer"; return CCS_E_ARG;
+  }
+  if (!src) {
+    h->err = "that buffer exists only in the stencil-split P3M (ccs_set_pp_split)";
+    return CCS_E_STATE;
   }
   if (bytes != n) {
     h->err = "buffer size mismatch: expected " + std::to_string(n);
@@ -2382,7 +2504,7 @@ int ccs_advance_host(ccs_handle *h, const float *pos4, const float *vel4, const 
   cudaSetDevice(h->device);
   const size_t N = (size_t)h->N;
   const bool reads = pos4_out || vel4_out || aux4_out || q_out;
-  const bool overlapped = nsteps > 0 && reads && h->useGraphs && h->timing == 0;
+  const bool overlapped = nsteps > 0 && reads && h->useGraphs && h->timing == 0 && !h->ppSplit;
   // a one-step call: velocities and heat come over on the copy stream while the step's grid and mesh run
   const bool split = overlapped && nsteps == 1;
   if (split && (rc = ensure_copy_stream(h))) return rc;
@@ -2583,6 +2705,26 @@ int ccs_contact_pairs(ccs_handle *h, int cap, int32_t *counts, uint32_t *pairs) 
   }
   for (size_t i = 0; i < N; ++i) counts[i] = (int32_t)aux[i].w;
   return check_launch(h);
+}
+
+int ccs_set_pp_split(ccs_handle *h, int S) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (S < 0 || S > 3) {
+    h->err = "ccs_set_pp_split: the stencil is 0 (off) or 1..3 mesh cells";
+    return CCS_E_ARG;
+  }
+  if (S == h->ppSplit) return CCS_OK;
+  cudaSetDevice(h->device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  free_graphs(h);   // captured steps hold the other form's kernels
+  if (S) {
+    rc = ensure_split_buffers(h);
+    if (rc) return rc;
+    CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  }
+  h->ppSplit = S;
+  return CCS_OK;
 }
 
 int ccs_set_graphs(ccs_handle *h, int on) {

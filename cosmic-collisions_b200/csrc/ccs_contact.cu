@@ -126,9 +126,47 @@ __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const Si
   __syncwarp();   // every lane has read its entries before the queue is written again
 }
 
+// the stencil-split P3M's gravity at a particle: each of its 8 nodes' pull carried from the node's centre
+// of mass to the particle by the node's tidal tensor (first order), the strays' pull back and the other
+// box's as the reference gives them, and the particle's own pair sum (ccs_split.cu)
+__device__ __forceinline__ f3 gravity_tide(const ccs_uniforms &u, const SimArgs &a, int me, f3 p) {
+  f3 grav = mk(0.0f, 0.0f, 0.0f), g;
+  const int box = box_of(u, p, g);
+  if (box >= 0) {
+    const float4 *F = box == 0 ? a.forceA : a.forceB, *T0 = box == 0 ? a.tideA0 : a.tideB0,
+                 *T1 = box == 0 ? a.tideA1 : a.tideB1, *M = box == 0 ? a.fineA : a.fineB;
+    const float fx = floorf(g.x), fy = floorf(g.y), fz = floorf(g.z);
+    const f3 t = mk(g.x - fx, g.y - fy, g.z - fz);
+    const int bx = (int)fx, by = (int)fy, bz = (int)fz;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
+      const float wgt = (ox ? t.x : 1.0f - t.x) * (oy ? t.y : 1.0f - t.y) * (oz ? t.z : 1.0f - t.z);
+      const int c = fine_index(min(bx + ox, 63), min(by + oy, 63), min(bz + oz, 63));
+      const float4 m = __ldg(M + c);
+      if (!(m.w > 0.0f)) continue;   // a node nothing was deposited on (a corner past the mesh's edge)
+      const f3 d = p - xyz(m) * fdiv(1.0f, m.w);
+      const float4 f = __ldg(F + c), t0 = __ldg(T0 + c), t1 = __ldg(T1 + c);
+      const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
+                       t1.x * d.x + t1.y * d.y + t0.z * d.z);
+      grav = grav + (xyz(f) + Td) * wgt;
+    }
+    grav = grav - xyz(__ldg(F + kFine)) * u.Gm;   // the strays in neither box pull back
+    if (u.boxB > 0.5f) {
+      const float4 mA = __ldg(a.monoA), mB = __ldg(a.monoB);
+      grav = grav + (box == 0 ? cross_at(u, mB, mA) : cross_at(u, mA, mB));
+    }
+  } else {
+    grav = mass_at(u, p, __ldg(a.monoA));
+    if (u.boxB > 0.5f) grav = grav + mass_at(u, p, __ldg(a.monoB));
+  }
+  return grav + xyz(__ldg(a.ppAll + me));
+}
+
 // a particle's gravity (the mesh gather and the pairwise add, or the field), settle/kick, heat and kick/drift
-// from its contact sums: the end of the contact step, and all of a split mesh step's tail
-template <bool FIELD>
+// from its contact sums: the end of the contact step, and all of a split mesh step's tail (TIDE: the
+// stencil-split P3M's gravity instead of the reference's gather and loose-list add)
+template <bool FIELD, bool TIDE = false>
 __device__ __forceinline__ void finish_particle(const ccs_uniforms &u, const SimArgs &a, int me, float4 P, float4 V,
                                                 float ri, float ci, f3 push, float lost, float flow, float nb) {
   const f3 p = xyz(P);
@@ -136,6 +174,8 @@ __device__ __forceinline__ void finish_particle(const ccs_uniforms &u, const Sim
   f3 grav = mk(0.0f, 0.0f, 0.0f), g;
   if (FIELD) {
     grav = ld3(u.gField);   // SIM_GRAV_FIELD, src/glsl-sim.js:490-492: the whole of gravity
+  } else if (TIDE) {
+    grav = gravity_tide(u, a, me, p);
   } else {
     // SIM_GRAV_MESH, src/glsl-sim.js:469-488
     const int box = box_of(u, p, g);
@@ -315,6 +355,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
 
 // the tail of a split mesh step, one thread a particle: the contact sums the contact walk left in part, then
 // the same gravity, settle/kick, heat and kick/drift as the whole step's
+template <bool TIDE>
 __global__ void __launch_bounds__(256) k_contact_tail(const ccs_uniforms u, const SimArgs a) {
   const int me = a.first + blockIdx.x * blockDim.x + threadIdx.x;
   if (me >= u.N) return;
@@ -323,7 +364,7 @@ __global__ void __launch_bounds__(256) k_contact_tail(const ccs_uniforms u, cons
   const float ci = ri * (is_iron(P.w) ? u.cpIron : 1.0f);
   const float4 s = a.part[me];
   const float2 s2 = a.part2[me];
-  finish_particle<false>(u, a, me, P, V, ri, ci, mk(s.x, s.y, s.z), s2.x, s2.y, s.w);
+  finish_particle<false, TIDE>(u, a, me, P, V, ri, ci, mk(s.x, s.y, s.z), s2.x, s2.y, s.w);
 }
 
 size_t contact_smem_bytes(int warps) { return sizeof(ContactWarp) * warps; }
@@ -378,9 +419,12 @@ int launch_contact_pairs(const ccs_uniforms &u, int N, const SimArgs &a, cudaStr
   return 1;
 }
 
-int launch_contact_tail(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st) {
+int launch_contact_tail(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, bool tide) {
   if (N <= 0) return 0;
-  k_contact_tail<<<blocks_for(N, 256), 256, 0, st>>>(u, a);
+  if (tide)
+    k_contact_tail<true><<<blocks_for(N, 256), 256, 0, st>>>(u, a);
+  else
+    k_contact_tail<false><<<blocks_for(N, 256), 256, 0, st>>>(u, a);
   return 1;
 }
 

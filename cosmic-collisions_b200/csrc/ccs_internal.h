@@ -12,6 +12,7 @@ namespace ccs {
 constexpr uint32_t kEmpty = CCS_SEAT_EMPTY;   // -1.0f bit pattern: an empty seat
 constexpr uint32_t kNoCell = 0xFFFFFFFFu;     // no cell recorded for this particle
 constexpr int kFine = 64 * 64 * 64;           // 64^3 mesh; index kFine is the scratch texel
+constexpr int kSplitKeys = 2 * kFine;         // the stencil-split pair pass's sort keys: (box, base node); this one: neither box
 constexpr int kCoarse = 4096;                 // 16^3 blocks
 constexpr int kCellChunks = 8;                // CTAs of the cell pass per occupied block, each a source chunk
 constexpr int kSeats = CCS_SEATS;
@@ -66,6 +67,9 @@ struct MeshBuf {
   int *occAscN = nullptr;      // ... and how many
   float4 *cellPart = nullptr;  // the cell pass's partial sums: [listed block][source chunk][cell]
   int *cellDone = nullptr;     // per listed block: the chunks done (the last one adds them up)
+  // the stencil-split P3M's mesh (allocated when that form is switched on): each cell's tidal tensor, and
+  // the cell pass's partial sums of pull, potential and tide: [listed block][source chunk][3][cell]
+  float4 *tide0 = nullptr, *tide1 = nullptr, *cellPartT = nullptr;
 };
 
 // Arguments of the contact step (simFS, src/glsl-sim.js:354-512).
@@ -84,6 +88,9 @@ struct SimArgs {
   float2 *part2 = nullptr;  // and dissipation, heat flow
   uint32_t *pairs = nullptr;  // the contact-pair read-out: per owner pairCap words, neighbour | touching << 31
   int pairCap = 0;
+  // the stencil-split P3M's gather: each box's tides and deposit (centres of mass), and each particle's pairs
+  const float4 *tideA0 = nullptr, *tideA1 = nullptr, *tideB0 = nullptr, *tideB1 = nullptr;
+  const float4 *fineA = nullptr, *fineB = nullptr, *ppAll = nullptr;
 };
 
 struct DiagArgs {
@@ -95,6 +102,7 @@ struct DiagArgs {
   const float4 *ppForce;
   int cap;
   float4 *diag;
+  const float4 *ppAll = nullptr;   // the stencil-split P3M's per-particle pair sums (uniform ppSplit > 0)
 };
 
 // per-device kernel attributes (dynamic shared memory limits); call once per
@@ -115,7 +123,8 @@ int launch_simulate(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t
 // a split mesh step: the contact walk alone (its sums into a.part, a.part2), then, after the mesh and the
 // pairwise pass, the tail that turns them and the gravity into the step's outputs
 int launch_contacts_only(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps);
-int launch_contact_tail(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st);
+// tide: the stencil-split P3M's gather (first order from each node's centre of mass, the particle's pairs)
+int launch_contact_tail(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, bool tide = false);
 // the contact step with its pair sets written out (a.pairs, a.pairCap): the same walk, outputs to a's buffers
 int launch_contact_pairs(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st);
 // the contact step for particles [first, first + count) only; first a multiple of 256
@@ -127,6 +136,15 @@ int launch_coarse(const MeshBuf &m, cudaStream_t st);
 int launch_far(const MeshBuf &m, cudaStream_t st);
 // split: threads per fine cell in the cell-gravity sums, 2, 4 or 8
 int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int split = 4);
+// the stencil-split P3M (S = 1, 2, 3 nodes): the cell pass without the stencil's node pairs, with tides
+int launch_cell_tide(const ccs_uniforms *u, int S, const MeshBuf &m, cudaStream_t st);
+// ... and the pair pass over every particle inside it: sort by (box, base node), then the stencil's pairs;
+// out gets each particle's (pull, potential) x Gm
+size_t split_start_ints();
+int launch_pp_split(const ccs_uniforms *U, int N, int S, const float4 *pos, const float *mat, uint32_t *keys,
+                    int32_t *vals, uint32_t *keysTmp, int32_t *valsTmp, uint32_t *hist, int *start, float4 *src,
+                    float4 *srcT, int *cells, int *nCells, float4 *out, cudaStream_t st);
+int pp_split_launches();
 int launch_pp_gather(const ccs_uniforms *u, const float4 *pos, const float *mat, const int *index, int cap,
                      float4 *list, float *box, cudaStream_t st);
 // the pairwise partials of the P3M pass: 4 quarters x chunks x cap float4

@@ -496,6 +496,188 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restr
 }
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// cell gravity of the stencil-split P3M (ccs_split.cu): the same work items, sources and chunk reduction as
+// k_cell, but a source cell within S cells of the target cell in every axis (the stencil, itself included)
+// is left to the pair pass, the rest is summed unsoftened (the pair pass takes everything near, so no
+// softening is needed to keep the sum finite), and each cell also gets its tidal tensor -- the gradient of
+// the pull, the near sources' exactly and the block's far field's as the block carries it -- so that the
+// gather can carry each node's pull from its centre of mass to the particle to first order.  Outputs (x Gm):
+// force = (pull, potential) at the cell's centre of mass, tide0 = (Txx, Tyy, Tzz, Txy), tide1 = (Txz, Tyz).
+// ---------------------------------------------------------------------------
+namespace {
+template <int SPLIT>
+__global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__restrict__ U, int S,
+                                                          const float4 *__restrict__ fine,
+                                                          const float4 *__restrict__ coarse,
+                                                          const float4 *__restrict__ occ,
+                                                          const uint8_t *__restrict__ occIdx,
+                                                          const int *__restrict__ occN,
+                                                          const int *__restrict__ occBlocks,
+                                                          const int *__restrict__ occCount,
+                                                          const float4 *__restrict__ farA,
+                                                          const float4 *__restrict__ farT0,
+                                                          const float4 *__restrict__ farT1,
+                                                          float4 *__restrict__ force, float4 *__restrict__ tide0,
+                                                          float4 *__restrict__ tide1, float4 *__restrict__ cellPart,
+                                                          int *__restrict__ cellDone) {
+  constexpr int kCellThreads = 64 * SPLIT;
+  __shared__ int nbK[128], nbOff[129];
+  __shared__ float4 src[kCellBatch];
+  __shared__ int sfc[kCellBatch];        // a source's fine cell, x | y << 6 | z << 12
+  __shared__ float4 part[3][SPLIT][64];  // (pull, potential), (Txx Tyy Tzz Txy), (Txz Tyz)
+  __shared__ int last;
+  const int t = threadIdx.x, cellT = t & 63, q = t >> 6, lane = t & 31;
+  if (blockIdx.x == 0 && t == 0) force[kFine] = fine[kFine];   // the scratch texel, carried through
+  const float Gm = U->Gm, eps2 = 1e-6f * U->eps2Mesh;
+  const int items = *occCount * kCellChunks;
+  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+    const int bi = it / kCellChunks, chunk = it % kCellChunks;
+    const int blk = occBlocks[bi];
+    const int ccx = blk & 15, ccy = (blk >> 4) & 15, ccz = blk >> 8;
+    if (t < 32) {   // the 125 neighbour blocks and where each one's occupied cells start (as k_cell)
+      int n[4], run = 0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int o = lane * 4 + r;
+        const int kx = ccx + o % 5 - 2, ky = ccy + (o / 5) % 5 - 2, kz = ccz + o / 25 - 2;
+        const bool in = o < 125 && kx >= 0 && ky >= 0 && kz >= 0 && kx <= 15 && ky <= 15 && kz <= 15;
+        const int k = in ? coarse_index(kx, ky, kz) : 0;
+        nbK[o] = k;
+        n[r] = in ? __ldg(occN + k) : 0;
+        run += n[r];
+      }
+      int incl = run;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) incl += y;
+      }
+      int at = incl - run;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        nbOff[lane * 4 + r] = at;
+        at += n[r];
+      }
+      if (lane == 31) nbOff[128] = at;
+    }
+    const int nOwn = __ldg(occN + blk);
+    const bool mine = cellT < nOwn;
+    const float4 tc = mine ? __ldg(occ + (size_t)blk * 64 + cellT) : make_float4(0, 0, 0, 0);
+    const int tl = mine ? (int)__ldg(occIdx + (size_t)blk * 64 + cellT) : 0;
+    const int tx = ccx * 4 + (tl & 3), ty = ccy * 4 + ((tl >> 2) & 3), tz = ccz * 4 + (tl >> 4);
+    const f3 x = xyz(tc);
+    f3 acc = mk(0, 0, 0);
+    float pot = 0.0f, txx = 0.0f, tyy = 0.0f, tzz = 0.0f, txy = 0.0f, txz = 0.0f, tyz = 0.0f;
+    __syncthreads();
+    const int total = nbOff[125];
+    const int c0 = (int)((long long)total * chunk / kCellChunks);
+    const int c1 = (int)((long long)total * (chunk + 1) / kCellChunks);
+    for (int b0 = c0; b0 < c1; b0 += kCellBatch) {
+      const int b1 = min(b0 + kCellBatch, c1);
+      for (int e = b0 + t; e < b1; e += kCellThreads) {
+        int lo = 0, hi = 125;
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (nbOff[mid] <= e) lo = mid;
+          else hi = mid;
+        }
+        const int k = nbK[lo], i = e - nbOff[lo];
+        src[e - b0] = __ldg(occ + (size_t)k * 64 + i);
+        const int ix = __ldg(occIdx + (size_t)k * 64 + i);
+        sfc[e - b0] = ((k & 15) * 4 + (ix & 3)) | (((k >> 4 & 15) * 4 + ((ix >> 2) & 3)) << 6) |
+                      (((k >> 8) * 4 + (ix >> 4)) << 12);
+      }
+      __syncthreads();
+      if (mine) {
+        const int n = b1 - b0;
+#pragma unroll 2
+        for (int i = q; i < n; i += SPLIT) {
+          const int f = sfc[i];
+          const int cheb = max(abs((f & 63) - tx), max(abs(((f >> 6) & 63) - ty), abs((f >> 12) - tz)));
+          if (cheb <= S) continue;   // the pair pass's
+          const float4 mf = src[i];
+          const f3 r = xyz(mf) - x;
+          // unsoftened beyond the stencil; eps2 (a thousandth of a cell, squared) only keeps two centres of mass
+          // that happen to coincide finite
+          const float inv = rsqrtf(dot(r, r) + eps2), inv2 = inv * inv, a3 = mf.w * inv * inv2, a5 = 3.0f * a3 * inv2;
+          acc = acc + r * a3;
+          pot -= mf.w * inv;
+          txx += a5 * r.x * r.x - a3;
+          tyy += a5 * r.y * r.y - a3;
+          tzz += a5 * r.z * r.z - a3;
+          txy += a5 * r.x * r.y;
+          txz += a5 * r.x * r.z;
+          tyz += a5 * r.y * r.z;
+        }
+      }
+      __syncthreads();
+    }
+    part[0][q][cellT] = make_float4(acc.x, acc.y, acc.z, pot);
+    part[1][q][cellT] = make_float4(txx, tyy, tzz, txy);
+    part[2][q][cellT] = make_float4(txz, tyz, 0.0f, 0.0f);
+    __syncthreads();
+    float4 *out = cellPart + ((size_t)bi * kCellChunks + chunk) * 64 * 3;
+    if (mine && q == 0) {
+      float4 s0 = part[0][0][cellT], s1 = part[1][0][cellT], s2 = part[2][0][cellT];
+#pragma unroll
+      for (int k = 1; k < SPLIT; ++k) {
+        const float4 p0 = part[0][k][cellT], p1 = part[1][k][cellT], p2 = part[2][k][cellT];
+        s0 = make_float4(s0.x + p0.x, s0.y + p0.y, s0.z + p0.z, s0.w + p0.w);
+        s1 = make_float4(s1.x + p1.x, s1.y + p1.y, s1.z + p1.z, s1.w + p1.w);
+        s2 = make_float4(s2.x + p2.x, s2.y + p2.y, s2.z, s2.w);
+      }
+      __stcg(out + cellT, s0);
+      __stcg(out + 64 + cellT, s1);
+      __stcg(out + 128 + cellT, s2);
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(cellDone + bi, 1) == kCellChunks - 1;
+    __syncthreads();
+    if (last) {   // every chunk is in: add them in chunk order, then the block's far field and its tide
+      __threadfence();
+      if (mine && q == 0) {
+        const float4 *pb = cellPart + (size_t)bi * kCellChunks * 64 * 3;
+        float4 s0 = __ldcg(pb + cellT), s1 = __ldcg(pb + 64 + cellT), s2 = __ldcg(pb + 128 + cellT);
+#pragma unroll
+        for (int c = 1; c < kCellChunks; ++c) {
+          const float4 p0 = __ldcg(pb + (size_t)c * 192 + cellT), p1 = __ldcg(pb + (size_t)c * 192 + 64 + cellT),
+                       p2 = __ldcg(pb + (size_t)c * 192 + 128 + cellT);
+          s0 = make_float4(s0.x + p0.x, s0.y + p0.y, s0.z + p0.z, s0.w + p0.w);
+          s1 = make_float4(s1.x + p1.x, s1.y + p1.y, s1.z + p1.z, s1.w + p1.w);
+          s2 = make_float4(s2.x + p2.x, s2.y + p2.y, s2.z, s2.w);
+        }
+        f3 a3 = mk(s0.x, s0.y, s0.z);
+        float pt = s0.w;
+        const float4 mb = coarse[blk];
+        const float4 fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
+        const f3 d = x - xyz(mb) * fdiv(1.0f, mb.w);
+        const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
+                         t1.x * d.x + t1.y * d.y + t0.z * d.z);
+        a3 = a3 + (xyz(fa) + Td);
+        pt += fa.w - dot(xyz(fa), d) - 0.5f * dot(d, Td);
+        const int fi = fine_index(tx, ty, tz);
+        force[fi] = make_float4(a3.x * Gm, a3.y * Gm, a3.z * Gm, pt * Gm);
+        tide0[fi] = make_float4((s1.x + t0.x) * Gm, (s1.y + t0.y) * Gm, (s1.z + t0.z) * Gm, (s1.w + t0.w) * Gm);
+        tide1[fi] = make_float4((s2.x + t1.x) * Gm, (s2.y + t1.y) * Gm, 0.0f, 0.0f);
+      }
+      if (t == 0) cellDone[bi] = 0;
+    }
+    __syncthreads();
+  }
+}
+}  // namespace
+
+int launch_cell_tide(const ccs_uniforms *u, int S, const MeshBuf &m, cudaStream_t st) {
+  const int sms = sm_count();
+  cudaMemsetAsync(m.force, 0, sizeof(float4) * kFine, st);
+  k_cell_tide<4><<<sms * 8, 256, 0, st>>>(u, S, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount,
+                                          m.farA, m.farT0, m.farT1, m.force, m.tide0, m.tide1, m.cellPartT,
+                                          m.cellDone);
+  return 1;
+}
+
 int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int split) {
   const int sms = sm_count();
   // a persistent grid over (block, chunk) items: four CTAs of 512 threads fill an SM, more of smaller ones

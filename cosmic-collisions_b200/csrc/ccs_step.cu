@@ -171,9 +171,13 @@ __global__ void __launch_bounds__(kBlock) k_diag(const ccs_uniforms *__restrict_
     if (u.boxB > 0.5f) phi += pot_at(u, p, *a.monoB);
     off = 2.0f;
   }
-  const int seat = a.ppSlot[me];
-  if (seat >= 0)
-    for (int s = 0; s < 4; ++s) phi += a.ppForce[(size_t)s * a.cap + seat].w;
+  if (u.ppSplit > 0) {
+    phi += a.ppAll[me].w;   // the stencil-split P3M: every particle's own pair sum
+  } else {
+    const int seat = a.ppSlot[me];
+    if (seat >= 0)
+      for (int s = 0; s < 4; ++s) phi += a.ppForce[(size_t)s * a.cap + seat].w;
+  }
   a.diag[me] = make_float4(phi, seated + off, taken, a.q[me]);
 }
 

@@ -264,7 +264,9 @@ class NBody:
                  "fineB": ((L.FINE + 1) * 4, np.float32), "forceB": ((L.FINE + 1) * 4, np.float32),
                  "monoB": (4, np.float32), "pplist": (PP_CAP * 4, np.float32),
                  "ppforce": (PP_CAP * 16, np.float32), "ppbox": (PP_CAP, np.float32), "ppslot": (N, np.int32),
-                 "diag": (N * 4, np.float32), "cellof": (N, np.uint32)}
+                 "diag": (N * 4, np.float32), "cellof": (N, np.uint32),
+                 "tide0A": ((L.FINE + 1) * 4, np.float32), "tide1A": ((L.FINE + 1) * 4, np.float32),
+                 "ppall": (N * 4, np.float32)}
         n, dt = sizes[name]
         a = np.empty(n, dt)
         self._check(lib().ccs_read_buffer(self._h, L.BUF[name], ptr(a), a.nbytes), "ccs_read_buffer")
@@ -434,6 +436,11 @@ class NBody:
                 for k in range(4):
                     b.mono[k] = float(d["mono"][k])
         self._check(lib().ccs_set_boxes(self._h, arr), "ccs_set_boxes")
+
+    def set_pp_split(self, S):
+        """The stencil-split P3M (ccs_set_pp_split): every pair of mesh nodes within S cells (1..3) summed
+        particle by particle, the rest on the mesh to first order; 0 returns to the reference's pass."""
+        self._check(lib().ccs_set_pp_split(self._h, int(S)), "ccs_set_pp_split")
 
     def contact_pairs(self, cap=64):
         """The contact-pair sets of the current state (ccs_contact_pairs): (counts, pairs), pairs an N x cap

@@ -55,6 +55,7 @@ typedef struct {
   float frozen;                                     /* the material held still (uFrozen); < 0: none */
   int ppCount;                                      /* loose-list length (pp.count) */
   float rot0[9], rot1[9], rdt;                      /* rigid carry (src/glsl-sim.js:537-570) */
+  int ppSplit;                                      /* 0: the reference's loose-list pass; S > 0: the stencil-split P3M */
 } ccs_uniforms;
 
 /* The run's scalars: the fields of the reference's `sim` object
@@ -287,6 +288,25 @@ int ccs_nn_grad(ccs_nn *nn, const float *rec6, const float *label3, int64_t n, f
 /* attach (or, with NULL, detach) a network to an engine's P3M pass */
 int ccs_set_pp_nn(ccs_handle *h, ccs_nn *nn);
 
+/* ---- the stencil-split P3M: gravity to a stated accuracy ----
+ * No counterpart in the reference.  The reference's pairwise pass corrects
+ * only the loose list (src/nbody.js:851-870, capped at PP_CAP) against the
+ * mesh's placement-averaged pair table (src/glsl-sim.js:700-754), so
+ * particles inside a body keep the mesh's near field, a cell-centre sum
+ * softened by FH^2/2 at every distance: a few per cent off Newton.  With
+ * S = 1, 2 or 3 the split form hands every pair of mesh nodes within S cells
+ * of each other (Chebyshev) to an exact pairwise sum over every particle --
+ * each particle pair weighted by the share of its cloud-in-cell node pairs
+ * that lie inside the stencil, so mesh and pairs partition the interaction
+ * exactly -- and keeps the rest on the mesh, unsoftened, gathered to first
+ * order from each node's centre of mass by the node's tidal tensor.  Pairs
+ * are Newton softened at the particle radius, the reference's own pairwise
+ * softening (src/glsl-sim.js:745); particles in neither box keep the boxes'
+ * monopoles.  The loose list is not used while the form is on.  S = 0
+ * returns to the reference's pass.  Applies from the next mesh step;
+ * allocates its buffers on first use (about 220 MB plus 80 B a particle). */
+int ccs_set_pp_split(ccs_handle *h, int S);
+
 /* ---- launch shapes by measurement ----
  * No counterpart in the reference (WebGL fixes its own shapes).  Times the
  * contact step at 8 and 4 warps per CTA and the cell gravity at 2, 4 and 8
@@ -341,7 +361,8 @@ int ccs_contact_pairs(ccs_handle *h, int cap, int32_t *counts, uint32_t *pairs);
 enum {
   CCS_BUF_SEATS = 5, CCS_BUF_FINE_A = 6, CCS_BUF_FORCE_A = 7, CCS_BUF_MONO_A = 8, CCS_BUF_COARSE_A = 9,
   CCS_BUF_FAR_A = 10, CCS_BUF_FINE_B = 11, CCS_BUF_FORCE_B = 12, CCS_BUF_MONO_B = 13, CCS_BUF_PP_LIST = 14,
-  CCS_BUF_PP_FORCE = 15, CCS_BUF_PP_BOX = 16, CCS_BUF_PP_SLOT = 17, CCS_BUF_DIAG = 18, CCS_BUF_CELL_OF = 19
+  CCS_BUF_PP_FORCE = 15, CCS_BUF_PP_BOX = 16, CCS_BUF_PP_SLOT = 17, CCS_BUF_DIAG = 18, CCS_BUF_CELL_OF = 19,
+  CCS_BUF_TIDE0_A = 20, CCS_BUF_TIDE1_A = 21, CCS_BUF_PP_ALL = 22   /* the stencil-split P3M's (ccs_set_pp_split) */
 };
 int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes);
 

@@ -750,6 +750,164 @@ void orc_cell(const orc_uni *u, const float *fine, const float *coarse, const fl
 }
 
 /* ------------------------------------------------------------------ */
+/* The stencil-split P3M (no counterpart in the reference; the library's ccs_set_pp_split).  The cell pass  */
+/* of CELL_FS (src/glsl-sim.js:303-352) with the node pairs within S cells (Chebyshev) left out, no         */
+/* softening, and the tidal tensor summed beside the pull; then every particle's pairs inside the stencil,  */
+/* each weighted by its share of cloud-in-cell node pairs within S; then the gather, first order from each  */
+/* node's centre of mass.                                                                                    */
+/* ------------------------------------------------------------------ */
+static v3 mass_at(const orc_uni *u, v3 p, const float *mono);
+static v3 cross_at(const orc_uni *u, const float *other, const float *mine);
+
+void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, const float *farA,
+                   const float *farT0, const float *farT1, float *force, float *tide0, float *tide1) {
+  const float eps2 = 1e-6f * u->eps2Mesh;   /* keeps two coinciding centres of mass finite, as the library's */
+  memcpy(force + 4 * ORC_FINE, fine + 4 * ORC_FINE, 16);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int ci = 0; ci < ORC_FINE; ci++) {
+    int c[3] = {ci & 63, (ci >> 6) & 63, ci >> 12};
+    const float *mc = fine + 4 * ci;
+    float *o = force + 4 * ci, *T0 = tide0 + 4 * ci, *T1 = tide1 + 4 * ci;
+    if (mc[3] <= 0.0f) {
+      o[0] = o[1] = o[2] = o[3] = 0.0f;
+      continue;
+    }
+    v3 x = vdivs(ld3(mc), mc[3]);
+    int cc[3] = {c[0] >> 2, c[1] >> 2, c[2] >> 2};
+    double acc[3] = {0, 0, 0}, pot = 0, T[6] = {0, 0, 0, 0, 0, 0};   /* Txx Tyy Tzz Txy Txz Tyz */
+    for (int kz = -2; kz <= 2; kz++)
+      for (int ky = -2; ky <= 2; ky++)
+        for (int kx = -2; kx <= 2; kx++) {
+          int k[3] = {cc[0] + kx, cc[1] + ky, cc[2] + kz};
+          if (k[0] < 0 || k[1] < 0 || k[2] < 0 || k[0] > 15 || k[1] > 15 || k[2] > 15) continue;
+          const float *m = coarse + 4 * coarse_index(k[0], k[1], k[2]);
+          if (m[3] <= 0.0f) continue;
+          for (int fz = 0; fz < 4; fz++)
+            for (int fy = 0; fy < 4; fy++)
+              for (int fx = 0; fx < 4; fx++) {
+                int f[3] = {k[0] * 4 + fx, k[1] * 4 + fy, k[2] * 4 + fz};
+                int dx = abs(f[0] - c[0]), dy = abs(f[1] - c[1]), dz = abs(f[2] - c[2]);
+                int cheb = dx > dy ? (dx > dz ? dx : dz) : (dy > dz ? dy : dz);
+                if (cheb <= S) continue;
+                const float *mf = fine + 4 * fine_index(f[0], f[1], f[2]);
+                if (mf[3] <= 0.0f) continue;
+                v3 r = vsub(vdivs(ld3(mf), mf[3]), x);
+                double rx = r.x, ry = r.y, rz = r.z, M = mf[3];
+                double inv = 1.0 / sqrt(rx * rx + ry * ry + rz * rz + eps2), inv2 = inv * inv;
+                double a3 = M * inv * inv2, a5 = 3.0 * a3 * inv2;
+                acc[0] += rx * a3; acc[1] += ry * a3; acc[2] += rz * a3;
+                pot -= M * inv;
+                T[0] += a5 * rx * rx - a3; T[1] += a5 * ry * ry - a3; T[2] += a5 * rz * rz - a3;
+                T[3] += a5 * rx * ry; T[4] += a5 * rx * rz; T[5] += a5 * ry * rz;
+              }
+        }
+    int ca = coarse_index(cc[0], cc[1], cc[2]);
+    const float *mb = coarse + 4 * ca, *fa = farA + 4 * ca, *t0 = farT0 + 4 * ca, *t1 = farT1 + 4 * ca;
+    v3 d = vsub(x, vdivs(ld3(mb), mb[3]));
+    v3 Td = V3(t0[0] * d.x + t0[3] * d.y + t1[0] * d.z,
+               t0[3] * d.x + t0[1] * d.y + t1[1] * d.z,
+               t1[0] * d.x + t1[1] * d.y + t0[2] * d.z);
+    acc[0] += fa[0] + Td.x; acc[1] += fa[1] + Td.y; acc[2] += fa[2] + Td.z;
+    pot += fa[3] - vdot(ld3(fa), d) - 0.5f * vdot(d, Td);
+    o[0] = (float)(acc[0] * u->Gm); o[1] = (float)(acc[1] * u->Gm); o[2] = (float)(acc[2] * u->Gm);
+    o[3] = (float)(pot * u->Gm);
+    T0[0] = (float)((T[0] + t0[0]) * u->Gm); T0[1] = (float)((T[1] + t0[1]) * u->Gm);
+    T0[2] = (float)((T[2] + t0[2]) * u->Gm); T0[3] = (float)((T[3] + t0[3]) * u->Gm);
+    T1[0] = (float)((T[4] + t1[0]) * u->Gm); T1[1] = (float)((T[5] + t1[1]) * u->Gm); T1[2] = T1[3] = 0.0f;
+  }
+}
+
+static double split_w(int D, int S, double ti, double tj) {
+  if (D <= S - 1 && D >= 1 - S) return 1.0;
+  if (D == S) return (1.0 - tj) + ti * tj;
+  if (D == -S) return (1.0 - ti) + ti * tj;
+  if (D == S + 1) return ti * (1.0 - tj);
+  if (D == -S - 1) return (1.0 - ti) * tj;
+  return 0.0;
+}
+
+void orc_pp_split(const orc_uni *u, int S, const float *pos4, const float *mat, float *out4) {
+  const int N = u->N;
+  int *box = (int *)malloc(sizeof(int) * N), *b = (int *)malloc(sizeof(int) * 3 * N);
+  double *t = (double *)malloc(sizeof(double) * 3 * N);
+  for (int i = 0; i < N; i++) {
+    float p[3] = {pos4[4 * (size_t)i], pos4[4 * (size_t)i + 1], pos4[4 * (size_t)i + 2]}, g[3];
+    box[i] = orc_box_of(u, p, g);
+    for (int k = 0; k < 3; k++) {
+      float f = floorf(g[k]);
+      b[3 * i + k] = (int)f;
+      t[3 * i + k] = (double)(g[k] - f);
+    }
+  }
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < N; i++) {
+    float *o = out4 + 4 * (size_t)i;
+    o[0] = o[1] = o[2] = o[3] = 0.0f;
+    if (box[i] < 0) continue;
+    double acc[3] = {0, 0, 0}, pot = 0;
+    const double px = pos4[4 * (size_t)i], py = pos4[4 * (size_t)i + 1], pz = pos4[4 * (size_t)i + 2];
+    for (int j = 0; j < N; j++) {
+      if (j == i || box[j] != box[i]) continue;
+      int D0 = b[3 * j] - b[3 * i], D1 = b[3 * j + 1] - b[3 * i + 1], D2 = b[3 * j + 2] - b[3 * i + 2];
+      if (abs(D0) > S + 1 || abs(D1) > S + 1 || abs(D2) > S + 1) continue;
+      double W = split_w(D0, S, t[3 * i], t[3 * j]) * split_w(D1, S, t[3 * i + 1], t[3 * j + 1]) *
+                 split_w(D2, S, t[3 * i + 2], t[3 * j + 2]);
+      double dx = pos4[4 * (size_t)j] - px, dy = pos4[4 * (size_t)j + 1] - py, dz = pos4[4 * (size_t)j + 2] - pz;
+      double inv = 1.0 / sqrt(dx * dx + dy * dy + dz * dz + (double)u->a2);
+      double w = mat[j] * W;
+      acc[0] += dx * w * inv * inv * inv; acc[1] += dy * w * inv * inv * inv; acc[2] += dz * w * inv * inv * inv;
+      pot -= w * inv;
+    }
+    o[0] = (float)(acc[0] * u->Gm); o[1] = (float)(acc[1] * u->Gm); o[2] = (float)(acc[2] * u->Gm);
+    o[3] = (float)(pot * u->Gm);
+  }
+  free(box); free(b); free(t);
+}
+
+void orc_gather_split(const orc_uni *u, const float *pos4, const float *fineA, const float *forceA,
+                      const float *tideA0, const float *tideA1, const float *fineB, const float *forceB,
+                      const float *tideB0, const float *tideB1, const float *monoA, const float *monoB,
+                      const float *ppAll, float *grav4) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < u->N; i++) {
+    v3 p = ld3(pos4 + 4 * (size_t)i), grav = V3(0, 0, 0);
+    float pp[3] = {p.x, p.y, p.z}, g[3];
+    int box = orc_box_of(u, pp, g);
+    if (box >= 0) {
+      const float *F = box == 0 ? forceA : forceB, *M = box == 0 ? fineA : fineB;
+      const float *T0 = box == 0 ? tideA0 : tideB0, *T1 = box == 0 ? tideA1 : tideB1;
+      float f[3], t[3];
+      int cf[3];
+      for (int k = 0; k < 3; k++) { f[k] = floorf(g[k]); t[k] = g[k] - f[k]; cf[k] = (int)f[k]; }
+      for (int k = 0; k < 8; k++) {
+        int o[3] = {k & 1, (k >> 1) & 1, k >> 2}, at[3];
+        float w3[3];
+        for (int d = 0; d < 3; d++) {
+          w3[d] = o[d] ? t[d] : 1.0f - t[d];
+          at[d] = cf[d] + o[d] < 63 ? cf[d] + o[d] : 63;
+        }
+        size_t c = (size_t)fine_index(at[0], at[1], at[2]);
+        const float *m = M + 4 * c, *fv = F + 4 * c, *t0 = T0 + 4 * c, *t1 = T1 + 4 * c;
+        if (!(m[3] > 0.0f)) continue;
+        v3 d = vsub(p, vdivs(ld3(m), m[3]));
+        v3 Td = V3(t0[0] * d.x + t0[3] * d.y + t1[0] * d.z,
+                   t0[3] * d.x + t0[1] * d.y + t1[1] * d.z,
+                   t1[0] * d.x + t1[1] * d.y + t0[2] * d.z);
+        grav = vadd(grav, vmuls(vadd(ld3(fv), Td), w3[0] * w3[1] * w3[2]));
+      }
+      grav = vsub(grav, vmuls(ld3(F + 4 * ORC_FINE), u->Gm));
+      if (u->boxB > 0.5f) grav = vadd(grav, box == 0 ? cross_at(u, monoB, monoA) : cross_at(u, monoA, monoB));
+    } else {
+      grav = mass_at(u, p, monoA);
+      if (u->boxB > 0.5f) grav = vadd(grav, mass_at(u, p, monoB));
+    }
+    grav = vadd(grav, ld3(ppAll + 4 * (size_t)i));
+    float *o = grav4 + 4 * (size_t)i;
+    o[0] = grav.x; o[1] = grav.y; o[2] = grav.z; o[3] = 0.0f;
+  }
+}
+
+/* ------------------------------------------------------------------ */
 /* src/glsl-sim.js:676-754 PPGATHER_FS, PPFORCE_FS                      */
 /* ------------------------------------------------------------------ */
 void orc_pp_gather(const orc_uni *u, const float *pos4, const float *mat, const int *index, int cap,

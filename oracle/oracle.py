@@ -145,6 +145,9 @@ def lib():
         L.orc_sim_pass.argtypes = [C.POINTER(Uni)] + [P] * 11 + [C.c_int] + [P] * 4
         L.orc_diag.argtypes = [C.POINTER(Uni)] + [P] * 9 + [C.c_int, P]
         L.orc_contact_pairs.argtypes = [C.POINTER(Uni), P, P, C.c_int, P, P]
+        L.orc_cell_tide.argtypes = [C.POINTER(Uni), C.c_int] + [P] * 8
+        L.orc_pp_split.argtypes = [C.POINTER(Uni), C.c_int, P, P, P]
+        L.orc_gather_split.argtypes = [C.POINTER(Uni)] + [P] * 13
         L.orc_rigid.argtypes = [C.c_int] + [P] * 10 + [C.c_float, P, P]
         L.orc_morton.argtypes = [C.c_int, P, P, P, P, P]
         L.orc_engine_new.restype = P
@@ -275,6 +278,33 @@ def contact_pairs(u, pos4, seats, cap=64):
     pairs = np.zeros((N, cap), np.uint32)
     lib().orc_contact_pairs(C.byref(u), ptr(pos4), ptr(seats), int(cap), ptr(counts), ptr(pairs))
     return counts, pairs
+
+
+def cell_tide(u, S, fine, coarse, farA, farT0, farT1):
+    """The stencil-split P3M's cell pass: (force, tide0, tide1), each (64^3 + 1) x 4."""
+    force = np.zeros((FINE + 1, 4), np.float32)
+    t0 = np.zeros((FINE + 1, 4), np.float32)
+    t1 = np.zeros((FINE + 1, 4), np.float32)
+    a = [np.ascontiguousarray(x, np.float32) for x in (fine, coarse, farA, farT0, farT1)]
+    lib().orc_cell_tide(C.byref(u), int(S), *[ptr(x) for x in a], ptr(force), ptr(t0), ptr(t1))
+    return force, t0, t1
+
+
+def pp_split(u, S, pos4, mat):
+    """The stencil-split P3M's pairs: every particle's (pull, potential) x Gm, N x 4."""
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    out = np.zeros((len(pos4), 4), np.float32)
+    lib().orc_pp_split(C.byref(u), int(S), ptr(pos4), ptr(np.ascontiguousarray(mat, np.float32)), ptr(out))
+    return out
+
+
+def gather_split(u, pos4, meshA, meshB, monoA, monoB, ppall):
+    """The stencil-split P3M's gravity at every particle; meshA/meshB = (fine, force, tide0, tide1)."""
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    out = np.zeros((len(pos4), 4), np.float32)
+    arrs = [np.ascontiguousarray(x, np.float32) for x in (*meshA, *meshB, monoA, monoB, ppall)]
+    lib().orc_gather_split(C.byref(u), ptr(pos4), *[ptr(x) for x in arrs], ptr(out))
+    return out
 
 
 def box_of(u, p):

@@ -1,0 +1,103 @@
+"""The oracle's stencil-split P3M, pinned on the CPU.
+
+The split form has no counterpart in the reference, so it is pinned by its own definition:
+1. a pair's weight is the share of its cloud-in-cell node pairs within S nodes of each other (Chebyshev),
+   checked against a brute-force enumeration of the 8 x 8 node pairs for random placements;
+2. when every particle lies within S - 1 nodes of every other, mesh and weights hand the whole interaction to
+   the pairs, so the split form's gravity is the direct sum (softened at the particle radius) to rounding.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+FH = 12.0 / 64
+
+
+def sweep_sim(orc, N, a=0.01):
+    from cosmic_collisions_b200 import _lib as L
+    s = L.Sim()
+    s.N, s.W = N, 128
+    s.H = N // 128
+    s.G = 64
+    s.m, s.a, s.cell = 1.0 / N, a, 2.6 * a
+    s.k, s.dt, s.c = 1.0, 1e-3, 0.0
+    s.M = 1.0
+    s.boxOn[0] = 1
+    sim = orc.Sim.from_buffer_copy(bytes(s))
+    u = orc.make_uni(sim)
+    orc.lib().orc_boxes(C.byref(sim), C.byref(u))
+    return sim, u
+
+
+def brute_weight(gi, gj, S):
+    """sum over node pairs (k, l), |k - l|_inf <= S, of w_i(k) w_j(l), the nodes and weights of CIC"""
+    bi, bj = np.floor(gi), np.floor(gj)
+    ti, tj = gi - bi, gj - bj
+    W = 0.0
+    for ki in range(8):
+        oi = np.array([ki & 1, (ki >> 1) & 1, ki >> 2])
+        wi = np.prod(np.where(oi, ti, 1 - ti))
+        for kj in range(8):
+            oj = np.array([kj & 1, (kj >> 1) & 1, kj >> 2])
+            wj = np.prod(np.where(oj, tj, 1 - tj))
+            if np.max(np.abs((bi + oi) - (bj + oj))) <= S:
+                W += wi * wj
+    return W
+
+
+@pytest.mark.parametrize("S", [1, 2, 3])
+def test_pair_weight_is_the_node_pair_share(orc, S):
+    rng = np.random.default_rng(7 + S)
+    N = 128
+    sim, u = sweep_sim(orc, N)
+    pos = np.zeros((N, 4), np.float32)
+    mat = np.zeros(N, np.float32)          # only particle 0 pulls: row i's pull is W_i0 x Newton
+    mat[0] = 1.0
+    centre = np.array([0.3, -0.2, 0.1])
+    pos[0, :3] = centre
+    off = rng.uniform(-(S + 2.5) * FH, (S + 2.5) * FH, size=(N - 1, 3))
+    pos[1:, :3] = centre + off
+    out = orc.pp_split(u, S, pos, mat)
+    LA = np.array(u.LA, np.float64)
+    g = (pos[:, :3].astype(np.float32) + np.array(u.LA, np.float32)) * np.float32(u.invH) - np.float32(0.5)
+    g = g.astype(np.float64)
+    a2 = float(np.float32(u.a2))
+    for i in range(1, N):
+        d = pos[0, :3].astype(np.float64) - pos[i, :3]
+        inv = 1.0 / math.sqrt(d @ d + a2)
+        want = brute_weight(g[i], g[0], S) * d * inv ** 3 * sim.m
+        assert np.allclose(out[i, :3], want, rtol=1e-5, atol=1e-6 * np.abs(d * inv ** 3 * sim.m).max()), i
+    assert np.any(np.abs(out[1:, 0]) > 0)
+
+
+def test_compact_cluster_is_the_direct_sum(orc):
+    """S = 3 and a cluster inside one node's neighbourhood (every base-node offset within 2): every pair has
+    weight 1 and the mesh keeps nothing near, so the gravity is the direct sum."""
+    rng = np.random.default_rng(3)
+    N = 512
+    sim, u = sweep_sim(orc, N)
+    pos = np.zeros((N, 4), np.float32)
+    pos[:, :3] = (np.array([0.05, 0.02, -0.03]) + rng.uniform(-0.9 * FH, 0.9 * FH, size=(N, 3))).astype(np.float32)
+    mat = np.ones(N, np.float32)
+    S = 3
+    fine = np.zeros((orc.FINE + 1, 4), np.float32)
+    z4 = np.zeros(4, np.float32)
+    P = orc.ptr
+    orc.lib().orc_deposit(C.byref(u), 0, P(pos), P(mat), P(z4), P(fine))
+    coarse = np.zeros((orc.COARSE, 4), np.float32)
+    mono = np.zeros(4, np.float32)
+    orc.lib().orc_coarse(P(fine), P(coarse), P(mono))
+    fa, t0, t1 = (np.zeros((orc.COARSE, 4), np.float32) for _ in range(3))
+    orc.lib().orc_far(P(coarse), P(fa), P(t0), P(t1))
+    force, tide0, tide1 = orc.cell_tide(u, S, fine, coarse, fa, t0, t1)
+    occ = fine[:-1, 3] > 0
+    assert occ.sum() >= 8
+    assert np.abs(force[:-1][occ]).max() == 0.0            # every node pair is inside the stencil
+    pp = orc.pp_split(u, S, pos, mat)
+    zeros = np.zeros((orc.FINE + 1, 4), np.float32)
+    grav = orc.gather_split(u, pos, (fine, force, tide0, tide1), (zeros, zeros, zeros, zeros), z4, z4, pp)
+    want, _ = orc.direct_sum(pos, np.full(N, sim.m), sim.a, np.arange(N, dtype=np.int32))
+    rel = np.linalg.norm(grav[:, :3] - want, axis=1) / np.linalg.norm(want, axis=1)
+    assert np.median(rel) < 1e-6 and rel.max() < 1e-4
