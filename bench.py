@@ -26,6 +26,11 @@ A step is one full-phase step of the reference schedule (contact grid every
            the same workload: full-phase steps from the same saved mid-impact
            state (the run prepared by the library, untimed, then handed over
            as a checkpoint).
+  plain_1e3  the plain P3M at the metric's operating point (median force error
+           <= 1e-3 against the binary64 direct sum on the gravity sweep): the
+           stencil-split form (ccs_set_pp_split), its own timed steps from the
+           same saved state and its force error.  `value` keeps the reference's
+           own P3M (mesh + the capped loose list), the form the CPU arm times.
   nn_corrected  the same timed steps with the learned pairwise correction
            attached (BF16 network on the tensor cores, half the plain cut),
            after training it on the device on pairs drawn from the same impact
@@ -266,10 +271,10 @@ def cpu_reference(ckpt, min_seconds=10.0, min_steps=8, threads=None, N=None):
                       % (steps, N, what, el, cores)}
 
 
-def force_error(cc, dev, N, sample=2048, seed=3, net=None):
+def force_error(cc, dev, N, sample=2048, seed=3, net=None, split=0):
     """The gravity-only sweep (Plummer sphere + 10 % debris, equal masses, 1 M_earth): one force evaluation
-    of the P3M step (plain, or with the learned correction `net`) against the library's binary64 direct sum
-    at a seeded sample of particles."""
+    of the P3M step (the reference's loose-list form, with the learned correction `net`, or the stencil-split
+    form with stencil `split`) against the library's binary64 direct sum at a seeded sample of particles."""
     import numpy as np
     from cosmic_collisions_b200 import configs
     sim, pos, vel, mat = configs.gravity_sweep(N=N)
@@ -284,6 +289,10 @@ def force_error(cc, dev, N, sample=2048, seed=3, net=None):
         s = nb.sim
         rep, lst, _ = cc.fof(s.N, s.m, s.a, pos, vel, mat, D, s.k, 2 * s.a)
         nb.set_pp(lst, rep.ppLoose)
+        if split:
+            nb.set_pp_split(split)
+            nb.pass_mesh()
+            nb.pass_pp()
         nb.pass_sim(False, False, 0.0)
         g = nb.read_state()["aux"][:, :3].astype(np.float64)
         idx = np.sort(np.random.default_rng(seed).choice(N, sample, replace=False)).astype(np.int32)
@@ -293,6 +302,8 @@ def force_error(cc, dev, N, sample=2048, seed=3, net=None):
     rel = np.linalg.norm(g[idx] - ref, axis=1) / np.linalg.norm(ref, axis=1)
     on = np.isin(idx, np.asarray(lst, np.int64))
     return {"median": float(np.median(rel)), "p99": float(np.percentile(rel, 99)), "sample": sample,
+            "method": ("stencil-split P3M, every mesh node pair within %d cells summed pairwise" % split
+                       if split else "the reference's P3M: mesh + the capped loose list's pairs"),
             "loose_list_members_in_sample": int(on.sum()),
             "loose_list_median": float(np.median(rel[on])) if on.any() else None,
             "workload": "gravity sweep, %d equal masses: Plummer sphere (scale 1 R_earth) + 10%% uniform debris" % N,
@@ -710,6 +721,28 @@ def run_ours(args, rank, world, log):
                    "kernels_us": {k: v["mean_us"] for k, v in nn_kt.items()}, "gpu_launches": int(nn_launches),
                    "clocks": nn_clk, "wall_s_timed_region": nn_wall, "force_error": nn_err, "training": info,
                    "state": "the plain leg's timed steps from the same saved state"}
+    # the plain P3M at the metric's operating point: the stencil-split form, the same timed steps from the
+    # same saved state, and its force error on the same gravity sweep
+    split_line = None
+    if args.split:
+        nb.load(snapshot)
+        nb.set_pp_split(args.split)
+        sp_ms, sp_kt, sp_launches, sp_wall, sp_clk = timed_steps(nb, lib, stream, flush, args.split_steps, dev, dist)
+        sp_total = max_over_ranks(sum(sp_ms))
+        sp_err = force_error(cc, dev, N, split=args.split) if rank == 0 else None
+        nb.set_pp_split(0)
+        split_line = {"value": world * N * args.split_steps / (sp_total / 1e3), "unit": "particle-steps/s",
+                      "ms_per_step": sp_total / args.split_steps, "steps": args.split_steps, "stencil": args.split,
+                      "kernels_us": {k: v["mean_us"] for k, v in sp_kt.items() if k != "simulate"},
+                      "gpu_launches": int(sp_launches), "clocks": sp_clk, "force_error": sp_err,
+                      "method": "stencil-split P3M: every pair of mesh nodes within %d cells (Chebyshev) summed "
+                                "particle by particle (each pair weighted by its share of cloud-in-cell node "
+                                "pairs inside the stencil), the rest on the mesh unsoftened, gathered to first "
+                                "order by each node's tidal tensor, far blocks as monopole + quadrupole at each "
+                                "cell; the plain form that reaches median force error <= 1e-3" % args.split,
+                      "state": "the plain leg's timed steps from the same saved state"}
+        log("stencil-split P3M (S=%d): %.3f ms a step, force error median %.3e"
+            % (args.split, sp_total / args.split_steps, sp_err["median"] if sp_err else float("nan")))
     peak, peak_kind = measured_peaks()
     sim_mean_us = kt["simulate"]["mean_us"]
     achieved = ALG_BYTES_SIM * N / (sim_mean_us * 1e-6) / 1e9 if sim_mean_us else None
@@ -759,6 +792,7 @@ def run_ours(args, rank, world, log):
         "force_error": ferr,
         "analysis": analysis,
         "nn_corrected": nn_line,
+        "plain_1e3": split_line,
     }
     nb.close()
     return line, snapshot
@@ -781,6 +815,9 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="ensemble: keep the default launch shapes")
     ap.add_argument("--nn-pairs", type=int, default=9_000_000, help="training pairs (three snapshots)")
     ap.add_argument("--nn-epochs", type=int, default=8)
+    ap.add_argument("--split", type=int, default=3, choices=[0, 1, 2, 3],
+                    help="stencil of the plain P3M leg at the metric's force-error operating point (0: skip)")
+    ap.add_argument("--split-steps", type=int, default=64, help="timed steps of that leg")
     ap.add_argument("--profile", action="store_true",
                     help="prepare, warm up, then run --steps steps inside cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no bench line")

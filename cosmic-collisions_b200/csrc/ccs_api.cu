@@ -546,7 +546,7 @@ int block_launches(const ccs_handle *h, const StepPlan *plans, int M, bool split
   for (int k = 0; k < M; ++k) {
     if (h->ppSplit && !h->field) {                  // the stencil-split P3M: walk + tail every step
       per += 2 + (plans[k].slots ? 1 : 0);
-      if (plans[k].mesh) per += 5 * (1 + (plans[k].u.boxB > 0.5f)) + pp_split_launches();
+      if (plans[k].mesh) per += 7 * (1 + (plans[k].u.boxB > 0.5f)) + pp_split_launches();
       continue;
     }
     per += 1;                                       // contact step
@@ -962,6 +962,8 @@ int ensure_split_buffers(ccs_handle *h) {
     rc |= dev_alloc(h, &m.tide0, kFine + 1);
     rc |= dev_alloc(h, &m.tide1, kFine + 1);
     rc |= dev_alloc(h, &m.cellPartT, (size_t)kCoarse * kCellChunks * 64 * 3);
+    rc |= dev_alloc(h, &m.quad0, kCoarse);
+    rc |= dev_alloc(h, &m.quad1, kCoarse);
   }
   rc |= dev_alloc(h, &h->splitStart, split_start_ints());
   rc |= dev_alloc(h, &h->splitCells, N);
@@ -972,6 +974,7 @@ int ensure_split_buffers(ccs_handle *h) {
   if (rc) {
     for (int b = 0; b < 2; ++b) {
       dev_free(h->pm[b].tide0); dev_free(h->pm[b].tide1); dev_free(h->pm[b].cellPartT);
+      dev_free(h->pm[b].quad0); dev_free(h->pm[b].quad1);
     }
     dev_free(h->splitStart); dev_free(h->splitCells); dev_free(h->splitNCells); dev_free(h->splitSrc);
     dev_free(h->splitSrcT); dev_free(h->ppAll);
@@ -995,7 +998,7 @@ void free_state(ccs_handle *h) {
     dev_free(m.farT1); dev_free(m.mono); dev_free(m.partial); dev_free(m.counter);
     dev_free(m.occ); dev_free(m.occIdx); dev_free(m.occN); dev_free(m.occBlocks); dev_free(m.occCount);
     dev_free(m.occAsc); dev_free(m.occAscN); dev_free(m.cellPart); dev_free(m.cellDone);
-    dev_free(m.tide0); dev_free(m.tide1); dev_free(m.cellPartT);
+    dev_free(m.tide0); dev_free(m.tide1); dev_free(m.cellPartT); dev_free(m.quad0); dev_free(m.quad1);
   }
   dev_free(h->splitStart); dev_free(h->splitCells); dev_free(h->splitNCells); dev_free(h->splitSrc);
   dev_free(h->splitSrcT); dev_free(h->ppAll);

@@ -70,6 +70,7 @@ struct MeshBuf {
   // the stencil-split P3M's mesh (allocated when that form is switched on): each cell's tidal tensor, and
   // the cell pass's partial sums of pull, potential and tide: [listed block][source chunk][3][cell]
   float4 *tide0 = nullptr, *tide1 = nullptr, *cellPartT = nullptr;
+  float4 *quad0 = nullptr, *quad1 = nullptr;   // each block's second moment about its centre of mass
 };
 
 // Arguments of the contact step (simFS, src/glsl-sim.js:354-512).

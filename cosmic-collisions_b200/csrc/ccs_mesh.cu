@@ -504,6 +504,9 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restr
 // the pull, the near sources' exactly and the block's far field's as the block carries it -- so that the
 // gather can carry each node's pull from its centre of mass to the particle to first order.  Outputs (x Gm):
 // force = (pull, potential) at the cell's centre of mass, tide0 = (Txx, Tyy, Tzz, Txy), tide1 = (Txz, Tyz).
+// The far field is k_far_cell's, added after: each far block's pull evaluated at the cell itself, with the
+// block's quadrupole (the reference carries a block's monopole field from the block's centre of mass by its
+// tidal tensor, which at a few blocks' distance is off by a per cent or two).
 // ---------------------------------------------------------------------------
 namespace {
 template <int SPLIT>
@@ -648,19 +651,10 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
           s1 = make_float4(s1.x + p1.x, s1.y + p1.y, s1.z + p1.z, s1.w + p1.w);
           s2 = make_float4(s2.x + p2.x, s2.y + p2.y, s2.z, s2.w);
         }
-        f3 a3 = mk(s0.x, s0.y, s0.z);
-        float pt = s0.w;
-        const float4 mb = coarse[blk];
-        const float4 fa = farA[blk], t0 = farT0[blk], t1 = farT1[blk];
-        const f3 d = x - xyz(mb) * fdiv(1.0f, mb.w);
-        const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
-                         t1.x * d.x + t1.y * d.y + t0.z * d.z);
-        a3 = a3 + (xyz(fa) + Td);
-        pt += fa.w - dot(xyz(fa), d) - 0.5f * dot(d, Td);
         const int fi = fine_index(tx, ty, tz);
-        force[fi] = make_float4(a3.x * Gm, a3.y * Gm, a3.z * Gm, pt * Gm);
-        tide0[fi] = make_float4((s1.x + t0.x) * Gm, (s1.y + t0.y) * Gm, (s1.z + t0.z) * Gm, (s1.w + t0.w) * Gm);
-        tide1[fi] = make_float4((s2.x + t1.x) * Gm, (s2.y + t1.y) * Gm, 0.0f, 0.0f);
+        force[fi] = make_float4(s0.x * Gm, s0.y * Gm, s0.z * Gm, s0.w * Gm);
+        tide0[fi] = make_float4(s1.x * Gm, s1.y * Gm, s1.z * Gm, s1.w * Gm);
+        tide1[fi] = make_float4(s2.x * Gm, s2.y * Gm, 0.0f, 0.0f);
       }
       if (t == 0) cellDone[bi] = 0;
     }
@@ -669,13 +663,136 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
 }
 }  // namespace
 
+// each occupied block's second moment about its centre of mass, from its occupied cells taken as points at
+// their own centres of mass: Q = sum m (x - X)(x - X)^T, q0 = (Qxx, Qyy, Qzz, Qxy), q1 = (Qxz, Qyz).  A warp a
+// block, the lanes over its (up to 64) cells.
+__global__ void __launch_bounds__(256) k_block_quad(const float4 *__restrict__ coarse,
+                                                    const float4 *__restrict__ occ, const int *__restrict__ occN,
+                                                    const int *__restrict__ occBlocks,
+                                                    const int *__restrict__ occCount, float4 *__restrict__ q0,
+                                                    float4 *__restrict__ q1) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (w >= *occCount) return;
+  const int b = occBlocks[w];
+  const float4 mb = coarse[b];
+  const f3 X = xyz(mb) * fdiv(1.0f, mb.w);
+  float s[6] = {0, 0, 0, 0, 0, 0};
+  const int n = occN[b];
+  for (int c = lane; c < n; c += 32) {
+    const float4 e = occ[(size_t)b * 64 + c];
+    const f3 d = xyz(e) - X;
+    s[0] += e.w * d.x * d.x; s[1] += e.w * d.y * d.y; s[2] += e.w * d.z * d.z;
+    s[3] += e.w * d.x * d.y; s[4] += e.w * d.x * d.z; s[5] += e.w * d.y * d.z;
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s[k] += __shfl_xor_sync(0xFFFFFFFFu, s[k], o);
+  if (lane == 0) {
+    q0[b] = make_float4(s[0], s[1], s[2], s[3]);
+    q1[b] = make_float4(s[4], s[5], 0.0f, 0.0f);
+  }
+}
+
+// the far field of the stencil-split P3M: at every occupied cell's centre of mass, the pull, potential and
+// tide of every occupied block more than two blocks from the cell's own (the blocks the near field leaves
+// out), each block as its monopole at its centre of mass plus its quadrupole; added to the near field.
+// A thread a cell: work items are (occupied block, its n-th occupied cell), the sources the ascending list
+// of occupied blocks, staged in shared memory a batch at a time.
+constexpr int kFarCellBatch = 256;
+__global__ void __launch_bounds__(256) k_far_cell(const ccs_uniforms *__restrict__ U,
+                                                  const float4 *__restrict__ coarse, const float4 *__restrict__ q0,
+                                                  const float4 *__restrict__ q1, const float4 *__restrict__ occ,
+                                                  const uint8_t *__restrict__ occIdx, const int *__restrict__ occN,
+                                                  const int *__restrict__ occBlocks, const int *__restrict__ occCount,
+                                                  const int *__restrict__ occAsc, const int *__restrict__ occAscN,
+                                                  float4 *__restrict__ force, float4 *__restrict__ tide0,
+                                                  float4 *__restrict__ tide1) {
+  __shared__ float4 sM[kFarCellBatch], sQ0[kFarCellBatch];
+  __shared__ float2 sQ1[kFarCellBatch];
+  __shared__ int sB[kFarCellBatch];
+  const float Gm = U->Gm;
+  const int nb = *occCount, ns = *occAscN;
+  const int items = nb * 64;
+  // every CTA walks the same rounds of 256 items (a block's 64 cell slots, four blocks a round), so the
+  // staging barriers are uniform; slots past a block's occupied cells idle
+  for (int base = blockIdx.x * 256; base < items; base += gridDim.x * 256) {
+    const int it = base + threadIdx.x;
+    const int bi = it >> 6, c = it & 63;
+    const bool live = it < items && c < occN[occBlocks[min(bi, nb - 1)]];
+    int blk = 0, tl = 0;
+    f3 x = mk(0, 0, 0);
+    if (live) {
+      blk = occBlocks[bi];
+      const float4 e = occ[(size_t)blk * 64 + c];
+      x = xyz(e);
+      tl = occIdx[(size_t)blk * 64 + c];
+    }
+    const int bx = blk & 15, by = (blk >> 4) & 15, bz = blk >> 8;
+    float ax = 0, ay = 0, az = 0, pot = 0, txx = 0, tyy = 0, tzz = 0, txy = 0, txz = 0, tyz = 0;
+    for (int s0 = 0; s0 < ns; s0 += kFarCellBatch) {
+      const int sn = min(kFarCellBatch, ns - s0);
+      __syncthreads();
+      for (int j = threadIdx.x; j < sn; j += blockDim.x) {
+        const int k = occAsc[s0 + j];
+        const float4 m = coarse[k];
+        const float iw = fdiv(1.0f, m.w);
+        sM[j] = make_float4(m.x * iw, m.y * iw, m.z * iw, m.w);
+        sQ0[j] = q0[k];
+        const float4 t = q1[k];
+        sQ1[j] = make_float2(t.x, t.y);
+        sB[j] = k;
+      }
+      __syncthreads();
+      if (live) {
+        for (int j = 0; j < sn; ++j) {
+          const int k = sB[j];
+          if (max(abs((k & 15) - bx), max(abs(((k >> 4) & 15) - by), abs((k >> 8) - bz))) <= 2) continue;
+          const float4 m = sM[j], Q0 = sQ0[j];
+          const float2 Q1 = sQ1[j];
+          const f3 r = xyz(m) - x;   // from the cell to the block
+          const float r2 = dot(r, r), inv = rsqrtf(r2), inv2 = inv * inv, inv3 = inv * inv2, inv5 = inv3 * inv2;
+          const float a3 = m.w * inv3, a5 = 3.0f * a3 * inv2;
+          // monopole: pull, potential, tide
+          ax += r.x * a3; ay += r.y * a3; az += r.z * a3;
+          pot -= m.w * inv;
+          txx += a5 * r.x * r.x - a3; tyy += a5 * r.y * r.y - a3; tzz += a5 * r.z * r.z - a3;
+          txy += a5 * r.x * r.y; txz += a5 * r.x * r.z; tyz += a5 * r.y * r.z;
+          // quadrupole: a = -3 Q r / r^5 + 7.5 (r Q r) r / r^7 - 1.5 tr(Q) r / r^5,
+          // potential -0.5 (3 r Q r / r^5 - tr(Q) / r^3)
+          const f3 Qr = mk(Q0.x * r.x + Q0.w * r.y + Q1.x * r.z, Q0.w * r.x + Q0.y * r.y + Q1.y * r.z,
+                           Q1.x * r.x + Q1.y * r.y + Q0.z * r.z);
+          const float rQr = dot(r, Qr), tr = Q0.x + Q0.y + Q0.z;
+          const float c1 = 7.5f * rQr * inv5 * inv2 - 1.5f * tr * inv5;
+          ax += c1 * r.x - 3.0f * inv5 * Qr.x;
+          ay += c1 * r.y - 3.0f * inv5 * Qr.y;
+          az += c1 * r.z - 3.0f * inv5 * Qr.z;
+          pot -= 0.5f * (3.0f * rQr * inv5 - tr * inv3);
+        }
+      }
+    }
+    if (live) {
+      const int fi = fine_index((blk & 15) * 4 + (tl & 3), ((blk >> 4) & 15) * 4 + ((tl >> 2) & 3),
+                                (blk >> 8) * 4 + (tl >> 4));
+      const float4 f = force[fi], t0 = tide0[fi], t1 = tide1[fi];
+      force[fi] = make_float4(f.x + ax * Gm, f.y + ay * Gm, f.z + az * Gm, f.w + pot * Gm);
+      tide0[fi] = make_float4(t0.x + txx * Gm, t0.y + tyy * Gm, t0.z + tzz * Gm, t0.w + txy * Gm);
+      tide1[fi] = make_float4(t1.x + txz * Gm, t1.y + tyz * Gm, 0.0f, 0.0f);
+    }
+  }
+}
+
 int launch_cell_tide(const ccs_uniforms *u, int S, const MeshBuf &m, cudaStream_t st) {
   const int sms = sm_count();
   cudaMemsetAsync(m.force, 0, sizeof(float4) * kFine, st);
   k_cell_tide<4><<<sms * 8, 256, 0, st>>>(u, S, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount,
                                           m.farA, m.farT0, m.farT1, m.force, m.tide0, m.tide1, m.cellPartT,
                                           m.cellDone);
-  return 1;
+  k_block_quad<<<kCoarse / 8, 256, 0, st>>>(m.coarse, m.occ, m.occN, m.occBlocks, m.occCount, m.quad0, m.quad1);
+  k_far_cell<<<sms * 4, 256, 0, st>>>(u, m.coarse, m.quad0, m.quad1, m.occ, m.occIdx, m.occN, m.occBlocks,
+                                      m.occCount, m.occAsc, m.occAscN, m.force, m.tide0, m.tide1);
+  return 3;
 }
 
 int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int split) {

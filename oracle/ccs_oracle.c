@@ -759,10 +759,26 @@ void orc_cell(const orc_uni *u, const float *fine, const float *coarse, const fl
 static v3 mass_at(const orc_uni *u, v3 p, const float *mono);
 static v3 cross_at(const orc_uni *u, const float *other, const float *mine);
 
-void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, const float *farA,
-                   const float *farT0, const float *farT1, float *force, float *tide0, float *tide1) {
+void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, float *force, float *tide0,
+                   float *tide1) {
   const float eps2 = 1e-6f * u->eps2Mesh;   /* keeps two coinciding centres of mass finite, as the library's */
   memcpy(force + 4 * ORC_FINE, fine + 4 * ORC_FINE, 16);
+  /* each occupied block's centre of mass and second moment, from its occupied cells at their centres of mass */
+  double *bq = (double *)calloc((size_t)ORC_COARSE * 10, sizeof(double));   /* X[3], M, Q[6] */
+  for (int b = 0; b < ORC_COARSE; b++) {
+    const float *m = coarse + 4 * b;
+    double *q = bq + 10 * b;
+    if (m[3] <= 0.0f) continue;
+    q[0] = m[0] / m[3]; q[1] = m[1] / m[3]; q[2] = m[2] / m[3]; q[3] = m[3];
+    int bx = b & 15, by = (b >> 4) & 15, bz = b >> 8;
+    for (int c = 0; c < 64; c++) {
+      const float *f = fine + 4 * fine_index(bx * 4 + (c & 3), by * 4 + ((c >> 2) & 3), bz * 4 + (c >> 4));
+      if (f[3] <= 0.0f) continue;
+      double d[3] = {f[0] / f[3] - q[0], f[1] / f[3] - q[1], f[2] / f[3] - q[2]};
+      q[4] += f[3] * d[0] * d[0]; q[5] += f[3] * d[1] * d[1]; q[6] += f[3] * d[2] * d[2];
+      q[7] += f[3] * d[0] * d[1]; q[8] += f[3] * d[0] * d[2]; q[9] += f[3] * d[1] * d[2];
+    }
+  }
 #pragma omp parallel for schedule(dynamic, 256)
   for (int ci = 0; ci < ORC_FINE; ci++) {
     int c[3] = {ci & 63, (ci >> 6) & 63, ci >> 12};
@@ -775,6 +791,7 @@ void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coar
     v3 x = vdivs(ld3(mc), mc[3]);
     int cc[3] = {c[0] >> 2, c[1] >> 2, c[2] >> 2};
     double acc[3] = {0, 0, 0}, pot = 0, T[6] = {0, 0, 0, 0, 0, 0};   /* Txx Tyy Tzz Txy Txz Tyz */
+    /* near: the fine cells of the 5^3 blocks around, beyond the stencil, unsoftened */
     for (int kz = -2; kz <= 2; kz++)
       for (int ky = -2; ky <= 2; ky++)
         for (int kx = -2; kx <= 2; kx++) {
@@ -801,20 +818,34 @@ void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coar
                 T[3] += a5 * rx * ry; T[4] += a5 * rx * rz; T[5] += a5 * ry * rz;
               }
         }
-    int ca = coarse_index(cc[0], cc[1], cc[2]);
-    const float *mb = coarse + 4 * ca, *fa = farA + 4 * ca, *t0 = farT0 + 4 * ca, *t1 = farT1 + 4 * ca;
-    v3 d = vsub(x, vdivs(ld3(mb), mb[3]));
-    v3 Td = V3(t0[0] * d.x + t0[3] * d.y + t1[0] * d.z,
-               t0[3] * d.x + t0[1] * d.y + t1[1] * d.z,
-               t1[0] * d.x + t1[1] * d.y + t0[2] * d.z);
-    acc[0] += fa[0] + Td.x; acc[1] += fa[1] + Td.y; acc[2] += fa[2] + Td.z;
-    pot += fa[3] - vdot(ld3(fa), d) - 0.5f * vdot(d, Td);
+    /* far: every occupied block more than two from the cell's own, monopole + quadrupole, at the cell */
+    for (int b = 0; b < ORC_COARSE; b++) {
+      const double *q = bq + 10 * b;
+      if (q[3] <= 0.0) continue;
+      int bx = b & 15, by = (b >> 4) & 15, bz = b >> 8;
+      int dx = abs(bx - cc[0]), dy = abs(by - cc[1]), dz = abs(bz - cc[2]);
+      if ((dx > dy ? (dx > dz ? dx : dz) : (dy > dz ? dy : dz)) <= 2) continue;
+      double r[3] = {q[0] - x.x, q[1] - x.y, q[2] - x.z};
+      double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2], inv = 1.0 / sqrt(r2), inv2 = inv * inv;
+      double inv3 = inv * inv2, inv5 = inv3 * inv2, M = q[3], a3 = M * inv3, a5 = 3.0 * a3 * inv2;
+      acc[0] += r[0] * a3; acc[1] += r[1] * a3; acc[2] += r[2] * a3;
+      pot -= M * inv;
+      T[0] += a5 * r[0] * r[0] - a3; T[1] += a5 * r[1] * r[1] - a3; T[2] += a5 * r[2] * r[2] - a3;
+      T[3] += a5 * r[0] * r[1]; T[4] += a5 * r[0] * r[2]; T[5] += a5 * r[1] * r[2];
+      double Qr[3] = {q[4] * r[0] + q[7] * r[1] + q[8] * r[2], q[7] * r[0] + q[5] * r[1] + q[9] * r[2],
+                      q[8] * r[0] + q[9] * r[1] + q[6] * r[2]};
+      double rQr = r[0] * Qr[0] + r[1] * Qr[1] + r[2] * Qr[2], tr = q[4] + q[5] + q[6];
+      double c1 = 7.5 * rQr * inv5 * inv2 - 1.5 * tr * inv5;
+      for (int a = 0; a < 3; a++) acc[a] += c1 * r[a] - 3.0 * inv5 * Qr[a];
+      pot -= 0.5 * (3.0 * rQr * inv5 - tr * inv3);
+    }
     o[0] = (float)(acc[0] * u->Gm); o[1] = (float)(acc[1] * u->Gm); o[2] = (float)(acc[2] * u->Gm);
     o[3] = (float)(pot * u->Gm);
-    T0[0] = (float)((T[0] + t0[0]) * u->Gm); T0[1] = (float)((T[1] + t0[1]) * u->Gm);
-    T0[2] = (float)((T[2] + t0[2]) * u->Gm); T0[3] = (float)((T[3] + t0[3]) * u->Gm);
-    T1[0] = (float)((T[4] + t1[0]) * u->Gm); T1[1] = (float)((T[5] + t1[1]) * u->Gm); T1[2] = T1[3] = 0.0f;
+    T0[0] = (float)(T[0] * u->Gm); T0[1] = (float)(T[1] * u->Gm); T0[2] = (float)(T[2] * u->Gm);
+    T0[3] = (float)(T[3] * u->Gm);
+    T1[0] = (float)(T[4] * u->Gm); T1[1] = (float)(T[5] * u->Gm); T1[2] = T1[3] = 0.0f;
   }
+  free(bq);
 }
 
 static double split_w(int D, int S, double ti, double tj) {

@@ -106,11 +106,12 @@ void orc_far(const float *coarse, float *farA, float *farT0, float *farT1);
 void orc_cell(const orc_uni *u, const float *fine, const float *coarse, const float *farA,
               const float *farT0, const float *farT1, float *force);
 /* the stencil-split P3M (the library's ccs_set_pp_split; no counterpart in the reference): the cell pass
- * without the node pairs within S cells, unsoftened, with tides (force, tide0 = Txx Tyy Tzz Txy, tide1 = Txz
+ * without the node pairs within S cells, unsoftened, with tides, and the far field at each cell from every
+ * block more than two away as its monopole and quadrupole (force, tide0 = Txx Tyy Tzz Txy, tide1 = Txz
  * Tyz, all x Gm); every particle's pairs inside the stencil (out4: pull, potential x Gm); the first-order
  * gather from each node's centre of mass plus the particle's pairs (grav4) */
-void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, const float *farA,
-                   const float *farT0, const float *farT1, float *force, float *tide0, float *tide1);
+void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, float *force, float *tide0,
+                   float *tide1);
 void orc_pp_split(const orc_uni *u, int S, const float *pos4, const float *mat, float *out4);
 void orc_gather_split(const orc_uni *u, const float *pos4, const float *fineA, const float *forceA,
                       const float *tideA0, const float *tideA1, const float *fineB, const float *forceB,

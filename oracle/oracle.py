@@ -145,7 +145,7 @@ def lib():
         L.orc_sim_pass.argtypes = [C.POINTER(Uni)] + [P] * 11 + [C.c_int] + [P] * 4
         L.orc_diag.argtypes = [C.POINTER(Uni)] + [P] * 9 + [C.c_int, P]
         L.orc_contact_pairs.argtypes = [C.POINTER(Uni), P, P, C.c_int, P, P]
-        L.orc_cell_tide.argtypes = [C.POINTER(Uni), C.c_int] + [P] * 8
+        L.orc_cell_tide.argtypes = [C.POINTER(Uni), C.c_int] + [P] * 5
         L.orc_pp_split.argtypes = [C.POINTER(Uni), C.c_int, P, P, P]
         L.orc_gather_split.argtypes = [C.POINTER(Uni)] + [P] * 13
         L.orc_rigid.argtypes = [C.c_int] + [P] * 10 + [C.c_float, P, P]
@@ -280,12 +280,12 @@ def contact_pairs(u, pos4, seats, cap=64):
     return counts, pairs
 
 
-def cell_tide(u, S, fine, coarse, farA, farT0, farT1):
-    """The stencil-split P3M's cell pass: (force, tide0, tide1), each (64^3 + 1) x 4."""
+def cell_tide(u, S, fine, coarse):
+    """The stencil-split P3M's cell pass, near and far: (force, tide0, tide1), each (64^3 + 1) x 4."""
     force = np.zeros((FINE + 1, 4), np.float32)
     t0 = np.zeros((FINE + 1, 4), np.float32)
     t1 = np.zeros((FINE + 1, 4), np.float32)
-    a = [np.ascontiguousarray(x, np.float32) for x in (fine, coarse, farA, farT0, farT1)]
+    a = [np.ascontiguousarray(x, np.float32) for x in (fine, coarse)]
     lib().orc_cell_tide(C.byref(u), int(S), *[ptr(x) for x in a], ptr(force), ptr(t0), ptr(t1))
     return force, t0, t1
 

@@ -5,8 +5,11 @@
   restatement of meshPairTable's field(), src/nbody.js:60-91);
 * the network's forward pass and its gradients, both through the tensor-core
   kernels, equal the numpy oracle's with the BF16 roundings at the same places;
-* training on the device learns the mesh's pair force where the two
-  particles share a mesh node, to about the pair table's accuracy;
+* training on the device converges on synthetic pairs, and on pairs drawn
+  from the impact the trained network's error where the two particles share
+  a mesh node is below the placement-averaged pair table's; the learned pass
+  at half the cut is no worse on the loose list than the plain pass at the
+  full cut;
 * the learned P3M pass over a loose list equals the oracle's pass.
 """
 import ctypes as C
@@ -105,12 +108,97 @@ def test_training_learns_the_mesh_pair_force(net, orc):
         print("loss %.3e -> %.3e; pairs sharing a node: label rms %.3e, table error %.3e, network error %.3e"
               % (loss[0], loss[-1], rms(lab[near]), e_tab, e_net))
         assert loss[-1] < loss[0] / 5
-        # the network learns the mesh's pair force to about the table's accuracy where the two share nodes
-        # (the placement-dependent rest is too fine-grained for 64 x 64 units); it must not be much worse
-        assert e_net < 1.5 * e_tab
+        assert e_net < 2 * e_tab          # synthetic pairs, uniform in the ball: training converges
     finally:
         net.set_params(p0)
         net.clear()
+
+
+@pytest.fixture(scope="module")
+def impact_net(ccmod):
+    """A network trained as the benchmark trains it, on a smaller pool: pairs drawn from the full impact at
+    262,144 particles at full-phase steps 0, 1000 and 3000 (1 M each), 8 epochs; a held-out draw from the
+    last snapshot.  Returns (network, held-out records, labels, the run's particle radius in cells)."""
+    from cosmic_collisions_b200 import configs
+    from cosmic_collisions_b200.learned import LearnedCorrection
+    n = LearnedCorrection(0, seed=2024)
+    nb = ccmod.NBody(0)
+    try:
+        nb.build(ccmod.make_opt(**configs.full_impact_opt(262144)))
+        while nb.sim.phase == 0:
+            nb.settle_some(64)
+        nb.analyze(True)
+        while nb.sim.phase == 1:
+            nb.rigid_step(0.01)
+        done = 0
+        for k, snap in enumerate((0, 1000, 3000)):
+            while done < snap:
+                step = min(360, snap - done)
+                nb.steps(step)
+                done += step
+                nb.analyze(True)
+            n.sample_state(nb, 1_000_000, seed=1000 + k)
+        n.sample_state(nb, 262_144, seed=9999)
+        a_cells = nb.sim.a / (12.0 / 64.0)
+    finally:
+        nb.close()
+    n.train(0, 3_000_000, epochs=8, tiles_per_cta=1, lr=2e-3)
+    rec, lab = n.read_pool(3_000_000, 262_144)
+    live = np.isfinite(rec[:, 0])
+    yield n, rec[live], lab[live], a_cells
+    n.close()
+
+
+def test_network_beats_the_table_on_impact_pairs(impact_net, orc):
+    """Where the two particles share a mesh node -- the only place the mesh's pair force is not the
+    node-softened Newton force -- the trained network's error is below the placement-averaged table's
+    (meshPairTable, src/nbody.js:48-109) on held-out pairs of the impact."""
+    net, rec, lab, a_cells = impact_net
+    y = net.forward(rec)
+    near = shares_a_node(rec)
+    mesh = lab + NO.softened_newton(rec)
+    f, _ = orc.pair_table()
+    tab = NO.table_model(rec, f, a_cells)
+    rms = lambda v: float(np.sqrt((v ** 2).sum(1).mean()))
+    e_net, e_tab = rms((y - lab)[near]), rms((mesh - tab)[near])
+    print("held-out impact pairs sharing a node: %d; table error %.4e, network error %.4e (%.1f %% lower)"
+          % (near.sum(), e_tab, e_net, 100 * (1 - e_net / e_tab)))
+    assert near.sum() > 10000
+    assert e_net < e_tab
+
+
+def test_learned_pass_at_half_the_cut_is_no_worse_than_the_plain_pass(impact_net, ccmod):
+    """On the gravity sweep, the loose list's force error (against the binary64 direct sum) with the learned
+    pass at half the cut is no worse than the plain pass's at the full cut: the network pays for the
+    pairs between 2.5 and 5 cells that it no longer corrects."""
+    from cosmic_collisions_b200 import configs
+    net = impact_net[0]
+    N = 262144
+    sim, pos, vel, mat = configs.gravity_sweep(N=N)
+    out = {}
+    for learned in (False, True):
+        nb = ccmod.NBody(0)
+        try:
+            nb.upload(sim, pos, vel, mat)
+            if learned:
+                nb.set_pp_nn(net)
+            nb.pass_slots()
+            nb.pass_diag()
+            D = nb.buffer("diag")
+            s = nb.sim
+            rep, lst, _ = ccmod.fof(s.N, s.m, s.a, pos, vel, mat, D, s.k, 2 * s.a)
+            nb.set_pp(lst, rep.ppLoose)
+            nb.pass_sim(False, False, 0.0)
+            g = nb.read_state()["aux"][:, :3].astype(np.float64)
+            idx = np.sort(np.asarray(lst, np.int64)[::8]).astype(np.int32)     # a sample of the loose list
+            ref, _ = nb.direct_sum(idx)
+            if learned:
+                nb.set_pp_nn(None)
+        finally:
+            nb.close()
+        out[learned] = float(np.median(np.linalg.norm(g[idx] - ref, axis=1) / np.linalg.norm(ref, axis=1)))
+    print("loose-list median force error: plain at 5 cells %.4e, learned at 2.5 cells %.4e" % (out[False], out[True]))
+    assert out[True] <= out[False]
 
 
 def test_learned_pass_matches_the_oracle(net, ccmod, orc):

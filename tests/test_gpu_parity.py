@@ -111,6 +111,7 @@ def test_contact_step(nb, ccmod, orc, settle, kick):
     nb.upload(to_lib_sim(ccmod, osim), pos, vel, mat)
     nb.write_state(q=q)
     nb.pass_slots()
+    gc, gp = nb.contact_pairs(64)            # the pair sets of this state, before the step moves it
     nb.pass_sim(settle, kick, 0.0)
     got = nb.read_state()
     # the oracle: same seats, zero meshes, gdt = 0
@@ -134,7 +135,6 @@ def test_contact_step(nb, ccmod, orc, settle, kick):
     assert np.array_equal(got["aux"][:, 3], ao[:, 3])
     assert ao[:, 3].mean() > 5          # the contact loop found neighbours
     # ... and the same ones: every owner's neighbours and which of them touch, as sets
-    gc, gp = nb.contact_pairs(64)
     oc, op = orc.contact_pairs(u, pos, seats, 64)
     assert np.array_equal(gc, oc) and gc.max() <= 64
     assert np.array_equal(np.sort(gp, axis=1), np.sort(op, axis=1))

@@ -68,7 +68,7 @@ def test_split_passes_match_the_oracle(ccmod, orc, S):
     P = orc.ptr
     fa, ft0, ft1 = (np.zeros((orc.COARSE, 4), np.float32) for _ in range(3))
     orc.lib().orc_far(P(coarse), P(fa), P(ft0), P(ft1))
-    of, ot0, ot1 = orc.cell_tide(u, S, fine, coarse, fa, ft0, ft1)
+    of, ot0, ot1 = orc.cell_tide(u, S, fine, coarse)
     occ = fine[:-1, 3] > 0
     assert occ.sum() > 500
     g = per_particle(force[:-1][occ, :3], of[:-1][occ, :3])
@@ -111,12 +111,14 @@ def sweep_error(ccmod, S, sample=2048, seed=3):
 
 def test_split_accuracy_on_the_gravity_sweep(ccmod):
     """One force evaluation of the split form against the binary64 direct sum: each wider stencil is more
-    accurate, and all are far more accurate than the mesh without pairs."""
+    accurate, all far more than the mesh without pairs, and the three-cell stencil reaches the metric's
+    operating point, median relative force error <= 1e-3."""
     plain = sweep_error(ccmod, 0)
     errs = {S: sweep_error(ccmod, S) for S in (1, 2, 3)}
     print("gravity sweep median / p99 relative error: mesh only", plain, "split", errs)
     assert plain[0] > 1e-2
-    assert errs[1][0] < 5e-3 and errs[3][0] < errs[2][0] < errs[1][0]
+    assert errs[3][0] < errs[2][0] < errs[1][0] < 5e-3
+    assert errs[3][0] <= 1e-3
 
 
 def test_split_steps_replay_as_launched(ccmod, orc):

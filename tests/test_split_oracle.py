@@ -91,7 +91,7 @@ def test_compact_cluster_is_the_direct_sum(orc):
     orc.lib().orc_coarse(P(fine), P(coarse), P(mono))
     fa, t0, t1 = (np.zeros((orc.COARSE, 4), np.float32) for _ in range(3))
     orc.lib().orc_far(P(coarse), P(fa), P(t0), P(t1))
-    force, tide0, tide1 = orc.cell_tide(u, S, fine, coarse, fa, t0, t1)
+    force, tide0, tide1 = orc.cell_tide(u, S, fine, coarse)
     occ = fine[:-1, 3] > 0
     assert occ.sum() >= 8
     assert np.abs(force[:-1][occ]).max() == 0.0            # every node pair is inside the stencil
@@ -101,3 +101,53 @@ def test_compact_cluster_is_the_direct_sum(orc):
     want, _ = orc.direct_sum(pos, np.full(N, sim.m), sim.a, np.arange(N, dtype=np.int32))
     rel = np.linalg.norm(grav[:, :3] - want, axis=1) / np.linalg.norm(want, axis=1)
     assert np.median(rel) < 1e-6 and rel.max() < 1e-4
+
+
+def test_far_blocks_with_quadrupoles_converge_to_the_direct_sum(orc):
+    """A cluster of particles more than two blocks away from a small target group: the split form's far
+    field (the cluster's blocks as monopole + quadrupole at the target cells) matches the direct sum of the
+    cluster to the octupole's order, an order of magnitude better than the monopole alone."""
+    rng = np.random.default_rng(5)
+    N = 2048
+    sim, u = sweep_sim(orc, N)
+    pos = np.zeros((N, 4), np.float32)
+    pos[:64, :3] = (np.array([-2.0, 0.1, 0.0]) + rng.normal(scale=0.02, size=(64, 3))).astype(np.float32)
+    pos[64:, :3] = (np.array([1.2, 0.4, -0.3]) + rng.uniform(-0.5, 0.5, size=(N - 64, 3))).astype(np.float32)
+    mat = np.ones(N, np.float32)
+    fine = np.zeros((orc.FINE + 1, 4), np.float32)
+    z4 = np.zeros(4, np.float32)
+    P = orc.ptr
+    orc.lib().orc_deposit(C.byref(u), 0, P(pos), P(mat), P(z4), P(fine))
+    coarse = np.zeros((orc.COARSE, 4), np.float32)
+    mono = np.zeros(4, np.float32)
+    orc.lib().orc_coarse(P(fine), P(coarse), P(mono))
+    force, _, _ = orc.cell_tide(u, 3, fine, coarse)
+    # the target cells: those the small group deposited on; their pull is all far (the cluster is 3+ blocks off)
+    tgt = np.zeros_like(fine)
+    m0 = mat.copy()
+    m0[64:] = 0
+    orc.lib().orc_deposit(C.byref(u), 0, P(pos), P(m0), P(z4), P(tgt))
+    cells = np.nonzero(tgt[:-1, 3] > 0)[0]
+    X = fine[cells, :3].astype(np.float64) / fine[cells, 3:4]
+    src = pos[64:, :3].astype(np.float64)
+    d = src[None, :, :] - X[:, None, :]
+    r = np.linalg.norm(d, axis=2)
+    want = (d / r[:, :, None] ** 3).sum(1) * sim.m
+    got = force[cells, :3].astype(np.float64)
+    # the group's own cells pull each other too (near, beyond the stencil or not): take them out
+    own = fine[cells].astype(np.float64) - tgt[cells]          # the cluster's share of these cells is none
+    assert np.abs(own[:, 3]).max() < 1e-6
+    near = np.zeros_like(got)
+    Xs = X
+    for a_, c in enumerate(cells):
+        cz, cy, cx = c // 4096, (c // 64) % 64, c % 64
+        for b_, c2 in enumerate(cells):
+            if c2 == c:
+                continue
+            z2, y2, x2 = c2 // 4096, (c2 // 64) % 64, c2 % 64
+            if max(abs(cx - x2), abs(cy - y2), abs(cz - z2)) <= 3:
+                continue
+            dd = Xs[b_] - Xs[a_]
+            near[a_] += fine[c2, 3] * dd / np.linalg.norm(dd) ** 3 * sim.m
+    rel = np.linalg.norm(got - near - want, axis=1) / np.linalg.norm(want, axis=1)
+    assert np.median(rel) < 2e-3, np.median(rel)
