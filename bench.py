@@ -348,7 +348,7 @@ def advance(nb, steps):
     return done
 
 
-def learned_correction(cc, dev, N, log, pairs=9_000_000, epochs=8, snaps=(0, 1000, 3000), held=262_144):
+def learned_correction(cc, dev, N, log, pairs=12_000_000, epochs=24, snaps=(0, 1000, 3000), held=262_144, lr=4e-3):
     """The learned P3M correction (config 4): a network trained on the device on pairs drawn from the full
     plain impact at full-phase steps 0, 1000 and 3000, labelled by the binary64 mesh arithmetic of the
     isolated pair.  Returns the network and what its training and a held-out set say."""
@@ -370,7 +370,7 @@ def learned_correction(cc, dev, N, log, pairs=9_000_000, epochs=8, snaps=(0, 100
     t_sample = time.perf_counter() - t0
     n_train = pairs // len(snaps) * len(snaps)
     t1 = time.perf_counter()
-    loss = net.train(0, n_train, epochs=epochs, tiles_per_cta=1, lr=2e-3)
+    loss = net.train(0, n_train, epochs=epochs, tiles_per_cta=1, lr=lr)
     t_train = time.perf_counter() - t1
     rec, lab = net.read_pool(n_train, held)
     live = np.isfinite(rec[:, 0])
@@ -381,7 +381,8 @@ def learned_correction(cc, dev, N, log, pairs=9_000_000, epochs=8, snaps=(0, 100
     f, _ = cc.pair_table()
     tab = table_model(rec, f, a_cells)                      # the plain pass's model of it
     rms = lambda v: float(np.sqrt((v ** 2).sum(1).mean())) if len(v) else None
-    info = {"pairs": int(n_train), "epochs": epochs, "snapshots_full_steps": list(snaps),
+    info = {"pairs": int(n_train), "epochs": epochs, "lr": lr, "snapshots_full_steps": list(snaps),
+            "train_tflops": 3.0 * 12288 * n_train * epochs / t_train / 1e12,
             "loss_first_epoch": float(loss[0]), "loss_last_epoch": float(loss[-1]),
             "sample_s": t_sample, "train_s": t_train,
             "held_out": {"pairs": int(len(rec)), "pairs_sharing_a_mesh_node": int(near.sum()),
@@ -813,8 +814,8 @@ def main():
     ap.add_argument("--ens-steps", type=int, default=2000)
     ap.add_argument("--no-nn", action="store_true", help="skip the learned-correction leg")
     ap.add_argument("--no-tune", action="store_true", help="ensemble: keep the default launch shapes")
-    ap.add_argument("--nn-pairs", type=int, default=9_000_000, help="training pairs (three snapshots)")
-    ap.add_argument("--nn-epochs", type=int, default=8)
+    ap.add_argument("--nn-pairs", type=int, default=12_000_000, help="training pairs (three snapshots)")
+    ap.add_argument("--nn-epochs", type=int, default=24)
     ap.add_argument("--split", type=int, default=3, choices=[0, 1, 2, 3],
                     help="stencil of the plain P3M leg at the metric's force-error operating point (0: skip)")
     ap.add_argument("--split-steps", type=int, default=64, help="timed steps of that leg")

@@ -116,9 +116,10 @@ def test_training_learns_the_mesh_pair_force(net, orc):
 
 @pytest.fixture(scope="module")
 def impact_net(ccmod):
-    """A network trained as the benchmark trains it, on a smaller pool: pairs drawn from the full impact at
-    262,144 particles at full-phase steps 0, 1000 and 3000 (1 M each), 8 epochs; a held-out draw from the
-    last snapshot.  Returns (network, held-out records, labels, the run's particle radius in cells)."""
+    """A network trained as the benchmark trains it: pairs drawn from the full impact at 262,144 particles
+    at full-phase steps 0, 1000 and 3000 (4 M each), 24 epochs at a learning rate of 4e-3; a held-out draw
+    from the last snapshot.  Returns (network, held-out records, labels, the run's particle radius in
+    cells)."""
     from cosmic_collisions_b200 import configs
     from cosmic_collisions_b200.learned import LearnedCorrection
     n = LearnedCorrection(0, seed=2024)
@@ -137,13 +138,13 @@ def impact_net(ccmod):
                 nb.steps(step)
                 done += step
                 nb.analyze(True)
-            n.sample_state(nb, 1_000_000, seed=1000 + k)
+            n.sample_state(nb, 4_000_000, seed=1000 + k)
         n.sample_state(nb, 262_144, seed=9999)
         a_cells = nb.sim.a / (12.0 / 64.0)
     finally:
         nb.close()
-    n.train(0, 3_000_000, epochs=8, tiles_per_cta=1, lr=2e-3)
-    rec, lab = n.read_pool(3_000_000, 262_144)
+    n.train(0, 12_000_000, epochs=24, tiles_per_cta=1, lr=4e-3)
+    rec, lab = n.read_pool(12_000_000, 262_144)
     live = np.isfinite(rec[:, 0])
     yield n, rec[live], lab[live], a_cells
     n.close()
@@ -164,7 +165,7 @@ def test_network_beats_the_table_on_impact_pairs(impact_net, orc):
     print("held-out impact pairs sharing a node: %d; table error %.4e, network error %.4e (%.1f %% lower)"
           % (near.sum(), e_tab, e_net, 100 * (1 - e_net / e_tab)))
     assert near.sum() > 10000
-    assert e_net < e_tab
+    assert e_net < 0.8 * e_tab       # measured: about a third below the table
 
 
 def test_learned_pass_at_half_the_cut_is_no_worse_than_the_plain_pass(impact_net, ccmod):
