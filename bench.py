@@ -492,6 +492,50 @@ def run_ensemble(args, log, rank=0, world=1):
     return line
 
 
+def conservation_run(cc, dev, N, steps=5000, log=None):
+    """The full impact's books over a long run (src/nbody.js:837-850 and the readout of index.html:335-349):
+    the run built, settled and brought in, then `steps` full-phase steps with runTo's synchronous analysis
+    every 360 steps (on the device), the books read at every analysis against the first look in the full
+    phase.  Returns the worst drifts seen and the last ones."""
+    nb = cc.NBody(dev)
+    nb.device_fof = True
+    t0 = time.perf_counter()
+    try:
+        nb.build(cc.make_opt(**impact_opt(N)))
+        while nb.sim.phase == 0:
+            nb.settle_some(64)
+        nb.analyze(True)
+        while nb.sim.phase == 1:
+            nb.rigid_step(0.01)
+        nb.analyze(True)
+        ref = nb.ref
+        rows = []
+        done = 0
+        while done < steps:
+            n = max(1, min(360 - (nb.sim.stepNo - nb.analyzed_at), steps - done))
+            nb.steps(n)
+            done += n
+            if nb.sim.stepNo - nb.analyzed_at >= 360 or done == steps:
+                nb.analyze(True)
+                r = nb.report
+                rows.append({"steps": done, "t": nb.sim.t, "L": (r.L - ref["L"]) / ref["L"],
+                             "balance": ((r.KE + r.PE + r.EL + r.Q) - ref["EQ"]) / ref["scale"],
+                             "drift": r.drift, "largest": r.largest})
+        nb.sync()
+    finally:
+        nb.close()
+    worst = {k: max(abs(x[k]) for x in rows) for k in ("L", "balance", "drift")}
+    out = {"steps": steps, "particles": N, "analyses": len(rows), "t_end": rows[-1]["t"], "wall_s":
+           time.perf_counter() - t0, "worst": worst, "last": rows[-1],
+           "what": "L: angular momentum against the first look of the full phase; balance: (KE + PE + elastic "
+                   "+ heat) less the first look's, over KE - PE; drift: |momentum| / M (the readout's books)"}
+    if log:
+        log("books over %d steps: worst |dL/L| %.2e, |balance| %.2e, drift %.2e" % (steps, worst["L"],
+                                                                                 worst["balance"],
+                                                                                 worst["drift"]))
+    return out
+
+
 def analysis_timing(cc, nb, reps=5):
     """The worker's fof (src/nbody.js:646-893) on the bench's state, with the Morton sort: on the device
     (ccs_fof_device, wall time of the call: it returns the report on the host) and on one host core
@@ -705,6 +749,7 @@ def run_ours(args, rank, world, log):
 
     ferr = force_error(cc, dev, N) if rank == 0 else None
     analysis = analysis_timing(cc, nb) if rank == 0 and not args.no_cpu else None
+    books = conservation_run(cc, dev, N, args.books_steps, log) if rank == 0 and args.books_steps else None
 
     # the learned correction (config 4): train, attach, the same timed steps, the same force sweep
     nn_line = None
@@ -794,6 +839,7 @@ def run_ours(args, rank, world, log):
         "analysis": analysis,
         "nn_corrected": nn_line,
         "plain_1e3": split_line,
+        "conservation": books,
     }
     nb.close()
     return line, snapshot
@@ -819,6 +865,8 @@ def main():
     ap.add_argument("--split", type=int, default=3, choices=[0, 1, 2, 3],
                     help="stencil of the plain P3M leg at the metric's force-error operating point (0: skip)")
     ap.add_argument("--split-steps", type=int, default=64, help="timed steps of that leg")
+    ap.add_argument("--books-steps", type=int, default=5000,
+                    help="full-phase steps of the conservation run (0: skip)")
     ap.add_argument("--profile", action="store_true",
                     help="prepare, warm up, then run --steps steps inside cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no bench line")

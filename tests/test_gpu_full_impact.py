@@ -1,0 +1,86 @@
+"""The full giant impact at 262,144 particles: its books over a long run, and case B's outcome.
+
+The reference keeps momentum, angular momentum and energy "to a fraction of a percent" (README.md:72,187)
+and shows them in its readout (index.html:335-349): angular momentum against the first look, the energy
+balance (KE + PE + elastic + heat) as a fraction of KE - PE, and the barycentre's drift.  Here the full
+impact is taken through settle and approach and then 5,000 full-phase steps with runTo's synchronous
+analysis every 360 steps (index.html:592-600), the books read at every analysis.  Case B (0.15 M_earth at
+30 degrees, 1.4 v_esc) is run at full size with the same cadence and whether the second mesh box goes up
+(placeBoxes, src/nbody.js:361-374) is recorded.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def advance(nb, steps, rows, ref):
+    done = 0
+    while done < steps:
+        n = max(1, min(360 - (nb.sim.stepNo - nb.analyzed_at), steps - done))
+        nb.steps(n)
+        done += n
+        if nb.sim.stepNo - nb.analyzed_at >= 360 or done == steps:
+            nb.analyze(True)
+            r = nb.report
+            rows.append((nb.sim.stepNo, nb.sim.t, (r.L - ref["L"]) / ref["L"],
+                         ((r.KE + r.PE + r.EL + r.Q) - ref["EQ"]) / ref["scale"], r.drift, r.largest,
+                         int(nb.sim.boxOn[1]), r.secMass))
+
+
+def into_full_phase(ccmod, opt):
+    nb = ccmod.NBody(0)
+    nb.device_fof = True
+    nb.build(opt)
+    while nb.sim.phase == 0:
+        nb.settle_some(64)
+    nb.analyze(True)
+    while nb.sim.phase == 1:
+        nb.rigid_step(0.01)
+    nb.analyze(True)
+    return nb
+
+
+def test_full_impact_5000_steps_keeps_its_books(ccmod):
+    from cosmic_collisions_b200 import configs
+    nb = into_full_phase(ccmod, configs.full_impact_opt(262144))
+    rows = []
+    try:
+        ref = dict(nb.ref)
+        advance(nb, 5000, rows, ref)
+        st = nb.read_state()
+    finally:
+        nb.close()
+    rows = np.array([r[:6] for r in rows])
+    worst = np.abs(rows[:, 2:5]).max(0)
+    print("262k impact, 5000 steps to t = %.2f: worst |dL/L| %.3e, |balance| %.3e, drift %.3e; largest %.4f"
+          % (rows[-1, 1], worst[0], worst[1], worst[2], rows[-1, 5]))
+    assert np.isfinite(st["pos"]).all() and np.isfinite(st["vel"]).all()
+    assert len(rows) >= 13
+    assert worst[0] < 1e-3          # angular momentum to a tenth of a per cent
+    assert worst[1] < 1e-2          # the energy balance to a per cent of KE - PE
+    assert worst[2] < 1e-4          # the barycentre barely moves
+
+
+def test_case_b_at_full_size(ccmod):
+    """Case B at 262,144 particles to t = 16: the outcome recorded, the step sound throughout; the second
+    box's rule is exercised either way (it goes up only on a separating body above 0.05 M_earth)."""
+    from cosmic_collisions_b200 import configs
+    nb = into_full_phase(ccmod, configs.full_impact_opt(262144, case="B"))
+    rows = []
+    try:
+        ref = dict(nb.ref)
+        while nb.sim.t < 16.0:
+            advance(nb, 720, rows, ref)
+        st = nb.read_state()
+    finally:
+        nb.close()
+    up = [r for r in rows if r[6]]
+    print("case B at 262k: %d analyses to t = %.2f; second box up at %s; last: largest %.4f, second %.4f, "
+          "|dL/L| %.2e" % (len(rows), rows[-1][1], ("t = %.2f" % up[0][1]) if up else "never",
+                           rows[-1][5], rows[-1][7], rows[-1][2]))
+    assert np.isfinite(st["pos"]).all() and np.isfinite(st["vel"]).all()
+    for r in rows:
+        if r[6]:
+            assert r[7] > 0.05      # the second box rides only a body the mesh can hold on its own
+    assert max(abs(r[2]) for r in rows) < 5e-3
