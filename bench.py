@@ -492,7 +492,7 @@ def run_ensemble(args, log, rank=0, world=1):
     return line
 
 
-def conservation_run(cc, dev, N, steps=5000, log=None):
+def conservation_run(cc, dev, N, steps=5000, log=None, split=0):
     """The full impact's books over a long run (src/nbody.js:837-850 and the readout of index.html:335-349):
     the run built, settled and brought in, then `steps` full-phase steps with runTo's synchronous analysis
     every 360 steps (on the device), the books read at every analysis against the first look in the full
@@ -507,6 +507,10 @@ def conservation_run(cc, dev, N, steps=5000, log=None):
         nb.analyze(True)
         while nb.sim.phase == 1:
             nb.rigid_step(0.01)
+        if split:
+            nb.set_pp_split(split)     # the books' first look is taken with the form's own potential
+            nb.steps(8)
+            nb.ref = None
         nb.analyze(True)
         ref = nb.ref
         rows = []
@@ -525,7 +529,7 @@ def conservation_run(cc, dev, N, steps=5000, log=None):
     finally:
         nb.close()
     worst = {k: max(abs(x[k]) for x in rows) for k in ("L", "balance", "drift")}
-    out = {"steps": steps, "particles": N, "analyses": len(rows), "t_end": rows[-1]["t"], "wall_s":
+    out = {"steps": steps, "particles": N, "stencil": split, "analyses": len(rows), "t_end": rows[-1]["t"], "wall_s":
            time.perf_counter() - t0, "worst": worst, "last": rows[-1],
            "what": "L: angular momentum against the first look of the full phase; balance: (KE + PE + elastic "
                    "+ heat) less the first look's, over KE - PE; drift: |momentum| / M (the readout's books)"}
@@ -749,7 +753,12 @@ def run_ours(args, rank, world, log):
 
     ferr = force_error(cc, dev, N) if rank == 0 else None
     analysis = analysis_timing(cc, nb) if rank == 0 and not args.no_cpu else None
-    books = conservation_run(cc, dev, N, args.books_steps, log) if rank == 0 and args.books_steps else None
+    books = None
+    if rank == 0 and args.books_steps:
+        books = conservation_run(cc, dev, N, args.books_steps, log)
+        if args.split:
+            books = {"reference_form": books,
+                     "stencil_split": conservation_run(cc, dev, N, args.books_steps, log, split=args.split)}
 
     # the learned correction (config 4): train, attach, the same timed steps, the same force sweep
     nn_line = None

@@ -701,9 +701,11 @@ __global__ void k_nn_image(const float *__restrict__ params, uint8_t *__restrict
 
 // ---------------------------------------------------------------------------
 // the learned P3M pass over the loose list (the pass of src/glsl-sim.js:
-// 676-754 with the table's force replaced): pairs inside half the cut are
-// enumerated in (target, source) order, the network evaluates the mesh part of
-// every pair, and each target's pairs are summed by one warp.
+// 676-754 with the table's force replaced by the network's inside half the
+// cut): pairs inside half the cut are enumerated in (target, source) order,
+// the network evaluates the mesh part of every one, and each target's pairs --
+// those and the list members out to the full cut, with the table -- are summed
+// by one warp.
 // ---------------------------------------------------------------------------
 // count pass (pairs == nullptr) and fill pass: one warp per target, the lanes test 32 consecutive sources
 // at a time; ballot prefix sums keep each target's pairs in ascending source order
@@ -778,7 +780,10 @@ __global__ void __launch_bounds__(1024) k_nn_pp_scan(const ccs_uniforms *__restr
   }
 }
 
-// one warp per target: the lanes take every 32nd of its pairs, then a fixed shuffle tree adds the lanes
+// one warp per target: the lanes take every 32nd of its pairs inside half the cut (the network's model of
+// the mesh's pull, blended into the table's by tau_in from 0.8 of the half cut out to it), then every 32nd
+// list member between the half cut and the cut (the plain pass's table, tapered to the cut); a fixed
+// shuffle tree adds the lanes
 __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__restrict__ U,
                                                       const float4 *__restrict__ list, const float *__restrict__ box,
                                                       int cap, const float2 *__restrict__ tab,
@@ -793,34 +798,55 @@ __global__ void __launch_bounds__(256) k_nn_pp_reduce(const ccs_uniforms *__rest
   const float4 P = list[me];
   if (P.w != 0.0f) {
     const float myBox = box[me];
-    const float cutN = xmul(0.5f, u.cut), a2 = u.a2, a = fsqrt(a2);
-    const float binScale = fdiv(64.0f, u.cut), taperScale = fdiv(1.0f, 0.8f * cutN - cutN);
+    const float cut = u.cut, cutN = xmul(0.5f, cut), a2 = u.a2, a = fsqrt(a2);
+    const float cut2 = xmul(cut, cut), cutN2 = xmul(cutN, cutN);
+    const float binScale = fdiv(64.0f, cut), inScale = fdiv(1.0f, 0.8f * cutN - cutN),
+                outScale = fdiv(1.0f, 0.8f * cut - cut);
     const float invH2 = u.invH * u.invH, eps2Cell = u.eps2Cell;
     f3 acc = mk(0, 0, 0);
     float pot = 0.0f;
+    // a pair's pull and potential: Newton softened at a, less the mesh's own as the network (weight tin) and
+    // the table (the rest) model it, tapered to the cut
+    auto pair = [&](const float4 Q, const f3 d, float r2, float tin, const float4 R, float bj) {
+      const float r = fsqrt(r2);
+      const float invN = rsqrtf(r2 + a2);
+      const float to = clampf((r - cut) * outScale, 0.0f, 1.0f);
+      const float tout = to * to * (3.0f - 2.0f * to);
+      f3 f = d * (invN * invN * invN * tout);
+      float Ty = 0.0f;
+      if (myBox >= 0.0f && bj == myBox) {
+        const float xx = clampf(r * binScale - 0.5f, 0.0f, 63.0f);
+        const int k = (int)xx, k1 = min(k + 1, 63);
+        const float tt = xx - (float)k;
+        const float2 ta = tab[k], tb = tab[k1];
+        const float Tx = ta.x + (tb.x - ta.x) * tt;
+        Ty = ta.y + (tb.y - ta.y) * tt;
+        const f3 table = d * (fdiv(1.0f, fmaxf(r, 1e-6f)) * fdiv(Tx, fmaxf(r2, a2)));
+        f = f - table * ((1.0f - tin) * tout);
+        if (tin > 0.0f) {
+          const float qn = rsqrtf(r2 + eps2Cell);
+          f = f - (d * (qn * qn * qn) + mk(R.x, R.y, R.z) * invH2) * tin;
+        }
+      }
+      acc = acc + f * Q.w;
+      pot += Q.w * (-invN - fdiv(Ty, fmaxf(r, a))) * tout;
+    };
     const int q0 = offs[me], q1 = offs[me + 1];
-    for (int q = q0 + lane; q < q1; q += 32) {
+    for (int q = q0 + lane; q < q1; q += 32) {   // inside half the cut: the network's pairs
       const int j = pairs[q].y;
       const float4 Q = list[j];
       const f3 d = xsub3(xyz(Q), xyz(P));
       const float r2 = xdot(d, d);
-      const float r = fsqrt(r2);
-      const float invN = rsqrtf(r2 + a2);
-      const float ts = clampf((r - cutN) * taperScale, 0.0f, 1.0f);
-      const float taper = ts * ts * (3.0f - 2.0f * ts);
-      const bool same = myBox >= 0.0f && box[j] == myBox;
-      f3 f = d * (invN * invN * invN);
-      float Ty = 0.0f;
-      if (same) {   // the mesh's own pull: node-softened Newton plus what the network learned
-        const float qn = rsqrtf(r2 + eps2Cell);
-        const float4 R = mesh[q];
-        f = f - d * (qn * qn * qn) - mk(R.x, R.y, R.z) * invH2;
-        const float xx = clampf(r * binScale - 0.5f, 0.0f, 63.0f);
-        const int k = (int)xx, k1 = min(k + 1, 63);
-        Ty = tab[k].y + (tab[k1].y - tab[k].y) * (xx - (float)k);
-      }
-      acc = acc + f * (Q.w * taper);
-      pot += Q.w * (-invN - fdiv(Ty, fmaxf(r, a))) * taper;
+      const float ti = clampf((fsqrt(r2) - cutN) * inScale, 0.0f, 1.0f);
+      pair(Q, d, r2, ti * ti * (3.0f - 2.0f * ti), mesh[q], box[j]);
+    }
+    for (int j = lane; j < count; j += 32) {     // between half the cut and the cut: the table
+      if (j == me) continue;
+      const float4 Q = list[j];
+      const f3 d = xsub3(xyz(Q), xyz(P));
+      const float r2 = xdot(d, d);
+      if (r2 < cutN2 || r2 >= cut2) continue;
+      pair(Q, d, r2, 0.0f, make_float4(0, 0, 0, 0), box[j]);
     }
 #pragma unroll
     for (int sh = 16; sh >= 1; sh >>= 1) {

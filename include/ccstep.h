@@ -249,10 +249,12 @@ int ccs_pp_force_static(const float *list4, const float *box, int n, const float
  * the rest: d the pair offset in mesh cells (source - target), s the source's
  * position in its cell; 6 -> 64 -> 64 -> 3 with SiLU, BF16 weights, FP32
  * accumulation, run and trained on the tensor cores.  With a network
- * attached, the P3M pass of an engine corrects the loose pairs inside
- * CCS_NN_CUT_CELLS cells (half the plain pass's 5) by m_j (N_a(d) -
- * d/(r^2 + FH^2/2)^(3/2) - R(d, s)/FH^2) taper (the potential keeps the
- * table's); detaching it restores the plain pass.  Flat parameter order:
+ * attached, the P3M pass of an engine models the mesh's pull on the loose
+ * pairs inside CCS_NN_CUT_CELLS cells (half the plain pass's 5) by
+ * d/(r^2 + FH^2/2)^(3/2) + R(d, s)/FH^2 instead of the table (blended into
+ * the table by a smoothstep from 0.8 of those cells out to them) and keeps the
+ * table beyond, out to the plain cut; the potential keeps the table's.
+ * Detaching it restores the plain pass.  Flat parameter order:
  * W1[64][6] b1[64] W2[64][64] b2[64] W3[3][64] b3[3]. */
 #define CCS_NN_PARAMS 4803
 #define CCS_NN_CUT_CELLS 2.5

@@ -16,9 +16,12 @@ gradients and the learned P3M pass can be checked against it:
 The network's target is the isolated pair's mesh force (meshPairTable's
 field(), src/nbody.js:60-91; orc_nn_label) less the node-softened Newton
 force d / (r^2 + 1/2)^1.5 in cells (softened_newton).  The learned P3M pass
-follows src/glsl-sim.js:676-754 at half the cut: for loose pairs inside 2.5
-cells, acc += m_j (d / (r^2 + a^2)^1.5 - same * (d / (r^2 + FH^2/2)^1.5 +
-y(d, s) / FH^2)) taper; pot is the plain pass's; times Gm; one slice.
+follows src/glsl-sim.js:676-754 with the table's model of the mesh's pull
+replaced by the network's inside half the cut: acc += m_j (N_a(d) tau_out -
+same * (tau_in (d / (r^2 + FH^2/2)^1.5 + y(d, s) / FH^2) + (1 - tau_in)
+tau_out T(r))), tau_in the smoothstep from 0.8 of the half cut to it, tau_out
+the plain pass's taper to the full cut; pot is the plain pass's; times Gm;
+one slice.
 """
 import numpy as np
 
@@ -125,21 +128,30 @@ def target(rec, mesh):
 
 def pp_nn(u, list4, box, count, tab, params, box_of):
     """The learned P3M pass over a loose list of `count` entries: force slice 0 (count x 4, binary64).
+    The network's model of the mesh's pull replaces the pair table's inside half the cut (weight tau_in,
+    smoothstep from 0.8 of the half cut to the half cut); beyond it the pass is the plain one (the table,
+    tapered to the full cut as PPFORCE_FS does, src/glsl-sim.js:738-750).
     u: the oracle's uniforms; box_of(u, p) -> (box, g) the oracle's GLSL_BOX."""
     list4 = np.asarray(list4, np.float32)
     cut = np.float32(u.cut)
     cutN = np.float32(np.float32(0.5) * cut)
-    cut2 = np.float32(cutN * cutN)
+    cutN2 = np.float32(cutN * cutN)
+    cut2 = np.float32(cut * cut)
     a2 = float(u.a2)
     a = np.sqrt(a2)
     invH = float(u.invH)
     out = np.zeros((count, 4))
     g = [box_of(u, list4[j, :3])[1] for j in range(count)]
+
+    def smooth(e0, e1, x):
+        t = min(max((x - e0) / (e1 - e0), 0.0), 1.0)
+        return t * t * (3.0 - 2.0 * t)
+
     for i in range(count):
         P = list4[i]
         if P[3] == 0.0:
             continue
-        js, recs = [], []
+        js, recs, inner = [], [], []
         for j in range(count):
             if j == i:
                 continue
@@ -148,6 +160,7 @@ def pp_nn(u, list4, box, count, tab, params, box_of):
             if r2 >= cut2:
                 continue
             js.append(j)
+            inner.append(r2 < cutN2)
             dc = (list4[j, :3].astype(np.float64) - P[:3]) * invH
             s = g[j] - np.floor(g[j])
             recs.append([dc[0], dc[1], dc[2], s[0], s[1], s[2]])
@@ -162,19 +175,22 @@ def pp_nn(u, list4, box, count, tab, params, box_of):
             r2 = float(d @ d)
             r = np.sqrt(r2)
             invN = 1.0 / np.sqrt(r2 + a2)
-            ts = min(max((r - cutN) / (0.8 * cutN - cutN), 0.0), 1.0)
-            taper = ts * ts * (3.0 - 2.0 * ts)
+            tau_out = smooth(float(cut), 0.8 * float(cut), r)
+            tau_in = smooth(float(cutN), 0.8 * float(cutN), r) if inner[q] else 0.0
             same = box[i] >= 0 and box[j] == box[i]
-            f = d * invN ** 3
+            f = d * invN ** 3 * tau_out
             Ty = 0.0
             if same:
-                f = f - d / (r2 + float(u.eps2Cell)) ** 1.5 - y[q] * invH * invH
                 xx = min(max(r * 64.0 / cut - 0.5, 0.0), 63.0)
                 k = int(xx)
                 k1 = min(k + 1, 63)
+                Tx = tab[k, 0] + (tab[k1, 0] - tab[k, 0]) * (xx - k)
                 Ty = tab[k, 1] + (tab[k1, 1] - tab[k, 1]) * (xx - k)
-            acc += f * (Q[3] * taper)
-            pot += Q[3] * (-invN - Ty / max(r, a)) * taper
+                table = d / max(r, 1e-6) * Tx / max(r2, a2)
+                learned = d / (r2 + float(u.eps2Cell)) ** 1.5 + y[q] * invH * invH
+                f = f - tau_in * learned - (1.0 - tau_in) * tau_out * table
+            acc += f * Q[3]
+            pot += Q[3] * (-invN - Ty / max(r, a)) * tau_out
         out[i, :3] = acc * u.Gm
         out[i, 3] = pot * u.Gm
     return out
