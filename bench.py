@@ -655,25 +655,39 @@ def run_ours(args, rank, world, log):
     nb.steps(args.warmup)
     nb.sync()
     if args.profile:
-        # for `ncu --profile-from-start off`: only these steps are profiled; without --no-nn the learned
-        # pass is attached (a network trained briefly on the same impact)
+        # for `ncu --profile-from-start off`: only the chosen leg's work between cudaProfilerStart and Stop is
+        # profiled -- plain: --steps steps of the reference's P3M; split: one warm 8-step block, then --steps
+        # steps of the stencil-split form (--split); learned: the learned pass attached (a network trained
+        # briefly on the same impact), then --steps steps; train: one training epoch of that network over 1 M
+        # pairs drawn from the state and a forward pass over 131,072 of them
         net = None
-        if not args.no_nn:
-            net, _ = learned_correction(cc, dev, N, log, pairs=300_000, epochs=2, snaps=(0,), held=16384)
+        if args.profile_leg in ("learned", "train"):
+            net, _ = learned_correction(cc, dev, N, log, pairs=1_000_000 if args.profile_leg == "train" else 300_000,
+                                        epochs=2, snaps=(0,), held=131072)
+        if args.profile_leg == "learned":
             nb.set_pp_nn(net)
-            for _ in range(args.warmup):
-                nb.step(False, False)
-                nb.sim.t += nb.sim.dt
-            nb.sync()
-        l0 = lib.ccs_launch_count(nb.handle)
-        torch.cuda.profiler.start()
-        for _ in range(args.steps):
+        if args.profile_leg == "split":
+            nb.set_pp_split(args.split or 3)
+            nb.steps(8)
+        for _ in range(args.warmup):
             nb.step(False, False)
             nb.sim.t += nb.sim.dt
         nb.sync()
+        l0 = lib.ccs_launch_count(nb.handle)
+        torch.cuda.profiler.start()
+        if args.profile_leg == "train":
+            rec, _ = net.read_pool(0, 131072)
+            net.train(0, 1_000_000, epochs=1, tiles_per_cta=1, lr=4e-3)
+            net.forward(rec)
+        else:
+            for _ in range(args.steps):
+                nb.step(False, False)
+                nb.sim.t += nb.sim.dt
+        nb.sync()
         torch.cuda.profiler.stop()
-        out = {"profile": True, "steps": args.steps, "gpu_launches": int(lib.ccs_launch_count(nb.handle) - l0),
-               "stepNo": nb.sim.stepNo, "loose_list": nb.pp["count"], "learned": net is not None}
+        out = {"profile": True, "leg": args.profile_leg, "steps": args.steps,
+               "gpu_launches": int(lib.ccs_launch_count(nb.handle) - l0), "stepNo": nb.sim.stepNo,
+               "loose_list": nb.pp["count"]}
         nb.set_pp_nn(None)
         nb.close()
         if net is not None:
@@ -876,6 +890,8 @@ def main():
     ap.add_argument("--split-steps", type=int, default=64, help="timed steps of that leg")
     ap.add_argument("--books-steps", type=int, default=5000,
                     help="full-phase steps of the conservation run (0: skip)")
+    ap.add_argument("--profile-leg", default="plain", choices=["plain", "split", "learned", "train"],
+                    help="what --profile runs between cudaProfilerStart and Stop")
     ap.add_argument("--profile", action="store_true",
                     help="prepare, warm up, then run --steps steps inside cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no bench line")
