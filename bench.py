@@ -62,13 +62,11 @@ METRIC = "particle-steps/s @262k, plain vs NN-corrected P\u00b3M at \u22641e-3 f
 
 
 def sample_every(steps):
-    """The stride of the contact-step sample inside the timed region: odd, so coprime with the 8-step cycle
-    and the samples cover every step of it; 9 when that still gives MIN_SAMPLES samples, else the largest
-    odd stride that does (1: every launch)."""
-    for every in (9, 7, 5, 3):
-        if steps // every >= MIN_SAMPLES:
-            return every
-    return 1
+    """The stride of the contact-step sample inside the timed region: 9 (coprime with the 8-step cycle, so the
+    samples cover every step of it) when that gives MIN_SAMPLES samples; 0 for a shorter run, whose contact
+    step is timed in a pass of its own after the region instead (a sampled launch leaves its step's graph
+    for a direct launch between two events, which a short run would feel)."""
+    return 9 if steps // 9 >= MIN_SAMPLES else 0
 
 
 def impact_opt(N):
@@ -590,15 +588,15 @@ def timed_steps(nb, lib, stream, flush, steps, dev, dist):
     import ctypes as C
     import torch
     every = sample_every(steps)
-    warm_step_graphs(nb, lib, every)
+    warm_step_graphs(nb, lib, every or 1)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     clocks = Clocks(dev)
     if dist:
         import torch.distributed as td
         td.barrier()
     torch.cuda.synchronize()
-    lib.ccs_timing_every(nb.handle, every)
-    lib.ccs_timing(nb.handle, 1)            # kernel id 0, the contact step
+    lib.ccs_timing_every(nb.handle, max(every, 1))
+    lib.ccs_timing(nb.handle, 1 if every else 0)   # kernel id 0, the contact step (sampled) or nothing
     l0 = lib.ccs_launch_count(nb.handle)
     clocks.start()
     w0 = time.perf_counter()
@@ -625,6 +623,15 @@ def timed_steps(nb, lib, stream, flush, steps, dev, dist):
             lib.ccs_timing_read(nb.handle, kid, C.byref(tot), C.byref(cnt))
             kt[names[kid]] = {"launches": cnt.value, "total_ms": tot.value,
                               "mean_us": 1e3 * tot.value / cnt.value if cnt.value else None}
+    if not every:   # a short region: the contact step on MIN_SAMPLES + 8 launches of its own, L2 flushed before each
+        lib.ccs_timing_every(nb.handle, 1)
+        lib.ccs_timing(nb.handle, 1)
+        for k in range(MIN_SAMPLES + 8):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+            nb.step(False, False)
+            nb.sim.t += nb.sim.dt
+        nb.sync()
     read([0])
     kt["simulate"]["every"] = every
     lib.ccs_timing_every(nb.handle, 1)
@@ -853,8 +860,10 @@ def run_ours(args, rank, world, log):
                      "traffic": tpp * N if tpp else None,
                      "algorithmic_bytes_per_launch": ALG_BYTES_SIM * N,
                      "timed_launches": kt["simulate"]["launches"],
-                     "timing": "CUDA events on the library's stream around every %d-th contact step of the timed "
-                               "region" % kt["simulate"]["every"],
+                     "timing": ("CUDA events on the library's stream around every %d-th contact step of the timed "
+                                "region" % kt["simulate"]["every"]) if kt["simulate"]["every"] else
+                               "CUDA events on the library's stream around each of %d contact steps in a pass of their "
+                               "own after the timed region, L2 flushed before each" % kt["simulate"]["launches"],
                      "limiter": limiter_note()},
         "gpu_launches": int(launches),
         "clocks": clk,
