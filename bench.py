@@ -565,12 +565,12 @@ def analysis_timing(cc, nb, reps=5):
 
 def warm_step_graphs(nb, lib, every):
     """Capture, before anything is timed, every step graph the timed loop replays: the loop times the contact
-    step on every `every`-th launch (a graph that stops before it) and replays whole-step graphs otherwise,
-    keyed by the step's place in the 8-step cycle and the buffers it touches, so 2 x 8 x every steps of the
-    same loop visit every key."""
-    lib.ccs_timing_every(nb.handle, every)
-    lib.ccs_timing(nb.handle, 1)
-    for _ in range(2 * 8 * every):
+    step on every `every`-th launch (a graph that stops before it; every = 0: none) and replays whole-step
+    graphs otherwise, keyed by the step's place in the 8-step cycle and the buffers it touches, so
+    2 x 8 x max(every, 1) steps of the same loop visit every key."""
+    lib.ccs_timing_every(nb.handle, max(every, 1))
+    lib.ccs_timing(nb.handle, 1 if every else 0)
+    for _ in range(2 * 8 * max(every, 1)):
         nb.step(False, False)
         nb.sim.t += nb.sim.dt
     nb.sync()
@@ -588,7 +588,7 @@ def timed_steps(nb, lib, stream, flush, steps, dev, dist):
     import ctypes as C
     import torch
     every = sample_every(steps)
-    warm_step_graphs(nb, lib, every or 1)
+    warm_step_graphs(nb, lib, every)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     clocks = Clocks(dev)
     if dist:
