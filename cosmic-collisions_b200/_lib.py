@@ -26,7 +26,7 @@ COARSE = 4096
 
 BUF = {"seats": 5, "fineA": 6, "forceA": 7, "monoA": 8, "coarseA": 9, "farA": 10, "fineB": 11, "forceB": 12,
        "monoB": 13, "pplist": 14, "ppforce": 15, "ppbox": 16, "ppslot": 17, "diag": 18, "cellof": 19,
-       "tide0A": 20, "tide1A": 21, "ppall": 22}
+       "tide0A": 20, "tide1A": 21, "ppall": 22, "walkstats": 23, "walkcount": 24}
 
 # every symbol include/ccstep.h declares
 EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_make_bodies", "ccs_make_bodies_device",
@@ -43,7 +43,8 @@ EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_ma
            "ccs_ensemble_create", "ccs_ensemble_destroy", "ccs_ensemble_last_error", "ccs_ensemble_steps",
            "ccs_ensemble_sync", "ccs_ensemble_autotune", "ccs_fof_device", "ccs_set_field",
            "ccs_checkpoint_size", "ccs_checkpoint_save", "ccs_checkpoint_load", "ccs_timing_every",
-           "ccs_set_boxes", "ccs_set_graphs", "ccs_contact_pairs", "ccs_set_pp_split"]
+           "ccs_set_boxes", "ccs_set_graphs", "ccs_contact_pairs", "ccs_set_pp_split",
+           "ccs_set_contact_walk"]
 NN_PARAMS = 4803
 NN_CUT_CELLS = 2.5
 
@@ -220,6 +221,7 @@ def lib():
         "ccs_set_graphs": (I, [H, I]),
         "ccs_contact_pairs": (I, [H, I, P, P]),
         "ccs_set_pp_split": (I, [H, I]),
+        "ccs_set_contact_walk": (I, [H, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

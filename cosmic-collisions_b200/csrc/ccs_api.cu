@@ -68,7 +68,7 @@ struct GraphSlot {
 
 // one step's launches captured as a graph (ccs_step): its schedule, the buffers it reads and writes
 struct StepKey {
-  int slots, mesh, boxB, pp, nn, seatCur, cur, ping, field, timed;
+  int slots, mesh, boxB, pp, nn, seatCur, cur, ping, field, timed, walk;
   bool operator<(const StepKey &o) const {
     return std::memcmp(this, &o, sizeof *this) < 0;
   }
@@ -99,6 +99,14 @@ struct ccs_handle {
   float4 *home = nullptr, *homeTmp = nullptr;
   float4 *part = nullptr;   // a split mesh step's contact sums (SimArgs::part, part2)
   float2 *part2 = nullptr;
+  // the contact walk's record (SimArgs::rec ...): made by a step that rebuilt the grid, replayed by the next.
+  // recValid: the last step made it and nothing has moved or reordered the particles since
+  uint32_t *rec = nullptr;
+  int *recN = nullptr;
+  float4 *recP = nullptr;
+  unsigned *recMax = nullptr, *recStats = nullptr;
+  int walkMode = 1;   // ccs_set_contact_walk
+  bool recValid = false;
   // contact grid: two seat tables used in turn, and the cell each particle went to
   uint32_t *seats[2] = {}, *hk[2] = {};
   int seatCur = 0;
@@ -114,6 +122,7 @@ struct ccs_handle {
   // pass's sorted sources, start offsets and occupied target nodes, and every particle's pair sum
   int ppSplit = 0;
   int *splitStart = nullptr, *splitCells = nullptr, *splitNCells = nullptr;
+  unsigned char *splitWork = nullptr;   // the pair pass's items and counters (split_work_bytes)
   float4 *splitSrc = nullptr, *splitSrcT = nullptr, *ppAll = nullptr;
   // the learned form of the P3M pass (borrowed network; pair buffers sized for the list)
   ccs_nn *nn = nullptr;
@@ -396,8 +405,8 @@ void pass_slots(ccs_handle *h, const ccs_uniforms &u) {
   cudaEvent_t b, e;
   time_begin(h, 1, &b, &e);
   h->launches += launch_contact_grid(u, h->N, h->pos[h->cur], h->seats[nxt], h->hk[nxt], h->seats[h->seatCur],
-                                     h->hk[h->seatCur], h->status, h->st);
-  record_uniform_node(h, 7);
+                                     h->hk[h->seatCur], h->status, h->recMax, h->st);
+  record_uniform_node(h, 8);
   time_end(h, e);
   h->seatCur = nxt;
 }
@@ -431,7 +440,7 @@ void pass_pp(ccs_handle *h, const ccs_uniforms *U, int count) {
     time_begin(h, 4, &b, &e);
     h->launches += launch_pp_split(U, h->N, h->ppSplit, h->pos[h->cur], h->mat, h->keys, h->vals, h->keysTmp,
                                    h->valsTmp, h->hist, h->splitStart, h->splitSrc, h->splitSrcT, h->splitCells,
-                                   h->splitNCells, h->ppAll, h->st);
+                                   h->splitNCells, h->splitWork, h->ppAll, h->st);
     time_end(h, e);
     return;
   }
@@ -477,11 +486,37 @@ SimArgs sim_args(const ccs_handle *h) {
   a.fineA = h->pm[0].fine;
   a.fineB = h->pm[1].fine;
   a.ppAll = h->ppAll;
+  a.rec = h->rec;
+  a.recN = h->recN;
+  a.recP = h->recP;
+  a.recMax = h->recMax;
+  a.recStats = h->walkMode == 2 ? h->recStats : nullptr;
+  // The record holds every pair the next step's walk can find while the owner has moved at most mu and
+  // every particle at most D since the rebuild, mu + D below the margin by which the cull's reach (cell +
+  // SEAT_SLACK a) exceeds the link radius (cell) plus the seat's quantisation (half the diagonal of a
+  // fifteenth of a cell), less rounding.  Without that margin nothing is recorded or replayed.
+  const double margin = kSeatSlack * h->sim.a - std::sqrt(3.0) / 30.0 * h->sim.cell - 1e-4 * h->sim.cell;
+  if (margin > 0.0) {
+    const double mu = 0.35 * margin, D = 0.55 * margin;
+    a.recLink2 = (float)((h->sim.cell + mu) * (h->sim.cell + mu));
+    a.recMove2 = (float)(0.95 * mu * 0.95 * mu);
+    a.recAll2 = (float)(0.95 * D * 0.95 * D);
+  }
+  a.walk = 0;
   return a;
 }
 
-void pass_sim(ccs_handle *h, const ccs_uniforms &u) {
-  const SimArgs a = sim_args(h);
+// the walk a step's contact step runs (SimArgs::walk): a step that rebuilds the grid records, the next one
+// replays what was recorded, while the record is good (ccs_set_contact_walk 1 or 2)
+int step_walk(const ccs_handle *h, bool slots) {
+  if (!h->walkMode || !h->rec) return 0;
+  if (kSeatSlack * h->sim.a - std::sqrt(3.0) / 30.0 * h->sim.cell - 1e-4 * h->sim.cell <= 0.0) return 0;
+  return slots ? 1 : (h->recValid ? 2 : 0);
+}
+
+void pass_sim(ccs_handle *h, const ccs_uniforms &u, int walk = 0) {
+  SimArgs a = sim_args(h);
+  a.walk = walk;
   if (h->ppSplit && !h->field && h->part && h->part2) {   // the stencil-split P3M's contact step: walk + tail
     h->launches += launch_contacts_only(u, h->N, a, h->st, h->tuneWarps);
     h->launches += launch_contact_tail(u, h->N, a, h->st, true);
@@ -519,6 +554,7 @@ void pass_diag_kernel(ccs_handle *h, const ccs_uniforms *U) {
 struct StepPlan {
   ccs_uniforms u;
   bool slots, mesh;
+  int walk;   // SimArgs::walk of its contact step
 };
 StepPlan plan_step(ccs_handle *h, int settle, int kick) {
   ccs_sim &s = h->sim;
@@ -528,6 +564,8 @@ StepPlan plan_step(ccs_handle *h, int settle, int kick) {
     p.slots = n % 2 == 0;
     p.mesh = false;
     p.u = pass_uniforms(h, settle, kick, s.dt);
+    p.walk = step_walk(h, p.slots);
+    h->recValid = p.walk == 1;
     return p;
   }
   if (!settle && !kick && !s.soft && s.t - s.impactT > 1.5) soften(h);
@@ -536,6 +574,8 @@ StepPlan plan_step(ccs_handle *h, int settle, int kick) {
   p.mesh = n % h->meshEvery == 0;
   if (p.mesh) set_boxes(h);
   p.u = pass_uniforms(h, settle, kick, p.mesh ? h->meshEvery * s.dt : 0.0);
+  p.walk = step_walk(h, p.slots);
+  h->recValid = p.walk == 1;
   return p;
 }
 
@@ -608,7 +648,8 @@ void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
       h->st = h->side;
     }
     if (p.slots) pass_slots(h, p.u);
-    const SimArgs a = sim_args(h);
+    SimArgs a = sim_args(h);
+    a.walk = p.walk;
     cudaEvent_t b, e;
     time_begin(h, 5, &b, &e);
     h->launches += launch_contacts_only(p.u, h->N, a, h->st, h->tuneWarps);
@@ -634,7 +675,8 @@ void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
     // the split mesh step with its two halves timed (kernel ids 5 and 6): everything in order on st, so
     // each half sits alone between its events
     if (p.slots) pass_slots(h, p.u);
-    const SimArgs a = sim_args(h);
+    SimArgs a = sim_args(h);
+    a.walk = p.walk;
     cudaEvent_t b, e;
     time_begin(h, 5, &b, &e);
     h->launches += launch_contacts_only(p.u, h->N, a, h->st, h->tuneWarps);
@@ -649,7 +691,7 @@ void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
   }
   if (!p.mesh || !can_split(h) || h->timing || h->inEnsemble) {
     enqueue_pre(h, p, U);
-    pass_sim(h, p.u);
+    pass_sim(h, p.u, p.walk);
     return;
   }
   cudaEventRecord(h->forkEv, h->st);
@@ -657,7 +699,8 @@ void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
   const cudaStream_t main = h->st;
   h->st = h->side;
   if (p.slots) pass_slots(h, p.u);
-  const SimArgs a = sim_args(h);   // the table the grid has just filled
+  SimArgs a = sim_args(h);   // the table the grid has just filled
+  a.walk = p.walk;
   h->launches += launch_contacts_only(p.u, h->N, a, h->st, h->tuneWarps);
   record_uniform_node(h, 2);
   h->st = main;
@@ -714,11 +757,11 @@ int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false) {
   const bool timed = (time_this(h, 0) && !h->ppSplit) || simOutside;
   const bool pre = p.mesh;   // kernels that read the uniforms from device memory (the mesh and pairwise passes)
   if (timed && !p.slots && !p.mesh) {   // nothing to replay: the contact step alone, launched directly
-    if (!simOutside) pass_sim(h, p.u);
+    if (!simOutside) pass_sim(h, p.u, p.walk);
     return check_launch(h);
   }
   const StepKey key{(int)p.slots, (int)p.mesh, (int)(p.u.boxB > 0.5f), h->ppCount > 0, h->nn != nullptr,
-                    h->seatCur, h->cur, h->ping, (int)h->field, (int)timed};
+                    h->seatCur, h->cur, h->ping, (int)h->field, (int)timed, p.walk};
   GraphSlot &g = h->stepGraphs[key];
   const int seatCur0 = h->seatCur, cur0 = h->cur;
   if (!g.exec) {
@@ -792,7 +835,7 @@ int step_graph(ccs_handle *h, const StepPlan &p, bool simOutside = false) {
     --h->launches;            // the caller launches the contact step
   } else if (timed) {
     --h->launches;            // pass_sim counts its own
-    pass_sim(h, p.u);
+    pass_sim(h, p.u, p.walk);
   } else {
     h->cur = cur0 ^ 1;
     if (h->timing & 1) ++h->timingSeq;   // a contact step that was not this sample's
@@ -968,6 +1011,7 @@ int ensure_split_buffers(ccs_handle *h) {
   rc |= dev_alloc(h, &h->splitStart, split_start_ints());
   rc |= dev_alloc(h, &h->splitCells, N);
   rc |= dev_alloc(h, &h->splitNCells, 1);
+  rc |= dev_alloc(h, &h->splitWork, split_work_bytes(h->N));
   rc |= dev_alloc(h, &h->splitSrc, N);
   rc |= dev_alloc(h, &h->splitSrcT, N);
   rc |= dev_alloc(h, &h->ppAll, N);
@@ -977,7 +1021,7 @@ int ensure_split_buffers(ccs_handle *h) {
       dev_free(h->pm[b].quad0); dev_free(h->pm[b].quad1);
     }
     dev_free(h->splitStart); dev_free(h->splitCells); dev_free(h->splitNCells); dev_free(h->splitSrc);
-    dev_free(h->splitSrcT); dev_free(h->ppAll);
+    dev_free(h->splitSrcT); dev_free(h->ppAll); dev_free(h->splitWork);
     return CCS_E_NOMEM;
   }
   for (int b = 0; b < 2; ++b) {
@@ -1001,9 +1045,11 @@ void free_state(ccs_handle *h) {
     dev_free(m.tide0); dev_free(m.tide1); dev_free(m.cellPartT); dev_free(m.quad0); dev_free(m.quad1);
   }
   dev_free(h->splitStart); dev_free(h->splitCells); dev_free(h->splitNCells); dev_free(h->splitSrc);
-  dev_free(h->splitSrcT); dev_free(h->ppAll);
+  dev_free(h->splitSrcT); dev_free(h->ppAll); dev_free(h->splitWork);
   dev_free(h->mat); dev_free(h->matTmp); dev_free(h->home); dev_free(h->homeTmp);
   dev_free(h->part); dev_free(h->part2);
+  dev_free(h->rec); dev_free(h->recN); dev_free(h->recP); dev_free(h->recMax); dev_free(h->recStats);
+  h->recValid = false;
   dev_free(h->ppIndex); dev_free(h->ppSlot); dev_free(h->ppList); dev_free(h->ppForce); dev_free(h->ppBox);
   dev_free(h->ppPart);
   dev_free(h->nnCounts); dev_free(h->nnOffs); dev_free(h->nnTotal); dev_free(h->nnPairs); dev_free(h->nnMesh);
@@ -1113,6 +1159,9 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
   rc |= dev_alloc(h, &h->mat, N); rc |= dev_alloc(h, &h->matTmp, N);
   rc |= dev_alloc(h, &h->home, N); rc |= dev_alloc(h, &h->homeTmp, N);
   rc |= dev_alloc(h, &h->part, N); rc |= dev_alloc(h, &h->part2, N);
+  rc |= dev_alloc(h, &h->rec, (N + 31) / 32 * kRecWarp); rc |= dev_alloc(h, &h->recN, (N + 31) / 32);
+  rc |= dev_alloc(h, &h->recP, N);
+  rc |= dev_alloc(h, &h->recMax, 1); rc |= dev_alloc(h, &h->recStats, 3);
   make_static(h);
   h->ncell = (size_t)h->stat.AW * (size_t)h->stat.AH;
   for (int b = 0; b < 2; ++b) {
@@ -1184,6 +1233,9 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
   CUDA_TRY(h, cudaMemsetAsync(h->ppBox, 0, sizeof(float) * CCS_PP_CAP, st));
   CUDA_TRY(h, cudaMemsetAsync(h->booksPartial, 0, sizeof(double) * books_partial_doubles(h->N), st));
   CUDA_TRY(h, cudaMemsetAsync(h->status, 0, sizeof(unsigned), st));
+  CUDA_TRY(h, cudaMemsetAsync(h->recMax, 0xFF, sizeof(unsigned), st));   // no record yet (a NaN: replay nothing)
+  CUDA_TRY(h, cudaMemsetAsync(h->recStats, 0, 3 * sizeof(unsigned), st));
+  h->recValid = false;
   float f[CCS_PP_BINS], p[CCS_PP_BINS];
   ccs_pair_table(CCS_PP_BINS, kPPCut, f, p);
   float2 tab[CCS_PP_BINS];
@@ -1225,12 +1277,14 @@ int ccs_get_uniforms(ccs_handle *h, ccs_uniforms *out) {
 int ccs_set_mesh_every(ccs_handle *h, int n) {
   if (!h || n < 1 || n > kMaxBlock) return CCS_E_ARG;
   h->meshEvery = n;
+  h->recValid = false;
   return CCS_OK;
 }
 
 int ccs_set_field(ccs_handle *h, int on, const double g[3], double frozen, double invM, double cpIron) {
   if (!h || (on && (!g || !(invM > 0) || !(cpIron > 0)))) return CCS_E_ARG;
   h->field = on != 0;
+  h->recValid = false;
   if (on) {
     for (int k = 0; k < 3; ++k) h->gField[k] = g[k];
     h->frozen = frozen;
@@ -1717,6 +1771,7 @@ int ccs_rigid_step(ccs_handle *h, double dtF) {
   if (rc) return rc;
   if (!(dtF > 0)) return CCS_E_ARG;
   cudaSetDevice(h->device);
+  h->recValid = false;   // the particles move without a contact step
   ccs_sim &s = h->sim;
   double *r = s.relr, *v = s.relv;
   const double M = s.M, M1 = s.M1, M2 = s.M2;
@@ -1892,6 +1947,7 @@ int ccs_set_boxes(ccs_handle *h, const ccs_box boxes[2]) {
 
 static int apply_perm_device(ccs_handle *h, const int32_t *permDev) {
   const int s = h->cur, d = h->cur ^ 1;
+  h->recValid = false;   // the record names particles by their old places
   h->launches += launch_permute(h->N, permDev, h->pos[s], h->vel[s], h->aux[s], h->q[s], h->mat, h->home, h->pos[d],
                                 h->vel[d], h->aux[d], h->q[d], h->matTmp, h->homeTmp, h->st);
   std::swap(h->mat, h->matTmp);
@@ -1941,6 +1997,7 @@ int ccs_sort_morton(ccs_handle *h, const double core[3], int32_t *perm_out, int3
   if (rc) return rc;
   if (!core) return CCS_E_ARG;
   cudaSetDevice(h->device);
+  h->recValid = false;
   const int N = h->N;
   h->launches += launch_morton_keys(N, h->pos[h->cur], core[0], core[1], core[2], h->keys, h->vals, h->st);
   h->launches += launch_radix_sort(N, 21, h->keys, h->vals, h->keysTmp, h->valsTmp, h->hist, h->st);
@@ -2071,6 +2128,7 @@ int ccs_fof_device(ccs_handle *h, double spring, double touch, int cap, int sort
   if (rc) return rc;
   if (!rep || cap < 0 || cap > CCS_PP_CAP || (cap > 0 && !list) || (sort && !perm)) return CCS_E_ARG;
   cudaSetDevice(h->device);
+  if (sort) h->recValid = false;
   rc = ensure_fof_buffers(h);
   if (rc) return rc;
   rc = diag_pass(h);   // the read-outs the books need, as the reference's analysis reads them
@@ -2292,6 +2350,7 @@ int ccs_write_state(ccs_handle *h, const float *pos4, const float *vel4, const f
   int rc = ensure_built(h);
   if (rc) return rc;
   cudaSetDevice(h->device);
+  h->recValid = false;
   const size_t N = (size_t)h->N;
   if (pos4) CUDA_TRY(h, cudaMemcpyAsync(h->pos[h->cur], pos4, 16 * N, cudaMemcpyHostToDevice, h->st));
   if (vel4) CUDA_TRY(h, cudaMemcpyAsync(h->vel[h->cur], vel4, 16 * N, cudaMemcpyHostToDevice, h->st));
@@ -2397,6 +2456,8 @@ int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes) {
     case CCS_BUF_TIDE0_A: src = h->pm[0].tide0; n = 16 * (size_t)(kFine + 1); break;
     case CCS_BUF_TIDE1_A: src = h->pm[0].tide1; n = 16 * (size_t)(kFine + 1); break;
     case CCS_BUF_PP_ALL: src = h->ppAll; n = 16 * N; break;
+    case CCS_BUF_WALK_STATS: src = h->recStats; n = 12; break;
+    case CCS_BUF_WALK_COUNT: src = h->recN; n = 4 * ((N + 31) / 32); break;
     default: h->err = "unknown buffer"; return CCS_E_ARG;
   }
   if (!src) {
@@ -2415,6 +2476,7 @@ int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes) {
 int ccs_pass_slots(ccs_handle *h) {
   int rc = ensure_built(h);
   if (rc) return rc;
+  h->recValid = false;   // passes run by hand neither record nor replay
   pass_slots(h, pass_uniforms(h, 0, 0, 0.0));
   return check_launch(h);
 }
@@ -2422,6 +2484,7 @@ int ccs_pass_slots(ccs_handle *h) {
 int ccs_pass_mesh(ccs_handle *h) {
   int rc = ensure_built(h);
   if (rc) return rc;
+  h->recValid = false;
   set_boxes(h);
   const ccs_uniforms *U;
   rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
@@ -2433,6 +2496,7 @@ int ccs_pass_mesh(ccs_handle *h) {
 int ccs_pass_pp(ccs_handle *h) {
   int rc = ensure_built(h);
   if (rc) return rc;
+  h->recValid = false;
   const ccs_uniforms *U;
   rc = push_uniforms(h, pass_uniforms(h, 0, 0, 0.0), &U);
   if (rc) return rc;
@@ -2443,6 +2507,7 @@ int ccs_pass_pp(ccs_handle *h) {
 int ccs_pass_sim(ccs_handle *h, int settle, int kick, double gdt) {
   int rc = ensure_built(h);
   if (rc) return rc;
+  h->recValid = false;
   pass_sim(h, pass_uniforms(h, settle, kick, gdt));
   return check_launch(h);
 }
@@ -2475,7 +2540,8 @@ static int last_step_overlapped(ccs_handle *h, float *pos4_out, float *vel4_out,
   rc = step_graph(h, p, true);   // the grid, the mesh and the pairwise pass
   if (rc) return rc;
   if (inputsOnCopyStream) CUDA_TRY(h, cudaStreamWaitEvent(h->st, h->inEv, 0));
-  const SimArgs a = sim_args(h);
+  SimArgs a = sim_args(h);
+  a.walk = p.walk;
   const int N = h->N, half = std::min(N, (N / 2 + 255) / 256 * 256), d = h->cur ^ 1;
   h->launches += launch_simulate_range(p.u, N, a, h->st, h->tuneWarps, h->field, 0, half);
   CUDA_TRY(h, cudaEventRecord(h->halfEv, h->st));
@@ -2505,6 +2571,7 @@ int ccs_advance_host(ccs_handle *h, const float *pos4, const float *vel4, const 
   if (rc) return rc;
   if (nsteps < 0) return CCS_E_ARG;
   cudaSetDevice(h->device);
+  if (pos4 || vel4 || q) h->recValid = false;   // a new state: nothing recorded for it
   const size_t N = (size_t)h->N;
   const bool reads = pos4_out || vel4_out || aux4_out || q_out;
   const bool overlapped = nsteps > 0 && reads && h->useGraphs && h->timing == 0 && !h->ppSplit;
@@ -2624,6 +2691,7 @@ int ccs_checkpoint_save(ccs_handle *h, const void *extra, size_t extraBytes, voi
 
 int ccs_checkpoint_load(ccs_handle *h, const void *buf, size_t bytes) {
   if (!h || !buf) return CCS_E_ARG;
+  h->recValid = false;
   ccs_checkpoint_header hd;
   if (bytes < sizeof hd) {
     h->err = "checkpoint: shorter than its header";
@@ -2693,6 +2761,7 @@ int ccs_contact_pairs(ccs_handle *h, int cap, int32_t *counts, uint32_t *pairs) 
   rc = dev_alloc(h, &dp, N * (size_t)cap);
   if (rc) return rc;
   SimArgs a = sim_args(h);   // the current state in, the spare buffers out (the run does not advance)
+  a.walk = step_walk(h, false);   // the walk the next step runs when it does not rebuild the grid
   a.pairs = dp;
   a.pairCap = cap;
   CUDA_TRY(h, cudaMemsetAsync(dp, 0xFF, sizeof(uint32_t) * N * (size_t)cap, h->st));
@@ -2733,6 +2802,18 @@ int ccs_set_pp_split(ccs_handle *h, int S) {
 int ccs_set_graphs(ccs_handle *h, int on) {
   if (!h || (on != 0 && on != 1)) return CCS_E_ARG;
   h->useGraphs = on != 0;
+  return CCS_OK;
+}
+
+int ccs_set_contact_walk(ccs_handle *h, int mode) {
+  if (!h || mode < 0 || mode > 2) return CCS_E_ARG;
+  if (mode == h->walkMode) return CCS_OK;
+  cudaSetDevice(h->device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  free_graphs(h);   // captured steps hold the other walk's kernels and arguments
+  h->walkMode = mode;
+  h->recValid = false;
+  if (mode == 2 && h->recStats) CUDA_TRY(h, cudaMemsetAsync(h->recStats, 0, 3 * sizeof(unsigned), h->st));
   return CCS_OK;
 }
 

@@ -27,6 +27,27 @@
 // The pair set and the neighbour counts are decided with exact arithmetic and
 // integer counts; force, dissipation and heat flow are summed in the order the
 // list was filled, to tolerance.
+//
+// The seat tables are rebuilt every second step (src/nbody.js:554), so the
+// step after a rebuild walks the same tables again.  The rebuilding step's
+// walk records what the next one needs (SimArgs::walk 1): for each warp, every
+// seat the cull keeps in the cells within cell + mu of an owner, each with its
+// owner and which of the owner's 27 cells it came from.  They go through the
+// stage-2 queue (tagged whether their cell passed the nearest-point test, as
+// only those are this step's candidates), and each 64 the queue drains are
+// copied to the record with two contiguous stores.  The next step
+// (walk 2) replays that record in place of stage 1, 32 entries at a time, with
+// the reference's decisions recomputed: the seat's cell must be one of the
+// 27 around where the owner is now and pass its nearest-point test, and then
+// the pair the link test.  The quantised cull is not repeated: it can only
+// drop a seat whose particle is beyond the link radius while every particle
+// has moved less than SEAT_SLACK a less the quantisation's half-diagonal
+// since the rebuild.  The record holds every pair the walk can find when the
+// owner has moved at most mu and every particle at most D, mu + D within that
+// same margin (the host sets both, and checks the margin is there).  Owners
+// that moved further walk as the reference does; owners that changed cell
+// replay and walk the cells their new neighbourhood adds; a warp whose record
+// did not fit, and every warp when any particle moved further than D, walks.
 #include "ccs_device.cuh"
 #include "ccs_internal.h"
 
@@ -35,6 +56,9 @@ namespace ccs {
 namespace {
 constexpr int kQCap = 32 * kSeats + 64;      // seat candidates: one stage-1 round plus what is left
 constexpr int kTCap = 16;                    // touching neighbours listed per owner
+// a queue entry: particle | owner lane << 18, and when the walk records, the owner's cell it came from << 23
+// and whether that cell passed the owner's nearest-point test (kNearCell); the record keeps the first three
+constexpr uint32_t kNearCell = 1u << 28, kRecEntry = kNearCell - 1u;
 inline int blocks_for(long n, int b) { return (int)((n + b - 1) / b); }
 }  // namespace
 
@@ -47,6 +71,7 @@ struct ContactWarp {
   int nb[32];          // neighbours inside the link radius, per owner
   int tn[32];          // touching neighbours listed, per owner
   uint32_t tl[kTCap][32];   // the touching neighbours of owner o: tl[k][o]
+  uint32_t near[32];   // walk 2: per owner, its record's cells that its walk would take now (near_cells)
   uint32_t q[kQCap];   // particle index | owner << 18
 };
 
@@ -102,27 +127,34 @@ __device__ __forceinline__ void take_near(const ccs_uniforms &u, const SimArgs &
 }
 
 // stage 2: queued seats, two per lane when there are 64 (two position loads in flight), else one
-// (lanes >= n idle); pairs inside the link radius are counted, touching ones listed for their owner
-template <bool PAIRS>
+// (lanes >= n idle); pairs inside the link radius are counted, touching ones listed for their owner.
+// MODE 1: the entries are first copied to the warp's record (rec from rbase, rc entries so far), and only
+// those tagged as in a cell past the nearest-point test are candidates
+template <bool PAIRS, int MODE>
 __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, int base,
-                                                 int n, int lane, int first) {
+                                                 int n, int lane, int first, size_t rbase, int &rc) {
   if (lane < n) {
     const bool two = n == 64;
     const uint32_t e0 = w.q[base + lane];
     const uint32_t e1 = two ? w.q[base + 32 + lane] : 0u;
+    if (MODE == 1) {
+      if (rc + lane < kRecWarp) a.rec[rbase + rc + lane] = e0 & kRecEntry;
+      if (two && rc + 32 + lane < kRecWarp) a.rec[rbase + rc + 32 + lane] = e1 & kRecEntry;
+    }
     const float4 Pj0 = __ldg(a.pos + (e0 & 0x3FFFFu));
     const float4 Pj1 = two ? __ldg(a.pos + (e1 & 0x3FFFFu)) : Pj0;
-    const float4 Po0 = w.P[e0 >> 18];
+    const float4 Po0 = w.P[(e0 >> 18) & 31u];
     const f3 d0 = xsub3(xyz(Pj0), xyz(Po0));
     const float r20 = xdot(d0, d0);
-    if (r20 < u.link2) take_near<PAIRS>(u, a, w, e0, r20, first);
+    if ((MODE != 1 || (e0 & kNearCell)) && r20 < u.link2) take_near<PAIRS>(u, a, w, e0 & 0x7FFFFFu, r20, first);
     if (two) {
-      const float4 Po1 = w.P[e1 >> 18];
+      const float4 Po1 = w.P[(e1 >> 18) & 31u];
       const f3 d1 = xsub3(xyz(Pj1), xyz(Po1));
       const float r21 = xdot(d1, d1);
-      if (r21 < u.link2) take_near<PAIRS>(u, a, w, e1, r21, first);
+      if ((MODE != 1 || (e1 & kNearCell)) && r21 < u.link2) take_near<PAIRS>(u, a, w, e1 & 0x7FFFFFu, r21, first);
     }
   }
+  if (MODE == 1) rc += n;
   __syncwarp();   // every lane has read its entries before the queue is written again
 }
 
@@ -168,7 +200,8 @@ __device__ __forceinline__ f3 gravity_tide(const ccs_uniforms &u, const SimArgs 
 // stencil-split P3M's gravity instead of the reference's gather and loose-list add)
 template <bool FIELD, bool TIDE = false>
 __device__ __forceinline__ void finish_particle(const ccs_uniforms &u, const SimArgs &a, int me, float4 P, float4 V,
-                                                float ri, float ci, f3 push, float lost, float flow, float nb) {
+                                                float ri, float ci, f3 push, float lost, float flow, float nb,
+                                                unsigned *recMax = nullptr) {
   const f3 p = xyz(P);
   const float body = P.w;
   f3 grav = mk(0.0f, 0.0f, 0.0f), g;
@@ -221,10 +254,73 @@ __device__ __forceinline__ void finish_particle(const ccs_uniforms &u, const Sim
   // simFS({frozen: true}), src/glsl-sim.js:523-526: the material that does not move
   if (FIELD && u.frozen >= 0.0f && fabsf(xsub(body, u.frozen)) < 0.5f) v = mk(0.0f, 0.0f, 0.0f);
   const f3 pn = p + v * dt;
+  if (recMax) {   // the walk recorded: how far any particle moves before the record is replayed
+    const f3 dd = pn - p;
+    const unsigned live = __activemask();
+    const unsigned m = __reduce_max_sync(live, __float_as_uint(dot(dd, dd)));   // >= 0 (NaN above all)
+    if ((threadIdx.x & 31) == __ffs(live) - 1) atomicMax(recMax, m);
+  }
   a.posO[me] = make_float4(pn.x, pn.y, pn.z, body);
   a.velO[me] = make_float4(v.x, v.y, v.z, fdiv(u.tK * Q, ci));
   a.auxO[me] = make_float4(grav.x, grav.y, grav.z, nb);
   a.qO[me] = Q;
+}
+
+// the cells that pass the owner's nearest-point test (src/glsl-sim.js:415-418) from where it is now (its
+// cell's corner c0x, c0y, c0z), with the arithmetic of the walk's own test, as bits e_x + 3 e_y + 9 e_z
+// over the 27 cells around another cell of the owner's, the one it had when its record was made, d cells
+// off this one (each of dx, dy, dz in -1..1): a cell outside the 27 around the present one has no bit
+__device__ __forceinline__ uint32_t near_cells(const ccs_uniforms &u, f3 p, float c0x, float c0y, float c0z, int dx,
+                                               int dy, int dz) {
+  const float cell = u.cell;
+  float sx[3], sy[3], sz[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float off = xmul((float)(d - 1), cell);
+    const float lx = xadd(c0x, off), ly = xadd(c0y, off), lz = xadd(c0z, off);
+    const float qx = xsub(clampf(p.x, lx, xadd(lx, cell)), p.x);
+    const float qy = xsub(clampf(p.y, ly, xadd(ly, cell)), p.y);
+    const float qz = xsub(clampf(p.z, lz, xadd(lz, cell)), p.z);
+    sx[d] = xmul(qx, qx);
+    sy[d] = xmul(qy, qy);
+    sz[d] = xmul(qz, qz);
+  }
+  // the record's cell e (0..2 an axis) is the present frame's o = e + d
+  float tx[3], ty[3], tz[3];
+  bool vx[3], vy[3], vz[3];
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    const int ox = e + dx, oy = e + dy, oz = e + dz;
+    vx[e] = ox >= 0 && ox <= 2;
+    vy[e] = oy >= 0 && oy <= 2;
+    vz[e] = oz >= 0 && oz <= 2;
+    tx[e] = ox <= 0 ? sx[0] : ox == 1 ? sx[1] : sx[2];
+    ty[e] = oy <= 0 ? sy[0] : oy == 1 ? sy[1] : sy[2];
+    tz[e] = oz <= 0 ? sz[0] : oz == 1 ? sz[1] : sz[2];
+  }
+  uint32_t m = 0;
+#pragma unroll
+  for (int ez = 0; ez < 3; ++ez)
+#pragma unroll
+    for (int ey = 0; ey < 3; ++ey)
+#pragma unroll
+      for (int ex = 0; ex < 3; ++ex)
+        if (vx[ex] && vy[ey] && vz[ez] && !(xadd(xadd(tx[ex], ty[ey]), tz[ez]) > u.link2))
+          m |= 1u << (ex + 3 * ey + 9 * ez);
+  return m;
+}
+
+// one record entry (particle | owner << 18 | the owner's cell it came from << 23): the walk's decisions
+// for it -- the cell one of the owner's 27 now, past the nearest-point test (near, the owner's bits), the
+// pair inside the link radius
+template <bool PAIRS>
+__device__ __forceinline__ void replay_entry(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, uint32_t e,
+                                             float4 Pj, int first) {
+  const int o = (int)((e >> 18) & 31u);
+  if (!((w.near[o] >> ((e >> 23) & 31u)) & 1u)) return;
+  const f3 d = xsub3(xyz(Pj), xyz(w.P[o]));
+  const float r2 = xdot(d, d);
+  if (r2 < u.link2) take_near<PAIRS>(u, a, w, e & 0x7FFFFFu, r2, first);
 }
 
 // W warps per CTA (8 or 4: the autotuner's choice; 4 CTAs of 8 or 8 of 4 share an SM); FIELD: the crater
@@ -232,9 +328,12 @@ __device__ __forceinline__ void finish_particle(const ccs_uniforms &u, const Sim
 // The uniforms come by value: every field is then an operand from the constant bank, where through a pointer
 // each was a load and a register held across the walk (5.7 % of the launch's time at 262k).
 // SPLIT: stop at the contact sums (a mesh step whose mesh runs beside the contact walk; k_contact_tail ends it).
-template <int W, bool FIELD, bool SPLIT = false, bool PAIRS = false>
+// MODE: 0 the walk; 1 the walk and its record for the next step; 2 the next step, which replays the record
+// (SimArgs::walk).
+template <int W, bool FIELD, bool SPLIT = false, bool PAIRS = false, int MODE = 0>
 __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_uniforms u, const SimArgs a) {
   constexpr int kThreads = 32 * W;
+  constexpr unsigned kAll = 0xFFFFFFFFu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ float spc[16];   // seatPos(q) * uCell, exact
   if (threadIdx.x < 16) spc[threadIdx.x] = xmul(__fdiv_rn((float)threadIdx.x + 0.5f, 15.0f), u.cell);
@@ -258,6 +357,25 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
   int cx, cy, cz;
   cell_of(u, p, gx, gy, gz, cx, cy, cz);
   const float c0x = xmul((float)cx, cell), c0y = xmul((float)cy, cell), c0z = xmul((float)cz, cell);
+  // MODE 2: how this lane's owner finds its pairs -- 0 its record; 1 its record, and a walk of the cells its
+  // new cell adds (ecx, ecy, ecz: its cell when the record was made); 2 the walk.  The warp's record: rn
+  // entries from rec[first / 32 * kRecWarp] (more than kRecWarp: it did not fit, and the warp walks)
+  int how = 2, ecx = cx, ecy = cy, ecz = cz, rn = 0;
+  const size_t rbase = (size_t)(first >> 5) * kRecWarp;
+  if (MODE == 2) {
+    rn = __ldg(a.recN + (first >> 5));
+    if (live && rn <= kRecWarp && __uint_as_float(__ldg(a.recMax)) <= a.recAll2) {
+      const float4 Pe = __ldg(a.recP + me);
+      const float mx = p.x - Pe.x, my = p.y - Pe.y, mz = p.z - Pe.z;
+      if (mx * mx + my * my + mz * mz <= a.recMove2) {
+        float ex, ey, ez;
+        cell_of(u, xyz(Pe), ex, ey, ez, ecx, ecy, ecz);
+        how = (ecx == cx && ecy == cy && ecz == cz) ? 0 : 1;
+      }
+    }
+    w.near[lane] = how < 2 ? near_cells(u, p, c0x, c0y, c0z, ecx - cx, ecy - cy, ecz - cz) : 0u;
+    if (rn > kRecWarp) rn = 0;
+  }
   w.P[lane] = P;
   w.V[lane] = V;
   w.C0[lane] = make_float4(c0x, c0y, c0z, ri);
@@ -266,11 +384,39 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
   w.nb[lane] = 0;
   w.tn[lane] = 0;
   __syncthreads();   // spc, and every owner slot
+  if (MODE == 2) {
+    if (a.recStats) {   // a diagnostic: how many owners took each way
+      const unsigned b0 = __ballot_sync(kAll, live && how == 0), b1 = __ballot_sync(kAll, live && how == 1),
+                     b2 = __ballot_sync(kAll, live && how == 2);
+      if (lane == 0) {
+        atomicAdd(a.recStats + 0, (unsigned)__popc(b0));
+        atomicAdd(a.recStats + 1, (unsigned)__popc(b1));
+        atomicAdd(a.recStats + 2, (unsigned)__popc(b2));
+      }
+    }
+    // the replay: the warp's record 64 entries at a time, two a lane (two position loads in flight); the
+    // entries of owners that walk find no bits in near
+#pragma unroll 1
+    for (int b = 0; b < rn; b += 64) {
+      const int k0 = b + lane, k1 = k0 + 32;
+      const uint32_t e0 = k0 < rn ? __ldg(a.rec + rbase + k0) : 0u;
+      const uint32_t e1 = k1 < rn ? __ldg(a.rec + rbase + k1) : 0u;
+      const float4 Pj0 = k0 < rn ? __ldg(a.pos + (e0 & 0x3FFFFu)) : make_float4(0, 0, 0, 0);
+      const float4 Pj1 = k1 < rn ? __ldg(a.pos + (e1 & 0x3FFFFu)) : Pj0;
+      if (k0 < rn) replay_entry<PAIRS>(u, a, w, e0, Pj0, first);
+      if (k1 < rn) replay_entry<PAIRS>(u, a, w, e1, Pj1, first);
+    }
+    __syncwarp();
+  }
   const int sh = u.GShift;
   const uint32_t gm = (uint32_t)u.GMask;
   const uint4 *seats = reinterpret_cast<const uint4 *>(a.seats);
   int qn = 0;   // queue fill (warp-uniform)
-  // stage 1: the 27 neighbour cells in the reference's order, the warp in lockstep
+  int rc = 0;   // MODE 1: entries of the warp's record (warp-uniform)
+  // stage 1: the 27 neighbour cells in the reference's order, the warp in lockstep (MODE 2: the lanes whose
+  // owners walk, over the cells they walk; none, and no walk, in most warps)
+  const bool walks = live && how > 0;
+  if (MODE != 2 || __any_sync(kAll, walks)) {
 #pragma unroll 1
   for (int dz = 0; dz < 3; ++dz) {
     const int z = cz + dz - 1;
@@ -289,8 +435,16 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
         const int x = cx + dx - 1;
         const float lx = xadd(c0x, xmul((float)(dx - 1), cell));
         const float qx = xsub(clampf(p.x, lx, xadd(lx, cell)), p.x);
+        const float d2 = xadd(xadd(xmul(qx, qx), qy2), qz2);
+        const bool nearCell = !(d2 > u.link2);   // the nearest-point test
+        bool walk = live;
+        if (MODE == 2)   // a lane that moved to another cell walks only the cells its old one did not have
+          walk = walks && (how == 2 || abs(x - ecx) > 1 || abs(y - ecy) > 1 || abs(z - ecz) > 1);
+        // MODE 1 loads the cells a little further out too, for the record (their seats are not this step's)
+        const bool load = walk && (MODE == 1 ? !(d2 > a.recLink2) : nearCell);
+        const uint32_t tag = MODE == 1 ? ((uint32_t)(dx + 3 * dy + 9 * dz) << 23) | (nearCell ? kNearCell : 0u) : 0u;
         uint4 s0 = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty), s1 = s0;
-        if (live && !(xadd(xadd(xmul(qx, qx), qy2), qz2) > u.link2)) {   // the nearest-point test
+        if (load) {
           const uint32_t yy = ((uint32_t)y + ((uint32_t)(x >> sh) << (sh - 1)) + wz) & gm;   // the x period skews y by half
           const uint32_t h = (row + yy) * (uint32_t)u.AW + col + ((uint32_t)x & gm);
           const uint4 *cp = seats + (size_t)h * 2;
@@ -302,7 +456,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
 #pragma unroll
           for (int k = 0; k < kSeats; ++k) {
             // a cell's seats fill from the front: the walk ends at the first seat empty in every lane's cell
-            if (!__any_sync(0xFFFFFFFFu, !(sv[k] & 0x80000000u))) break;
+            if (!__any_sync(kAll, !(sv[k] & 0x80000000u))) break;
             bool seat = !(sv[k] & 0x80000000u) && (int)(sv[k] & 0x3FFFFu) != me;
             if (seat) {   // the quantised cull: where the seat sat at the rebuild, against this particle now
               const f3 dq = mk(xsub(xadd(lx, spc[(sv[k] >> 18) & 15u]), p.x),
@@ -310,25 +464,30 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
                                xsub(xadd(lz, spc[(sv[k] >> 26) & 15u]), p.z));
               seat = !(xdot(dq, dq) > u.reach2);
             }
-            const unsigned bal = __ballot_sync(0xFFFFFFFFu, seat);
-            if (seat) w.q[qn + __popc(bal & ((1u << lane) - 1u))] = (sv[k] & 0x3FFFFu) | ((uint32_t)lane << 18);
+            const unsigned bal = __ballot_sync(kAll, seat);
+            if (seat) w.q[qn + __popc(bal & ((1u << lane) - 1u))] = (sv[k] & 0x3FFFFu) | ((uint32_t)lane << 18) | tag;
             qn += __popc(bal);
           }
         }
         __syncwarp();
         while (qn >= 64) {
           qn -= 64;
-          drain_candidates<PAIRS>(u, a, w, qn, 64, lane, first);
+          drain_candidates<PAIRS, MODE>(u, a, w, qn, 64, lane, first, rbase, rc);
         }
       }
     }
   }
+  }
   if (qn >= 32) {
     qn -= 32;
-    drain_candidates<PAIRS>(u, a, w, qn, 32, lane, first);
+    drain_candidates<PAIRS, MODE>(u, a, w, qn, 32, lane, first, rbase, rc);
   }
-  if (qn > 0) drain_candidates<PAIRS>(u, a, w, 0, qn, lane, first);
+  if (qn > 0) drain_candidates<PAIRS, MODE>(u, a, w, 0, qn, lane, first, rbase, rc);
   __syncwarp();
+  if (MODE == 1) {
+    if (lane == 0) a.recN[first >> 5] = min(rc, kRecWarp + 1);
+    if (live) a.recP[me] = P;
+  }
   if (!live) return;
   // stage 3: each owner's touching neighbours in its own lane, the sums in registers
   f3 push = mk(w.fx[lane], w.fy[lane], w.fz[lane]);
@@ -350,11 +509,12 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
     a.part2[me] = make_float2(lost, flow);
     return;
   }
-  finish_particle<FIELD>(u, a, me, P, V, ri, ci, push, lost, flow, nb);
+  finish_particle<FIELD>(u, a, me, P, V, ri, ci, push, lost, flow, nb, MODE == 1 ? a.recMax : nullptr);
 }
 
 // the tail of a split mesh step, one thread a particle: the contact sums the contact walk left in part, then
-// the same gravity, settle/kick, heat and kick/drift as the whole step's
+// the same gravity, settle/kick, heat and kick/drift as the whole step's (and, after a walk that recorded,
+// the displacement its record is good for)
 template <bool TIDE>
 __global__ void __launch_bounds__(256) k_contact_tail(const ccs_uniforms u, const SimArgs a) {
   const int me = a.first + blockIdx.x * blockDim.x + threadIdx.x;
@@ -364,23 +524,47 @@ __global__ void __launch_bounds__(256) k_contact_tail(const ccs_uniforms u, cons
   const float ci = ri * (is_iron(P.w) ? u.cpIron : 1.0f);
   const float4 s = a.part[me];
   const float2 s2 = a.part2[me];
-  finish_particle<false, TIDE>(u, a, me, P, V, ri, ci, mk(s.x, s.y, s.z), s2.x, s2.y, s.w);
+  finish_particle<false, TIDE>(u, a, me, P, V, ri, ci, mk(s.x, s.y, s.z), s2.x, s2.y, s.w,
+                               a.walk == 1 ? a.recMax : nullptr);
 }
 
 size_t contact_smem_bytes(int warps) { return sizeof(ContactWarp) * warps; }
 
+namespace {
+template <int W, bool FIELD, bool SPLIT, bool PAIRS, int MODE>
+cudaError_t set_smem() {
+  return cudaFuncSetAttribute(k_contact_step<W, FIELD, SPLIT, PAIRS, MODE>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)contact_smem_bytes(W));
+}
+template <int W, bool FIELD, bool SPLIT, bool PAIRS>
+cudaError_t set_modes() {
+  cudaError_t e = set_smem<W, FIELD, SPLIT, PAIRS, 0>();
+  if (e == cudaSuccess) e = set_smem<W, FIELD, SPLIT, PAIRS, 1>();
+  if (e == cudaSuccess) e = set_smem<W, FIELD, SPLIT, PAIRS, 2>();
+  return e;
+}
+// one launch of the contact step over [a.first, a.first + count) in the walk a.walk names
+template <int W, bool FIELD, bool SPLIT, bool PAIRS>
+void launch_walk(const ccs_uniforms &u, const SimArgs &a, int count, cudaStream_t st) {
+  const dim3 grid(blocks_for(count, 32 * W)), block(32 * W);
+  const size_t smem = contact_smem_bytes(W);
+  if (a.walk == 1)
+    k_contact_step<W, FIELD, SPLIT, PAIRS, 1><<<grid, block, smem, st>>>(u, a);
+  else if (a.walk == 2)
+    k_contact_step<W, FIELD, SPLIT, PAIRS, 2><<<grid, block, smem, st>>>(u, a);
+  else
+    k_contact_step<W, FIELD, SPLIT, PAIRS, 0><<<grid, block, smem, st>>>(u, a);
+}
+}  // namespace
+
 cudaError_t init_kernels() {
-  const cudaFuncAttribute smem = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute(k_contact_step<8, false>, smem, (int)contact_smem_bytes(8));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_contact_step<4, false>, smem, (int)contact_smem_bytes(4));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_contact_step<8, true>, smem, (int)contact_smem_bytes(8));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_contact_step<4, true>, smem, (int)contact_smem_bytes(4));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_contact_step<8, false, true>, smem, (int)contact_smem_bytes(8));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_contact_step<4, false, true>, smem, (int)contact_smem_bytes(4));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_contact_step<4, false, false, true>, smem, (int)contact_smem_bytes(4));
+  cudaError_t e = set_modes<8, false, false, false>();
+  if (e == cudaSuccess) e = set_modes<4, false, false, false>();
+  if (e == cudaSuccess) e = set_modes<8, true, false, false>();
+  if (e == cudaSuccess) e = set_modes<4, true, false, false>();
+  if (e == cudaSuccess) e = set_modes<8, false, true, false>();
+  if (e == cudaSuccess) e = set_modes<4, false, true, false>();
+  if (e == cudaSuccess) e = set_modes<4, false, false, true>();
   return e;
 }
 
@@ -390,13 +574,13 @@ int launch_simulate_range(const ccs_uniforms &u, int N, SimArgs a, cudaStream_t 
   a.first = first;
   if (count <= 0) return 0;
   if (warps == 4 && field)
-    k_contact_step<4, true><<<blocks_for(count, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+    launch_walk<4, true, false, false>(u, a, count, st);
   else if (warps == 4)
-    k_contact_step<4, false><<<blocks_for(count, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+    launch_walk<4, false, false, false>(u, a, count, st);
   else if (field)
-    k_contact_step<8, true><<<blocks_for(count, 256), 256, contact_smem_bytes(8), st>>>(u, a);
+    launch_walk<8, true, false, false>(u, a, count, st);
   else
-    k_contact_step<8, false><<<blocks_for(count, 256), 256, contact_smem_bytes(8), st>>>(u, a);
+    launch_walk<8, false, false, false>(u, a, count, st);
   return 1;
 }
 
@@ -407,15 +591,19 @@ int launch_simulate(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t
 int launch_contacts_only(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps) {
   if (N <= 0) return 0;
   if (warps == 4)
-    k_contact_step<4, false, true><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+    launch_walk<4, false, true, false>(u, a, N, st);
   else
-    k_contact_step<8, false, true><<<blocks_for(N, 256), 256, contact_smem_bytes(8), st>>>(u, a);
+    launch_walk<8, false, true, false>(u, a, N, st);
   return 1;
 }
 
+// the read-out never records (it is not a step); after a step that recorded it replays as the next step will
 int launch_contact_pairs(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st) {
   if (N <= 0) return 0;
-  k_contact_step<4, false, false, true><<<blocks_for(N, 128), 128, contact_smem_bytes(4), st>>>(u, a);
+  SimArgs b = a;
+  if (b.walk == 1) b.walk = 0;
+  b.recStats = nullptr;
+  launch_walk<4, false, false, true>(u, b, N, st);
   return 1;
 }
 

@@ -19,6 +19,7 @@ constexpr int kSeats = CCS_SEATS;
 constexpr unsigned kStatusGrid = 1u;          // a contact-cell insertion gave up (degenerate pile)
 constexpr unsigned kStatusNN = 2u;            // a tensor-core wait of the learned P3M pass gave up
 constexpr unsigned kStatusFof = 4u;           // a union of the device analysis gave up its retries
+constexpr int kRecWarp = 1536;                // seats a grid step's contact walk records per warp for the next step
 
 // the analysis on the device (ccs_fof.cu): src/nbody.js:646-893
 constexpr int kFofBuckets = 1 << 20;          // hashed cells of side 2.4 a, as the host restatement hashes them
@@ -92,6 +93,20 @@ struct SimArgs {
   // the stencil-split P3M's gather: each box's tides and deposit (centres of mass), and each particle's pairs
   const float4 *tideA0 = nullptr, *tideA1 = nullptr, *tideB0 = nullptr, *tideB1 = nullptr;
   const float4 *fineA = nullptr, *fineB = nullptr, *ppAll = nullptr;
+  // the contact walk's record (ccs_contact.cu).  walk 1, a step that rebuilt the grid: the walk also writes,
+  // per warp, every seat its cull kept in the cells within recLink2 of an owner (rec[warp * kRecWarp + k],
+  // particle | owner lane << 18 | the owner's cell it came from << 23), how many (recN[warp]; kRecWarp + 1
+  // when they did not fit), where each owner was (recP), and the largest squared displacement of the
+  // step's kick/drift (recMax, the bits of a float; the grid zeroes it).  walk 2, the next step (same
+  // seats): owners that moved less than sqrt(recMove2) replay the record instead of walking the seat
+  // tables, while recMax is at most recAll2.  walk 0: the walk alone
+  uint32_t *rec = nullptr;
+  int *recN = nullptr;
+  float4 *recP = nullptr;
+  unsigned *recMax = nullptr;
+  unsigned *recStats = nullptr;   // walk 2, optional: owners that replayed, replayed and walked new cells, walked
+  int walk = 0;
+  float recLink2 = 0.0f, recMove2 = 0.0f, recAll2 = 0.0f;
 };
 
 struct DiagArgs {
@@ -115,10 +130,13 @@ int sm_count();
 // kernel launchers (ccs_kernels.cu); all enqueue on `st` and return the
 // number of kernels launched.
 int launch_fill_u32(uint32_t *p, size_t n, uint32_t v, cudaStream_t st);
-// u by value (the kernel's first argument, as for the contact step)
+// u by value (the kernel's first argument, as for the contact step); recMax, if not null, is zeroed for the
+// contact walk that records (SimArgs::walk 1)
 int launch_contact_grid(const ccs_uniforms &u, int N, const float4 *pos, uint32_t *seats, uint32_t *hk,
-                        uint32_t *seatsOld, const uint32_t *hkOld, unsigned *status, cudaStream_t st);
-// warps: CTA width of the contact step, 8 or 4; u by value (the kernel's first argument)
+                        uint32_t *seatsOld, const uint32_t *hkOld, unsigned *status, unsigned *recMax,
+                        cudaStream_t st);
+// warps: CTA width of the contact step, 8 or 4; u by value (the kernel's first argument); every contact-step
+// launcher runs the walk a.walk names (0 the walk, 1 the walk and its record, 2 the record's replay)
 int launch_simulate(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps = 8,
                     bool field = false);
 // a split mesh step: the contact walk alone (its sums into a.part, a.part2), then, after the mesh and the
@@ -141,10 +159,12 @@ int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int sp
 int launch_cell_tide(const ccs_uniforms *u, int S, const MeshBuf &m, cudaStream_t st);
 // ... and the pair pass over every particle inside it: sort by (box, base node), then the stencil's pairs;
 // out gets each particle's (pull, potential) x Gm
+// (work: split_work_bytes(N) of scratch for the pair pass's items and counters)
 size_t split_start_ints();
+size_t split_work_bytes(int N);
 int launch_pp_split(const ccs_uniforms *U, int N, int S, const float4 *pos, const float *mat, uint32_t *keys,
                     int32_t *vals, uint32_t *keysTmp, int32_t *valsTmp, uint32_t *hist, int *start, float4 *src,
-                    float4 *srcT, int *cells, int *nCells, float4 *out, cudaStream_t st);
+                    float4 *srcT, int *cells, int *nCells, void *work, float4 *out, cudaStream_t st);
 int pp_split_launches();
 int launch_pp_gather(const ccs_uniforms *u, const float4 *pos, const float *mat, const int *index, int cap,
                      float4 *list, float *box, cudaStream_t st);

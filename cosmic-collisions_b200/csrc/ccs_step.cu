@@ -94,8 +94,9 @@ __device__ __forceinline__ void seat_insert(uint32_t *cell, uint32_t w, unsigned
 __global__ void __launch_bounds__(kBlock) k_contact_grid(const ccs_uniforms u, const float4 *__restrict__ pos,
                                                          uint32_t *seats, uint32_t *__restrict__ hk,
                                                          uint32_t *seatsOld, const uint32_t *__restrict__ hkOld,
-                                                         unsigned *status) {
+                                                         unsigned *status, unsigned *recMax) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (recMax && i == 0) *recMax = 0u;   // the displacement the contact walk's record is good for, from none
   const bool live = i < u.N;
   float4 P = make_float4(0, 0, 0, 0);
   if (live) P = pos[i];
@@ -123,8 +124,9 @@ __global__ void __launch_bounds__(kBlock) k_contact_grid(const ccs_uniforms u, c
 }
 
 int launch_contact_grid(const ccs_uniforms &u, int N, const float4 *pos, uint32_t *seats, uint32_t *hk,
-                        uint32_t *seatsOld, const uint32_t *hkOld, unsigned *status, cudaStream_t st) {
-  k_contact_grid<<<blocks_for(N), kBlock, 0, st>>>(u, pos, seats, hk, seatsOld, hkOld, status);
+                        uint32_t *seatsOld, const uint32_t *hkOld, unsigned *status, unsigned *recMax,
+                        cudaStream_t st) {
+  k_contact_grid<<<blocks_for(N), kBlock, 0, st>>>(u, pos, seats, hk, seatsOld, hkOld, status, recMax);
   return 1;
 }
 

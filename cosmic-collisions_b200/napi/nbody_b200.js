@@ -146,6 +146,7 @@ CC.nbody = {
   get buffers() { return B.deviceBuffers(h); },
   // the stencil-split P3M (no counterpart in the reference): S = 1..3, or 0 for the reference's pass
   set ppSplit(S) { B.setPPSplit(h, S); },
+  set contactWalk(mode) { B.setContactWalk(h, mode); },
   books: function (withDiag) { return B.books(h, withDiag !== false); },
   T_UNIT: T_UNIT, V_UNIT: V_UNIT, E_KG: E_KG, CP_ROCK: CP_ROCK, CP_IRON: CP_IRON, L_EM: L_EM, JAM: JAM,
   PP_CAP: PP_CAP, meanK: meanK, ANALYZE_EVERY: ANALYZE_EVERY

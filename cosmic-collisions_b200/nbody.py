@@ -266,7 +266,7 @@ class NBody:
                  "ppforce": (PP_CAP * 16, np.float32), "ppbox": (PP_CAP, np.float32), "ppslot": (N, np.int32),
                  "diag": (N * 4, np.float32), "cellof": (N, np.uint32),
                  "tide0A": ((L.FINE + 1) * 4, np.float32), "tide1A": ((L.FINE + 1) * 4, np.float32),
-                 "ppall": (N * 4, np.float32)}
+                 "ppall": (N * 4, np.float32), "walkstats": (3, np.uint32), "walkcount": ((N + 31) // 32, np.int32)}
         n, dt = sizes[name]
         a = np.empty(n, dt)
         self._check(lib().ccs_read_buffer(self._h, L.BUF[name], ptr(a), a.nbytes), "ccs_read_buffer")
@@ -441,6 +441,13 @@ class NBody:
         """The stencil-split P3M (ccs_set_pp_split): every pair of mesh nodes within S cells (1..3) summed
         particle by particle, the rest on the mesh to first order; 0 returns to the reference's pass."""
         self._check(lib().ccs_set_pp_split(self._h, int(S)), "ccs_set_pp_split")
+
+    def set_contact_walk(self, mode):
+        """How the step after a grid rebuild finds its contact pairs (ccs_set_contact_walk): 1 (the default)
+        replays the rebuilding step's record where it is good, 0 walks the seat tables every step, 2 is 1
+        counting how each particle found its pairs (buffer "walkstats": replayed, replayed and walked the
+        cells a new cell added, walked)."""
+        self._check(lib().ccs_set_contact_walk(self._h, int(mode)), "ccs_set_contact_walk")
 
     def contact_pairs(self, cap=64):
         """The contact-pair sets of the current state (ccs_contact_pairs): (counts, pairs), pairs an N x cap

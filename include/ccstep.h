@@ -364,7 +364,13 @@ enum {
   CCS_BUF_SEATS = 5, CCS_BUF_FINE_A = 6, CCS_BUF_FORCE_A = 7, CCS_BUF_MONO_A = 8, CCS_BUF_COARSE_A = 9,
   CCS_BUF_FAR_A = 10, CCS_BUF_FINE_B = 11, CCS_BUF_FORCE_B = 12, CCS_BUF_MONO_B = 13, CCS_BUF_PP_LIST = 14,
   CCS_BUF_PP_FORCE = 15, CCS_BUF_PP_BOX = 16, CCS_BUF_PP_SLOT = 17, CCS_BUF_DIAG = 18, CCS_BUF_CELL_OF = 19,
-  CCS_BUF_TIDE0_A = 20, CCS_BUF_TIDE1_A = 21, CCS_BUF_PP_ALL = 22   /* the stencil-split P3M's (ccs_set_pp_split) */
+  CCS_BUF_TIDE0_A = 20, CCS_BUF_TIDE1_A = 21, CCS_BUF_PP_ALL = 22,  /* the stencil-split P3M's (ccs_set_pp_split) */
+  /* the contact walk's record (ccs_set_contact_walk): 3 uint32 -- particles
+   * whose step replayed the record, replayed it and walked the cells a new
+   * cell added, walked -- counted while the mode is 2; (N + 31) / 32 int32 --
+   * seats recorded per warp of 32 particles by the last step that rebuilt the
+   * grid (1537: more than fit) */
+  CCS_BUF_WALK_STATS = 23, CCS_BUF_WALK_COUNT = 24
 };
 int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes);
 
@@ -414,6 +420,19 @@ int ccs_sync(ccs_handle *h);
 /* CUDA-graph replay of steps on (1, the default) or off (0: every kernel
  * launched directly), for comparing the two paths and for debugging */
 int ccs_set_graphs(ccs_handle *h, int on);
+/* How the contact step finds its pairs (src/glsl-sim.js:415-450) on the step
+ * after a grid rebuild, which walks the same seat tables.  1 (the default):
+ * the rebuilding step's walk records, per particle, the seats its cull kept
+ * in the cells within the link radius and a margin; the next step replays
+ * that record (every decision of the walk recomputed, the pair sets and the
+ * neighbour counts the same) for the particles that moved less than the
+ * margin, and walks the seat tables for the others and for every particle
+ * after any call that moves or reorders them between the two steps (state
+ * writes, permutations, rigid steps, checkpoint loads, passes run by hand).
+ * 0: every step walks the seat tables.  2: as 1, and the replaying steps
+ * count how each particle found its pairs (CCS_BUF_WALK_STATS; the counts
+ * start from zero when this mode is set). */
+int ccs_set_contact_walk(ccs_handle *h, int mode);
 /* average device time (ms) of the kernels named by `kernel` launched since the
  * last reset, measured with CUDA events on the handle's stream; kernel ids:
  * 0 contact step (simulate), 1 contact grid, 2 deposit, 3 cell, 4 P3M force,

@@ -238,3 +238,55 @@ def test_contact_step_at_262k_mid_impact(ccmod, orc, mid_impact):
     dv = per_particle(dv_g, dv_o, floor=rms)
     print("per-particle relative error, 262k contact step:", quantiles(dv))
     assert np.median(dv) < REL and np.percentile(dv, 99.9) < 10 * REL, quantiles(dv)
+
+
+def test_replayed_step_at_262k_mid_impact(ccmod, orc, mid_impact):
+    """The step after a grid rebuild, on the same seats: its pairs come from the rebuilding step's record
+    (ccs_set_contact_walk) for the particles that moved little, from the walk for the rest.  The pair sets
+    equal the oracle walk's over those seats, and the step equals the same step walking the seat tables
+    from the same state: every neighbour count, each particle's velocity change to 1e-5 (the contacts
+    summed in another order)."""
+    import os
+    from cosmic_collisions_b200 import checkpoint
+    orc.set_threads(os.cpu_count())
+    ck = checkpoint.read(mid_impact)
+    nb = ccmod.NBody(0)
+    try:
+        nb.load(mid_impact)
+        nb.set_contact_walk(2)
+        nb.step(False, False)                      # grid, mesh, pairwise pass, contacts; the record
+        mid = nb.read_state()
+        seats = nb.buffer("seats")
+        stepNo, t = nb.sim.stepNo, nb.sim.t
+        gc, gp = nb.contact_pairs(64)              # replayed, as the next step finds them
+        nb.step(False, False)                      # the same seats, replayed
+        end = nb.read_state()
+        stats, rec = nb.buffer("walkstats"), nb.buffer("walkcount")
+        # the same step from the same state, walking the seat tables (a state write: nothing is replayed)
+        nb.set_contact_walk(0)
+        nb.sim.stepNo, nb.sim.t = stepNo, t
+        nb.write_state(pos=mid["pos"], vel=mid["vel"], aux=mid["aux"], q=mid["q"])
+        wc, wp = nb.contact_pairs(64)
+        nb.step(False, False)
+        end_w = nb.read_state()
+        assert np.array_equal(nb.buffer("seats"), seats)
+    finally:
+        nb.close()
+    u = orc.make_uni(orc.Sim.from_buffer_copy(bytes(ck["sim"])))
+    oc, op = orc.contact_pairs(u, mid["pos"], seats, 64)
+    assert np.array_equal(gc, oc) and oc.max() <= 64
+    assert np.array_equal(np.sort(gp, axis=1), np.sort(op, axis=1))
+    assert np.array_equal(wc, oc) and np.array_equal(np.sort(wp, axis=1), np.sort(op, axis=1))
+    assert np.array_equal(end["aux"][:, 3], end_w["aux"][:, 3])
+    assert np.array_equal(end["aux"][:, 3], oc.astype(np.float32))
+    dv = end["vel"][:, :3].astype(np.float64) - mid["vel"][:, :3]
+    dvw = end_w["vel"][:, :3].astype(np.float64) - mid["vel"][:, :3]
+    rms = np.sqrt((dvw ** 2).sum(1).mean())
+    rel = per_particle(dv, dvw, floor=rms)
+    N = len(rel)
+    print("262k replayed step: replayed / replayed and walked new cells / walked", stats.tolist(),
+          "; seats recorded per particle %.1f, warps whose record did not fit: %d" % (rec.mean() / 32,
+                                                                                   int((rec > 1536).sum())),
+          "; dv vs walking step:", quantiles(rel))
+    assert stats.sum() == N and stats[0] > N // 2
+    assert np.median(rel) < REL and np.percentile(rel, 99.9) < 10 * REL, quantiles(rel)
