@@ -394,17 +394,29 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
         atomicAdd(a.recStats + 2, (unsigned)__popc(b2));
       }
     }
-    // the replay: the warp's record 64 entries at a time, two a lane (two position loads in flight); the
-    // entries of owners that walk find no bits in near
+    // the replay: the warp's record 128 entries at a time, four a lane (four position loads in flight),
+    // the next 128 entries loaded while these are worked; the entries of owners that walk find no bits in near
+    constexpr int kPer = 4;
+    uint32_t e[kPer];
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) e[q] = lane + 32 * q < rn ? __ldg(a.rec + rbase + lane + 32 * q) : 0u;
 #pragma unroll 1
-    for (int b = 0; b < rn; b += 64) {
-      const int k0 = b + lane, k1 = k0 + 32;
-      const uint32_t e0 = k0 < rn ? __ldg(a.rec + rbase + k0) : 0u;
-      const uint32_t e1 = k1 < rn ? __ldg(a.rec + rbase + k1) : 0u;
-      const float4 Pj0 = k0 < rn ? __ldg(a.pos + (e0 & 0x3FFFFu)) : make_float4(0, 0, 0, 0);
-      const float4 Pj1 = k1 < rn ? __ldg(a.pos + (e1 & 0x3FFFFu)) : Pj0;
-      if (k0 < rn) replay_entry<PAIRS>(u, a, w, e0, Pj0, first);
-      if (k1 < rn) replay_entry<PAIRS>(u, a, w, e1, Pj1, first);
+    for (int b = 0; b < rn; b += 32 * kPer) {
+      float4 Pj[kPer];
+#pragma unroll
+      for (int q = 0; q < kPer; ++q)
+        Pj[q] = b + lane + 32 * q < rn ? __ldg(a.pos + (e[q] & 0x3FFFFu)) : make_float4(0, 0, 0, 0);
+      uint32_t en[kPer];
+#pragma unroll
+      for (int q = 0; q < kPer; ++q) {
+        const int k = b + 32 * kPer + lane + 32 * q;
+        en[q] = k < rn ? __ldg(a.rec + rbase + k) : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < kPer; ++q)
+        if (b + lane + 32 * q < rn) replay_entry<PAIRS>(u, a, w, e[q], Pj[q], first);
+#pragma unroll
+      for (int q = 0; q < kPer; ++q) e[q] = en[q];
     }
     __syncwarp();
   }
