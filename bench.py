@@ -674,7 +674,7 @@ def run_ours(args, rank, world, log):
         if args.profile_leg == "learned":
             nb.set_pp_nn(net)
         if args.profile_leg == "split":
-            nb.set_pp_split(args.split or 3)
+            nb.set_pp_split(args.split or 1)
             nb.steps(8)
         for _ in range(args.warmup):
             nb.step(False, False)
@@ -813,9 +813,10 @@ def run_ours(args, rank, world, log):
                       "gpu_launches": int(sp_launches), "clocks": sp_clk, "force_error": sp_err,
                       "method": "stencil-split P3M: every pair of mesh nodes within %d cells (Chebyshev) summed "
                                 "particle by particle (each pair weighted by its share of cloud-in-cell node "
-                                "pairs inside the stencil), the rest on the mesh unsoftened, gathered to first "
-                                "order by each node's tidal tensor, far blocks as monopole + quadrupole at each "
-                                "cell; the plain form that reaches median force error <= 1e-3" % args.split,
+                                "pairs inside the stencil), the rest on the mesh unsoftened, gathered to second "
+                                "order by each node's tidal tensor and the pull's second gradient, far blocks as "
+                                "monopole + quadrupole at each cell; the plain form that reaches median force "
+                                "error <= 1e-3" % args.split,
                       "state": "the plain leg's timed steps from the same saved state"}
         log("stencil-split P3M (S=%d): %.3f ms a step, force error median %.3e"
             % (args.split, sp_total / args.split_steps, sp_err["median"] if sp_err else float("nan")))
@@ -894,7 +895,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="ensemble: keep the default launch shapes")
     ap.add_argument("--nn-pairs", type=int, default=12_000_000, help="training pairs (three snapshots)")
     ap.add_argument("--nn-epochs", type=int, default=24)
-    ap.add_argument("--split", type=int, default=3, choices=[0, 1, 2, 3],
+    ap.add_argument("--split", type=int, default=1, choices=[0, 1, 2, 3],
                     help="stencil of the plain P3M leg at the metric's force-error operating point (0: skip)")
     ap.add_argument("--split-steps", type=int, default=64, help="timed steps of that leg")
     ap.add_argument("--books-steps", type=int, default=5000,

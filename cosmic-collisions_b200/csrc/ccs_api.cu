@@ -483,6 +483,8 @@ SimArgs sim_args(const ccs_handle *h) {
   a.tideA1 = h->pm[0].tide1;
   a.tideB0 = h->pm[1].tide0;
   a.tideB1 = h->pm[1].tide1;
+  a.tideA2 = h->pm[0].tide2;
+  a.tideB2 = h->pm[1].tide2;
   a.fineA = h->pm[0].fine;
   a.fineB = h->pm[1].fine;
   a.ppAll = h->ppAll;
@@ -637,7 +639,7 @@ void enqueue_pre(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
 void enqueue_step(ccs_handle *h, const StepPlan &p, const ccs_uniforms *U) {
   if (h->ppSplit && !h->field && h->part && h->part2) {
     // the stencil-split P3M: every step's contact step as its walk and its tail, whose gravity is the
-    // first-order gather plus the particle's own pair sum.  On a mesh step the grid and the walk run on the
+    // second-order gather plus the particle's own pair sum.  On a mesh step the grid and the walk run on the
     // side stream beside the mesh chain and the pair pass (unless kernels are timed or the step is an
     // ensemble member's), as in the reference form's split mesh step.
     const bool fork = p.mesh && h->side && !h->inEnsemble && !h->timing;
@@ -1004,7 +1006,8 @@ int ensure_split_buffers(ccs_handle *h) {
     MeshBuf &m = h->pm[b];
     rc |= dev_alloc(h, &m.tide0, kFine + 1);
     rc |= dev_alloc(h, &m.tide1, kFine + 1);
-    rc |= dev_alloc(h, &m.cellPartT, (size_t)kCoarse * kCellChunks * 64 * 3);
+    rc |= dev_alloc(h, &m.tide2, 3 * (size_t)(kFine + 1));
+    rc |= dev_alloc(h, &m.cellPartT, (size_t)kCoarse * kCellChunks * 64 * 5);
     rc |= dev_alloc(h, &m.quad0, kCoarse);
     rc |= dev_alloc(h, &m.quad1, kCoarse);
   }
@@ -1018,7 +1021,7 @@ int ensure_split_buffers(ccs_handle *h) {
   if (rc) {
     for (int b = 0; b < 2; ++b) {
       dev_free(h->pm[b].tide0); dev_free(h->pm[b].tide1); dev_free(h->pm[b].cellPartT);
-      dev_free(h->pm[b].quad0); dev_free(h->pm[b].quad1);
+      dev_free(h->pm[b].quad0); dev_free(h->pm[b].quad1); dev_free(h->pm[b].tide2);
     }
     dev_free(h->splitStart); dev_free(h->splitCells); dev_free(h->splitNCells); dev_free(h->splitSrc);
     dev_free(h->splitSrcT); dev_free(h->ppAll); dev_free(h->splitWork);
@@ -1027,6 +1030,7 @@ int ensure_split_buffers(ccs_handle *h) {
   for (int b = 0; b < 2; ++b) {
     CUDA_TRY(h, cudaMemsetAsync(h->pm[b].tide0, 0, sizeof(float4) * (kFine + 1), h->st));
     CUDA_TRY(h, cudaMemsetAsync(h->pm[b].tide1, 0, sizeof(float4) * (kFine + 1), h->st));
+    CUDA_TRY(h, cudaMemsetAsync(h->pm[b].tide2, 0, sizeof(float4) * 3 * (kFine + 1), h->st));
   }
   CUDA_TRY(h, cudaMemsetAsync(h->ppAll, 0, sizeof(float4) * N, h->st));
   return CCS_OK;
@@ -1043,6 +1047,7 @@ void free_state(ccs_handle *h) {
     dev_free(m.occ); dev_free(m.occIdx); dev_free(m.occN); dev_free(m.occBlocks); dev_free(m.occCount);
     dev_free(m.occAsc); dev_free(m.occAscN); dev_free(m.cellPart); dev_free(m.cellDone);
     dev_free(m.tide0); dev_free(m.tide1); dev_free(m.cellPartT); dev_free(m.quad0); dev_free(m.quad1);
+    dev_free(m.tide2);
   }
   dev_free(h->splitStart); dev_free(h->splitCells); dev_free(h->splitNCells); dev_free(h->splitSrc);
   dev_free(h->splitSrcT); dev_free(h->ppAll); dev_free(h->splitWork);
@@ -2458,6 +2463,7 @@ int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes) {
     case CCS_BUF_PP_ALL: src = h->ppAll; n = 16 * N; break;
     case CCS_BUF_WALK_STATS: src = h->recStats; n = 12; break;
     case CCS_BUF_WALK_COUNT: src = h->recN; n = 4 * ((N + 31) / 32); break;
+    case CCS_BUF_TIDE2_A: src = h->pm[0].tide2; n = 16 * 3 * (size_t)(kFine + 1); break;
     default: h->err = "unknown buffer"; return CCS_E_ARG;
   }
   if (!src) {

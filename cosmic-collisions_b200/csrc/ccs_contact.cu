@@ -159,14 +159,16 @@ __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const Si
 }
 
 // the stencil-split P3M's gravity at a particle: each of its 8 nodes' pull carried from the node's centre
-// of mass to the particle by the node's tidal tensor (first order), the strays' pull back and the other
-// box's as the reference gives them, and the particle's own pair sum (ccs_split.cu)
+// of mass to the particle by the node's tidal tensor and the pull's second gradient (second order), the
+// strays' pull back and the other box's as the reference gives them, and the particle's own pair sum
+// (ccs_split.cu)
 __device__ __forceinline__ f3 gravity_tide(const ccs_uniforms &u, const SimArgs &a, int me, f3 p) {
   f3 grav = mk(0.0f, 0.0f, 0.0f), g;
   const int box = box_of(u, p, g);
   if (box >= 0) {
     const float4 *F = box == 0 ? a.forceA : a.forceB, *T0 = box == 0 ? a.tideA0 : a.tideB0,
-                 *T1 = box == 0 ? a.tideA1 : a.tideB1, *M = box == 0 ? a.fineA : a.fineB;
+                 *T1 = box == 0 ? a.tideA1 : a.tideB1, *M = box == 0 ? a.fineA : a.fineB,
+                 *T2 = box == 0 ? a.tideA2 : a.tideB2;
     const float fx = floorf(g.x), fy = floorf(g.y), fz = floorf(g.z);
     const f3 t = mk(g.x - fx, g.y - fy, g.z - fz);
     const int bx = (int)fx, by = (int)fy, bz = (int)fz;
@@ -179,8 +181,14 @@ __device__ __forceinline__ f3 gravity_tide(const ccs_uniforms &u, const SimArgs 
       if (!(m.w > 0.0f)) continue;   // a node nothing was deposited on (a corner past the mesh's edge)
       const f3 d = p - xyz(m) * fdiv(1.0f, m.w);
       const float4 f = __ldg(F + c), t0 = __ldg(T0 + c), t1 = __ldg(T1 + c);
-      const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z, t0.w * d.x + t0.y * d.y + t1.y * d.z,
-                       t1.x * d.x + t1.y * d.y + t0.z * d.z);
+      const float4 g0 = __ldg(T2 + c), g1 = __ldg(T2 + kFine + 1 + c), g2 = __ldg(T2 + 2 * (kFine + 1) + c);
+      const float xx = d.x * d.x, yy = d.y * d.y, zz = d.z * d.z, xy = d.x * d.y, xz = d.x * d.z, yz = d.y * d.z;
+      const f3 Td = mk(t0.x * d.x + t0.w * d.y + t1.x * d.z + 0.5f * (g0.x * xx + g1.z * yy + g2.x * zz) +
+                           g1.x * xy + g1.y * xz + g0.w * yz,
+                       t0.w * d.x + t0.y * d.y + t1.y * d.z + 0.5f * (g1.x * xx + g0.y * yy + g2.y * zz) +
+                           g1.z * xy + g0.w * xz + g1.w * yz,
+                       t1.x * d.x + t1.y * d.y + t0.z * d.z + 0.5f * (g1.y * xx + g1.w * yy + g0.z * zz) +
+                           g0.w * xy + g2.x * xz + g2.y * yz);
       grav = grav + (xyz(f) + Td) * wgt;
     }
     grav = grav - xyz(__ldg(F + kFine)) * u.Gm;   // the strays in neither box pull back

@@ -68,9 +68,10 @@ struct MeshBuf {
   int *occAscN = nullptr;      // ... and how many
   float4 *cellPart = nullptr;  // the cell pass's partial sums: [listed block][source chunk][cell]
   int *cellDone = nullptr;     // per listed block: the chunks done (the last one adds them up)
-  // the stencil-split P3M's mesh (allocated when that form is switched on): each cell's tidal tensor, and
-  // the cell pass's partial sums of pull, potential and tide: [listed block][source chunk][3][cell]
-  float4 *tide0 = nullptr, *tide1 = nullptr, *cellPartT = nullptr;
+  // the stencil-split P3M's mesh (allocated when that form is switched on): each cell's tidal tensor, the
+  // pull's second gradient (tide2: three planes of kFine + 1), and the cell pass's partial sums of pull,
+  // potential, tide and second gradient: [listed block][source chunk][5][cell]
+  float4 *tide0 = nullptr, *tide1 = nullptr, *tide2 = nullptr, *cellPartT = nullptr;
   float4 *quad0 = nullptr, *quad1 = nullptr;   // each block's second moment about its centre of mass
 };
 
@@ -92,6 +93,7 @@ struct SimArgs {
   int pairCap = 0;
   // the stencil-split P3M's gather: each box's tides and deposit (centres of mass), and each particle's pairs
   const float4 *tideA0 = nullptr, *tideA1 = nullptr, *tideB0 = nullptr, *tideB1 = nullptr;
+  const float4 *tideA2 = nullptr, *tideB2 = nullptr;   // the second gradient's three planes (kFine + 1 apart)
   const float4 *fineA = nullptr, *fineB = nullptr, *ppAll = nullptr;
   // the contact walk's record (ccs_contact.cu).  walk 1, a step that rebuilt the grid: the walk also writes,
   // per warp, every seat its cull kept in the cells within recLink2 of an owner (rec[warp * kRecWarp + k],
@@ -142,7 +144,7 @@ int launch_simulate(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t
 // a split mesh step: the contact walk alone (its sums into a.part, a.part2), then, after the mesh and the
 // pairwise pass, the tail that turns them and the gravity into the step's outputs
 int launch_contacts_only(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, int warps);
-// tide: the stencil-split P3M's gather (first order from each node's centre of mass, the particle's pairs)
+// tide: the stencil-split P3M's gather (second order from each node's centre of mass, the particle's pairs)
 int launch_contact_tail(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st, bool tide = false);
 // the contact step with its pair sets written out (a.pairs, a.pairCap): the same walk, outputs to a's buffers
 int launch_contact_pairs(const ccs_uniforms &u, int N, const SimArgs &a, cudaStream_t st);

@@ -502,13 +502,35 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell(const ccs_uniforms *__restr
 // is left to the pair pass, the rest is summed unsoftened (the pair pass takes everything near, so no
 // softening is needed to keep the sum finite), and each cell also gets its tidal tensor -- the gradient of
 // the pull, the near sources' exactly and the block's far field's as the block carries it -- so that the
-// gather can carry each node's pull from its centre of mass to the particle to first order.  Outputs (x Gm):
-// force = (pull, potential) at the cell's centre of mass, tide0 = (Txx, Tyy, Tzz, Txy), tide1 = (Txz, Tyz).
+// gather can carry each node's pull from its centre of mass to the particle, and the pull's second gradient
+// for the second-order term.  Outputs (x Gm): force = (pull, potential) at the cell's centre of mass, tide0 =
+// (Txx, Tyy, Tzz, Txy), tide1 = (Txz, Tyz), and tide2's three planes (Gxxx Gyyy Gzzz Gxyz), (Gxxy Gxxz Gxyy
+// Gyyz), (Gxzz Gyzz), G_abc = d2 F_a / dx_b dx_c.
 // The far field is k_far_cell's, added after: each far block's pull evaluated at the cell itself, with the
 // block's quadrupole (the reference carries a block's monopole field from the block's centre of mass by its
 // tidal tensor, which at a few blocks' distance is off by a per cent or two).
 // ---------------------------------------------------------------------------
 namespace {
+// one source at r from the cell (r = source - cell, a5 = 3 M / r^5, a7 = 15 M / r^7): its second gradient
+// of the pull, G_abc = a7 r_a r_b r_c - a5 (d_ab r_c + d_ac r_b + d_bc r_a), onto g0 = (Gxxx Gyyy Gzzz Gxyz),
+// g1 = (Gxxy Gxxz Gxyy Gyyz), g2 = (Gxzz Gyzz)
+__device__ __forceinline__ void add_tide2(float4 &g0, float4 &g1, float2 &g2, f3 r, float a5, float a7) {
+  const float xx = r.x * r.x, yy = r.y * r.y, zz = r.z * r.z;
+  g0.x += r.x * (a7 * xx - 3.0f * a5);
+  g0.y += r.y * (a7 * yy - 3.0f * a5);
+  g0.z += r.z * (a7 * zz - 3.0f * a5);
+  g0.w += a7 * r.x * r.y * r.z;
+  g1.x += r.y * (a7 * xx - a5);
+  g1.y += r.z * (a7 * xx - a5);
+  g1.z += r.x * (a7 * yy - a5);
+  g1.w += r.z * (a7 * yy - a5);
+  g2.x += r.x * (a7 * zz - a5);
+  g2.y += r.y * (a7 * zz - a5);
+}
+__device__ __forceinline__ float4 add4(float4 a, float4 b) {
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+
 template <int SPLIT>
 __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__restrict__ U, int S,
                                                           const float4 *__restrict__ fine,
@@ -522,13 +544,14 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
                                                           const float4 *__restrict__ farT0,
                                                           const float4 *__restrict__ farT1,
                                                           float4 *__restrict__ force, float4 *__restrict__ tide0,
-                                                          float4 *__restrict__ tide1, float4 *__restrict__ cellPart,
-                                                          int *__restrict__ cellDone) {
+                                                          float4 *__restrict__ tide1, float4 *__restrict__ tide2,
+                                                          float4 *__restrict__ cellPart, int *__restrict__ cellDone) {
   constexpr int kCellThreads = 64 * SPLIT;
+  constexpr int kRows = 5;               // partial rows a cell: pull + potential, the tide (2), G (2 + 1 in row 2's zw)
   __shared__ int nbK[128], nbOff[129];
   __shared__ float4 src[kCellBatch];
   __shared__ int sfc[kCellBatch];        // a source's fine cell, x | y << 6 | z << 12
-  __shared__ float4 part[3][SPLIT][64];  // (pull, potential), (Txx Tyy Tzz Txy), (Txz Tyz)
+  __shared__ float4 part[kRows][SPLIT][64];
   __shared__ int last;
   const int t = threadIdx.x, cellT = t & 63, q = t >> 6, lane = t & 31;
   if (blockIdx.x == 0 && t == 0) force[kFine] = fine[kFine];   // the scratch texel, carried through
@@ -572,6 +595,8 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
     const f3 x = xyz(tc);
     f3 acc = mk(0, 0, 0);
     float pot = 0.0f, txx = 0.0f, tyy = 0.0f, tzz = 0.0f, txy = 0.0f, txz = 0.0f, tyz = 0.0f;
+    float4 g0 = make_float4(0, 0, 0, 0), g1 = g0;
+    float2 g2 = make_float2(0, 0);
     __syncthreads();
     const int total = nbOff[125];
     const int c0 = (int)((long long)total * chunk / kCellChunks);
@@ -612,27 +637,26 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
           txy += a5 * r.x * r.y;
           txz += a5 * r.x * r.z;
           tyz += a5 * r.y * r.z;
+          add_tide2(g0, g1, g2, r, a5, 5.0f * a5 * inv2);
         }
       }
       __syncthreads();
     }
     part[0][q][cellT] = make_float4(acc.x, acc.y, acc.z, pot);
     part[1][q][cellT] = make_float4(txx, tyy, tzz, txy);
-    part[2][q][cellT] = make_float4(txz, tyz, 0.0f, 0.0f);
+    part[2][q][cellT] = make_float4(txz, tyz, g2.x, g2.y);
+    part[3][q][cellT] = g0;
+    part[4][q][cellT] = g1;
     __syncthreads();
-    float4 *out = cellPart + ((size_t)bi * kCellChunks + chunk) * 64 * 3;
+    float4 *out = cellPart + ((size_t)bi * kCellChunks + chunk) * 64 * kRows;
     if (mine && q == 0) {
-      float4 s0 = part[0][0][cellT], s1 = part[1][0][cellT], s2 = part[2][0][cellT];
 #pragma unroll
-      for (int k = 1; k < SPLIT; ++k) {
-        const float4 p0 = part[0][k][cellT], p1 = part[1][k][cellT], p2 = part[2][k][cellT];
-        s0 = make_float4(s0.x + p0.x, s0.y + p0.y, s0.z + p0.z, s0.w + p0.w);
-        s1 = make_float4(s1.x + p1.x, s1.y + p1.y, s1.z + p1.z, s1.w + p1.w);
-        s2 = make_float4(s2.x + p2.x, s2.y + p2.y, s2.z, s2.w);
+      for (int r = 0; r < kRows; ++r) {
+        float4 sr = part[r][0][cellT];
+#pragma unroll
+        for (int k = 1; k < SPLIT; ++k) sr = add4(sr, part[r][k][cellT]);
+        __stcg(out + 64 * r + cellT, sr);
       }
-      __stcg(out + cellT, s0);
-      __stcg(out + 64 + cellT, s1);
-      __stcg(out + 128 + cellT, s2);
     }
     __threadfence();
     __syncthreads();
@@ -641,20 +665,22 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
     if (last) {   // every chunk is in: add them in chunk order, then the block's far field and its tide
       __threadfence();
       if (mine && q == 0) {
-        const float4 *pb = cellPart + (size_t)bi * kCellChunks * 64 * 3;
-        float4 s0 = __ldcg(pb + cellT), s1 = __ldcg(pb + 64 + cellT), s2 = __ldcg(pb + 128 + cellT);
+        const float4 *pb = cellPart + (size_t)bi * kCellChunks * 64 * kRows;
+        float4 s[kRows];
 #pragma unroll
+        for (int r = 0; r < kRows; ++r) s[r] = __ldcg(pb + 64 * r + cellT);
+#pragma unroll 1
         for (int c = 1; c < kCellChunks; ++c) {
-          const float4 p0 = __ldcg(pb + (size_t)c * 192 + cellT), p1 = __ldcg(pb + (size_t)c * 192 + 64 + cellT),
-                       p2 = __ldcg(pb + (size_t)c * 192 + 128 + cellT);
-          s0 = make_float4(s0.x + p0.x, s0.y + p0.y, s0.z + p0.z, s0.w + p0.w);
-          s1 = make_float4(s1.x + p1.x, s1.y + p1.y, s1.z + p1.z, s1.w + p1.w);
-          s2 = make_float4(s2.x + p2.x, s2.y + p2.y, s2.z, s2.w);
+#pragma unroll
+          for (int r = 0; r < kRows; ++r) s[r] = add4(s[r], __ldcg(pb + (size_t)c * 64 * kRows + 64 * r + cellT));
         }
         const int fi = fine_index(tx, ty, tz);
-        force[fi] = make_float4(s0.x * Gm, s0.y * Gm, s0.z * Gm, s0.w * Gm);
-        tide0[fi] = make_float4(s1.x * Gm, s1.y * Gm, s1.z * Gm, s1.w * Gm);
-        tide1[fi] = make_float4(s2.x * Gm, s2.y * Gm, 0.0f, 0.0f);
+        force[fi] = make_float4(s[0].x * Gm, s[0].y * Gm, s[0].z * Gm, s[0].w * Gm);
+        tide0[fi] = make_float4(s[1].x * Gm, s[1].y * Gm, s[1].z * Gm, s[1].w * Gm);
+        tide1[fi] = make_float4(s[2].x * Gm, s[2].y * Gm, 0.0f, 0.0f);
+        tide2[fi] = make_float4(s[3].x * Gm, s[3].y * Gm, s[3].z * Gm, s[3].w * Gm);
+        tide2[kFine + 1 + fi] = make_float4(s[4].x * Gm, s[4].y * Gm, s[4].z * Gm, s[4].w * Gm);
+        tide2[2 * (kFine + 1) + fi] = make_float4(s[2].z * Gm, s[2].w * Gm, 0.0f, 0.0f);
       }
       if (t == 0) cellDone[bi] = 0;
     }
@@ -708,7 +734,7 @@ __global__ void __launch_bounds__(256) k_far_cell(const ccs_uniforms *__restrict
                                                   const int *__restrict__ occBlocks, const int *__restrict__ occCount,
                                                   const int *__restrict__ occAsc, const int *__restrict__ occAscN,
                                                   float4 *__restrict__ force, float4 *__restrict__ tide0,
-                                                  float4 *__restrict__ tide1) {
+                                                  float4 *__restrict__ tide1, float4 *__restrict__ tide2) {
   __shared__ float4 sM[kFarCellBatch], sQ0[kFarCellBatch];
   __shared__ float2 sQ1[kFarCellBatch];
   __shared__ int sB[kFarCellBatch];
@@ -731,6 +757,8 @@ __global__ void __launch_bounds__(256) k_far_cell(const ccs_uniforms *__restrict
     }
     const int bx = blk & 15, by = (blk >> 4) & 15, bz = blk >> 8;
     float ax = 0, ay = 0, az = 0, pot = 0, txx = 0, tyy = 0, tzz = 0, txy = 0, txz = 0, tyz = 0;
+    float4 g0 = make_float4(0, 0, 0, 0), g1 = g0;
+    float2 g2 = make_float2(0, 0);
     for (int s0 = 0; s0 < ns; s0 += kFarCellBatch) {
       const int sn = min(kFarCellBatch, ns - s0);
       __syncthreads();
@@ -759,6 +787,7 @@ __global__ void __launch_bounds__(256) k_far_cell(const ccs_uniforms *__restrict
           pot -= m.w * inv;
           txx += a5 * r.x * r.x - a3; tyy += a5 * r.y * r.y - a3; tzz += a5 * r.z * r.z - a3;
           txy += a5 * r.x * r.y; txz += a5 * r.x * r.z; tyz += a5 * r.y * r.z;
+          add_tide2(g0, g1, g2, r, a5, 5.0f * a5 * inv2);   // the monopole's second gradient
           // quadrupole: a = -3 Q r / r^5 + 7.5 (r Q r) r / r^7 - 1.5 tr(Q) r / r^5,
           // potential -0.5 (3 r Q r / r^5 - tr(Q) / r^3)
           const f3 Qr = mk(Q0.x * r.x + Q0.w * r.y + Q1.x * r.z, Q0.w * r.x + Q0.y * r.y + Q1.y * r.z,
@@ -779,6 +808,11 @@ __global__ void __launch_bounds__(256) k_far_cell(const ccs_uniforms *__restrict
       force[fi] = make_float4(f.x + ax * Gm, f.y + ay * Gm, f.z + az * Gm, f.w + pot * Gm);
       tide0[fi] = make_float4(t0.x + txx * Gm, t0.y + tyy * Gm, t0.z + tzz * Gm, t0.w + txy * Gm);
       tide1[fi] = make_float4(t1.x + txz * Gm, t1.y + tyz * Gm, 0.0f, 0.0f);
+      float4 *G0 = tide2 + fi, *G1 = tide2 + kFine + 1 + fi, *G2 = tide2 + 2 * (kFine + 1) + fi;
+      const float4 h0 = *G0, h1 = *G1, h2 = *G2;
+      *G0 = make_float4(h0.x + g0.x * Gm, h0.y + g0.y * Gm, h0.z + g0.z * Gm, h0.w + g0.w * Gm);
+      *G1 = make_float4(h1.x + g1.x * Gm, h1.y + g1.y * Gm, h1.z + g1.z * Gm, h1.w + g1.w * Gm);
+      *G2 = make_float4(h2.x + g2.x * Gm, h2.y + g2.y * Gm, 0.0f, 0.0f);
     }
   }
 }
@@ -787,11 +821,11 @@ int launch_cell_tide(const ccs_uniforms *u, int S, const MeshBuf &m, cudaStream_
   const int sms = sm_count();
   cudaMemsetAsync(m.force, 0, sizeof(float4) * kFine, st);
   k_cell_tide<4><<<sms * 8, 256, 0, st>>>(u, S, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount,
-                                          m.farA, m.farT0, m.farT1, m.force, m.tide0, m.tide1, m.cellPartT,
+                                          m.farA, m.farT0, m.farT1, m.force, m.tide0, m.tide1, m.tide2, m.cellPartT,
                                           m.cellDone);
   k_block_quad<<<kCoarse / 8, 256, 0, st>>>(m.coarse, m.occ, m.occN, m.occBlocks, m.occCount, m.quad0, m.quad1);
   k_far_cell<<<sms * 4, 256, 0, st>>>(u, m.coarse, m.quad0, m.quad1, m.occ, m.occIdx, m.occN, m.occBlocks,
-                                      m.occCount, m.occAsc, m.occAscN, m.force, m.tide0, m.tide1);
+                                      m.occCount, m.occAsc, m.occAscN, m.force, m.tide0, m.tide1, m.tide2);
   return 3;
 }
 

@@ -7,8 +7,9 @@
 // cent off Newton.  This form splits the interaction exactly instead.  A particle's cloud-in-cell weights
 // w_i(k) over its 8 nodes and a source's w_j(l) over its 8 make a partition of unity over node pairs
 // (k, l); the mesh keeps the pairs of nodes more than S cells apart in every axis' Chebyshev sense
-// (k_cell_tide, unsoftened, with the tidal tensor so the gather is first order in the offset from each
-// node's centre of mass), and this pass keeps the rest, each particle pair weighted by
+// (k_cell_tide, unsoftened, with the tidal tensor and the pull's second gradient so the gather is second
+// order in the offset from each node's centre of mass), and this pass keeps the rest, each particle pair
+// weighted by
 //   W_ij = sum over (k, l) with |k - l|_inf <= S of w_i(k) w_j(l) = prod over axes of W_a(D_a, t_ia, t_ja),
 // D_a = b_ja - b_ia the base nodes' offset: 1 for |D| <= S - 1, (1 - t_j) + t_i t_j for D = S,
 // (1 - t_i) + t_i t_j for D = -S, t_i (1 - t_j) for D = S + 1, (1 - t_i) t_j for D = -S - 1, 0 beyond.

@@ -266,7 +266,8 @@ class NBody:
                  "ppforce": (PP_CAP * 16, np.float32), "ppbox": (PP_CAP, np.float32), "ppslot": (N, np.int32),
                  "diag": (N * 4, np.float32), "cellof": (N, np.uint32),
                  "tide0A": ((L.FINE + 1) * 4, np.float32), "tide1A": ((L.FINE + 1) * 4, np.float32),
-                 "ppall": (N * 4, np.float32), "walkstats": (3, np.uint32), "walkcount": ((N + 31) // 32, np.int32)}
+                 "ppall": (N * 4, np.float32), "walkstats": (3, np.uint32), "walkcount": ((N + 31) // 32, np.int32),
+                 "tide2A": (3 * (L.FINE + 1) * 4, np.float32)}
         n, dt = sizes[name]
         a = np.empty(n, dt)
         self._check(lib().ccs_read_buffer(self._h, L.BUF[name], ptr(a), a.nbytes), "ccs_read_buffer")
@@ -439,7 +440,7 @@ class NBody:
 
     def set_pp_split(self, S):
         """The stencil-split P3M (ccs_set_pp_split): every pair of mesh nodes within S cells (1..3) summed
-        particle by particle, the rest on the mesh to first order; 0 returns to the reference's pass."""
+        particle by particle, the rest on the mesh to second order; 0 returns to the reference's pass."""
         self._check(lib().ccs_set_pp_split(self._h, int(S)), "ccs_set_pp_split")
 
     def set_contact_walk(self, mode):

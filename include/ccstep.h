@@ -370,7 +370,11 @@ enum {
    * cell added, walked -- counted while the mode is 2; (N + 31) / 32 int32 --
    * seats recorded per warp of 32 particles by the last step that rebuilt the
    * grid (1537: more than fit) */
-  CCS_BUF_WALK_STATS = 23, CCS_BUF_WALK_COUNT = 24
+  CCS_BUF_WALK_STATS = 23, CCS_BUF_WALK_COUNT = 24,
+  /* the stencil-split P3M's second gradient of the pull at each cell of box A:
+   * three planes of 64^3 + 1 float4 (Gxxx Gyyy Gzzz Gxyz), (Gxxy Gxxz Gxyy
+   * Gyyz), (Gxzz Gyzz) */
+  CCS_BUF_TIDE2_A = 25
 };
 int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes);
 

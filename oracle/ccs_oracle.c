@@ -759,8 +759,25 @@ void orc_cell(const orc_uni *u, const float *fine, const float *coarse, const fl
 static v3 mass_at(const orc_uni *u, v3 p, const float *mono);
 static v3 cross_at(const orc_uni *u, const float *other, const float *mine);
 
+/* one source of mass M at offset r from the cell's centre of mass (r = source - cell): the second gradient
+ * of its pull at the cell, G_abc = d2 F_a / dx_b dx_c = M (15 r_a r_b r_c / r^7 - 3 (d_ab r_c + d_ac r_b +
+ * d_bc r_a) / r^5), added to G = (Gxxx Gyyy Gzzz Gxyz, Gxxy Gxxz Gxyy Gyyz, Gxzz Gyzz); a5 = 3 M / r^5 and
+ * a7 = 15 M / r^7 */
+static void add_tide2(double *G, double rx, double ry, double rz, double a5, double a7) {
+  G[0] += a7 * rx * rx * rx - 3.0 * a5 * rx;
+  G[1] += a7 * ry * ry * ry - 3.0 * a5 * ry;
+  G[2] += a7 * rz * rz * rz - 3.0 * a5 * rz;
+  G[3] += a7 * rx * ry * rz;
+  G[4] += a7 * rx * rx * ry - a5 * ry;
+  G[5] += a7 * rx * rx * rz - a5 * rz;
+  G[6] += a7 * rx * ry * ry - a5 * rx;
+  G[7] += a7 * ry * ry * rz - a5 * rz;
+  G[8] += a7 * rx * rz * rz - a5 * rx;
+  G[9] += a7 * ry * rz * rz - a5 * ry;
+}
+
 void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, float *force, float *tide0,
-                   float *tide1) {
+                   float *tide1, float *tide2) {
   const float eps2 = 1e-6f * u->eps2Mesh;   /* keeps two coinciding centres of mass finite, as the library's */
   memcpy(force + 4 * ORC_FINE, fine + 4 * ORC_FINE, 16);
   /* each occupied block's centre of mass and second moment, from its occupied cells at their centres of mass */
@@ -791,6 +808,7 @@ void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coar
     v3 x = vdivs(ld3(mc), mc[3]);
     int cc[3] = {c[0] >> 2, c[1] >> 2, c[2] >> 2};
     double acc[3] = {0, 0, 0}, pot = 0, T[6] = {0, 0, 0, 0, 0, 0};   /* Txx Tyy Tzz Txy Txz Tyz */
+    double G[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     /* near: the fine cells of the 5^3 blocks around, beyond the stencil, unsoftened */
     for (int kz = -2; kz <= 2; kz++)
       for (int ky = -2; ky <= 2; ky++)
@@ -816,6 +834,7 @@ void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coar
                 pot -= M * inv;
                 T[0] += a5 * rx * rx - a3; T[1] += a5 * ry * ry - a3; T[2] += a5 * rz * rz - a3;
                 T[3] += a5 * rx * ry; T[4] += a5 * rx * rz; T[5] += a5 * ry * rz;
+                add_tide2(G, rx, ry, rz, a5, 5.0 * a5 * inv2);
               }
         }
     /* far: every occupied block more than two from the cell's own, monopole + quadrupole, at the cell */
@@ -832,6 +851,7 @@ void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coar
       pot -= M * inv;
       T[0] += a5 * r[0] * r[0] - a3; T[1] += a5 * r[1] * r[1] - a3; T[2] += a5 * r[2] * r[2] - a3;
       T[3] += a5 * r[0] * r[1]; T[4] += a5 * r[0] * r[2]; T[5] += a5 * r[1] * r[2];
+      add_tide2(G, r[0], r[1], r[2], a5, 5.0 * a5 * inv2);
       double Qr[3] = {q[4] * r[0] + q[7] * r[1] + q[8] * r[2], q[7] * r[0] + q[5] * r[1] + q[9] * r[2],
                       q[8] * r[0] + q[9] * r[1] + q[6] * r[2]};
       double rQr = r[0] * Qr[0] + r[1] * Qr[1] + r[2] * Qr[2], tr = q[4] + q[5] + q[6];
@@ -844,6 +864,11 @@ void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coar
     T0[0] = (float)(T[0] * u->Gm); T0[1] = (float)(T[1] * u->Gm); T0[2] = (float)(T[2] * u->Gm);
     T0[3] = (float)(T[3] * u->Gm);
     T1[0] = (float)(T[4] * u->Gm); T1[1] = (float)(T[5] * u->Gm); T1[2] = T1[3] = 0.0f;
+    if (tide2) {   /* three planes of (64^3 + 1) float4, as the library's */
+      for (int k = 0; k < 10; k++) tide2[(size_t)(k >> 2) * 4 * (ORC_FINE + 1) + 4 * (size_t)ci + (k & 3)] = (float)(G[k] * u->Gm);
+      tide2[2 * 4 * (size_t)(ORC_FINE + 1) + 4 * (size_t)ci + 2] = 0.0f;
+      tide2[2 * 4 * (size_t)(ORC_FINE + 1) + 4 * (size_t)ci + 3] = 0.0f;
+    }
   }
   free(bq);
 }
@@ -896,9 +921,9 @@ void orc_pp_split(const orc_uni *u, int S, const float *pos4, const float *mat, 
 }
 
 void orc_gather_split(const orc_uni *u, const float *pos4, const float *fineA, const float *forceA,
-                      const float *tideA0, const float *tideA1, const float *fineB, const float *forceB,
-                      const float *tideB0, const float *tideB1, const float *monoA, const float *monoB,
-                      const float *ppAll, float *grav4) {
+                      const float *tideA0, const float *tideA1, const float *tideA2, const float *fineB,
+                      const float *forceB, const float *tideB0, const float *tideB1, const float *tideB2,
+                      const float *monoA, const float *monoB, const float *ppAll, float *grav4) {
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < u->N; i++) {
     v3 p = ld3(pos4 + 4 * (size_t)i), grav = V3(0, 0, 0);
@@ -907,6 +932,7 @@ void orc_gather_split(const orc_uni *u, const float *pos4, const float *fineA, c
     if (box >= 0) {
       const float *F = box == 0 ? forceA : forceB, *M = box == 0 ? fineA : fineB;
       const float *T0 = box == 0 ? tideA0 : tideB0, *T1 = box == 0 ? tideA1 : tideB1;
+      const float *T2 = box == 0 ? tideA2 : tideB2;
       float f[3], t[3];
       int cf[3];
       for (int k = 0; k < 3; k++) { f[k] = floorf(g[k]); t[k] = g[k] - f[k]; cf[k] = (int)f[k]; }
@@ -924,6 +950,13 @@ void orc_gather_split(const orc_uni *u, const float *pos4, const float *fineA, c
         v3 Td = V3(t0[0] * d.x + t0[3] * d.y + t1[0] * d.z,
                    t0[3] * d.x + t0[1] * d.y + t1[1] * d.z,
                    t1[0] * d.x + t1[1] * d.y + t0[2] * d.z);
+        if (T2) {   /* second order: half the pull's second gradient along d, twice */
+          const float *g0 = T2 + 4 * c, *g1 = T2 + 4 * ((size_t)(ORC_FINE + 1) + c), *g2 = T2 + 4 * (2 * (size_t)(ORC_FINE + 1) + c);
+          float xx = d.x * d.x, yy = d.y * d.y, zz = d.z * d.z, xy = d.x * d.y, xz = d.x * d.z, yz = d.y * d.z;
+          Td = vadd(Td, V3(0.5f * (g0[0] * xx + g1[2] * yy + g2[0] * zz) + g1[0] * xy + g1[1] * xz + g0[3] * yz,
+                           0.5f * (g1[0] * xx + g0[1] * yy + g2[1] * zz) + g1[2] * xy + g0[3] * xz + g1[3] * yz,
+                           0.5f * (g1[1] * xx + g1[3] * yy + g0[2] * zz) + g0[3] * xy + g2[0] * xz + g2[1] * yz));
+        }
         grav = vadd(grav, vmuls(vadd(ld3(fv), Td), w3[0] * w3[1] * w3[2]));
       }
       grav = vsub(grav, vmuls(ld3(F + 4 * ORC_FINE), u->Gm));

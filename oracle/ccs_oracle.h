@@ -108,15 +108,18 @@ void orc_cell(const orc_uni *u, const float *fine, const float *coarse, const fl
 /* the stencil-split P3M (the library's ccs_set_pp_split; no counterpart in the reference): the cell pass
  * without the node pairs within S cells, unsoftened, with tides, and the far field at each cell from every
  * block more than two away as its monopole and quadrupole (force, tide0 = Txx Tyy Tzz Txy, tide1 = Txz
- * Tyz, all x Gm); every particle's pairs inside the stencil (out4: pull, potential x Gm); the first-order
- * gather from each node's centre of mass plus the particle's pairs (grav4) */
+ * Tyz, tide2 = the pull's second gradient, three planes of (64^3 + 1) float4: Gxxx Gyyy Gzzz Gxyz, Gxxy
+ * Gxxz Gxyy Gyyz, Gxzz Gyzz -- the near sources' and the far blocks' monopoles'; all x Gm; tide2 may be
+ * NULL); every particle's pairs inside the stencil (out4: pull, potential x Gm); the gather from each
+ * node's centre of mass, second order (first order where tideA2 / tideB2 is NULL), plus the particle's
+ * pairs (grav4) */
 void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, float *force, float *tide0,
-                   float *tide1);
+                   float *tide1, float *tide2);
 void orc_pp_split(const orc_uni *u, int S, const float *pos4, const float *mat, float *out4);
 void orc_gather_split(const orc_uni *u, const float *pos4, const float *fineA, const float *forceA,
-                      const float *tideA0, const float *tideA1, const float *fineB, const float *forceB,
-                      const float *tideB0, const float *tideB1, const float *monoA, const float *monoB,
-                      const float *ppAll, float *grav4);
+                      const float *tideA0, const float *tideA1, const float *tideA2, const float *fineB,
+                      const float *forceB, const float *tideB0, const float *tideB1, const float *tideB2,
+                      const float *monoA, const float *monoB, const float *ppAll, float *grav4);
 void orc_pp_gather(const orc_uni *u, const float *pos4, const float *mat, const int *index, int cap,
                    float *list4, float *box);
 void orc_pp_force(const orc_uni *u, const float *list4, const float *box, int count, int cap,

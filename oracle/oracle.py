@@ -145,9 +145,9 @@ def lib():
         L.orc_sim_pass.argtypes = [C.POINTER(Uni)] + [P] * 11 + [C.c_int] + [P] * 4
         L.orc_diag.argtypes = [C.POINTER(Uni)] + [P] * 9 + [C.c_int, P]
         L.orc_contact_pairs.argtypes = [C.POINTER(Uni), P, P, C.c_int, P, P]
-        L.orc_cell_tide.argtypes = [C.POINTER(Uni), C.c_int] + [P] * 5
+        L.orc_cell_tide.argtypes = [C.POINTER(Uni), C.c_int] + [P] * 6
         L.orc_pp_split.argtypes = [C.POINTER(Uni), C.c_int, P, P, P]
-        L.orc_gather_split.argtypes = [C.POINTER(Uni)] + [P] * 13
+        L.orc_gather_split.argtypes = [C.POINTER(Uni)] + [P] * 15
         L.orc_rigid.argtypes = [C.c_int] + [P] * 10 + [C.c_float, P, P]
         L.orc_morton.argtypes = [C.c_int, P, P, P, P, P]
         L.orc_engine_new.restype = P
@@ -281,13 +281,15 @@ def contact_pairs(u, pos4, seats, cap=64):
 
 
 def cell_tide(u, S, fine, coarse):
-    """The stencil-split P3M's cell pass, near and far: (force, tide0, tide1), each (64^3 + 1) x 4."""
+    """The stencil-split P3M's cell pass, near and far: (force, tide0, tide1), each (64^3 + 1) x 4, and
+    tide2, the pull's second gradient, 3 x (64^3 + 1) x 4 (the library's three planes)."""
     force = np.zeros((FINE + 1, 4), np.float32)
     t0 = np.zeros((FINE + 1, 4), np.float32)
     t1 = np.zeros((FINE + 1, 4), np.float32)
+    t2 = np.zeros((3, FINE + 1, 4), np.float32)
     a = [np.ascontiguousarray(x, np.float32) for x in (fine, coarse)]
-    lib().orc_cell_tide(C.byref(u), int(S), *[ptr(x) for x in a], ptr(force), ptr(t0), ptr(t1))
-    return force, t0, t1
+    lib().orc_cell_tide(C.byref(u), int(S), *[ptr(x) for x in a], ptr(force), ptr(t0), ptr(t1), ptr(t2))
+    return force, t0, t1, t2
 
 
 def pp_split(u, S, pos4, mat):
@@ -299,11 +301,16 @@ def pp_split(u, S, pos4, mat):
 
 
 def gather_split(u, pos4, meshA, meshB, monoA, monoB, ppall):
-    """The stencil-split P3M's gravity at every particle; meshA/meshB = (fine, force, tide0, tide1)."""
+    """The stencil-split P3M's gravity at every particle; meshA/meshB = (fine, force, tide0, tide1[, tide2]):
+    with tide2 the second-order gather, without it the first-order one."""
     pos4 = np.ascontiguousarray(pos4, np.float32)
     out = np.zeros((len(pos4), 4), np.float32)
-    arrs = [np.ascontiguousarray(x, np.float32) for x in (*meshA, *meshB, monoA, monoB, ppall)]
-    lib().orc_gather_split(C.byref(u), ptr(pos4), *[ptr(x) for x in arrs], ptr(out))
+
+    def mesh(m):
+        m = [np.ascontiguousarray(x, np.float32) for x in m]
+        return [m[0], m[1], m[2], m[3], m[4] if len(m) > 4 else None]
+    arrs = mesh(meshA) + mesh(meshB) + [np.ascontiguousarray(x, np.float32) for x in (monoA, monoB, ppall)]
+    lib().orc_gather_split(C.byref(u), ptr(pos4), *[None if x is None else ptr(x) for x in arrs], ptr(out))
     return out
 
 

@@ -31,7 +31,7 @@ def moving_state(orc, target_move, impactor_move):
     """A settled 16k state on the impact's schedule whose first step is a kick: every particle takes its
     body's bulk velocity (no spin), which moves the target's particles `target_move` and the impactor's
     `impactor_move` radii in the step, each body in its own direction.  The record lets its owner have moved
-    about 0.085 of a radius, and every particle about 0.3."""
+    about 0.15 of a radius, and every particle about 0.23."""
     osim, pos, vel, mat = settled(orc)
     assert (pos[:, 3] < 3.5).sum() > 1000 and (pos[:, 3] > 3.5).sum() > 1000     # both bodies
     com = (pos[:, :3].astype(np.float64) * mat[:, None]).sum(0) / mat.sum()
