@@ -26,7 +26,7 @@ COARSE = 4096
 
 BUF = {"seats": 5, "fineA": 6, "forceA": 7, "monoA": 8, "coarseA": 9, "farA": 10, "fineB": 11, "forceB": 12,
        "monoB": 13, "pplist": 14, "ppforce": 15, "ppbox": 16, "ppslot": 17, "diag": 18, "cellof": 19,
-       "tide0A": 20, "tide1A": 21, "ppall": 22, "walkstats": 23, "walkcount": 24, "tide2A": 25}
+       "tide0A": 20, "tide1A": 21, "ppall": 22, "walkstats": 23, "walkcount": 24, "tide2A": 25, "fineQA": 26}
 
 # every symbol include/ccstep.h declares
 EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_make_bodies", "ccs_make_bodies_device",

@@ -417,6 +417,7 @@ void pass_mesh_box(ccs_handle *h, const ccs_uniforms *U, int b) {
   cudaEvent_t eb, ee;
   time_begin(h, 2, &eb, &ee);
   h->launches += launch_deposit(U, h->N, b, h->pos[h->cur], h->mat, m.mono, m.fine, h->st);
+  if (h->ppSplit) h->launches += launch_node_moments(U, h->N, b, h->pos[h->cur], h->mat, m, h->st);
   time_end(h, ee);
   cudaMemsetAsync(m.occCount, 0, sizeof(int), h->st);
   h->launches += launch_coarse(m, h->st);
@@ -588,7 +589,7 @@ int block_launches(const ccs_handle *h, const StepPlan *plans, int M, bool split
   for (int k = 0; k < M; ++k) {
     if (h->ppSplit && !h->field) {                  // the stencil-split P3M: walk + tail every step
       per += 2 + (plans[k].slots ? 1 : 0);
-      if (plans[k].mesh) per += 7 * (1 + (plans[k].u.boxB > 0.5f)) + pp_split_launches();
+      if (plans[k].mesh) per += 8 * (1 + (plans[k].u.boxB > 0.5f)) + pp_split_launches();
       continue;
     }
     per += 1;                                       // contact step
@@ -1007,6 +1008,7 @@ int ensure_split_buffers(ccs_handle *h) {
     rc |= dev_alloc(h, &m.tide0, kFine + 1);
     rc |= dev_alloc(h, &m.tide1, kFine + 1);
     rc |= dev_alloc(h, &m.tide2, 3 * (size_t)(kFine + 1));
+    rc |= dev_alloc(h, &m.fineQ, 2 * (size_t)(kFine + 1));
     rc |= dev_alloc(h, &m.cellPartT, (size_t)kCoarse * kCellChunks * 64 * 5);
     rc |= dev_alloc(h, &m.quad0, kCoarse);
     rc |= dev_alloc(h, &m.quad1, kCoarse);
@@ -1021,7 +1023,7 @@ int ensure_split_buffers(ccs_handle *h) {
   if (rc) {
     for (int b = 0; b < 2; ++b) {
       dev_free(h->pm[b].tide0); dev_free(h->pm[b].tide1); dev_free(h->pm[b].cellPartT);
-      dev_free(h->pm[b].quad0); dev_free(h->pm[b].quad1); dev_free(h->pm[b].tide2);
+      dev_free(h->pm[b].quad0); dev_free(h->pm[b].quad1); dev_free(h->pm[b].tide2); dev_free(h->pm[b].fineQ);
     }
     dev_free(h->splitStart); dev_free(h->splitCells); dev_free(h->splitNCells); dev_free(h->splitSrc);
     dev_free(h->splitSrcT); dev_free(h->ppAll); dev_free(h->splitWork);
@@ -1047,7 +1049,7 @@ void free_state(ccs_handle *h) {
     dev_free(m.occ); dev_free(m.occIdx); dev_free(m.occN); dev_free(m.occBlocks); dev_free(m.occCount);
     dev_free(m.occAsc); dev_free(m.occAscN); dev_free(m.cellPart); dev_free(m.cellDone);
     dev_free(m.tide0); dev_free(m.tide1); dev_free(m.cellPartT); dev_free(m.quad0); dev_free(m.quad1);
-    dev_free(m.tide2);
+    dev_free(m.tide2); dev_free(m.fineQ);
   }
   dev_free(h->splitStart); dev_free(h->splitCells); dev_free(h->splitNCells); dev_free(h->splitSrc);
   dev_free(h->splitSrcT); dev_free(h->ppAll); dev_free(h->splitWork);
@@ -2464,6 +2466,7 @@ int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes) {
     case CCS_BUF_WALK_STATS: src = h->recStats; n = 12; break;
     case CCS_BUF_WALK_COUNT: src = h->recN; n = 4 * ((N + 31) / 32); break;
     case CCS_BUF_TIDE2_A: src = h->pm[0].tide2; n = 16 * 3 * (size_t)(kFine + 1); break;
+    case CCS_BUF_FINEQ_A: src = h->pm[0].fineQ; n = 16 * 2 * (size_t)(kFine + 1); break;
     default: h->err = "unknown buffer"; return CCS_E_ARG;
   }
   if (!src) {

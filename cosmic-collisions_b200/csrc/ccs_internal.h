@@ -72,6 +72,7 @@ struct MeshBuf {
   // pull's second gradient (tide2: three planes of kFine + 1), and the cell pass's partial sums of pull,
   // potential, tide and second gradient: [listed block][source chunk][5][cell]
   float4 *tide0 = nullptr, *tide1 = nullptr, *tide2 = nullptr, *cellPartT = nullptr;
+  float4 *fineQ = nullptr;   // each cell's second moment about its centre of mass: two planes of kFine + 1
   float4 *quad0 = nullptr, *quad1 = nullptr;   // each block's second moment about its centre of mass
 };
 
@@ -159,6 +160,9 @@ int launch_far(const MeshBuf &m, cudaStream_t st);
 int launch_cell(const ccs_uniforms *u, const MeshBuf &m, cudaStream_t st, int split = 4);
 // the stencil-split P3M (S = 1, 2, 3 nodes): the cell pass without the stencil's node pairs, with tides
 int launch_cell_tide(const ccs_uniforms *u, int S, const MeshBuf &m, cudaStream_t st);
+// ... after the deposit of box `box`: each cell's second moment about its centre of mass (m.fineQ)
+int launch_node_moments(const ccs_uniforms *u, int N, int box, const float4 *pos, const float *mat,
+                        const MeshBuf &m, cudaStream_t st);
 // ... and the pair pass over every particle inside it: sort by (box, base node), then the stencil's pairs;
 // out gets each particle's (pull, potential) x Gm
 // (work: split_work_bytes(N) of scratch for the pair pass's items and counters)

@@ -134,6 +134,109 @@ int launch_deposit(const ccs_uniforms *u, int N, int box, const float4 *pos, con
 }
 
 // ---------------------------------------------------------------------------
+// the stencil-split P3M's node moments: each fine cell's second moment about its own centre of mass, from
+// the particles' cloud-in-cell weights, Q = sum w m (x - X)(x - X)^T as two planes of kFine + 1 float4,
+// (Qxx, Qyy, Qzz, Qxy) and (Qxz, Qyz).  With them the split form's mesh carries each node's quadrupole as a
+// source, the reaction to the second-order gather's pull on the node's spread (without it that pull has
+// no counterpart, and momentum drifts).  After the deposit (the centres of mass); the same grouping by
+// base cell as the deposit, its 8 corners x 6 moments reduce-scattered over the warp in two rounds.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_node_moments(const ccs_uniforms *__restrict__ U, int box,
+                                                         const float4 *__restrict__ pos,
+                                                         const float *__restrict__ mat,
+                                                         const float4 *__restrict__ fine, float4 *fineQ) {
+  const ccs_uniforms &u = *U;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  bool in = false;
+  int bx = 0, by = 0, bz = 0;
+  f3 t = mk(0, 0, 0), p = mk(0, 0, 0);
+  float mr = 0.0f;
+  if (i < u.N) {
+    p = xyz(pos[i]);
+    mr = mat[i];
+    f3 g;
+    if (box_of(u, p, g) == box) {
+      in = true;
+      const float fx = floorf(g.x), fy = floorf(g.y), fz = floorf(g.z);
+      t = mk(g.x - fx, g.y - fy, g.z - fz);
+      bx = (int)fx;
+      by = (int)fy;
+      bz = (int)fz;
+    }
+  }
+  const unsigned inMask = __ballot_sync(0xFFFFFFFFu, in);
+  if (inMask == 0u) return;
+  // corner k's moments of this particle (zero where the corner is past the mesh or the lane is out)
+  auto corner = [&](int k, bool on, float (&m6)[6]) {
+    const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
+    const bool ok = on && bx + ox <= 63 && by + oy <= 63 && bz + oz <= 63;
+    float w = 0.0f;
+    f3 d = mk(0, 0, 0);
+    if (ok) {
+      w = (ox ? t.x : 1.0f - t.x) * (oy ? t.y : 1.0f - t.y) * (oz ? t.z : 1.0f - t.z) * mr;
+      const float4 c = __ldg(fine + fine_index(bx + ox, by + oy, bz + oz));
+      d = p - xyz(c) * fdiv(1.0f, c.w);
+    }
+    m6[0] = w * d.x * d.x; m6[1] = w * d.y * d.y; m6[2] = w * d.z * d.z;
+    m6[3] = w * d.x * d.y; m6[4] = w * d.x * d.z; m6[5] = w * d.y * d.z;
+  };
+  const int key = in ? (bz << 16) | (by << 8) | bx : -1 - lane;
+  constexpr int kGroups = 4;
+  unsigned todo = inMask, lone = 0u;
+#pragma unroll 1
+  for (int gi = 0; gi < kGroups && todo; ++gi) {
+    const int key0 = __shfl_sync(0xFFFFFFFFu, key, __ffs(todo) - 1);
+    const bool member = in && key == key0;
+    const unsigned gm = __ballot_sync(0xFFFFFFFFu, member);
+    todo &= ~gm;
+    if (__popc(gm) == 1) {
+      lone |= gm;
+      continue;
+    }
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {   // corners 4 half .. 4 half + 3, 8 slots a corner (6 used)
+      float v[32];
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        float m6[6];
+        corner(4 * half + kk, member, m6);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[8 * kk + c] = c < 6 ? m6[c] : 0.0f;
+      }
+      reduce_scatter32(v, lane);
+      const int k = 4 * half + (lane >> 3), comp = lane & 7;
+      const int cx = (key0 & 0xFF) + (k & 1), cy = ((key0 >> 8) & 0xFF) + ((k >> 1) & 1), cz = (key0 >> 16) + (k >> 2);
+      if (comp < 6 && cx <= 63 && cy <= 63 && cz <= 63 && v[0] != 0.0f)
+        atomicAdd(reinterpret_cast<float *>(fineQ + (size_t)(comp >> 2) * (kFine + 1) + fine_index(cx, cy, cz)) +
+                      (comp & 3),
+                  v[0]);
+    }
+  }
+  if (((todo | lone) >> lane) & 1u) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
+      const int cx = bx + ox, cy = by + oy, cz = bz + oz;
+      if (cx > 63 || cy > 63 || cz > 63) continue;
+      float m6[6];
+      corner(k, true, m6);
+      const int fi = fine_index(cx, cy, cz);
+      atomicAdd(fineQ + fi, make_float4(m6[0], m6[1], m6[2], m6[3]));
+      atomicAdd(reinterpret_cast<float *>(fineQ + kFine + 1 + fi) + 0, m6[4]);
+      atomicAdd(reinterpret_cast<float *>(fineQ + kFine + 1 + fi) + 1, m6[5]);
+    }
+  }
+}
+
+int launch_node_moments(const ccs_uniforms *u, int N, int box, const float4 *pos, const float *mat,
+                        const MeshBuf &m, cudaStream_t st) {
+  cudaMemsetAsync(m.fineQ, 0, sizeof(float4) * 2 * (kFine + 1), st);
+  k_node_moments<<<blocks_for(N), kBlock, 0, st>>>(u, box, pos, mat, m.fine, m.fineQ);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
 // coarse and monopole: src/glsl-sim.js:222-251.  One warp per coarse block:
 // its lanes load the block's 4^3 fine cells together into shared memory, and
 // lane 0 sums them in the reference's loop order (bit for bit).  The same warp
@@ -543,14 +646,18 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
                                                           const float4 *__restrict__ farA,
                                                           const float4 *__restrict__ farT0,
                                                           const float4 *__restrict__ farT1,
+                                                          const float4 *__restrict__ fineQ,
                                                           float4 *__restrict__ force, float4 *__restrict__ tide0,
                                                           float4 *__restrict__ tide1, float4 *__restrict__ tide2,
                                                           float4 *__restrict__ cellPart, int *__restrict__ cellDone) {
   constexpr int kCellThreads = 64 * SPLIT;
   constexpr int kRows = 5;               // partial rows a cell: pull + potential, the tide (2), G (2 + 1 in row 2's zw)
+  constexpr int kBatch = 512;
   __shared__ int nbK[128], nbOff[129];
-  __shared__ float4 src[kCellBatch];
-  __shared__ int sfc[kCellBatch];        // a source's fine cell, x | y << 6 | z << 12
+  __shared__ float4 src[kBatch];
+  __shared__ float4 sq0[kBatch];         // a source's second moment about its centre of mass: Qxx Qyy Qzz Qxy
+  __shared__ float2 sq1[kBatch];         // Qxz Qyz
+  __shared__ int sfc[kBatch];            // a source's fine cell, x | y << 6 | z << 12
   __shared__ float4 part[kRows][SPLIT][64];
   __shared__ int last;
   const int t = threadIdx.x, cellT = t & 63, q = t >> 6, lane = t & 31;
@@ -601,8 +708,8 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
     const int total = nbOff[125];
     const int c0 = (int)((long long)total * chunk / kCellChunks);
     const int c1 = (int)((long long)total * (chunk + 1) / kCellChunks);
-    for (int b0 = c0; b0 < c1; b0 += kCellBatch) {
-      const int b1 = min(b0 + kCellBatch, c1);
+    for (int b0 = c0; b0 < c1; b0 += kBatch) {
+      const int b1 = min(b0 + kBatch, c1);
       for (int e = b0 + t; e < b1; e += kCellThreads) {
         int lo = 0, hi = 125;
         while (hi - lo > 1) {
@@ -613,8 +720,12 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
         const int k = nbK[lo], i = e - nbOff[lo];
         src[e - b0] = __ldg(occ + (size_t)k * 64 + i);
         const int ix = __ldg(occIdx + (size_t)k * 64 + i);
-        sfc[e - b0] = ((k & 15) * 4 + (ix & 3)) | (((k >> 4 & 15) * 4 + ((ix >> 2) & 3)) << 6) |
-                      (((k >> 8) * 4 + (ix >> 4)) << 12);
+        const int fx = (k & 15) * 4 + (ix & 3), fy = (k >> 4 & 15) * 4 + ((ix >> 2) & 3), fz = (k >> 8) * 4 + (ix >> 4);
+        sfc[e - b0] = fx | (fy << 6) | (fz << 12);
+        const int fi = fine_index(fx, fy, fz);
+        sq0[e - b0] = __ldg(fineQ + fi);
+        const float4 q1 = __ldg(fineQ + kFine + 1 + fi);
+        sq1[e - b0] = make_float2(q1.x, q1.y);
       }
       __syncthreads();
       if (mine) {
@@ -638,6 +749,16 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
           txz += a5 * r.x * r.z;
           tyz += a5 * r.y * r.z;
           add_tide2(g0, g1, g2, r, a5, 5.0f * a5 * inv2);
+          // the source's spread about its centre of mass as a quadrupole (the reaction to the second-order
+          // gather's pull on a node's spread): a = -3 Q r / r^5 + 7.5 (r Q r) r / r^7 - 1.5 tr(Q) r / r^5
+          const float4 q0 = sq0[i];
+          const float2 q1 = sq1[i];
+          const f3 Qr = mk(q0.x * r.x + q0.w * r.y + q1.x * r.z, q0.w * r.x + q0.y * r.y + q1.y * r.z,
+                           q1.x * r.x + q1.y * r.y + q0.z * r.z);
+          const float rQr = dot(r, Qr), tr = q0.x + q0.y + q0.z, inv5 = inv2 * inv2 * inv;
+          const float cq = 7.5f * rQr * inv5 * inv2 - 1.5f * tr * inv5;
+          acc = acc + r * cq - Qr * (3.0f * inv5);
+          pot -= 0.5f * (3.0f * rQr * inv5 - tr * inv2 * inv);
         }
       }
       __syncthreads();
@@ -689,13 +810,16 @@ __global__ void __launch_bounds__(64 * SPLIT) k_cell_tide(const ccs_uniforms *__
 }
 }  // namespace
 
-// each occupied block's second moment about its centre of mass, from its occupied cells taken as points at
-// their own centres of mass: Q = sum m (x - X)(x - X)^T, q0 = (Qxx, Qyy, Qzz, Qxy), q1 = (Qxz, Qyz).  A warp a
-// block, the lanes over its (up to 64) cells.
+// each occupied block's second moment about its centre of mass, from its occupied cells' own moments and
+// their centres of mass (parallel axes): Q = sum (m (x - X)(x - X)^T + Q_cell), q0 = (Qxx, Qyy, Qzz, Qxy), q1 =
+// (Qxz, Qyz).  A warp a block, the lanes over its (up to 64) cells.
 __global__ void __launch_bounds__(256) k_block_quad(const float4 *__restrict__ coarse,
-                                                    const float4 *__restrict__ occ, const int *__restrict__ occN,
+                                                    const float4 *__restrict__ occ,
+                                                    const uint8_t *__restrict__ occIdx,
+                                                    const int *__restrict__ occN,
                                                     const int *__restrict__ occBlocks,
-                                                    const int *__restrict__ occCount, float4 *__restrict__ q0,
+                                                    const int *__restrict__ occCount,
+                                                    const float4 *__restrict__ fineQ, float4 *__restrict__ q0,
                                                     float4 *__restrict__ q1) {
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -705,11 +829,15 @@ __global__ void __launch_bounds__(256) k_block_quad(const float4 *__restrict__ c
   const f3 X = xyz(mb) * fdiv(1.0f, mb.w);
   float s[6] = {0, 0, 0, 0, 0, 0};
   const int n = occN[b];
+  const int bx = b & 15, by = (b >> 4) & 15, bz = b >> 8;
   for (int c = lane; c < n; c += 32) {
     const float4 e = occ[(size_t)b * 64 + c];
     const f3 d = xyz(e) - X;
-    s[0] += e.w * d.x * d.x; s[1] += e.w * d.y * d.y; s[2] += e.w * d.z * d.z;
-    s[3] += e.w * d.x * d.y; s[4] += e.w * d.x * d.z; s[5] += e.w * d.y * d.z;
+    const int ix = occIdx[(size_t)b * 64 + c];
+    const int fi = fine_index(bx * 4 + (ix & 3), by * 4 + ((ix >> 2) & 3), bz * 4 + (ix >> 4));
+    const float4 Q0 = fineQ[fi], Q1 = fineQ[kFine + 1 + fi];   // the cell's own spread, by parallel axes
+    s[0] += e.w * d.x * d.x + Q0.x; s[1] += e.w * d.y * d.y + Q0.y; s[2] += e.w * d.z * d.z + Q0.z;
+    s[3] += e.w * d.x * d.y + Q0.w; s[4] += e.w * d.x * d.z + Q1.x; s[5] += e.w * d.y * d.z + Q1.y;
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k)
@@ -821,9 +949,10 @@ int launch_cell_tide(const ccs_uniforms *u, int S, const MeshBuf &m, cudaStream_
   const int sms = sm_count();
   cudaMemsetAsync(m.force, 0, sizeof(float4) * kFine, st);
   k_cell_tide<4><<<sms * 8, 256, 0, st>>>(u, S, m.fine, m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount,
-                                          m.farA, m.farT0, m.farT1, m.force, m.tide0, m.tide1, m.tide2, m.cellPartT,
-                                          m.cellDone);
-  k_block_quad<<<kCoarse / 8, 256, 0, st>>>(m.coarse, m.occ, m.occN, m.occBlocks, m.occCount, m.quad0, m.quad1);
+                                          m.farA, m.farT0, m.farT1, m.fineQ, m.force, m.tide0, m.tide1, m.tide2,
+                                          m.cellPartT, m.cellDone);
+  k_block_quad<<<kCoarse / 8, 256, 0, st>>>(m.coarse, m.occ, m.occIdx, m.occN, m.occBlocks, m.occCount, m.fineQ,
+                                            m.quad0, m.quad1);
   k_far_cell<<<sms * 4, 256, 0, st>>>(u, m.coarse, m.quad0, m.quad1, m.occ, m.occIdx, m.occN, m.occBlocks,
                                       m.occCount, m.occAsc, m.occAscN, m.force, m.tide0, m.tide1, m.tide2);
   return 3;

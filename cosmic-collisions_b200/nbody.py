@@ -267,7 +267,7 @@ class NBody:
                  "diag": (N * 4, np.float32), "cellof": (N, np.uint32),
                  "tide0A": ((L.FINE + 1) * 4, np.float32), "tide1A": ((L.FINE + 1) * 4, np.float32),
                  "ppall": (N * 4, np.float32), "walkstats": (3, np.uint32), "walkcount": ((N + 31) // 32, np.int32),
-                 "tide2A": (3 * (L.FINE + 1) * 4, np.float32)}
+                 "tide2A": (3 * (L.FINE + 1) * 4, np.float32), "fineQA": (2 * (L.FINE + 1) * 4, np.float32)}
         n, dt = sizes[name]
         a = np.empty(n, dt)
         self._check(lib().ccs_read_buffer(self._h, L.BUF[name], ptr(a), a.nbytes), "ccs_read_buffer")

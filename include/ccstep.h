@@ -374,7 +374,10 @@ enum {
   /* the stencil-split P3M's second gradient of the pull at each cell of box A:
    * three planes of 64^3 + 1 float4 (Gxxx Gyyy Gzzz Gxyz), (Gxxy Gxxz Gxyy
    * Gyyz), (Gxzz Gyzz) */
-  CCS_BUF_TIDE2_A = 25
+  CCS_BUF_TIDE2_A = 25,
+  /* ... and each cell's second moment about its centre of mass: two planes
+   * of 64^3 + 1 float4 (Qxx Qyy Qzz Qxy), (Qxz Qyz) */
+  CCS_BUF_FINEQ_A = 26
 };
 int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes);
 

@@ -759,6 +759,53 @@ void orc_cell(const orc_uni *u, const float *fine, const float *coarse, const fl
 static v3 mass_at(const orc_uni *u, v3 p, const float *mono);
 static v3 cross_at(const orc_uni *u, const float *other, const float *mine);
 
+/* each fine cell's second moment about its own centre of mass (fine, after orc_deposit), from the particles'
+ * cloud-in-cell weights: Q = sum w m (x - X)(x - X)^T, two planes of (64^3 + 1) float4, (Qxx Qyy Qzz Qxy) and
+ * (Qxz Qyz) -- the split form's node quadrupoles (binary64 sums, stored as binary32) */
+void orc_node_moments(const orc_uni *u, int box, const float *pos4, const float *mat, const float *fine,
+                      float *fineQ) {
+  double *q = (double *)calloc((size_t)ORC_FINE * 6, sizeof(double));
+  for (int i = 0; i < u->N; i++) {
+    float pp[3] = {pos4[4 * (size_t)i], pos4[4 * (size_t)i + 1], pos4[4 * (size_t)i + 2]}, g[3];
+    if (orc_box_of(u, pp, g) != box) continue;
+    float f[3], t[3];
+    for (int k = 0; k < 3; k++) { f[k] = floorf(g[k]); t[k] = g[k] - f[k]; }
+    for (int k = 0; k < 8; k++) {
+      int o[3] = {k & 1, (k >> 1) & 1, k >> 2}, c[3];
+      double w = mat[i];
+      for (int d = 0; d < 3; d++) { c[d] = (int)f[d] + o[d]; w *= o[d] ? t[d] : 1.0 - t[d]; }
+      if (c[0] > 63 || c[1] > 63 || c[2] > 63) continue;
+      int ci = fine_index(c[0], c[1], c[2]);
+      const float *m = fine + 4 * (size_t)ci;
+      double d[3] = {pp[0] - (double)m[0] / m[3], pp[1] - (double)m[1] / m[3], pp[2] - (double)m[2] / m[3]};
+      double *Q = q + 6 * (size_t)ci;
+      Q[0] += w * d[0] * d[0]; Q[1] += w * d[1] * d[1]; Q[2] += w * d[2] * d[2];
+      Q[3] += w * d[0] * d[1]; Q[4] += w * d[0] * d[2]; Q[5] += w * d[1] * d[2];
+    }
+  }
+  memset(fineQ, 0, sizeof(float) * 8 * (ORC_FINE + 1));
+  for (int ci = 0; ci < ORC_FINE; ci++) {
+    const double *Q = q + 6 * (size_t)ci;
+    float *a = fineQ + 4 * (size_t)ci, *b = fineQ + 4 * ((size_t)ORC_FINE + 1 + ci);
+    a[0] = (float)Q[0]; a[1] = (float)Q[1]; a[2] = (float)Q[2]; a[3] = (float)Q[3];
+    b[0] = (float)Q[4]; b[1] = (float)Q[5];
+  }
+  free(q);
+}
+
+/* one source's second moment Q (Qxx Qyy Qzz Qxy Qxz Qyz) at offset r from the cell (r = source - cell): its
+ * quadrupole pull a = -3 Q r / r^5 + 7.5 (r Q r) r / r^7 - 1.5 tr(Q) r / r^5 and potential
+ * -0.5 (3 r Q r / r^5 - tr(Q) / r^3), added to acc and pot */
+static void add_quad(double *acc, double *pot, const double *r, const double *Q, double inv) {
+  double inv2 = inv * inv, inv3 = inv * inv2, inv5 = inv3 * inv2;
+  double Qr[3] = {Q[0] * r[0] + Q[3] * r[1] + Q[4] * r[2], Q[3] * r[0] + Q[1] * r[1] + Q[5] * r[2],
+                  Q[4] * r[0] + Q[5] * r[1] + Q[2] * r[2]};
+  double rQr = r[0] * Qr[0] + r[1] * Qr[1] + r[2] * Qr[2], tr = Q[0] + Q[1] + Q[2];
+  double c1 = 7.5 * rQr * inv5 * inv2 - 1.5 * tr * inv5;
+  for (int a = 0; a < 3; a++) acc[a] += c1 * r[a] - 3.0 * inv5 * Qr[a];
+  *pot -= 0.5 * (3.0 * rQr * inv5 - tr * inv3);
+}
+
 /* one source of mass M at offset r from the cell's centre of mass (r = source - cell): the second gradient
  * of its pull at the cell, G_abc = d2 F_a / dx_b dx_c = M (15 r_a r_b r_c / r^7 - 3 (d_ab r_c + d_ac r_b +
  * d_bc r_a) / r^5), added to G = (Gxxx Gyyy Gzzz Gxyz, Gxxy Gxxz Gxyy Gyyz, Gxzz Gyzz); a5 = 3 M / r^5 and
@@ -776,8 +823,8 @@ static void add_tide2(double *G, double rx, double ry, double rz, double a5, dou
   G[9] += a7 * ry * rz * rz - a5 * ry;
 }
 
-void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, float *force, float *tide0,
-                   float *tide1, float *tide2) {
+void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, const float *fineQ,
+                   float *force, float *tide0, float *tide1, float *tide2) {
   const float eps2 = 1e-6f * u->eps2Mesh;   /* keeps two coinciding centres of mass finite, as the library's */
   memcpy(force + 4 * ORC_FINE, fine + 4 * ORC_FINE, 16);
   /* each occupied block's centre of mass and second moment, from its occupied cells at their centres of mass */
@@ -794,6 +841,11 @@ void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coar
       double d[3] = {f[0] / f[3] - q[0], f[1] / f[3] - q[1], f[2] / f[3] - q[2]};
       q[4] += f[3] * d[0] * d[0]; q[5] += f[3] * d[1] * d[1]; q[6] += f[3] * d[2] * d[2];
       q[7] += f[3] * d[0] * d[1]; q[8] += f[3] * d[0] * d[2]; q[9] += f[3] * d[1] * d[2];
+      if (fineQ) {   /* the cell's own spread, by parallel axes */
+        size_t fi = (size_t)fine_index(bx * 4 + (c & 3), by * 4 + ((c >> 2) & 3), bz * 4 + (c >> 4));
+        const float *a = fineQ + 4 * fi, *b = fineQ + 4 * ((size_t)ORC_FINE + 1 + fi);
+        q[4] += a[0]; q[5] += a[1]; q[6] += a[2]; q[7] += a[3]; q[8] += b[0]; q[9] += b[1];
+      }
     }
   }
 #pragma omp parallel for schedule(dynamic, 256)
@@ -835,6 +887,12 @@ void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coar
                 T[0] += a5 * rx * rx - a3; T[1] += a5 * ry * ry - a3; T[2] += a5 * rz * rz - a3;
                 T[3] += a5 * rx * ry; T[4] += a5 * rx * rz; T[5] += a5 * ry * rz;
                 add_tide2(G, rx, ry, rz, a5, 5.0 * a5 * inv2);
+                if (fineQ) {   /* the source's spread as a quadrupole */
+                  size_t fi = (size_t)fine_index(f[0], f[1], f[2]);
+                  const float *qa = fineQ + 4 * fi, *qb = fineQ + 4 * ((size_t)ORC_FINE + 1 + fi);
+                  double Q[6] = {qa[0], qa[1], qa[2], qa[3], qb[0], qb[1]}, rr[3] = {rx, ry, rz};
+                  add_quad(acc, &pot, rr, Q, inv);
+                }
               }
         }
     /* far: every occupied block more than two from the cell's own, monopole + quadrupole, at the cell */

@@ -113,8 +113,13 @@ void orc_cell(const orc_uni *u, const float *fine, const float *coarse, const fl
  * NULL); every particle's pairs inside the stencil (out4: pull, potential x Gm); the gather from each
  * node's centre of mass, second order (first order where tideA2 / tideB2 is NULL), plus the particle's
  * pairs (grav4) */
-void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, float *force, float *tide0,
-                   float *tide1, float *tide2);
+void orc_cell_tide(const orc_uni *u, int S, const float *fine, const float *coarse, const float *fineQ,
+                   float *force, float *tide0, float *tide1, float *tide2);
+/* each cell's second moment about its centre of mass (after orc_deposit): fineQ, two planes of (64^3 + 1)
+ * float4 (Qxx Qyy Qzz Qxy), (Qxz Qyz); given to orc_cell_tide, the near cells act as quadrupoles and the
+ * blocks' quadrupoles include the cells' own (NULL: monopoles at their centres of mass) */
+void orc_node_moments(const orc_uni *u, int box, const float *pos4, const float *mat, const float *fine,
+                      float *fineQ);
 void orc_pp_split(const orc_uni *u, int S, const float *pos4, const float *mat, float *out4);
 void orc_gather_split(const orc_uni *u, const float *pos4, const float *fineA, const float *forceA,
                       const float *tideA0, const float *tideA1, const float *tideA2, const float *fineB,

@@ -145,7 +145,8 @@ def lib():
         L.orc_sim_pass.argtypes = [C.POINTER(Uni)] + [P] * 11 + [C.c_int] + [P] * 4
         L.orc_diag.argtypes = [C.POINTER(Uni)] + [P] * 9 + [C.c_int, P]
         L.orc_contact_pairs.argtypes = [C.POINTER(Uni), P, P, C.c_int, P, P]
-        L.orc_cell_tide.argtypes = [C.POINTER(Uni), C.c_int] + [P] * 6
+        L.orc_cell_tide.argtypes = [C.POINTER(Uni), C.c_int] + [P] * 7
+        L.orc_node_moments.argtypes = [C.POINTER(Uni), C.c_int] + [P] * 4
         L.orc_pp_split.argtypes = [C.POINTER(Uni), C.c_int, P, P, P]
         L.orc_gather_split.argtypes = [C.POINTER(Uni)] + [P] * 15
         L.orc_rigid.argtypes = [C.c_int] + [P] * 10 + [C.c_float, P, P]
@@ -280,16 +281,26 @@ def contact_pairs(u, pos4, seats, cap=64):
     return counts, pairs
 
 
-def cell_tide(u, S, fine, coarse):
+def cell_tide(u, S, fine, coarse, fineQ=None):
     """The stencil-split P3M's cell pass, near and far: (force, tide0, tide1), each (64^3 + 1) x 4, and
-    tide2, the pull's second gradient, 3 x (64^3 + 1) x 4 (the library's three planes)."""
+    tide2, the pull's second gradient, 3 x (64^3 + 1) x 4 (the library's three planes).  fineQ (node_moments):
+    the near cells act as quadrupoles and the blocks' quadrupoles include the cells' own."""
     force = np.zeros((FINE + 1, 4), np.float32)
     t0 = np.zeros((FINE + 1, 4), np.float32)
     t1 = np.zeros((FINE + 1, 4), np.float32)
     t2 = np.zeros((3, FINE + 1, 4), np.float32)
     a = [np.ascontiguousarray(x, np.float32) for x in (fine, coarse)]
-    lib().orc_cell_tide(C.byref(u), int(S), *[ptr(x) for x in a], ptr(force), ptr(t0), ptr(t1), ptr(t2))
+    q = None if fineQ is None else np.ascontiguousarray(fineQ, np.float32)
+    lib().orc_cell_tide(C.byref(u), int(S), *[ptr(x) for x in a], ptr(q), ptr(force), ptr(t0), ptr(t1), ptr(t2))
     return force, t0, t1, t2
+
+
+def node_moments(u, box, pos4, mat, fine):
+    """Each fine cell's second moment about its centre of mass: 2 x (64^3 + 1) x 4 (Qxx Qyy Qzz Qxy; Qxz Qyz)."""
+    out = np.zeros((2, FINE + 1, 4), np.float32)
+    a = [np.ascontiguousarray(x, np.float32) for x in (pos4, mat, fine)]
+    lib().orc_node_moments(C.byref(u), int(box), *[ptr(x) for x in a], ptr(out))
+    return out
 
 
 def pp_split(u, S, pos4, mat):

@@ -57,6 +57,7 @@ def test_split_passes_match_the_oracle(ccmod, orc, S):
         fine, coarse, far = nb.buffer("fineA"), nb.buffer("coarseA"), nb.buffer("farA")
         force, t0, t1 = nb.buffer("forceA"), nb.buffer("tide0A"), nb.buffer("tide1A")
         t2 = nb.buffer("tide2A").reshape(3, -1, 4)
+        fq = nb.buffer("fineQA").reshape(2, -1, 4)
         ppall = nb.buffer("ppall")
         mono = nb.buffer("monoA")[0]
         nb.pass_slots()
@@ -69,9 +70,17 @@ def test_split_passes_match_the_oracle(ccmod, orc, S):
     P = orc.ptr
     fa, ft0, ft1 = (np.zeros((orc.COARSE, 4), np.float32) for _ in range(3))
     orc.lib().orc_far(P(coarse), P(fa), P(ft0), P(ft1))
-    of, ot0, ot1, ot2 = orc.cell_tide(u, S, fine, coarse)
+    ofq = orc.node_moments(u, 0, pos, mat, fine)
     occ = fine[:-1, 3] > 0
     assert occ.sum() > 500
+    # each cell's second moment about its centre of mass (float atomics: to the moments' own scale)
+    Q = np.c_[fq[0][:-1][occ], fq[1][:-1][occ, :2]].astype(np.float64)
+    oQ = np.c_[ofq[0][:-1][occ], ofq[1][:-1][occ, :2]].astype(np.float64)
+    qs = np.abs(oQ[:, :3]).sum(1)
+    big = qs > 1e-3 * np.median(qs)
+    qr = np.abs(Q - oQ).max(1)[big] / qs[big]
+    assert np.median(qr) < REL and np.percentile(qr, 99) < 1e-3, (np.median(qr), np.percentile(qr, 99))
+    of, ot0, ot1, ot2 = orc.cell_tide(u, S, fine, coarse, fq)
     g = per_particle(force[:-1][occ, :3], of[:-1][occ, :3])
     assert np.median(g) < REL and np.percentile(g, 99) < 10 * REL, (np.median(g), np.percentile(g, 99))
     tide = np.c_[t0[:-1][occ], t1[:-1][occ, :2]].astype(np.float64)

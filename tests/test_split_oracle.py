@@ -8,7 +8,9 @@ The split form has no counterpart in the reference, so it is pinned by its own d
 3. the far blocks' quadrupoles converge to the direct sum of a distant cluster;
 4. the second gradient of a node's pull is the derivative of its tidal tensor (central differences of the
    tide of a single source), and the second-order gather is closer to the direct sum than the first-order
-   one on a Plummer sphere with debris.
+   one on a Plummer sphere with debris;
+5. the node quadrupoles are the reaction to the second-order gather: with them the net force over all
+   particles returns to the first-order form's level.
 """
 import ctypes as C
 import math
@@ -235,3 +237,43 @@ def test_second_order_gather_is_closer_to_the_direct_sum(orc):
     e2 = np.linalg.norm(second[idx, :3] - want, axis=1) / np.linalg.norm(want, axis=1)
     print("S = 1 at 16k: median error first order %.3e, second order %.3e" % (np.median(e1), np.median(e2)))
     assert np.median(e2) < 0.95 * np.median(e1)     # measured 2.42e-3 against 2.75e-3
+
+
+def test_node_quadrupoles_restore_the_net_force(orc):
+    """Two spread-out clumps five cells apart (every pair between them beyond the stencil, so their pull on
+    each other is all the mesh's): any exact pairwise sum gives them equal and opposite forces.  The
+    first-order gather is reciprocal node by node; the second-order gather pulls on each node's spread about
+    its centre of mass (G : Q / 2 net on the node), which point sources do not return; with every node's second
+    moment acting as a quadrupole source the two clumps' forces balance again."""
+    rng = np.random.default_rng(21)
+    N = 1024
+    sim, u = sweep_sim(orc, N)
+    pos = np.zeros((N, 4), np.float32)
+    pos[:512, :3] = (np.array([0.02, -0.01, 0.03]) + rng.normal(scale=0.6 * FH, size=(512, 3))).astype(np.float32)
+    pos[512:, :3] = (np.array([0.02 + 5 * FH, 0.9 * FH, 0.03]) + rng.normal(scale=0.6 * FH, size=(512, 3))).astype(np.float32)
+    mat = np.ones(N, np.float32)
+    mat[512:] = 0.5
+    P = orc.ptr
+    fine = np.zeros((orc.FINE + 1, 4), np.float32)
+    z4 = np.zeros(4, np.float32)
+    orc.lib().orc_deposit(C.byref(u), 0, P(pos), P(mat), P(z4), P(fine))
+    coarse = np.zeros((orc.COARSE, 4), np.float32)
+    mono = np.zeros(4, np.float32)
+    orc.lib().orc_coarse(P(fine), P(coarse), P(mono))
+    fq = orc.node_moments(u, 0, pos, mat, fine)
+    pp = orc.pp_split(u, 1, pos, mat)
+    zeros = np.zeros_like(fine)
+    zeros2 = np.zeros((3, orc.FINE + 1, 4), np.float32)
+    m = mat.astype(np.float64)
+    net = {}
+    for name, q, second in (("first", None, False), ("second", None, True), ("second+Q", fq, True)):
+        force, t0, t1, t2 = orc.cell_tide(u, 1, fine, coarse, q)
+        meshA = (fine, force, t0, t1, t2) if second else (fine, force, t0, t1)
+        meshB = (zeros, zeros, zeros, zeros, zeros2) if second else (zeros, zeros, zeros, zeros)
+        g = orc.gather_split(u, pos, meshA, meshB, mono, mono, pp)[:, :3].astype(np.float64)
+        fa = (m[:512, None] * g[:512]).sum(0)          # the first clump's pull (its own pairs cancel)
+        fb = (m[512:, None] * g[512:]).sum(0)
+        net[name] = float(np.linalg.norm(fa + fb) / np.linalg.norm(fa))
+    print("net force over the pull between the clumps:", net)
+    assert net["second"] > 1e-4                        # the unreturned pull on the nodes' spread
+    assert net["second+Q"] < 0.1 * net["second"]
