@@ -36,9 +36,15 @@ A step is one full-phase step of the reference schedule (contact grid every
            after training it on the device on pairs drawn from the same impact
            at full-phase steps 0, 1000 and 3000; its force error on the same
            gravity sweep as force_error.
+  ensemble  the batched ensemble of 64 impacts of uneven size, 2,000 steps
+           each (--ens-count 0 skips it): aggregate particle-steps/s with
+           each round one persistent launch over every instance's contact
+           grids and contact steps (value), beside the branch-graph form and
+           one stream per instance, and the per-instance step times.
 
 Multi-GPU: one process per GPU, independent replicas of the impact (the step
 has no partition worth a data-path collective at this size): weak scaling.
+The ensemble sub-line shards its impacts by instance across the ranks.
 """
 import argparse
 import json
@@ -470,20 +476,44 @@ def run_ensemble(args, log, rank=0, world=1):
     ens.steps(8 * blocks)
     ens.sync()
     wall_graph = max_over_ranks(time.perf_counter() - w1)
+    # and again with every round one persistent launch over all instances' grids and contact steps
+    # (ccs_ensemble_set_persistent), after the instances' mesh chains
+    ens.set_persistent(True)
+    ens.steps(8)                                          # capture the round's graphs
+    ens.step_ms()                                         # (waits; the sums start at the timed rounds)
+    torch.cuda.synchronize()
+    barrier()
+    l0 = ens.launch_count()
+    w2 = time.perf_counter()
+    ens.steps(8 * blocks)
+    ens.sync()
+    wall_pers = max_over_ranks(time.perf_counter() - w2)
+    pers_ms = ens.step_ms()                               # each instance's step time inside the rounds
+    pers_launches = ens.launch_count() - l0
     ens.close()
     p50 = max_over_ranks(float(np.percentile(per_step_ms, 50)))
     p99 = max_over_ranks(float(np.percentile(per_step_ms, 99)))
-    line = {"metric": "ensemble aggregate particle-steps/s", "value": total / wall_graph, "unit": "particle-steps/s",
+    pp50 = max_over_ranks(float(np.percentile(pers_ms, 50)))
+    pp99 = max_over_ranks(float(np.percentile(pers_ms, 99)))
+    line = {"metric": "ensemble aggregate particle-steps/s", "value": total / wall_pers, "unit": "particle-steps/s",
             "instances": int(sum_over_ranks(len(runs))), "n_gpus": world, "steps_each": 8 * blocks,
             "particles": int(sum_over_ranks(sum(nb.sim.N for nb in runs))),
             "sharding": "whole impacts per GPU (every world-th instance), no exchange during the run; the "
                         "slowest rank's wall time and the summed particle-steps",
-            "mode": "one CUDA graph per four 8-step rounds holding every instance's steps as a parallel branch "
-                    "(ccs_ensemble); wall clock over the rounds",
+            "mode": "persistent: each 8-step round one launch of k_ensemble_round over every instance's contact "
+                    "grids and contact steps (work items from per-instance queues), after the instances' mesh "
+                    "chains; four rounds a CUDA graph (ccs_ensemble_set_persistent); wall clock over the rounds",
+            "wall_s": wall_pers,
+            "persistent_launches": int(pers_launches),
+            "per_instance_step_ms": {"p50": pp50, "p99": pp99,
+                                     "what": "each instance's first work item to its last in a round "
+                                             "(%globaltimer), over 8 steps, averaged over the timed rounds"},
+            "branch_graph": {"value": total / wall_graph, "wall_s": wall_graph,
+                             "mode": "one CUDA graph per four 8-step rounds holding every instance's steps as a "
+                                     "parallel branch (ccs_ensemble)"},
             "per_handle_streams": {"value": total / wall, "wall_s": wall,
                                    "per_instance_step_ms": {"p50": p50, "p99": p99},
                                    "mode": "one handle and stream per impact, captured 8-step graphs interleaved"},
-            "wall_s": wall_graph,
             "autotuned": tuned}
     for nb in runs:
         nb.close()
@@ -891,6 +921,8 @@ def main():
     ap.add_argument("--ensemble", type=int, default=0,
                     help="run the batched ensemble of this many impacts instead and print its line")
     ap.add_argument("--ens-steps", type=int, default=2000)
+    ap.add_argument("--ens-count", type=int, default=64,
+                    help="impacts of the ensemble sub-line of the default run (0: skip it)")
     ap.add_argument("--no-nn", action="store_true", help="skip the learned-correction leg")
     ap.add_argument("--no-tune", action="store_true", help="ensemble: keep the default launch shapes")
     ap.add_argument("--nn-pairs", type=int, default=12_000_000, help="training pairs (three snapshots)")
@@ -948,6 +980,13 @@ def main():
             td.destroy_process_group()
         return
     line, snapshot = run_ours(args, rank, world, log)
+    if args.ens_count > 0 and not args.profile:
+        # config 5 beside the headline: the 64-impact ensemble, each instance 2,000 steps
+        ens_args = argparse.Namespace(**vars(args))
+        ens_args.ensemble = args.ens_count
+        ens = run_ensemble(ens_args, log, rank, world)
+        if rank == 0:
+            line["ensemble"] = ens
     if rank == 0:
         if world == 1 and not args.no_cpu and not args.profile:
             line["cpu_baseline"] = cpu_reference(snapshot, min_seconds=args.cpu_seconds)

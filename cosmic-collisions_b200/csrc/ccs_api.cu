@@ -1166,7 +1166,10 @@ int ccs_build(ccs_handle *h, const ccs_sim *sim, const float *pos4, const float 
   rc |= dev_alloc(h, &h->mat, N); rc |= dev_alloc(h, &h->matTmp, N);
   rc |= dev_alloc(h, &h->home, N); rc |= dev_alloc(h, &h->homeTmp, N);
   rc |= dev_alloc(h, &h->part, N); rc |= dev_alloc(h, &h->part2, N);
-  rc |= dev_alloc(h, &h->rec, (N + 31) / 32 * kRecWarp); rc |= dev_alloc(h, &h->recN, (N + 31) / 32);
+  // recN: a count for every warp of the contact step's last CTA (up to 8 warps of 32), also the warps wholly
+  // past N, which write (and read) a count of nothing
+  rc |= dev_alloc(h, &h->rec, (N + 31) / 32 * kRecWarp); rc |= dev_alloc(h, &h->recN, (N + 255) / 256 * 8);
+  if (h->recN) cudaMemset(h->recN, 0, sizeof(int) * ((N + 255) / 256 * 8));   // no warp has a record yet
   rc |= dev_alloc(h, &h->recP, N);
   rc |= dev_alloc(h, &h->recMax, 1); rc |= dev_alloc(h, &h->recStats, 3);
   make_static(h);
@@ -1438,6 +1441,11 @@ struct EnsembleGraph {
   std::vector<int> member;                 // the member each of them belongs to
   cudaEvent_t done = nullptr;
   bool used = false;
+  // the persistent form: every round's step arguments ([round][member][step]) and their pinned staging, and
+  // each round's counters ([round][member], with the round's abort flag after them)
+  EnsStepArgs *args = nullptr, *argsHost = nullptr;
+  unsigned char *state = nullptr;
+  size_t stateBytes = 0;
 };
 }  // namespace
 
@@ -1449,6 +1457,15 @@ struct ccs_ensemble {
   std::vector<cudaEvent_t> join, ready;
   std::map<std::pair<int, std::vector<GraphKey>>, EnsembleGraph> graphs;   // (rounds, members' keys)
   std::string err;
+  // the persistent form (ccs_ensemble_set_persistent): each round one launch of k_ensemble_round
+  bool persistent = false;
+  int ctas = 0;                          // its CTAs: the device's resident count
+  EnsMember *info = nullptr;             // per member: its round's segments
+  int *order = nullptr;                  // the members in priority order: largest first
+  unsigned long long *acc = nullptr;     // per member: ns and rounds (EnsLaunch::acc)
+  unsigned *status = nullptr;            // kStatusEnsemble
+  int64_t launches = 0;                  // persistent rounds launched
+  unsigned long long waitNs = 2000000000ull;   // the longest a CTA of the round waits (ccs_ensemble_set_wait_ns)
 };
 
 constexpr int kEnsRounds = 4;   // rounds of meshEvery steps one ensemble graph holds
@@ -1459,6 +1476,9 @@ void free_ensemble_graph(EnsembleGraph &g) {
   if (g.graph) cudaGraphDestroy(g.graph);
   for (auto p : g.dev) cudaFree(p);
   for (auto p : g.host) cudaFreeHost(p);
+  if (g.args) cudaFree(g.args);
+  if (g.argsHost) cudaFreeHost(g.argsHost);
+  if (g.state) cudaFree(g.state);
   if (g.done) cudaEventDestroy(g.done);
   g = EnsembleGraph();
 }
@@ -1477,8 +1497,144 @@ void free_ensemble_graphs(ccs_ensemble *e) {
     }                                                                                            \
   } while (0)
 
+// the persistent form: R rounds, each the members' mesh chains for the round's mesh step (parallel branches,
+// as in the branch form) and then one launch of k_ensemble_round over every member's steps of the round
+
+size_t ens_state_slice(int n) { return (sizeof(EnsState) * n + 255) / 256 * 256 + 256; }   // + the abort flag
+
+int ensemble_block_persistent(ccs_ensemble *e, int R) {
+  const int n = (int)e->m.size(), M = kEnsSteps * R;
+  for (ccs_handle *h : e->m)
+    if (h->field || h->ppSplit || h->nn || h->meshEvery != kEnsSteps) {
+      e->err = "persistent ensemble: a member left the impact's step with the reference's P3M and meshEvery 8";
+      return CCS_E_STATE;
+    }
+  std::vector<GraphKey> keys(n);
+  std::vector<std::vector<StepPlan>> plans(n, std::vector<StepPlan>(M));
+  std::vector<int> seat0(n), cur0(n);
+  for (int i = 0; i < n; ++i) {
+    ccs_handle *h = e->m[i];
+    for (int k = 0; k < M; ++k) {
+      plans[i][k] = plan_step(h, 0, 0);
+      h->sim.t += h->sim.dt;   // the frame loop's clock, index.html:372
+      if (plans[i][k].mesh != (k % kEnsSteps == 0) || plans[i][k].slots != (k % 2 == 0)) {
+        e->err = "persistent ensemble: a member's schedule is not the 8-step cycle";
+        return CCS_E_STATE;
+      }
+    }
+    keys[i] = GraphKey{(int)(plans[i][0].u.boxB > 0.5f), h->ppCount > 0, h->seatCur, h->cur, -kEnsSteps, 0, 0};
+    seat0[i] = h->seatCur;
+    cur0[i] = h->cur;
+  }
+  const size_t nArgs = (size_t)R * n * kEnsSteps, slice = ens_state_slice(n);
+  EnsembleGraph &g = e->graphs[std::make_pair(R, keys)];
+  if (!g.exec) {
+    g.stateBytes = slice * R;
+    ENS_TRY(e, cudaMalloc(&g.args, sizeof(EnsStepArgs) * nArgs));
+    ENS_TRY(e, cudaMallocHost(&g.argsHost, sizeof(EnsStepArgs) * nArgs));
+    ENS_TRY(e, cudaMalloc(&g.state, g.stateBytes));
+    ENS_TRY(e, cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+    cudaGraph_t graph;
+    ENS_TRY(e, cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(g.args, g.argsHost, sizeof(EnsStepArgs) * nArgs, cudaMemcpyHostToDevice, e->st);
+    cudaMemsetAsync(g.state, 0, g.stateBytes, e->st);
+    for (int r = 0; r < R; ++r) {
+      cudaEventRecord(e->fork, e->st);
+      for (int i = 0; i < n; ++i) {   // the round's mesh step: mesh and pairwise pass from the round's positions
+        ccs_handle *h = e->m[i];
+        const int timing = h->timing;
+        const int64_t l0 = h->launches;
+        h->timing = 0;
+        h->cur = cur0[i];
+        cudaStreamWaitEvent(h->st, e->fork, 0);
+        const StepPlan &p = plans[i][(size_t)r * kEnsSteps];
+        const ccs_uniforms *U = &g.args[((size_t)r * n + i) * kEnsSteps].u;
+        pass_mesh(h, U, p.u.boxB > 0.5f);
+        pass_pp(h, U, p.u.ppCount);
+        cudaEventRecord(e->join[i], h->st);
+        cudaStreamWaitEvent(e->st, e->join[i], 0);
+        h->timing = timing;
+        h->launches = l0;
+      }
+      EnsLaunch L;
+      L.members = n;
+      L.steps = kEnsSteps;
+      L.args = g.args + (size_t)r * n * kEnsSteps;
+      L.info = e->info;
+      L.state = reinterpret_cast<EnsState *>(g.state + slice * r);
+      L.abort = reinterpret_cast<int *>(g.state + slice * r + slice - 256);
+      L.front = L.abort + 1;
+      L.status = e->status;
+      L.acc = e->acc;
+      L.order = e->order;
+      L.limitNs = e->waitNs;
+      launch_ensemble_round(L, e->ctas, e->st);
+    }
+    cudaError_t ce = cudaStreamEndCapture(e->st, &graph);
+    if (ce == cudaSuccess) {
+      ce = cudaGraphInstantiate(&g.exec, graph, 0);
+      if (ce != cudaSuccess) {
+        g.exec = nullptr;
+        cudaGraphDestroy(graph);
+      } else {
+        g.graph = graph;
+      }
+    }
+    if (ce != cudaSuccess) {
+      e->err = std::string("persistent ensemble capture: ") + cudaGetErrorString(ce);
+      free_ensemble_graph(g);
+      e->graphs.erase(std::make_pair(R, keys));
+      return CCS_E_CUDA;
+    }
+  }
+  if (g.used) ENS_TRY(e, cudaEventSynchronize(g.done));   // the last replay has read the staging
+  for (int i = 0; i < n; ++i) {
+    ccs_handle *h = e->m[i];
+    for (int K = 0; K < M; ++K) {
+      const StepPlan &p = plans[i][K];
+      const int seatB = seat0[i] ^ (((K + 1) / 2) & 1);   // the table the step finds: a rebuild every 2nd step
+      h->cur = cur0[i] ^ (K & 1);
+      h->seatCur = p.slots ? seatB ^ 1 : seatB;
+      EnsStepArgs &A = g.argsHost[((size_t)(K / kEnsSteps) * n + i) * kEnsSteps + K % kEnsSteps];
+      A.u = p.u;
+      A.a = sim_args(h);
+      A.a.walk = p.walk;
+      A.gpos = h->pos[h->cur];
+      A.gseats = h->seats[seatB ^ 1];
+      A.ghk = h->hk[seatB ^ 1];
+      A.gseatsOld = h->seats[seatB];
+      A.ghkOld = h->hk[seatB];
+      A.gstatus = h->status;
+      A.grecMax = h->recMax;
+    }
+    h->cur = cur0[i];
+    h->seatCur = seat0[i];
+  }
+  for (int i = 0; i < n; ++i) {   // after whatever each member has queued
+    ENS_TRY(e, cudaEventRecord(e->ready[i], e->m[i]->st));
+    ENS_TRY(e, cudaStreamWaitEvent(e->st, e->ready[i], 0));
+  }
+  ENS_TRY(e, cudaGraphLaunch(g.exec, e->st));
+  g.used = true;
+  ENS_TRY(e, cudaEventRecord(g.done, e->st));
+  ENS_TRY(e, cudaEventRecord(e->after, e->st));
+  e->launches += R;
+  for (int i = 0; i < n; ++i) {   // and whatever they queue next comes after it
+    ccs_handle *h = e->m[i];
+    ENS_TRY(e, cudaStreamWaitEvent(h->st, e->after, 0));
+    h->cur = cur0[i] ^ (M & 1);
+    h->seatCur = seat0[i] ^ (((M + 1) / 2) & 1);
+    for (int r = 0; r < R; ++r) {   // the mesh chain's kernels (the round's steps are the ensemble's launch)
+      const StepPlan &p = plans[i][(size_t)r * kEnsSteps];
+      h->launches += 5 * (1 + (p.u.boxB > 0.5f)) + (p.u.ppCount ? 3 : 0);
+    }
+  }
+  return CCS_OK;
+}
+
 // R rounds: every member's next R x meshEvery steps, one graph launch
 int ensemble_block(ccs_ensemble *e, int R) {
+  if (e->persistent) return ensemble_block_persistent(e, R);
   const int n = (int)e->m.size(), M = e->M * R;
   std::vector<GraphKey> keys(n);
   std::vector<std::vector<StepPlan>> plans(n, std::vector<StepPlan>(M));
@@ -1581,6 +1737,7 @@ int ensemble_block(ccs_ensemble *e, int R) {
     ENS_TRY(e, cudaStreamWaitEvent(e->st, e->ready[i], 0));
   }
   ENS_TRY(e, cudaGraphLaunch(g.exec, e->st));
+  g.used = true;   // the next use of this graph waits for this replay before it rewrites the staging
   ENS_TRY(e, cudaEventRecord(g.done, e->st));
   ENS_TRY(e, cudaEventRecord(e->after, e->st));
   for (int i = 0; i < n; ++i) {   // and whatever they queue next comes after it
@@ -1640,6 +1797,10 @@ int ccs_ensemble_destroy(ccs_ensemble *e) {
   if (e->fork) cudaEventDestroy(e->fork);
   if (e->after) cudaEventDestroy(e->after);
   if (e->st) cudaStreamDestroy(e->st);
+  if (e->info) cudaFree(e->info);
+  if (e->order) cudaFree(e->order);
+  if (e->acc) cudaFree(e->acc);
+  if (e->status) cudaFree(e->status);
   delete e;
   return CCS_OK;
 }
@@ -1734,6 +1895,14 @@ int ccs_ensemble_sync(ccs_ensemble *e) {
   if (!e) return CCS_E_ARG;
   cudaSetDevice(e->device);
   ENS_TRY(e, cudaStreamSynchronize(e->st));
+  if (e->status) {
+    unsigned st = 0;
+    ENS_TRY(e, cudaMemcpy(&st, e->status, sizeof st, cudaMemcpyDeviceToHost));
+    if (st & kStatusEnsemble) {
+      e->err = "persistent ensemble round: a wait for work ran out (the round was abandoned)";
+      return CCS_E_KERNEL;
+    }
+  }
   for (ccs_handle *h : e->m) {
     int rc = check_status(h);
     if (rc) {
@@ -1741,6 +1910,91 @@ int ccs_ensemble_sync(ccs_ensemble *e) {
       return rc;
     }
   }
+  return CCS_OK;
+}
+
+int ccs_ensemble_set_persistent(ccs_ensemble *e, int on) {
+  if (!e || (on != 0 && on != 1)) return CCS_E_ARG;
+  cudaSetDevice(e->device);
+  if (on) {
+    if (e->M != kEnsSteps) {
+      e->err = "persistent ensemble: meshEvery must be 8";
+      return CCS_E_STATE;
+    }
+    for (ccs_handle *h : e->m)
+      if (h->field || h->ppSplit || h->nn) {
+        e->err = "persistent ensemble: members run the impact's step with the reference's P3M (no field step, "
+                 "stencil-split or learned pass)";
+        return CCS_E_STATE;
+      }
+  }
+  ENS_TRY(e, cudaStreamSynchronize(e->st));
+  free_ensemble_graphs(e);
+  e->persistent = on != 0;
+  if (!on || e->info) return CCS_OK;
+  const int n = (int)e->m.size();
+  std::vector<EnsMember> info(n);
+  long total = 0;
+  for (int i = 0; i < n; ++i) {   // the round's chain: grid, contact step on even steps; contact step on odd
+    EnsMember &I = info[i];
+    constexpr int kItem = kEnsContactItem;
+    const int N = e->m[i]->N, gi = (N + kEnsGridItem - 1) / kEnsGridItem, ci = (N + kItem - 1) / kItem;
+    I.nseg = 0;
+    int t = 0;
+    for (int k = 0; k < kEnsSteps; ++k) {
+      if (k % 2 == 0) {
+        t += gi;
+        I.end[I.nseg] = t;
+        I.step[I.nseg] = k;
+        I.grid[I.nseg++] = 1;
+      }
+      t += ci;
+      I.end[I.nseg] = t;
+      I.step[I.nseg] = k;
+      I.grid[I.nseg++] = 0;
+    }
+    I.total = t;
+    total += N;
+  }
+  (void)total;
+  e->ctas = ensemble_round_ctas();
+  std::vector<int> order(n);   // largest first (ties in member order): the longest chains start first
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return e->m[a]->N > e->m[b]->N; });
+  ENS_TRY(e, cudaMalloc(&e->info, sizeof(EnsMember) * n));
+  ENS_TRY(e, cudaMalloc(&e->order, sizeof(int) * n));
+  ENS_TRY(e, cudaMalloc(&e->acc, sizeof(unsigned long long) * 2 * n));
+  ENS_TRY(e, cudaMalloc(&e->status, sizeof(unsigned)));
+  ENS_TRY(e, cudaMemcpy(e->info, info.data(), sizeof(EnsMember) * n, cudaMemcpyHostToDevice));
+  ENS_TRY(e, cudaMemcpy(e->order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  ENS_TRY(e, cudaMemset(e->acc, 0, sizeof(unsigned long long) * 2 * n));
+  ENS_TRY(e, cudaMemset(e->status, 0, sizeof(unsigned)));
+  return CCS_OK;
+}
+
+int ccs_ensemble_step_ms(ccs_ensemble *e, double *ms, int count) {
+  if (!e || !ms || count != (int)e->m.size()) return CCS_E_ARG;
+  if (!e->acc) return CCS_E_STATE;
+  cudaSetDevice(e->device);
+  const int n = (int)e->m.size();
+  ENS_TRY(e, cudaStreamSynchronize(e->st));
+  std::vector<unsigned long long> acc(2 * n);
+  ENS_TRY(e, cudaMemcpy(acc.data(), e->acc, sizeof(unsigned long long) * 2 * n, cudaMemcpyDeviceToHost));
+  ENS_TRY(e, cudaMemset(e->acc, 0, sizeof(unsigned long long) * 2 * n));
+  for (int i = 0; i < n; ++i)
+    ms[i] = acc[n + i] ? (double)acc[i] / (double)acc[n + i] / kEnsSteps * 1e-6 : -1.0;
+  return CCS_OK;
+}
+
+int64_t ccs_ensemble_launch_count(const ccs_ensemble *e) { return e ? e->launches : -1; }
+
+int ccs_ensemble_set_wait_ns(ccs_ensemble *e, uint64_t ns) {
+  if (!e || ns == 0) return CCS_E_ARG;
+  cudaSetDevice(e->device);
+  ENS_TRY(e, cudaStreamSynchronize(e->st));
+  free_ensemble_graphs(e);   // the bound is an argument of the captured launches
+  e->waitNs = ns;
+  if (e->status) ENS_TRY(e, cudaMemset(e->status, 0, sizeof(unsigned)));
   return CCS_OK;
 }
 

@@ -49,6 +49,7 @@
 // replay and walk the cells their new neighbourhood adds; a warp whose record
 // did not fit, and every warp when any particle moved further than D, walks.
 #include "ccs_device.cuh"
+#include "ccs_grid.cuh"
 #include "ccs_internal.h"
 
 namespace ccs {
@@ -61,6 +62,15 @@ constexpr int kTCap = 16;                    // touching neighbours listed per o
 constexpr uint32_t kNearCell = 1u << 28, kRecEntry = kNearCell - 1u;
 inline int blocks_for(long n, int b) { return (int)((n + b - 1) / b); }
 }  // namespace
+
+// a load of state that other CTAs of the same launch may have written (COH, the ensemble's persistent round:
+// a plain load, ordered after the producer's release by the consumer's fence) or that no CTA of the launch
+// writes (the step's own kernels: the read-only path)
+template <bool COH, class T>
+__device__ __forceinline__ T ldr(const T *p) {
+  if constexpr (COH) return *p;
+  else return __ldg(p);
+}
 
 struct ContactWarp {
   float4 P[32];        // owner position, tag
@@ -80,10 +90,11 @@ struct Contact {
   f3 push;
   float lost, flow;
 };
+template <bool COH>
 __device__ __forceinline__ Contact contact_of(const ccs_uniforms &u, const SimArgs &a, float4 Po, float4 Vo, float ri,
                                               float ci, uint32_t j, float r) {
-  const float4 Pj = __ldg(a.pos + j);
-  const float4 Vj = __ldg(a.vel + j);
+  const float4 Pj = ldr<COH>(a.pos + j);
+  const float4 Vj = ldr<COH>(a.vel + j);
   const float rj = __ldg(a.mat + j);
   const f3 nrm = (xyz(Pj) - xyz(Po)) * fdiv(1.0f, fmaxf(r, 1e-6f));
   const float ov = u.touch - r;
@@ -102,7 +113,7 @@ __device__ __forceinline__ Contact contact_of(const ccs_uniforms &u, const SimAr
 // a pair inside the link radius: its owner's count; a touching one onto its owner's list (past the list's
 // end, rarely, its contact is worked out here and added to the owner's shared slots).  PAIRS: the pair is
 // also written to its owner's row of the pair read-out (the warp's first particle is `base`)
-template <bool PAIRS>
+template <bool PAIRS, bool COH>
 __device__ __forceinline__ void take_near(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, uint32_t e,
                                           float r2, int base) {
   const int o = (int)(e >> 18);
@@ -116,7 +127,7 @@ __device__ __forceinline__ void take_near(const ccs_uniforms &u, const SimArgs &
     if (k < kTCap) {
       w.tl[k][o] = e & 0x3FFFFu;
     } else {
-      const Contact c = contact_of(u, a, w.P[o], w.V[o], w.C0[o].w, w.ci[o], e & 0x3FFFFu, r);
+      const Contact c = contact_of<COH>(u, a, w.P[o], w.V[o], w.C0[o].w, w.ci[o], e & 0x3FFFFu, r);
       atomicAdd(&w.fx[o], c.push.x);
       atomicAdd(&w.fy[o], c.push.y);
       atomicAdd(&w.fz[o], c.push.z);
@@ -130,7 +141,7 @@ __device__ __forceinline__ void take_near(const ccs_uniforms &u, const SimArgs &
 // (lanes >= n idle); pairs inside the link radius are counted, touching ones listed for their owner.
 // MODE 1: the entries are first copied to the warp's record (rec from rbase, rc entries so far), and only
 // those tagged as in a cell past the nearest-point test are candidates
-template <bool PAIRS, int MODE>
+template <bool PAIRS, int MODE, bool COH>
 __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, int base,
                                                  int n, int lane, int first, size_t rbase, int &rc) {
   if (lane < n) {
@@ -141,17 +152,17 @@ __device__ __forceinline__ void drain_candidates(const ccs_uniforms &u, const Si
       if (rc + lane < kRecWarp) a.rec[rbase + rc + lane] = e0 & kRecEntry;
       if (two && rc + 32 + lane < kRecWarp) a.rec[rbase + rc + 32 + lane] = e1 & kRecEntry;
     }
-    const float4 Pj0 = __ldg(a.pos + (e0 & 0x3FFFFu));
-    const float4 Pj1 = two ? __ldg(a.pos + (e1 & 0x3FFFFu)) : Pj0;
+    const float4 Pj0 = ldr<COH>(a.pos + (e0 & 0x3FFFFu));
+    const float4 Pj1 = two ? ldr<COH>(a.pos + (e1 & 0x3FFFFu)) : Pj0;
     const float4 Po0 = w.P[(e0 >> 18) & 31u];
     const f3 d0 = xsub3(xyz(Pj0), xyz(Po0));
     const float r20 = xdot(d0, d0);
-    if ((MODE != 1 || (e0 & kNearCell)) && r20 < u.link2) take_near<PAIRS>(u, a, w, e0 & 0x7FFFFFu, r20, first);
+    if ((MODE != 1 || (e0 & kNearCell)) && r20 < u.link2) take_near<PAIRS, COH>(u, a, w, e0 & 0x7FFFFFu, r20, first);
     if (two) {
       const float4 Po1 = w.P[(e1 >> 18) & 31u];
       const f3 d1 = xsub3(xyz(Pj1), xyz(Po1));
       const float r21 = xdot(d1, d1);
-      if ((MODE != 1 || (e1 & kNearCell)) && r21 < u.link2) take_near<PAIRS>(u, a, w, e1 & 0x7FFFFFu, r21, first);
+      if ((MODE != 1 || (e1 & kNearCell)) && r21 < u.link2) take_near<PAIRS, COH>(u, a, w, e1 & 0x7FFFFFu, r21, first);
     }
   }
   if (MODE == 1) rc += n;
@@ -321,14 +332,14 @@ __device__ __forceinline__ uint32_t near_cells(const ccs_uniforms &u, f3 p, floa
 // one record entry (particle | owner << 18 | the owner's cell it came from << 23): the walk's decisions
 // for it -- the cell one of the owner's 27 now, past the nearest-point test (near, the owner's bits), the
 // pair inside the link radius
-template <bool PAIRS>
+template <bool PAIRS, bool COH>
 __device__ __forceinline__ void replay_entry(const ccs_uniforms &u, const SimArgs &a, ContactWarp &w, uint32_t e,
                                              float4 Pj, int first) {
   const int o = (int)((e >> 18) & 31u);
   if (!((w.near[o] >> ((e >> 23) & 31u)) & 1u)) return;
   const f3 d = xsub3(xyz(Pj), xyz(w.P[o]));
   const float r2 = xdot(d, d);
-  if (r2 < u.link2) take_near<PAIRS>(u, a, w, e & 0x7FFFFFu, r2, first);
+  if (r2 < u.link2) take_near<PAIRS, COH>(u, a, w, e & 0x7FFFFFu, r2, first);
 }
 
 // W warps per CTA (8 or 4: the autotuner's choice; 4 CTAs of 8 or 8 of 4 share an SM); FIELD: the crater
@@ -338,16 +349,20 @@ __device__ __forceinline__ void replay_entry(const ccs_uniforms &u, const SimArg
 // SPLIT: stop at the contact sums (a mesh step whose mesh runs beside the contact walk; k_contact_tail ends it).
 // MODE: 0 the walk; 1 the walk and its record for the next step; 2 the next step, which replays the record
 // (SimArgs::walk).
-template <int W, bool FIELD, bool SPLIT = false, bool PAIRS = false, int MODE = 0>
-__global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_uniforms u, const SimArgs a) {
+// One CTA's 32 W particles from a.first + blk 32 W: the contact step's body, shared by the kernel below
+// (blk = blockIdx.x) and the ensemble's persistent round (k_ensemble_round, one of its work items).  ws: the W
+// warps' shared-memory slots; spc: 16 floats of shared memory.  COH: the state it reads (positions,
+// velocities, seats, the record) may have been written by other CTAs of the same launch.
+template <int W, bool FIELD, bool SPLIT, bool PAIRS, int MODE, bool COH>
+__device__ __forceinline__ void contact_block(const ccs_uniforms &u, const SimArgs &a, int blk, ContactWarp *ws,
+                                              float *spc) {
   constexpr int kThreads = 32 * W;
   constexpr unsigned kAll = 0xFFFFFFFFu;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ float spc[16];   // seatPos(q) * uCell, exact
+  // spc: seatPos(q) * uCell, exact
   if (threadIdx.x < 16) spc[threadIdx.x] = xmul(__fdiv_rn((float)threadIdx.x + 0.5f, 15.0f), u.cell);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  ContactWarp &w = reinterpret_cast<ContactWarp *>(smem_raw)[wid];
-  const int me = a.first + blockIdx.x * kThreads + threadIdx.x;
+  ContactWarp &w = ws[wid];
+  const int me = a.first + blk * kThreads + threadIdx.x;
   const int first = me - lane;   // the warp's first particle (the pair read-out's rows)
   const bool live = me < u.N;
   const float cell = u.cell;
@@ -371,9 +386,9 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
   int how = 2, ecx = cx, ecy = cy, ecz = cz, rn = 0;
   const size_t rbase = (size_t)(first >> 5) * kRecWarp;
   if (MODE == 2) {
-    rn = __ldg(a.recN + (first >> 5));
-    if (live && rn <= kRecWarp && __uint_as_float(__ldg(a.recMax)) <= a.recAll2) {
-      const float4 Pe = __ldg(a.recP + me);
+    rn = ldr<COH>(a.recN + (first >> 5));
+    if (live && rn <= kRecWarp && __uint_as_float(ldr<COH>(a.recMax)) <= a.recAll2) {
+      const float4 Pe = ldr<COH>(a.recP + me);
       const float mx = p.x - Pe.x, my = p.y - Pe.y, mz = p.z - Pe.z;
       if (mx * mx + my * my + mz * mz <= a.recMove2) {
         float ex, ey, ez;
@@ -407,22 +422,22 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
     constexpr int kPer = 4;
     uint32_t e[kPer];
 #pragma unroll
-    for (int q = 0; q < kPer; ++q) e[q] = lane + 32 * q < rn ? __ldg(a.rec + rbase + lane + 32 * q) : 0u;
+    for (int q = 0; q < kPer; ++q) e[q] = lane + 32 * q < rn ? ldr<COH>(a.rec + rbase + lane + 32 * q) : 0u;
 #pragma unroll 1
     for (int b = 0; b < rn; b += 32 * kPer) {
       float4 Pj[kPer];
 #pragma unroll
       for (int q = 0; q < kPer; ++q)
-        Pj[q] = b + lane + 32 * q < rn ? __ldg(a.pos + (e[q] & 0x3FFFFu)) : make_float4(0, 0, 0, 0);
+        Pj[q] = b + lane + 32 * q < rn ? ldr<COH>(a.pos + (e[q] & 0x3FFFFu)) : make_float4(0, 0, 0, 0);
       uint32_t en[kPer];
 #pragma unroll
       for (int q = 0; q < kPer; ++q) {
         const int k = b + 32 * kPer + lane + 32 * q;
-        en[q] = k < rn ? __ldg(a.rec + rbase + k) : 0u;
+        en[q] = k < rn ? ldr<COH>(a.rec + rbase + k) : 0u;
       }
 #pragma unroll
       for (int q = 0; q < kPer; ++q)
-        if (b + lane + 32 * q < rn) replay_entry<PAIRS>(u, a, w, e[q], Pj[q], first);
+        if (b + lane + 32 * q < rn) replay_entry<PAIRS, COH>(u, a, w, e[q], Pj[q], first);
 #pragma unroll
       for (int q = 0; q < kPer; ++q) e[q] = en[q];
     }
@@ -468,8 +483,8 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
           const uint32_t yy = ((uint32_t)y + ((uint32_t)(x >> sh) << (sh - 1)) + wz) & gm;   // the x period skews y by half
           const uint32_t h = (row + yy) * (uint32_t)u.AW + col + ((uint32_t)x & gm);
           const uint4 *cp = seats + (size_t)h * 2;
-          s0 = __ldg(cp);       // both halves of the cell: one 32-byte sector, one round trip
-          s1 = __ldg(cp + 1);
+          s0 = ldr<COH>(cp);       // both halves of the cell: one 32-byte sector, one round trip
+          s1 = ldr<COH>(cp + 1);
         }
         {
           const uint32_t sv[kSeats] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
@@ -492,7 +507,7 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
         __syncwarp();
         while (qn >= 64) {
           qn -= 64;
-          drain_candidates<PAIRS, MODE>(u, a, w, qn, 64, lane, first, rbase, rc);
+          drain_candidates<PAIRS, MODE, COH>(u, a, w, qn, 64, lane, first, rbase, rc);
         }
       }
     }
@@ -500,9 +515,9 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
   }
   if (qn >= 32) {
     qn -= 32;
-    drain_candidates<PAIRS, MODE>(u, a, w, qn, 32, lane, first, rbase, rc);
+    drain_candidates<PAIRS, MODE, COH>(u, a, w, qn, 32, lane, first, rbase, rc);
   }
-  if (qn > 0) drain_candidates<PAIRS, MODE>(u, a, w, 0, qn, lane, first, rbase, rc);
+  if (qn > 0) drain_candidates<PAIRS, MODE, COH>(u, a, w, 0, qn, lane, first, rbase, rc);
   __syncwarp();
   if (MODE == 1) {
     if (lane == 0) a.recN[first >> 5] = min(rc, kRecWarp + 1);
@@ -517,9 +532,9 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
 #pragma unroll 4
   for (int k = 0; k < nt; ++k) {   // unrolled: the next contacts' loads are in flight with this one's math
     const uint32_t j = w.tl[k][lane];
-    const float4 Pj = __ldg(a.pos + j);
+    const float4 Pj = ldr<COH>(a.pos + j);
     const f3 d = xsub3(xyz(Pj), p);
-    const Contact c = contact_of(u, a, P, V, ri, ci, j, __fsqrt_rn(xdot(d, d)));
+    const Contact c = contact_of<COH>(u, a, P, V, ri, ci, j, __fsqrt_rn(xdot(d, d)));
     push = push + c.push;
     lost += c.lost;
     flow += c.flow;
@@ -530,6 +545,14 @@ __global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_unifo
     return;
   }
   finish_particle<FIELD>(u, a, me, P, V, ri, ci, push, lost, flow, nb, MODE == 1 ? a.recMax : nullptr);
+}
+
+template <int W, bool FIELD, bool SPLIT = false, bool PAIRS = false, int MODE = 0>
+__global__ void __launch_bounds__(32 * W, 32 / W) k_contact_step(const ccs_uniforms u, const SimArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ float spc[16];
+  contact_block<W, FIELD, SPLIT, PAIRS, MODE, false>(u, a, blockIdx.x, reinterpret_cast<ContactWarp *>(smem_raw),
+                                                     spc);
 }
 
 // the tail of a split mesh step, one thread a particle: the contact sums the contact walk left in part, then
@@ -549,6 +572,156 @@ __global__ void __launch_bounds__(256) k_contact_tail(const ccs_uniforms u, cons
 }
 
 size_t contact_smem_bytes(int warps) { return sizeof(ContactWarp) * warps; }
+
+// ---------------------------------------------------------------------------
+// The ensemble's persistent round: every member's kEnsSteps steps (contact grid on even steps, contact step
+// on each) in one launch of as many CTAs as the device holds at once.  Each member's work is a chain of
+// segments numbered by one ticket counter (EnsMember, EnsState): a CTA takes the next ticket of a member
+// whose current segment is ready (the segment before it finished), does that work item, and counts it done
+// after a fence.  A ticket only ever waits for tickets taken before it, by CTAs that are running and wait for
+// nothing later, so the round finishes whether or not every CTA is resident.  Every wait is bounded by
+// %globaltimer (limitNs): when one runs out the CTA raises kStatusEnsemble and the abort flag, and every CTA
+// leaves at its next pick.  State the round writes (positions, velocities, seats, the walk's record) is read
+// with plain loads after the fence that follows each wait (contact_block<..., COH = true>); the read-only
+// path is kept for what only the kernels before the launch wrote (the mesh force, the pairwise pass).
+// ---------------------------------------------------------------------------
+namespace {
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ int seg_of(const EnsMember &I, int t) {
+  int s = 0;
+  while (s < I.nseg - 1 && t >= I.end[s]) ++s;
+  return s;
+}
+__device__ __forceinline__ int seg_items(const EnsMember &I, int s) { return I.end[s] - (s ? I.end[s - 1] : 0); }
+__device__ __forceinline__ bool seg_ready(const EnsMember &I, const EnsState &S, int s) {
+  return s == 0 || *(volatile const int *)&S.done[s - 1] >= seg_items(I, s - 1);
+}
+
+// thread 0: the next work item (member, segment, item in the segment); member -1 when every member's work has
+// been taken or the round aborted.  Members are tried in the priority order L.order (largest first), from the
+// first one whose work is not all taken (L.front, a hint every CTA moves on): each CTA works for the earliest
+// member with a ready segment, so a few members are under way at a time -- their state stays in L2 -- and the
+// gaps at one member's step boundaries go to the next.
+__device__ int4 ens_pick(const EnsLaunch &L) {
+  const int M = L.members;
+  const unsigned long long t0 = gtime();
+  for (;;) {
+    if (*(volatile int *)L.abort) return make_int4(-1, 0, 0, 0);
+    bool left = false;
+    for (int k = *(volatile int *)L.front; k < M; ++k) {
+      const int m = L.order[k];
+      const EnsMember &I = L.info[m];
+      EnsState &S = L.state[m];
+      int t = *(volatile int *)&S.next;
+      if (t >= I.total) {
+        if (!left) atomicMax(L.front, k + 1);   // every member before it is taken too
+        continue;
+      }
+      left = true;
+      if (!seg_ready(I, S, seg_of(I, t))) continue;   // its next segment waits: work for another member
+      t = atomicAdd(&S.next, 1);
+      if (t >= I.total) continue;
+      const int s = seg_of(I, t);
+      if (t == 0) S.t0 = gtime();
+      // the ticket may lie past a segment boundary another CTA crossed meanwhile: wait for the segment before
+      while (!seg_ready(I, S, s)) {
+        if (*(volatile int *)L.abort) return make_int4(-1, 0, 0, 0);
+        if (gtime() - t0 > L.limitNs) {
+          atomicOr(L.status, kStatusEnsemble);
+          atomicExch(L.abort, 1);
+          return make_int4(-1, 0, 0, 0);
+        }
+        __nanosleep(100);
+      }
+      return make_int4(m, s, t - (s ? I.end[s - 1] : 0), 0);
+    }
+    if (!left) return make_int4(-1, 0, 0, 0);
+    if (gtime() - t0 > L.limitNs) {
+      atomicOr(L.status, kStatusEnsemble);
+      atomicExch(L.abort, 1);
+      return make_int4(-1, 0, 0, 0);
+    }
+    __nanosleep(200);
+  }
+}
+}  // namespace
+
+// 6 CTAs an SM: the walk's three forms and the grid in one kernel keep 80 registers without spilling (at 8
+// CTAs and 64 registers it spilled, and ran slower).  Work items are a CTA's: warp-sized items, each warp
+// picking its own, took four times the picks and ran slower.
+__global__ void __launch_bounds__(32 * kEnsWarps, 6) k_ensemble_round(const EnsLaunch L) {
+  constexpr int W = kEnsWarps;
+  extern __shared__ __align__(16) unsigned char smem_raw[];   // the contact step's W warp slots
+  __shared__ float spc[16];
+  __shared__ __align__(16) unsigned char argRaw[sizeof(EnsStepArgs)];   // the item's step, copied in
+  __shared__ int4 pick;
+  const EnsStepArgs &A = *reinterpret_cast<const EnsStepArgs *>(argRaw);
+  int held = -1;   // the (member, step) whose arguments argRaw holds
+  for (;;) {
+    if (threadIdx.x == 0) {
+      pick = ens_pick(L);
+      __threadfence();   // with the barrier: what the finished segments wrote is seen by the whole CTA
+    }
+    __syncthreads();
+    const int4 p = pick;
+    if (p.x < 0) break;
+    const EnsMember &I = L.info[p.x];
+    const int step = I.step[p.y];
+    if (p.x * L.steps + step != held) {   // items in a row mostly share their step
+      held = p.x * L.steps + step;
+      const int *src = reinterpret_cast<const int *>(L.args + held);
+      int *dst = reinterpret_cast<int *>(argRaw);
+      for (int k = threadIdx.x; k < (int)(sizeof(EnsStepArgs) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+      __syncthreads();
+    }
+    if (I.grid[p.y]) {
+#pragma unroll 1
+      for (int r = 0; r < kEnsGridItem / (32 * W); ++r)
+        grid_particle(A.u, p.z * kEnsGridItem + r * 32 * W + (int)threadIdx.x, A.gpos, A.gseats, A.ghk,
+                      A.gseatsOld, A.ghkOld, A.gstatus, A.grecMax);
+    } else {
+      ContactWarp *ws = reinterpret_cast<ContactWarp *>(smem_raw);
+      if (A.a.walk == 1)
+        contact_block<W, false, false, false, 1, true>(A.u, A.a, p.z, ws, spc);
+      else if (A.a.walk == 2)
+        contact_block<W, false, false, false, 2, true>(A.u, A.a, p.z, ws, spc);
+      else
+        contact_block<W, false, false, false, 0, true>(A.u, A.a, p.z, ws, spc);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();   // this item's writes before its count
+      const int d = atomicAdd(&L.state[p.x].done[p.y], 1) + 1;
+      if (d == seg_items(I, p.y) && p.y == I.nseg - 1) {   // the member's last item: its round's time
+        const unsigned long long t = gtime() - *(volatile unsigned long long *)&L.state[p.x].t0;
+        atomicAdd(L.acc + p.x, t);
+        atomicAdd(L.acc + L.members + p.x, 1ull);
+      }
+    }
+  }
+}
+
+namespace {
+size_t ensemble_smem() { return contact_smem_bytes(kEnsWarps); }
+}  // namespace
+
+int ensemble_round_ctas() {
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ensemble_round, 32 * kEnsWarps, ensemble_smem()) !=
+          cudaSuccess ||
+      per <= 0)
+    per = 1;
+  return per * sm_count();
+}
+
+int launch_ensemble_round(const EnsLaunch &L, int ctas, cudaStream_t st) {
+  k_ensemble_round<<<ctas, 32 * kEnsWarps, ensemble_smem(), st>>>(L);
+  return 1;
+}
 
 namespace {
 template <int W, bool FIELD, bool SPLIT, bool PAIRS, int MODE>
@@ -585,6 +758,8 @@ cudaError_t init_kernels() {
   if (e == cudaSuccess) e = set_modes<8, false, true, false>();
   if (e == cudaSuccess) e = set_modes<4, false, true, false>();
   if (e == cudaSuccess) e = set_modes<4, false, false, true>();
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_ensemble_round, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ensemble_smem());
   return e;
 }
 

@@ -112,6 +112,54 @@ struct SimArgs {
   float recLink2 = 0.0f, recMove2 = 0.0f, recAll2 = 0.0f;
 };
 
+// The ensemble's persistent round (k_ensemble_round, ccs_contact.cu): every member's steps of one round of
+// kEnsSteps in one launch.  Each member's round is a chain of segments -- on an even step the contact grid's,
+// then each step's contact step -- cut into work items (kEnsGridItem particles for the grid, kEnsContactItem
+// for the contact step) numbered by one ticket counter per member; a segment's items start once the segment
+// before it is finished.  The mesh and the pairwise pass of the round's mesh step run before the launch.
+constexpr int kEnsSteps = 8;          // steps a persistent round holds (the ensemble's meshEvery)
+constexpr int kEnsSegs = 2 * kEnsSteps;
+constexpr int kEnsWarps = 4;          // the contact step's CTA width in the round
+constexpr int kEnsContactItem = 32 * kEnsWarps;   // particles of a contact-step work item (one CTA's)
+constexpr int kEnsGridItem = 512;     // particles of a grid work item
+constexpr unsigned kStatusEnsemble = 8u;   // a wait of the ensemble's persistent round ran out
+struct EnsStepArgs {                  // one member's step
+  ccs_uniforms u;
+  SimArgs a;                          // the contact step's (the walk in a.walk)
+  // the contact grid's, on a step that rebuilds it: as launch_contact_grid takes them
+  const float4 *gpos;
+  uint32_t *gseats, *ghk, *gseatsOld;
+  const uint32_t *ghkOld;
+  unsigned *gstatus, *grecMax;
+};
+struct EnsMember {                    // a member's round: its segments (fixed by its size)
+  int nseg, total;                    // segments, work items
+  int end[kEnsSegs];                  // segment s holds tickets [s ? end[s - 1] : 0, end[s])
+  int step[kEnsSegs];                 // the step it belongs to
+  int grid[kEnsSegs];                 // 1: the contact grid; 0: the contact step
+};
+struct EnsState {                     // a member's counters in one launch, zeroed before it
+  int next;                           // the next ticket
+  int done[kEnsSegs];                 // work items finished, per segment
+  int pad;
+  unsigned long long t0;              // %globaltimer when its first item was taken
+};
+struct EnsLaunch {
+  int members, steps;                 // steps = kEnsSteps
+  const EnsStepArgs *args;            // [member][step]
+  const EnsMember *info;              // [member]
+  EnsState *state;                    // [member]
+  int *abort;                         // set when a wait runs out: every CTA leaves
+  unsigned *status;                   // kStatusEnsemble when a wait ran out
+  unsigned long long *acc;            // per member: ns its rounds took (acc[m]) and rounds (acc[members + m])
+  const int *order;                   // the members in priority order (largest first)
+  int *front;                         // in this launch: the first place in `order` whose work is not all taken
+  unsigned long long limitNs;         // the longest a CTA waits for work before it gives up
+};
+// the round's launch: `ctas` CTAs (ensemble_round_ctas(): the device's resident count)
+int launch_ensemble_round(const EnsLaunch &L, int ctas, cudaStream_t st);
+int ensemble_round_ctas();
+
 struct DiagArgs {
   const float4 *pos;
   const float *q;

@@ -561,6 +561,28 @@ class Ensemble:
     def sync(self):
         self._check(lib().ccs_ensemble_sync(self._h), "ccs_ensemble_sync")
 
+    def set_persistent(self, on=True):
+        """ccs_ensemble_set_persistent: each round of 8 steps as one persistent launch over every member (after
+        the members' mesh chains), work items taken from per-member queues; off: the branch form."""
+        self._check(lib().ccs_ensemble_set_persistent(self._h, 1 if on else 0), "ccs_ensemble_set_persistent")
+
+    def step_ms(self):
+        """ccs_ensemble_step_ms: per member, the mean ms of one step inside the persistent rounds since the last
+        call (-1 where none ran); waits for the rounds and resets the sums."""
+        import numpy as np
+        out = np.zeros(len(self.members), np.float64)
+        self._check(lib().ccs_ensemble_step_ms(self._h, out.ctypes.data_as(C.c_void_p), len(self.members)),
+                    "ccs_ensemble_step_ms")
+        return out
+
+    def launch_count(self):
+        """persistent rounds launched (one kernel launch each)"""
+        return int(lib().ccs_ensemble_launch_count(self._h))
+
+    def set_wait_ns(self, ns):
+        """ccs_ensemble_set_wait_ns: the bound on every wait of the persistent round (default 2 s)."""
+        self._check(lib().ccs_ensemble_set_wait_ns(self._h, int(ns)), "ccs_ensemble_set_wait_ns")
+
     def autotune(self, rounds=4):
         """ccs_ensemble_autotune: every launch-shape combination on all members, timed over real rounds (the
         members advance); the fastest aggregate is kept.  Returns the choice."""

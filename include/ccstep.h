@@ -346,6 +346,31 @@ int ccs_ensemble_sync(ccs_ensemble *e);   /* waits for the rounds; reports any m
  * can lose when many runs share the GPU, which is why the ensemble measures
  * its own.  choice (may be NULL) gets {warps, threads per cell}. */
 int ccs_ensemble_autotune(ccs_ensemble *e, int rounds, int choice[2]);
+/* The ensemble's persistent form (on = 1; 0 returns to the branch form).  No
+ * counterpart in the reference.  Each round of 8 steps is then one launch of
+ * a persistent kernel over every member: after the members' mesh chains for
+ * the round's mesh step (parallel branches, as before), the launch runs every
+ * member's contact grids and contact steps of the round, as many CTAs as the
+ * device holds at once taking work items from per-member queues (a member's
+ * next step starts as soon as its own previous one is finished; members never
+ * wait for one another).  The rounds stay CUDA graphs, four to a replay.  The
+ * members must run the impact's step with the reference's P3M (no field
+ * step, stencil-split or learned pass; CCS_E_STATE) and meshEvery 8.  Every
+ * wait in the kernel is bounded (2 s); one that runs out abandons the round,
+ * and ccs_ensemble_sync reports CCS_E_KERNEL. */
+int ccs_ensemble_set_persistent(ccs_ensemble *e, int on);
+/* Per member (count = the members), the mean time of one step inside the
+ * persistent rounds since the last call, in ms: from the member's first work
+ * item to its last in each round (%globaltimer), over 8; -1 for a member no
+ * persistent round has run.  Waits for the rounds; resets the sums. */
+int ccs_ensemble_step_ms(ccs_ensemble *e, double *ms, int count);
+/* persistent rounds launched (one kernel launch each) */
+int64_t ccs_ensemble_launch_count(const ccs_ensemble *e);
+/* The bound on every wait of the persistent round, in ns (default 2e9).  A
+ * bound shorter than the round's ordinary waits abandons the round: the way
+ * the time-out path is tested without a hang.  Also clears the ensemble's
+ * status word. */
+int ccs_ensemble_set_wait_ns(ccs_ensemble *e, uint64_t ns);
 
 /* The contact-pair sets of the current state, read out for checking: the
  * contact step's own walk over the current seat table (the 27 cells, the

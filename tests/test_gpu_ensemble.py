@@ -112,3 +112,103 @@ def test_ensemble_autotune_picks_a_shape_and_steps(ccmod):
     finally:
         for nb in members:
             nb.close()
+
+
+def test_persistent_round_steps_members_as_alone(ccmod):
+    """The persistent form: each round one launch over every member's grids and contact steps (after the
+    members' mesh chains), work items from per-member queues.  Members of different sizes step as they do
+    alone, to the same spread as the branch form; every member's step time inside the rounds is reported."""
+    sizes = [16384, 32768, 16384, 65536]
+    members = [settled(ccmod, N) for N in sizes]
+    lone = [settled(ccmod, N) for N in sizes]
+    lone2 = settled(ccmod, 16384)
+    try:
+        ens = ccmod.Ensemble(members)
+        ens.set_persistent(True)
+        ens.steps(16)
+        ens.sync()
+        assert ens.launch_count() == 2                  # one persistent launch a round
+        ms = ens.step_ms()
+        assert np.all(ms > 0) and np.all(ms < 50), ms
+        for nb in lone + [lone2]:
+            nb.steps(16)
+            nb.sync()
+        assert [nb.sim.stepNo for nb in members] == [nb.sim.stepNo for nb in lone]
+        l2 = lone2.read_state()
+        spread = {k: np.abs(l2[k][:, :3] - lone[0].read_state()[k][:, :3]).max() for k in ("pos", "vel")}
+        for a, b in zip(members, lone):
+            sa, sb = a.read_state(), b.read_state()
+            for k in ("pos", "vel"):
+                ref = sb[k][:, :3].astype(np.float64)
+                scale = np.abs(ref).max()
+                diff = np.abs(sa[k][:, :3] - ref).max()
+                print("persistent member N=%d %s: vs lone %.3e, lone vs lone %.3e, scale %.3e"
+                      % (a.sim.N, k, diff, spread[k], scale))
+                assert diff <= max(30 * spread[k], 2e-3 * scale), k
+            assert np.isfinite(sa["aux"]).all()
+        # back to the branch form and on again: the members stay engines throughout
+        ens.set_persistent(False)
+        ens.steps(8)
+        ens.set_persistent(True)
+        ens.steps(8)
+        ens.sync()
+        for nb in members:
+            assert np.isfinite(nb.read_state()["pos"]).all()
+        ens.close()
+    finally:
+        for nb in members + lone + [lone2]:
+            nb.close()
+
+
+def test_persistent_round_first_step_counts_as_alone(ccmod):
+    """After one persistent round the neighbour counts (the contact-pair sets' sizes, decided with exact
+    arithmetic) of almost every particle equal a lone run's: the rounds' launches find the pairs the
+    reference's walk finds.  (Float atomics in the mesh deposit move positions in the last bits, which can
+    move a pair across the link radius in a handful of particles over 8 steps.)"""
+    members = [settled(ccmod, N) for N in (16384, 32768)]
+    lone = [settled(ccmod, N) for N in (16384, 32768)]
+    try:
+        ens = ccmod.Ensemble(members)
+        ens.set_persistent(True)
+        ens.steps(8)
+        ens.sync()
+        for nb in lone:
+            nb.steps(8)
+            nb.sync()
+        for a, b in zip(members, lone):
+            ca, cb = a.read_state()["aux"][:, 3], b.read_state()["aux"][:, 3]
+            same = np.mean(ca == cb)
+            print("N=%d: neighbour counts equal for %.5f of particles" % (a.sim.N, same))
+            assert same > 0.999
+        ens.close()
+    finally:
+        for nb in members + lone:
+            nb.close()
+
+
+def test_persistent_round_wait_bound_reports_and_leaves_the_device_usable(ccmod):
+    """Every wait of the persistent round is bounded.  A bound far shorter than the round's ordinary waits for
+    work (1 us) makes CTAs give up: the round is abandoned, the kernel ends, ccs_ensemble_sync reports
+    CCS_E_KERNEL, and the device goes on working (a fresh engine steps and matches its twin)."""
+    members = [settled(ccmod, N) for N in (16384, 16384)]
+    try:
+        ens = ccmod.Ensemble(members)
+        ens.set_persistent(True)
+        ens.set_wait_ns(1000)
+        ens.steps(8)
+        with pytest.raises(ccmod.CCSError, match="CCS_E_KERNEL|wait"):
+            ens.sync()
+        ens.close()
+    finally:
+        for nb in members:
+            nb.close()
+    a, b = settled(ccmod, 16384), settled(ccmod, 16384)
+    try:
+        a.steps(8)
+        b.steps(8)
+        sa, sb = a.read_state(), b.read_state()
+        assert np.isfinite(sa["pos"]).all()
+        assert np.abs(sa["pos"][:, :3] - sb["pos"][:, :3]).max() <= 1e-3
+    finally:
+        a.close()
+        b.close()
