@@ -990,6 +990,10 @@ def main():
     if rank == 0:
         if world == 1 and not args.no_cpu and not args.profile:
             line["cpu_baseline"] = cpu_reference(snapshot, min_seconds=args.cpu_seconds)
+            # the single-thread form of the same sample (the oracle is one binary32 rounding per operation,
+            # so the one-thread and all-core runs compute the same steps)
+            one = cpu_reference(snapshot, min_seconds=args.cpu_seconds, min_steps=4, threads=1)
+            line["cpu_baseline"]["single_thread"] = {"value": one["value"], "cores": 1, "sample": one["sample"]}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as td

@@ -14,7 +14,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libccstep.so")
 SOURCES = ["ccs_step.cu", "ccs_contact.cu", "ccs_mesh.cu", "ccs_pp.cu", "ccs_split.cu", "ccs_nn.cu", "ccs_fof.cu",
            "ccs_order.cu", "ccs_api.cu", "ccs_build.cu", "ccs_host.cpp"]
-HEADERS = ["ccs_device.cuh", "ccs_internal.h", "ccs_umma.cuh", os.path.join("..", "..", "include", "ccstep.h")]
+HEADERS = ["ccs_device.cuh", "ccs_grid.cuh", "ccs_internal.h", "ccs_umma.cuh",
+           os.path.join("..", "..", "include", "ccstep.h")]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17",
