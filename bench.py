@@ -275,10 +275,12 @@ def cpu_reference(ckpt, min_seconds=10.0, min_steps=8, threads=None, N=None):
                       % (steps, N, what, el, cores)}
 
 
-def force_error(cc, dev, N, sample=2048, seed=3, net=None, split=0):
+def force_error(cc, dev, N, sample=2048, seed=3, net=None, split=0, uncapped=False):
     """The gravity-only sweep (Plummer sphere + 10 % debris, equal masses, 1 M_earth): one force evaluation
     of the P3M step (the reference's loose-list form, with the learned correction `net`, or the stencil-split
-    form with stencil `split`) against the library's binary64 direct sum at a seeded sample of particles."""
+    form with stencil `split`) against the library's binary64 direct sum at a seeded sample of particles.
+    uncapped: the reference's form with every loose particle on the list (its 8,192 cap lifted): the mesh
+    alone from the step, plus the pairwise correction over the whole list (ccs_pp_list_force)."""
     import numpy as np
     from cosmic_collisions_b200 import configs
     sim, pos, vel, mat = configs.gravity_sweep(N=N)
@@ -291,14 +293,16 @@ def force_error(cc, dev, N, sample=2048, seed=3, net=None, split=0):
         nb.pass_diag()
         D = nb.buffer("diag")
         s = nb.sim
-        rep, lst, _ = cc.fof(s.N, s.m, s.a, pos, vel, mat, D, s.k, 2 * s.a)
-        nb.set_pp(lst, rep.ppLoose)
+        rep, lst, _ = cc.fof(s.N, s.m, s.a, pos, vel, mat, D, s.k, 2 * s.a, cap=s.N if uncapped else cc.NBody.PP_CAP)
+        nb.set_pp(np.zeros(0, np.int32) if uncapped else lst, rep.ppLoose)
         if split:
             nb.set_pp_split(split)
             nb.pass_mesh()
             nb.pass_pp()
         nb.pass_sim(False, False, 0.0)
         g = nb.read_state()["aux"][:, :3].astype(np.float64)
+        if uncapped:
+            g[lst] += nb.pp_list_force(lst)[:, :3]
         idx = np.sort(np.random.default_rng(seed).choice(N, sample, replace=False)).astype(np.int32)
         ref, _ = nb.direct_sum(idx)
     finally:
@@ -307,7 +311,8 @@ def force_error(cc, dev, N, sample=2048, seed=3, net=None, split=0):
     on = np.isin(idx, np.asarray(lst, np.int64))
     return {"median": float(np.median(rel)), "p99": float(np.percentile(rel, 99)), "sample": sample,
             "method": ("stencil-split P3M, every mesh node pair within %d cells summed pairwise" % split
-                       if split else "the reference's P3M: mesh + the capped loose list's pairs"),
+                       if split else "the reference's P3M: mesh + the whole loose list's pairs (no cap)"
+                       if uncapped else "the reference's P3M: mesh + the capped loose list's pairs"),
             "loose_list_members_in_sample": int(on.sum()),
             "loose_list_median": float(np.median(rel[on])) if on.any() else None,
             "workload": "gravity sweep, %d equal masses: Plummer sphere (scale 1 R_earth) + 10%% uniform debris" % N,
@@ -803,6 +808,10 @@ def run_ours(args, rank, world, log):
     d2h = N * (16 + 16 + 16 + 4)
 
     ferr = force_error(cc, dev, N) if rank == 0 else None
+    if ferr is not None:
+        unc = force_error(cc, dev, N, uncapped=True)
+        ferr["uncapped"] = {k: unc[k] for k in ("median", "p99", "method", "loose_list", "loose_list_median",
+                                                 "loose_list_members_in_sample")}
     analysis = analysis_timing(cc, nb) if rank == 0 and not args.no_cpu else None
     books = None
     if rank == 0 and args.books_steps:

@@ -2690,6 +2690,43 @@ int ccs_direct_sum(ccs_handle *h, const int32_t *idx, int n, double *acc3, doubl
   return check_launch(h);
 }
 
+int ccs_pp_list_force(ccs_handle *h, const int32_t *list, int n, float *force4) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (n < 0 || n > h->N || (n > 0 && (!list || !force4))) return CCS_E_ARG;
+  for (int k = 0; k < n; ++k)
+    if (list[k] < 0 || list[k] >= h->N) {
+      h->err = "pairwise list: index out of range";
+      return CCS_E_ARG;
+    }
+  if (n == 0) return CCS_OK;
+  cudaSetDevice(h->device);
+  const ccs_uniforms u = pass_uniforms(h, 0, 0, 0.0);   // the boxes and constants the step's pass uses
+  int32_t *dIdx = nullptr;
+  float4 *dList = nullptr, *dOut = nullptr;
+  float *dBox = nullptr;
+  ccs_uniforms *dU = nullptr;
+  if (cudaMalloc(&dIdx, sizeof(int32_t) * n) != cudaSuccess || cudaMalloc(&dList, sizeof(float4) * n) != cudaSuccess ||
+      cudaMalloc(&dOut, sizeof(float4) * n) != cudaSuccess || cudaMalloc(&dBox, sizeof(float) * n) != cudaSuccess ||
+      cudaMalloc(&dU, sizeof(ccs_uniforms)) != cudaSuccess) {
+    cudaFree(dIdx); cudaFree(dList); cudaFree(dOut); cudaFree(dBox); cudaFree(dU);
+    h->err = "pairwise list: device allocation failed";
+    return CCS_E_NOMEM;
+  }
+  cudaMemcpyAsync(dIdx, list, sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->st);
+  cudaMemcpyAsync(dU, &u, sizeof u, cudaMemcpyHostToDevice, h->st);
+  h->launches += launch_pp_gather(dU, h->pos[h->cur], h->mat, dIdx, n, dList, dBox, h->st);
+  h->launches += launch_pp_list(u, dList, dBox, n, h->tab, dOut, h->st);
+  cudaMemcpyAsync(force4, dOut, sizeof(float4) * n, cudaMemcpyDeviceToHost, h->st);
+  const cudaError_t e = cudaStreamSynchronize(h->st);
+  cudaFree(dIdx); cudaFree(dList); cudaFree(dOut); cudaFree(dBox); cudaFree(dU);
+  if (e != cudaSuccess) {
+    h->err = std::string("pairwise list: ") + cudaGetErrorString(e);
+    return CCS_E_CUDA;
+  }
+  return check_launch(h);
+}
+
 int ccs_read_buffer(ccs_handle *h, int which, void *dst, size_t bytes) {
   int rc = ensure_built(h);
   if (rc) return rc;

@@ -226,6 +226,10 @@ int launch_pp_gather(const ccs_uniforms *u, const float4 *pos, const float *mat,
 size_t pp_partial_float4s();
 int launch_pp_force(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,
                     float4 *part, float4 *force, cudaStream_t st);
+// the same correction over a gathered list of any length n (no cap), the four slices in one: out[s] = Gm x
+// (pull, potential) of member s
+int launch_pp_list(const ccs_uniforms &u, const float4 *list, const float *box, int n, const float2 *tab,
+                   float4 *out, cudaStream_t st);
 // the learned P3M pass (ccs_nn.cu): count / scan / fill the pairs inside half
 // the cut, the network on the tensor cores, the per-target sums
 size_t nn_pp_count_ints();

@@ -61,6 +61,36 @@ __device__ __forceinline__ int pp_chunk_width(int share) {
   return min(max(w, 16), kPPJ);
 }
 
+// one pair's correction (PPFORCE_FS, src/glsl-sim.js:738-750): the softened Newton force less the mesh's own
+// (the table, zeroed unless both read the same box), tapered to zero at the cut, added to (acc, pot)
+struct PPConst {
+  float cut, a2, cut2, a, binScale, taperScale;
+  __device__ __forceinline__ explicit PPConst(const ccs_uniforms &u)
+      : cut(u.cut), a2(u.a2), cut2(xmul(u.cut, u.cut)), a(fsqrt(u.a2)), binScale(fdiv(64.0f, u.cut)),
+        taperScale(fdiv(1.0f, 0.8f * u.cut - u.cut)) {}
+};
+__device__ __forceinline__ void pp_pair(const PPConst &c, float4 P, float myBox, float4 Q, float qBox,
+                                        const float2 *stab, f3 &acc, float &pot) {
+  const f3 d = xsub3(xyz(Q), xyz(P));
+  const float r2 = xdot(d, d);
+  if (r2 >= c.cut2) return;
+  const float r = fsqrt(r2);
+  const float xx = clampf(r * c.binScale - 0.5f, 0.0f, 63.0f);
+  const int k = (int)xx, k1 = min(k + 1, 63);
+  const float tt = xx - (float)k;
+  const float invN = rsqrtf(r2 + c.a2);
+  const float ts = clampf((r - c.cut) * c.taperScale, 0.0f, 1.0f);
+  const float taper = ts * ts * (3.0f - 2.0f * ts);
+  const float same = (myBox >= 0.0f && qBox == myBox) ? 1.0f : 0.0f;
+  const float2 ta = stab[k], tb = stab[k1];
+  const float Tx = (ta.x + (tb.x - ta.x) * tt) * same;
+  const float Ty = (ta.y + (tb.y - ta.y) * tt) * same;
+  const float fn = invN * invN * invN * r - fdiv(Tx, fmaxf(r2, c.a2));
+  const float mj = Q.w;
+  acc = acc + d * (fdiv(1.0f, fmaxf(r, 1e-6f)) * mj * fn * taper);
+  pot += mj * (-invN - fdiv(Ty, fmaxf(r, c.a))) * taper;
+}
+
 // a persistent grid over (seat tile, quarter, chunk) work items, counted from the list's length on the
 // device, so a captured launch serves any length
 __global__ void __launch_bounds__(kPPI) k_pp_pairs(const ccs_uniforms *__restrict__ U,
@@ -77,8 +107,7 @@ __global__ void __launch_bounds__(kPPI) k_pp_pairs(const ccs_uniforms *__restric
   const int nCh = share > 0 ? (share + jw - 1) / jw : 0;
   const int items = (count + kPPI - 1) / kPPI * 4 * nCh;
   if (threadIdx.x < CCS_PP_BINS) stab[threadIdx.x] = tab[threadIdx.x];
-  const float cut = u.cut, a2 = u.a2, cut2 = xmul(cut, cut), a = fsqrt(a2);
-  const float binScale = fdiv(64.0f, cut), taperScale = fdiv(1.0f, 0.8f * cut - cut);
+  const PPConst c(u);
   for (int item = blockIdx.x; item < items; item += gridDim.x) {
     const int tile = item / (4 * nCh), rest = item % (4 * nCh);
     const int slice = rest / nCh, chunk = rest % nCh;
@@ -102,25 +131,7 @@ __global__ void __launch_bounds__(kPPI) k_pp_pairs(const ccs_uniforms *__restric
 #pragma unroll 4
       for (int jj = 0; jj < n; ++jj) {
         if (j0 + jj == me) continue;
-        const float4 Q = sq[jj];
-        const f3 d = xsub3(xyz(Q), xyz(P));
-        const float r2 = xdot(d, d);
-        if (r2 >= cut2) continue;
-        const float r = fsqrt(r2);
-        const float xx = clampf(r * binScale - 0.5f, 0.0f, 63.0f);
-        const int k = (int)xx, k1 = min(k + 1, 63);
-        const float tt = xx - (float)k;
-        const float invN = rsqrtf(r2 + a2);
-        const float ts = clampf((r - cut) * taperScale, 0.0f, 1.0f);
-        const float taper = ts * ts * (3.0f - 2.0f * ts);
-        const float same = (myBox >= 0.0f && sb[jj] == myBox) ? 1.0f : 0.0f;
-        const float2 ta = stab[k], tb = stab[k1];
-        const float Tx = (ta.x + (tb.x - ta.x) * tt) * same;
-        const float Ty = (ta.y + (tb.y - ta.y) * tt) * same;
-        const float fn = invN * invN * invN * r - fdiv(Tx, fmaxf(r2, a2));
-        const float mj = Q.w;
-        acc = acc + d * (fdiv(1.0f, fmaxf(r, 1e-6f)) * mj * fn * taper);
-        pot += mj * (-invN - fdiv(Ty, fmaxf(r, a))) * taper;
+        pp_pair(c, P, myBox, sq[jj], sb[jj], stab, acc, pot);
       }
     }
     if (me < count) part[((size_t)slice * kMaxChunks + chunk) * cap + me] = make_float4(acc.x, acc.y, acc.z, pot);
@@ -149,6 +160,50 @@ __global__ void __launch_bounds__(kBlock) k_pp_reduce(const ccs_uniforms *__rest
     o = make_float4(o.x * u.Gm, o.y * u.Gm, o.z * u.Gm, o.w * u.Gm);
   }
   force[(size_t)slice * cap + me] = o;
+}
+
+// the same correction over a list of any length (the reference caps it at 8,192): one thread a member, the
+// whole list staged kPPJ entries at a time and walked in list order, so no partial sums are kept; out[s] is
+// Gm x (pull, potential), the four slices of the capped pass in one
+__global__ void __launch_bounds__(kPPI) k_pp_list(const ccs_uniforms u, const float4 *__restrict__ list,
+                                                  const float *__restrict__ box, int n,
+                                                  const float2 *__restrict__ tab, float4 *__restrict__ out) {
+  __shared__ float4 sq[kPPJ];
+  __shared__ float sb[kPPJ];
+  __shared__ float2 stab[CCS_PP_BINS];
+  if (threadIdx.x < CCS_PP_BINS) stab[threadIdx.x] = tab[threadIdx.x];
+  const PPConst c(u);
+  const int me = blockIdx.x * kPPI + threadIdx.x;
+  const float4 P = me < n ? list[me] : make_float4(0, 0, 0, 0);
+  const bool active = me < n && P.w != 0.0f;
+  const float myBox = me < n ? box[me] : -1.0f;
+  f3 acc = mk(0, 0, 0);
+  float pot = 0.0f;
+  for (int j0 = 0; j0 < n; j0 += kPPJ) {
+    __syncthreads();   // the previous chunk's reads are done
+    if (j0 + (int)threadIdx.x < n) {
+      sq[threadIdx.x] = list[j0 + threadIdx.x];
+      sb[threadIdx.x] = box[j0 + threadIdx.x];
+    }
+    __syncthreads();
+    if (active) {
+      const int m = min(kPPJ, n - j0);
+#pragma unroll 4
+      for (int jj = 0; jj < m; ++jj) {
+        if (j0 + jj == me) continue;
+        pp_pair(c, P, myBox, sq[jj], sb[jj], stab, acc, pot);
+      }
+    }
+  }
+  if (me < n) out[me] = active ? make_float4(acc.x * u.Gm, acc.y * u.Gm, acc.z * u.Gm, pot * u.Gm)
+                               : make_float4(0, 0, 0, 0);
+}
+
+int launch_pp_list(const ccs_uniforms &u, const float4 *list, const float *box, int n, const float2 *tab,
+                   float4 *out, cudaStream_t st) {
+  if (n <= 0) return 0;
+  k_pp_list<<<(n + kPPI - 1) / kPPI, kPPI, 0, st>>>(u, list, box, n, tab, out);
+  return 1;
 }
 
 int launch_pp_force(const ccs_uniforms *u, const float4 *list, const float *box, int cap, const float2 *tab,

@@ -290,6 +290,15 @@ class NBody:
         self._check(lib().ccs_direct_sum(self._h, ptr(idx), len(idx), ptr(acc), ptr(pot)), "ccs_direct_sum")
         return acc, pot
 
+    def pp_list_force(self, lst):
+        """ccs_pp_list_force: the reference's pairwise correction over a list of any length (no 8,192 cap), per
+        member Gm x (pull xyz, potential), n x 4; the run is not changed."""
+        lst = np.ascontiguousarray(lst, np.int32)
+        out = np.zeros((len(lst), 4), np.float32)
+        self._check(lib().ccs_pp_list_force(self._h, ptr(lst) if len(lst) else None, len(lst),
+                                            ptr(out) if len(lst) else None), "ccs_pp_list_force")
+        return out
+
     def books(self, with_diag=True):
         """The conservation books on the device in binary64 (src/nbody.js:837-850)."""
         out = np.zeros(L.BOOKS, np.float64)

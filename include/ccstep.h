@@ -221,6 +221,16 @@ int ccs_books(ccs_handle *h, int with_diag, double out[CCS_BOOKS]);
  * Newton softened at the particle radius a (the P3M pass's softening,
  * src/glsl-sim.js:745), self term excluded, G = 1. */
 int ccs_direct_sum(ccs_handle *h, const int32_t *idx, int n, double *acc3, double *pot);
+/* The P3M pairwise correction of PPFORCE_FS (src/glsl-sim.js:700-754) over a
+ * list of any length n <= N (particle indices), without the reference's
+ * 8,192 cap (PP_CAP, src/nbody.js:38): for each member, the sum over every
+ * other member inside the cut, the four slices of the capped pass added
+ * together, x Gm, as (pull xyz, potential) in force4 (n x 4 floats), at the
+ * current positions with the boxes and table the step's pass uses.  The run
+ * is not changed.  For measuring the uncapped form of the reference's method
+ * (the gravity sweep's loose list exceeds the cap); allocates scratch for the
+ * call. */
+int ccs_pp_list_force(ccs_handle *h, const int32_t *list, int n, float *force4);
 
 /* The P3M pairwise pass with no allocation at all, for callers that may not
  * call cudaMalloc (a host running inside a device-memory budget it does not

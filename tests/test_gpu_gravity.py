@@ -68,3 +68,42 @@ def test_force_error_vs_direct_sum(ccmod, orc):
     # the 64^3 mesh at FH = 0.1875 R_earth smooths the pull below a cell: a few per cent at the median
     assert med < 0.05
     assert p99 < 0.5
+
+
+def test_uncapped_form_reports_its_error(ccmod, orc):
+    """The gravity sweep's loose list exceeds the reference's 8,192 cap; the uncapped form of the reference's
+    method puts every loose particle on the list (the mesh from the step, the pairwise correction over the
+    whole list by ccs_pp_list_force).  Its error is stated beside the capped form's."""
+    from cosmic_collisions_b200 import configs
+    N = 65536
+    sim, pos, vel, mat = configs.gravity_sweep(N=N)
+    nb = ccmod.NBody(0)
+    try:
+        nb.upload(sim, pos, vel, mat)
+        nb.pass_slots()
+        nb.pass_diag()
+        D = nb.buffer("diag")
+        s = nb.sim
+        m, a = float(s.m), float(s.a)
+        rep, lst, _ = ccmod.fof(s.N, s.m, s.a, pos, vel, mat, D, s.k, 2 * s.a, cap=N)
+        assert len(lst) == rep.ppLoose > ccmod.NBody.PP_CAP
+        nb.set_pp(np.zeros(0, np.int32), rep.ppLoose)
+        nb.pass_sim(False, False, 0.0)
+        g = nb.read_state()["aux"][:, :3].astype(np.float64)
+        corr = nb.pp_list_force(lst)
+        g[lst] += corr[:, :3]
+    finally:
+        nb.close()
+    assert np.isfinite(corr).all() and np.abs(corr[:, :3]).max() > 0
+    idx = np.sort(np.random.default_rng(3).choice(N, 1024, replace=False)).astype(np.int32)
+    ref, _ = orc.direct_sum(pos, m * mat.astype(np.float64), a, idx)
+    rel = np.linalg.norm(g[idx] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    loose = np.zeros(N, bool)
+    loose[lst] = True
+    capped, capped_loose, _ = force_error(ccmod, orc, N)
+    print("gravity sweep N=%d: uncapped (%d on the list) median %.3e p99 %.3e, loose members %.3e; "
+          "capped median %.3e, its list members %.3e"
+          % (N, len(lst), np.median(rel), np.percentile(rel, 99), np.median(rel[loose[idx]]), np.median(capped),
+             np.median(capped[capped_loose])))
+    assert np.all(np.isfinite(rel))
+    assert np.median(rel) < 0.05

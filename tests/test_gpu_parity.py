@@ -297,6 +297,49 @@ def test_pp(nb, ccmod, orc):
     assert np.array_equal(slot, want)
 
 
+def test_pp_list_beyond_the_cap_matches_the_oracle(nb, ccmod, orc):
+    """The reference's pairwise correction over a list longer than its 8,192 cap (ccs_pp_list_force, the
+    uncapped form the gravity sweep reports): 12,000 members, against the oracle's PPFORCE_FS restatement
+    run with the cap lifted (orc_pp_force with cap = the list's length), each member's four slices summed;
+    and over a list inside the cap, against the capped pass of the step itself."""
+    osim, pos, vel, mat, q = oracle_state(orc)
+    rng = np.random.default_rng(9)
+    pos = pos.copy()
+    n = 12000
+    assert n > orc.PP_CAP and n < osim.N
+    sel = rng.choice(osim.N, n, replace=False)
+    pos[sel, :3] *= np.float32(2.0)
+    com = (pos[:, :3].astype(np.float64) * mat[:, None]).sum(0) / mat.sum()
+    set_box(osim, com, on_b=True, cen_b=com + np.array([4.0, 0.0, 0.0]))
+    nb.upload(to_lib_sim(ccmod, osim), pos, vel, mat)
+    nb.pass_mesh()                                  # sets the box uniforms (boxes())
+    lst = np.sort(sel).astype(np.int32)
+    got = nb.pp_list_force(lst).astype(np.float64)
+    u = uni_for(orc, osim)
+    orc.lib().orc_boxes(C.byref(osim), C.byref(u))
+    P = orc.ptr
+    ol = np.zeros((n, 4), np.float32)
+    ob = np.zeros(n, np.float32)
+    orc.lib().orc_pp_gather(C.byref(u), P(pos), P(mat), P(lst), n, P(ol), P(ob))
+    f, p = orc.pair_table()
+    tab = np.stack([f, p], 1).astype(np.float32).copy()
+    of = np.zeros((4 * n, 4), np.float32)
+    orc.lib().orc_pp_force(C.byref(u), P(ol), P(ob), n, n, P(tab), P(of))
+    want = of.reshape(4, n, 4).astype(np.float64).sum(0)   # x Gm already
+    assert np.abs(want[:, :3]).max() > 0
+    assert scaled_err(got, want) < TOL
+    big = np.linalg.norm(want[:, :3], axis=1) > 1e-3 * np.linalg.norm(want[:, :3], axis=1).max()
+    rel = np.linalg.norm(got[:, :3] - want[:, :3], axis=1)[big] / np.linalg.norm(want[:, :3], axis=1)[big]
+    print("uncapped list of %d: per-member median rel %.2e, p99.9 %.2e" % (n, np.median(rel),
+                                                                           np.percentile(rel, 99.9)))
+    assert np.median(rel) < 1e-5 and np.percentile(rel, 99.9) < 1e-4
+    # inside the cap: the same members as the step's own (capped, four-slice) pass
+    short = lst[:5000]
+    nb.set_pp(short)
+    slices = nb.buffer("ppforce").reshape(4, ccmod._lib.PP_CAP, 4)[:, :len(short)].astype(np.float64).sum(0)
+    assert scaled_err(nb.pp_list_force(short).astype(np.float64), slices) < TOL
+
+
 def test_rigid_carry_is_exact(nb, ccmod, orc):
     sim, pos, vel, mat, home = orc.build_run(orc.make_opt(16384))
     sim.phase = 1
