@@ -121,6 +121,7 @@ struct ccs_handle {
   // the stencil-split P3M (ccs_set_pp_split): the stencil S (0: the reference's loose-list pass), the pair
   // pass's sorted sources, start offsets and occupied target nodes, and every particle's pair sum
   int ppSplit = 0;
+  int splitSymMin = 128;   // ccs_set_pp_split_sym: nodes this full take their mutual pairs once, both ways
   int *splitStart = nullptr, *splitCells = nullptr, *splitNCells = nullptr;
   unsigned char *splitWork = nullptr;   // the pair pass's items and counters (split_work_bytes)
   float4 *splitSrc = nullptr, *splitSrcT = nullptr, *ppAll = nullptr;
@@ -441,7 +442,7 @@ void pass_pp(ccs_handle *h, const ccs_uniforms *U, int count) {
     time_begin(h, 4, &b, &e);
     h->launches += launch_pp_split(U, h->N, h->ppSplit, h->pos[h->cur], h->mat, h->keys, h->vals, h->keysTmp,
                                    h->valsTmp, h->hist, h->splitStart, h->splitSrc, h->splitSrcT, h->splitCells,
-                                   h->splitNCells, h->splitWork, h->ppAll, h->st);
+                                   h->splitNCells, h->splitWork, h->ppAll, h->splitSymMin, h->st);
     time_end(h, e);
     return;
   }
@@ -589,7 +590,7 @@ int block_launches(const ccs_handle *h, const StepPlan *plans, int M, bool split
   for (int k = 0; k < M; ++k) {
     if (h->ppSplit && !h->field) {                  // the stencil-split P3M: walk + tail every step
       per += 2 + (plans[k].slots ? 1 : 0);
-      if (plans[k].mesh) per += 8 * (1 + (plans[k].u.boxB > 0.5f)) + pp_split_launches();
+      if (plans[k].mesh) per += 8 * (1 + (plans[k].u.boxB > 0.5f)) + pp_split_launches(h->splitSymMin);
       continue;
     }
     per += 1;                                       // contact step
@@ -3096,6 +3097,21 @@ int ccs_set_pp_split(ccs_handle *h, int S) {
     CUDA_TRY(h, cudaStreamSynchronize(h->st));
   }
   h->ppSplit = S;
+  return CCS_OK;
+}
+
+int ccs_set_pp_split_sym(ccs_handle *h, int minNode) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (minNode < 0 || (minNode > 0 && minNode < kSymMinNode)) {
+    h->err = "ccs_set_pp_split_sym: 0 (every pair one way) or at least 16 particles a node";
+    return CCS_E_ARG;
+  }
+  if (minNode == h->splitSymMin) return CCS_OK;
+  cudaSetDevice(h->device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  free_graphs(h);   // captured pair passes hold the threshold as an argument
+  h->splitSymMin = minNode;
   return CCS_OK;
 }
 

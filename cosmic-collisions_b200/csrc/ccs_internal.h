@@ -13,6 +13,7 @@ constexpr uint32_t kEmpty = CCS_SEAT_EMPTY;   // -1.0f bit pattern: an empty sea
 constexpr uint32_t kNoCell = 0xFFFFFFFFu;     // no cell recorded for this particle
 constexpr int kFine = 64 * 64 * 64;           // 64^3 mesh; index kFine is the scratch texel
 constexpr int kSplitKeys = 2 * kFine;         // the stencil-split pair pass's sort keys: (box, base node); this one: neither box
+constexpr int kSymMinNode = 16;               // the least node size ccs_set_pp_split_sym accepts (its items' room)
 constexpr int kCoarse = 4096;                 // 16^3 blocks
 constexpr int kCellChunks = 8;                // CTAs of the cell pass per occupied block, each a source chunk
 constexpr int kSeats = CCS_SEATS;
@@ -216,10 +217,11 @@ int launch_node_moments(const ccs_uniforms *u, int N, int box, const float4 *pos
 // (work: split_work_bytes(N) of scratch for the pair pass's items and counters)
 size_t split_start_ints();
 size_t split_work_bytes(int N);
+// symMin: nodes of at least this many particles take their pairs with each other once, both ways (0: never)
 int launch_pp_split(const ccs_uniforms *U, int N, int S, const float4 *pos, const float *mat, uint32_t *keys,
                     int32_t *vals, uint32_t *keysTmp, int32_t *valsTmp, uint32_t *hist, int *start, float4 *src,
-                    float4 *srcT, int *cells, int *nCells, void *work, float4 *out, cudaStream_t st);
-int pp_split_launches();
+                    float4 *srcT, int *cells, int *nCells, void *work, float4 *out, int symMin, cudaStream_t st);
+int pp_split_launches(int symMin);
 int launch_pp_gather(const ccs_uniforms *u, const float4 *pos, const float *mat, const int *index, int cap,
                      float4 *list, float *box, cudaStream_t st);
 // the pairwise partials of the P3M pass: 4 quarters x chunks x cap float4

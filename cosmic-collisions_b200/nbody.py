@@ -452,6 +452,11 @@ class NBody:
         particle by particle, the rest on the mesh to second order; 0 returns to the reference's pass."""
         self._check(lib().ccs_set_pp_split(self._h, int(S)), "ccs_set_pp_split")
 
+    def set_pp_split_sym(self, min_node):
+        """ccs_set_pp_split_sym: nodes of at least min_node particles take their mutual pairs once, both ways
+        (default 128); 0: every pair one way."""
+        self._check(lib().ccs_set_pp_split_sym(self._h, int(min_node)), "ccs_set_pp_split_sym")
+
     def set_contact_walk(self, mode):
         """How the step after a grid rebuild finds its contact pairs (ccs_set_contact_walk): 1 (the default)
         replays the rebuilding step's record where it is good, 0 walks the seat tables every step, 2 is 1

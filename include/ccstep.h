@@ -318,6 +318,13 @@ int ccs_set_pp_nn(ccs_handle *h, ccs_nn *nn);
  * returns to the reference's pass.  Applies from the next mesh step;
  * allocates its buffers on first use (about 220 MB plus 80 B a particle). */
 int ccs_set_pp_split(ccs_handle *h, int S);
+/* The split form's pair pass takes the pairs between two mesh nodes that
+ * each hold at least minNode particles once, adding each pair's reaction to
+ * the other particle (Newton's third law), in float atomics; smaller nodes
+ * take every pair one way, in a fixed order.  minNode = 0 takes every pair
+ * one way (deterministic); otherwise at least 16 (CCS_E_ARG).  Default 128.
+ * No counterpart in the reference. */
+int ccs_set_pp_split_sym(ccs_handle *h, int minNode);
 
 /* ---- launch shapes by measurement ----
  * No counterpart in the reference (WebGL fixes its own shapes).  Times the

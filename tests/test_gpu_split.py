@@ -45,13 +45,16 @@ def loose_body(orc, N=16384):
     return s, pos, e.buf("vel"), mat
 
 
-@pytest.mark.parametrize("S", [1, 2])
-def test_split_passes_match_the_oracle(ccmod, orc, S):
+@pytest.mark.parametrize("S,sym", [(1, 128), (2, 128), (1, 16), (2, 16)])
+def test_split_passes_match_the_oracle(ccmod, orc, S, sym):
+    """sym: the node size from which pairs are taken once, both ways (16: most of this body's nodes, so the
+    pair pass's both-ways kernel is what the oracle checks; 128: none of them, the one-way kernel)."""
     s, pos, vel, mat = loose_body(orc)
     nb = ccmod.NBody(0)
     try:
         nb.upload(ccmod._lib.Sim.from_buffer_copy(bytes(s)), pos, vel, mat)
         nb.set_pp_split(S)
+        nb.set_pp_split_sym(sym)
         nb.pass_mesh()
         nb.pass_pp()
         fine, coarse, far = nb.buffer("fineA"), nb.buffer("coarseA"), nb.buffer("farA")
@@ -101,6 +104,41 @@ def test_split_passes_match_the_oracle(ccmod, orc, S):
     og = orc.gather_split(u, pos, (fine, force, t0, t1, t2), (zeros, zeros, zeros, zeros, zeros2), mono, mono, ppall)
     gr = per_particle(grav, og[:, :3])
     assert np.median(gr) < REL and np.percentile(gr, 99.9) < 10 * REL, (np.median(gr), np.percentile(gr, 99.9))
+
+
+@pytest.mark.parametrize("S", [1, 3])
+def test_both_ways_pair_pass_equals_one_way_at_full_size(ccmod, S):
+    """On the gravity sweep (262,144 particles, a dense Plummer core: most particles sit in nodes of 128 or
+    more) the pair pass that takes the big nodes' mutual pairs once, both ways, gives every particle the sum
+    the one-way pass gives it, to 1e-5 of its size (float atomics sum the both-ways part in any order)."""
+    from cosmic_collisions_b200 import configs
+    sim, pos, vel, mat = configs.gravity_sweep(N=262144)
+    nb = ccmod.NBody(0)
+    try:
+        nb.upload(sim, pos, vel, mat)
+        nb.set_pp_split(S)
+        nb.pass_mesh()
+        out = {}
+        for sym in (0, 128):
+            nb.set_pp_split_sym(sym)
+            nb.pass_pp()
+            out[sym] = nb.buffer("ppall").astype(np.float64)
+    finally:
+        nb.close()
+    one, both = out[0], out[128]
+    assert np.abs(one[:, :3]).max() > 0
+    floor = np.sqrt((one[:, :3] ** 2).sum(1).mean())
+    pr = per_particle(both[:, :3], one[:, :3], floor=floor)
+    pot = np.abs(both[:, 3] - one[:, 3]) / np.maximum(np.abs(one[:, 3]), 1e-30)
+    moved = np.mean(np.any(both != one, axis=1))   # the particles whose sums the both-ways kernel made
+    print("S=%d both ways vs one way (%.1f %% of particles summed both ways): pull median %.2e p99.9 %.2e max "
+          "%.2e; potential median %.2e p99.9 %.2e max %.2e" % (S, 100 * moved, np.median(pr), np.percentile(pr, 99.9),
+                                                            pr.max(), np.median(pot), np.percentile(pot, 99.9),
+                                                            pot.max()))
+    assert moved > 0.05
+    assert np.median(pr) < REL and np.percentile(pr, 99.9) < 10 * REL
+    # a potential sums some 1e5 binary32 terms a particle, here in another order: to 1e-4 but for a few
+    assert np.median(pot) < REL and np.percentile(pot, 99.9) < 10 * REL and pot.max() < 1e-3
 
 
 def sweep_error(ccmod, S, sample=2048, seed=3):
