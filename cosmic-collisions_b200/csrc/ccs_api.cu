@@ -121,7 +121,7 @@ struct ccs_handle {
   // the stencil-split P3M (ccs_set_pp_split): the stencil S (0: the reference's loose-list pass), the pair
   // pass's sorted sources, start offsets and occupied target nodes, and every particle's pair sum
   int ppSplit = 0;
-  int splitSymMin = 128;   // ccs_set_pp_split_sym: nodes this full take their mutual pairs once, both ways
+  int splitSymMin = 16;    // ccs_set_pp_split_sym: nodes this full take their mutual pairs once, both ways
   int *splitStart = nullptr, *splitCells = nullptr, *splitNCells = nullptr;
   unsigned char *splitWork = nullptr;   // the pair pass's items and counters (split_work_bytes)
   float4 *splitSrc = nullptr, *splitSrcT = nullptr, *ppAll = nullptr;

@@ -454,7 +454,7 @@ class NBody:
 
     def set_pp_split_sym(self, min_node):
         """ccs_set_pp_split_sym: nodes of at least min_node particles take their mutual pairs once, both ways
-        (default 128); 0: every pair one way."""
+        (default 16); 0: every pair one way."""
         self._check(lib().ccs_set_pp_split_sym(self._h, int(min_node)), "ccs_set_pp_split_sym")
 
     def set_contact_walk(self, mode):

@@ -322,7 +322,7 @@ int ccs_set_pp_split(ccs_handle *h, int S);
  * each hold at least minNode particles once, adding each pair's reaction to
  * the other particle (Newton's third law), in float atomics; smaller nodes
  * take every pair one way, in a fixed order.  minNode = 0 takes every pair
- * one way (deterministic); otherwise at least 16 (CCS_E_ARG).  Default 128.
+ * one way (deterministic); otherwise at least 16 (CCS_E_ARG).  Default 16.
  * No counterpart in the reference. */
 int ccs_set_pp_split_sym(ccs_handle *h, int minNode);
 

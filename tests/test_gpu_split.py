@@ -47,8 +47,9 @@ def loose_body(orc, N=16384):
 
 @pytest.mark.parametrize("S,sym", [(1, 128), (2, 128), (1, 16), (2, 16)])
 def test_split_passes_match_the_oracle(ccmod, orc, S, sym):
-    """sym: the node size from which pairs are taken once, both ways (16: most of this body's nodes, so the
-    pair pass's both-ways kernel is what the oracle checks; 128: none of them, the one-way kernel)."""
+    """sym: the node size from which pairs are taken once, both ways (16, the default: most of this body's
+    nodes, so the pair pass's both-ways items are what the oracle checks; 128: none of them, the one-way
+    items)."""
     s, pos, vel, mat = loose_body(orc)
     nb = ccmod.NBody(0)
     try:
@@ -108,9 +109,10 @@ def test_split_passes_match_the_oracle(ccmod, orc, S, sym):
 
 @pytest.mark.parametrize("S", [1, 3])
 def test_both_ways_pair_pass_equals_one_way_at_full_size(ccmod, S):
-    """On the gravity sweep (262,144 particles, a dense Plummer core: most particles sit in nodes of 128 or
-    more) the pair pass that takes the big nodes' mutual pairs once, both ways, gives every particle the sum
-    the one-way pass gives it, to 1e-5 of its size (float atomics sum the both-ways part in any order)."""
+    """On the gravity sweep (262,144 particles, a Plummer sphere in debris) the pair pass that takes the
+    mutual pairs of nodes holding 16 particles or more (the default) once, both ways, gives every particle
+    the sum the one-way pass gives it, to 1e-5 of its size (float atomics sum the both-ways part in any
+    order)."""
     from cosmic_collisions_b200 import configs
     sim, pos, vel, mat = configs.gravity_sweep(N=262144)
     nb = ccmod.NBody(0)
@@ -119,13 +121,13 @@ def test_both_ways_pair_pass_equals_one_way_at_full_size(ccmod, S):
         nb.set_pp_split(S)
         nb.pass_mesh()
         out = {}
-        for sym in (0, 128):
+        for sym in (0, 16):
             nb.set_pp_split_sym(sym)
             nb.pass_pp()
             out[sym] = nb.buffer("ppall").astype(np.float64)
     finally:
         nb.close()
-    one, both = out[0], out[128]
+    one, both = out[0], out[16]
     assert np.abs(one[:, :3]).max() > 0
     floor = np.sqrt((one[:, :3] ** 2).sum(1).mean())
     pr = per_particle(both[:, :3], one[:, :3], floor=floor)
