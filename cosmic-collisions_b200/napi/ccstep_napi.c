@@ -309,6 +309,7 @@ SIMPLE(SettleSome, ccs_settle_some(h, get_i32(env, a.argv[1])), "ccs_settle_some
 SIMPLE(RigidStep, ccs_rigid_step(h, get_f64(env, a.argv[1])), "ccs_rigid_step")
 SIMPLE(SetMeshEvery, ccs_set_mesh_every(h, get_i32(env, a.argv[1])), "ccs_set_mesh_every")
 SIMPLE(SetPPSplit, ccs_set_pp_split(h, get_i32(env, a.argv[1])), "ccs_set_pp_split")
+SIMPLE(SetPPSplitSym, ccs_set_pp_split_sym(h, get_i32(env, a.argv[1])), "ccs_set_pp_split_sym")
 SIMPLE(SetContactWalk, ccs_set_contact_walk(h, get_i32(env, a.argv[1])), "ccs_set_contact_walk")
 SIMPLE(DiagAsync, ccs_diag_async(h), "ccs_diag_async")
 SIMPLE(PassSlots, ccs_pass_slots(h), "ccs_pass_slots")
@@ -523,7 +524,8 @@ NAPI_MODULE_INIT() {
       FN("create", Create) FN("makeBodies", MakeBodies) FN("build", Build) FN("getSim", GetSim)
       FN("setSim", SetSim) FN("setStatic", SetStatic) FN("step", Step) FN("steps", Steps)
       FN("settleSome", SettleSome) FN("rigidStep", RigidStep) FN("setMeshEvery", SetMeshEvery)
-      FN("setPPSplit", SetPPSplit) FN("setContactWalk", SetContactWalk) FN("setPP", SetPP) FN("setBoxes", SetBoxes) FN("applyPerm", ApplyPerm)
+      FN("setPPSplit", SetPPSplit) FN("setPPSplitSym", SetPPSplitSym) FN("setContactWalk", SetContactWalk)
+      FN("setPP", SetPP) FN("setBoxes", SetBoxes) FN("applyPerm", ApplyPerm)
       FN("sortMorton", SortMorton) FN("diagAsync", DiagAsync) FN("poll", Poll) FN("fof", Fof)
       FN("fofDevice", FofDevice) FN("pairTable", PairTable) FN("readState", ReadState) FN("books", Books)
       FN("deviceBuffers", DeviceBuffers) FN("advanceHost", AdvanceHost) FN("passSlots", PassSlots)
