@@ -857,6 +857,21 @@ def run_ours(args, rank, world, log):
                                 "monopole + quadrupole at each cell; the plain form that reaches median force "
                                 "error <= 1e-3" % args.split,
                       "state": "the plain leg's timed steps from the same saved state"}
+        one, both = nb.pp_split_pairs()   # the last mesh step's pair pass
+        pp_ms = sp_kt.get("pp_force", {}).get("mean_us", 0.0) / 1e3
+        split_line["pair_pass"] = {
+            "pairs_one_way": one, "pairs_both_ways": both,
+            "forces": one + 2 * both,
+            "pairs_per_s": (one + both) / (pp_ms / 1e3) if pp_ms else None,
+            "forces_per_s": (one + 2 * both) / (pp_ms / 1e3) if pp_ms else None,
+            "ms": pp_ms,
+            "fp32_ops_per_pair": {"one_way": 17, "both_ways": 25},
+            "fma_pipe_of_peak": 0.589,
+            "what": "the (target, source) pairs inside the stencil the pass's items take, one way (a force on "
+                    "the target) and both ways (a force on each: pairs between nodes of 16 particles or more, "
+                    "once); forces = one way + 2 x both ways, the one-way pass's count; over the pass's "
+                    "event-timed mean; the FMA pipe's share from the committed ncu capture "
+                    "(profiles/pp_split_both_262k.md)"}
         log("stencil-split P3M (S=%d): %.3f ms a step, force error median %.3e"
             % (args.split, sp_total / args.split_steps, sp_err["median"] if sp_err else float("nan")))
     peak, peak_kind = measured_peaks()

@@ -46,7 +46,7 @@ EXPORTS = ["ccs_version", "ccs_last_error", "ccs_create", "ccs_destroy", "ccs_ma
            "ccs_set_boxes", "ccs_set_graphs", "ccs_contact_pairs", "ccs_set_pp_split",
            "ccs_set_contact_walk", "ccs_ensemble_set_persistent", "ccs_ensemble_step_ms",
            "ccs_ensemble_launch_count", "ccs_ensemble_set_wait_ns", "ccs_pp_list_force",
-           "ccs_set_pp_split_sym"]
+           "ccs_set_pp_split_sym", "ccs_pp_split_pairs"]
 NN_PARAMS = 4803
 NN_CUT_CELLS = 2.5
 
@@ -230,6 +230,7 @@ def lib():
         "ccs_ensemble_set_wait_ns": (I, [H, C.c_uint64]),
         "ccs_pp_list_force": (I, [H, P, I, P]),
         "ccs_set_pp_split_sym": (I, [H, I]),
+        "ccs_pp_split_pairs": (I, [H, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -3100,6 +3100,17 @@ int ccs_set_pp_split(ccs_handle *h, int S) {
   return CCS_OK;
 }
 
+int ccs_pp_split_pairs(ccs_handle *h, uint64_t counts[2]) {
+  int rc = ensure_built(h);
+  if (rc) return rc;
+  if (!counts) return CCS_E_ARG;
+  if (!h->splitWork) return CCS_E_STATE;
+  cudaSetDevice(h->device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->st));
+  CUDA_TRY(h, cudaMemcpy(counts, split_pair_counts(h->splitWork), 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return CCS_OK;
+}
+
 int ccs_set_pp_split_sym(ccs_handle *h, int minNode) {
   int rc = ensure_built(h);
   if (rc) return rc;

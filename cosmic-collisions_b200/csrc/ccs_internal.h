@@ -217,6 +217,8 @@ int launch_node_moments(const ccs_uniforms *u, int N, int box, const float4 *pos
 // (work: split_work_bytes(N) of scratch for the pair pass's items and counters)
 size_t split_start_ints();
 size_t split_work_bytes(int N);
+// where the last pass left its two 64-bit counts: pair evaluations one way, and both ways (each once)
+const void *split_pair_counts(const void *work);
 // symMin: nodes of at least this many particles take their pairs with each other once, both ways (0: never)
 int launch_pp_split(const ccs_uniforms *U, int N, int S, const float4 *pos, const float *mat, uint32_t *keys,
                     int32_t *vals, uint32_t *keysTmp, int32_t *valsTmp, uint32_t *hist, int *start, float4 *src,

@@ -61,7 +61,12 @@ constexpr int kSplitClasses = 32;    // cost classes of the items (log2 of a lan
 // the small items as made and in the order they are taken, the big items likewise, then the big nodes'
 // particles' sums (sorted order)
 constexpr int kCtrTmp = 0, kCtrTaken = 1, kCtrCount = 32, kCtrStart = 64, kCtrFill = 96, kCtrBig = 128;
-constexpr int kCtrInts = 256;
+// after both lists' counters (kCtrBig + kCtrFill + 31 = 255), two 64-bit counts: the pairs the items take one
+// way and both ways
+constexpr int kCtrPairs = 256;
+constexpr int kCtrInts = 264;   // a multiple of 4, so the items that follow stay 16-byte aligned
+static_assert(kCtrBig + kCtrFill + 32 <= kCtrPairs && kCtrPairs + 4 <= kCtrInts && kCtrInts % 4 == 0,
+              "the counters do not overlap, and the items after them are 16-byte aligned");
 inline size_t item_cap(int N) { return 2 * (size_t)N + (size_t)N / 64 + 64; }
 constexpr int kSymWarps = 4;                    // a big item's CTA
 constexpr int kSymTargets = 64 * kSymWarps;     // its targets: two a lane
@@ -170,22 +175,29 @@ __global__ void __launch_bounds__(kBlock) k_split_items(const int *__restrict__ 
     for (int dz = -R; dz <= R; ++dz) {
       const int z = bz + dz;
       if (z < 0 || z > 63) continue;
-      long srcs = 0;
+      long both = 0, one = 0;   // the slab's sources other than the node itself: big of higher key, small
+      bool own = false;
       for (int y = max(by - R, 0); y <= min(by + R, 63); ++y) {
         const int rowKey = box * kFine + fine_index(0, y, z);
         for (int x = x0; x <= x1; ++x) {
           const int X = rowKey + x, n = start[X + 1] - start[X];
-          if (X == key) srcs += n / 2 + 1;
-          else if (n > 0 && (n < symMin || X > key)) srcs += n;
+          if (X == key) own = true;
+          else if (n > 0 && n < symMin) one += n;
+          else if (n > 0 && X > key) both += n;
         }
       }
-      if (srcs == 0) continue;
+      if (both + one == 0 && !(own && k1 - k0 > 1)) continue;
       for (int f = k0; f < k1; f += kSymTargets) {
         const int nt = min(kSymTargets, k1 - f);
-        const long share = (long)nt * srcs / 64;   // a lane's pairs, as the small items count them
+        // targets f .. f + nt - 1 each meet the node's particles after them once
+        const long mine = own ? (long)nt * (k1 - 1 - f) - (long)nt * (nt - 1) / 2 : 0;
+        const long pairsBoth = (long)nt * both + mine, pairsOne = (long)nt * one;
+        const long share = (pairsBoth + pairsOne) / 64;   // a lane's pairs, as the small items count them
         const int cls = 31 - __clz((int)min(max(share, 1L), (long)INT_MAX));
         tmpBig[atomicAdd(ctr + kCtrBig + kCtrTmp, 1)] = make_int4(f, nt, cls, dz);
         atomicAdd(ctr + kCtrBig + kCtrCount + cls, 1);
+        atomicAdd(reinterpret_cast<unsigned long long *>(ctr + kCtrPairs), (unsigned long long)pairsOne);
+        atomicAdd(reinterpret_cast<unsigned long long *>(ctr + kCtrPairs + 2), (unsigned long long)pairsBoth);
       }
     }
     return;
@@ -204,6 +216,7 @@ __global__ void __launch_bounds__(kBlock) k_split_items(const int *__restrict__ 
     const int cls = 31 - __clz((int)min(max(share, 1L), (long)INT_MAX));
     tmp[atomicAdd(ctr + kCtrTmp, 1)] = make_int4(f, nt, cls, L);
     atomicAdd(ctr + kCtrCount + cls, 1);
+    atomicAdd(reinterpret_cast<unsigned long long *>(ctr + kCtrPairs), (unsigned long long)nt * sources);
     f += nt;
   }
 }
@@ -596,6 +609,8 @@ __global__ void __launch_bounds__(kBlock) k_split_finish(const ccs_uniforms *__r
 }
 
 size_t split_start_ints() { return (size_t)kSplitKeys + 2; }
+
+const void *split_pair_counts(const void *work) { return static_cast<const int *>(work) + kCtrPairs; }
 
 size_t split_work_bytes(int N) {
   return sizeof(int) * kCtrInts + 2 * sizeof(int4) * (item_cap(N) + big_cap(N)) + sizeof(float4) * (size_t)N;

@@ -452,6 +452,12 @@ class NBody:
         particle by particle, the rest on the mesh to second order; 0 returns to the reference's pass."""
         self._check(lib().ccs_set_pp_split(self._h, int(S)), "ccs_set_pp_split")
 
+    def pp_split_pairs(self):
+        """ccs_pp_split_pairs: the last split pair pass's pair evaluations (one way, both ways)."""
+        out = np.zeros(2, np.uint64)
+        self._check(lib().ccs_pp_split_pairs(self._h, ptr(out)), "ccs_pp_split_pairs")
+        return int(out[0]), int(out[1])
+
     def set_pp_split_sym(self, min_node):
         """ccs_set_pp_split_sym: nodes of at least min_node particles take their mutual pairs once, both ways
         (default 16); 0: every pair one way."""

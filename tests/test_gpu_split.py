@@ -120,14 +120,21 @@ def test_both_ways_pair_pass_equals_one_way_at_full_size(ccmod, S):
         nb.upload(sim, pos, vel, mat)
         nb.set_pp_split(S)
         nb.pass_mesh()
-        out = {}
+        out, counts = {}, {}
         for sym in (0, 16):
             nb.set_pp_split_sym(sym)
             nb.pass_pp()
             out[sym] = nb.buffer("ppall").astype(np.float64)
+            counts[sym] = nb.pp_split_pairs()
     finally:
         nb.close()
     one, both = out[0], out[16]
+    # the same pairs: the one-way pass's count less a both-ways pass's forces is the big nodes' particles,
+    # which the one-way pass also meets with themselves
+    assert counts[0][1] == 0 and counts[16][1] > 0
+    gap = counts[0][0] - (counts[16][0] + 2 * counts[16][1])
+    print("pairs one way %d; both ways %d + one way %d (gap %d)" % (counts[0][0], counts[16][1], counts[16][0], gap))
+    assert 0 < gap <= 262144
     assert np.abs(one[:, :3]).max() > 0
     floor = np.sqrt((one[:, :3] ** 2).sum(1).mean())
     pr = per_particle(both[:, :3], one[:, :3], floor=floor)
