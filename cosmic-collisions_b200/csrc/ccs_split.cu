@@ -31,19 +31,20 @@
 // share of the pairs) from one counter by a persistent grid, so the last items are short.  Sums run in a
 // fixed order per item (rows, then sorted order, then the shuffle tree): deterministic.
 //
-// Nodes holding at least symMin particles (the bodies' interiors) are "big", and a pair of particles in two
-// big nodes is evaluated once, by the node of the lower key, its reaction added to the other particle
-// (Newton's third law: the weight, the softened distance and the pull are the same both ways).  A big node's
-// work is cut into CTA items of up to 256 targets (64 a warp, two a lane) and one z slab of its stencil, taken
-// heaviest first by a persistent grid (k_pp_split_both, whose warps then take the small nodes' items, so those
-// fill the first phase's tail): the CTA stages 64 sources at a time; a source
-// chunk of big nodes of higher key (or the node itself, from the item's first target on, each pair once) is
-// walked by each lane in a rotating order, so the reaction owed to each source travels with it from lane to
-// lane (one shuffle a component a step) and is complete after 32 steps; the warps add theirs in shared memory
-// and the CTA adds the chunk's to the sources' sums with one vector atomic a source.  Small nodes in a big
-// node's stencil are sources one way only, and small nodes' own items (k_pp_split) take every source one way,
-// so every pair is counted once in each direction (k_split_finish writes the big nodes' sums out).  The big
-// nodes' sums are float atomics: summed in any order.  symMin = 0 takes every node one way (the form above).
+// Nodes holding at least symMin particles (16 by default: the bodies and most of their surfaces) are "big",
+// and a pair of particles in two big nodes is evaluated once, by the node of the lower key, its reaction
+// added to the other particle (Newton's third law: the weight, the softened distance and the pull are the
+// same both ways).  A big node's work is cut into CTA items of up to 256 targets (64 a warp, two a lane) and
+// one z slab of its stencil, taken heaviest first by a persistent grid (k_pp_split_both, whose warps then
+// take the small nodes' items, so those fill the first phase's tail): the CTA stages 64 sources at a time; a
+// source chunk of big nodes of higher key (or the node itself, from the item's first target on, each pair
+// once) is walked by each lane in a rotating order, so the reaction owed to each source travels with it from
+// lane to lane (one shuffle a component a step) and is complete after 32 steps; the warps add theirs in
+// shared memory and the CTA adds the chunk's to the sources' sums with one vector atomic a source.  Small
+// nodes in a big node's stencil are sources one way only, and small nodes' own items take every source one
+// way, so every pair is counted once in each direction (k_split_finish writes the big nodes' sums out).  The
+// big nodes' sums are float atomics: summed in any order.  symMin = 0 takes every node one way (the form
+// above, k_pp_split: deterministic).  The items count the pairs they take, one way and both ways.
 #include <algorithm>
 
 #include "ccs_device.cuh"
