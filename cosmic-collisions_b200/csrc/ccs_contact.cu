@@ -650,10 +650,10 @@ __device__ int4 ens_pick(const EnsLaunch &L) {
 }
 }  // namespace
 
-// 6 CTAs an SM: the walk's three forms and the grid in one kernel keep 80 registers without spilling (at 8
-// CTAs and 64 registers it spilled, and ran slower).  Work items are a CTA's: warp-sized items, each warp
-// picking its own, took four times the picks and ran slower.
-__global__ void __launch_bounds__(32 * kEnsWarps, 6) k_ensemble_round(const EnsLaunch L) {
+// 3 CTAs of 8 warps an SM: the walk's three forms and the grid in one kernel keep 80 registers without
+// spilling (at 64 registers it spilled, and ran slower).  Work items are a CTA's: warp-sized items, each warp
+// picking its own, took four times the picks and ran slower; CTAs of 4 warps 4 % slower than of 8.
+__global__ void __launch_bounds__(32 * kEnsWarps, 24 / kEnsWarps) k_ensemble_round(const EnsLaunch L) {
   constexpr int W = kEnsWarps;
   extern __shared__ __align__(16) unsigned char smem_raw[];   // the contact step's W warp slots
   __shared__ float spc[16];
