@@ -1036,6 +1036,7 @@ int ensure_split_buffers(ccs_handle *h) {
     CUDA_TRY(h, cudaMemsetAsync(h->pm[b].tide2, 0, sizeof(float4) * 3 * (kFine + 1), h->st));
   }
   CUDA_TRY(h, cudaMemsetAsync(h->ppAll, 0, sizeof(float4) * N, h->st));
+  CUDA_TRY(h, cudaMemsetAsync(h->splitWork, 0, split_work_bytes(h->N), h->st));   // no pass counted yet
   return CCS_OK;
 }
 

@@ -327,8 +327,9 @@ int ccs_set_pp_split(ccs_handle *h, int S);
 int ccs_set_pp_split_sym(ccs_handle *h, int minNode);
 /* The split form's last pair pass, counted: counts[0] the (target, source)
  * pair evaluations taken one way, counts[1] those taken once for both
- * particles (each a force on both); waits for the pass.  CCS_E_STATE before
- * the form's first pass.  No counterpart in the reference. */
+ * particles (each a force on both); waits for the pass.  Zeros before the
+ * form's first pass; CCS_E_STATE before the form was ever switched on.  No
+ * counterpart in the reference. */
 int ccs_pp_split_pairs(ccs_handle *h, uint64_t counts[2]);
 
 /* ---- launch shapes by measurement ----
