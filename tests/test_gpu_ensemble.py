@@ -212,3 +212,43 @@ def test_persistent_round_wait_bound_reports_and_leaves_the_device_usable(ccmod)
     finally:
         a.close()
         b.close()
+
+
+def test_persistent_round_with_the_second_box_up(ccmod):
+    """Members whose second mesh box is up (one box on each body: the gather from box B, the cross pull
+    between the boxes, each particle reading the box whose centre is nearer) step in the persistent rounds
+    as their lone twins do, to the same spread as the other ensemble tests."""
+    def two_boxes(nb):
+        s = nb.sim
+        nb.set_boxes([{"on": 1, "cen": tuple(s.cen0), "t": s.t}, {"on": 1, "cen": tuple(s.cen1), "t": s.t}])
+
+    sizes = [16384, 32768]
+    members = [settled(ccmod, N) for N in sizes]
+    lone = [settled(ccmod, N) for N in sizes]
+    lone2 = settled(ccmod, 16384)
+    try:
+        for nb in members + lone + [lone2]:
+            two_boxes(nb)
+        ens = ccmod.Ensemble(members)
+        ens.set_persistent(True)
+        ens.steps(16)
+        ens.sync()
+        for nb in lone + [lone2]:
+            nb.steps(16)
+            nb.sync()
+        assert all(nb.uniforms().boxB > 0.5 for nb in members)
+        l2 = lone2.read_state()
+        spread = {k: np.abs(l2[k][:, :3] - lone[0].read_state()[k][:, :3]).max() for k in ("pos", "vel")}
+        for a, b in zip(members, lone):
+            sa, sb = a.read_state(), b.read_state()
+            for k in ("pos", "vel"):
+                ref = sb[k][:, :3].astype(np.float64)
+                scale = np.abs(ref).max()
+                diff = np.abs(sa[k][:, :3] - ref).max()
+                print("two boxes, persistent member N=%d %s: vs lone %.3e, lone vs lone %.3e, scale %.3e"
+                      % (a.sim.N, k, diff, spread[k], scale))
+                assert diff <= max(30 * spread[k], 2e-3 * scale), k
+        ens.close()
+    finally:
+        for nb in members + lone + [lone2]:
+            nb.close()
