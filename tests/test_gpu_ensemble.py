@@ -23,6 +23,26 @@ def settled(ccmod, N, steps=64):
     return nb
 
 
+def twin_spread(ccmod, sizes, lone, steps, prepare=None):
+    """Per size, how far two lone runs of the same start drift apart in `steps` steps (float atomics sum in
+    any order): a second lone twin of each size against the first one in `lone`."""
+    out = {}
+    for N, first in zip(sizes, lone):
+        if N in out:
+            continue
+        twin = settled(ccmod, N)
+        try:
+            if prepare:
+                prepare(twin)
+            twin.steps(steps)
+            twin.sync()
+            st, s0 = twin.read_state(), first.read_state()
+            out[N] = {k: np.abs(st[k][:, :3] - s0[k][:, :3]).max() for k in ("pos", "vel")}
+        finally:
+            twin.close()
+    return out
+
+
 def spread_ok(a, b, lone, scale):
     return np.abs(a - b).max() <= max(30 * lone, 2e-3 * scale)
 
@@ -121,7 +141,6 @@ def test_persistent_round_steps_members_as_alone(ccmod):
     sizes = [16384, 32768, 16384, 65536]
     members = [settled(ccmod, N) for N in sizes]
     lone = [settled(ccmod, N) for N in sizes]
-    lone2 = settled(ccmod, 16384)
     try:
         ens = ccmod.Ensemble(members)
         ens.set_persistent(True)
@@ -130,21 +149,21 @@ def test_persistent_round_steps_members_as_alone(ccmod):
         assert ens.launch_count() == 2                  # one persistent launch a round
         ms = ens.step_ms()
         assert np.all(ms > 0) and np.all(ms < 50), ms
-        for nb in lone + [lone2]:
+        for nb in lone:
             nb.steps(16)
             nb.sync()
         assert [nb.sim.stepNo for nb in members] == [nb.sim.stepNo for nb in lone]
-        l2 = lone2.read_state()
-        spread = {k: np.abs(l2[k][:, :3] - lone[0].read_state()[k][:, :3]).max() for k in ("pos", "vel")}
+        spread = twin_spread(ccmod, sizes, lone, 16)
         for a, b in zip(members, lone):
             sa, sb = a.read_state(), b.read_state()
             for k in ("pos", "vel"):
                 ref = sb[k][:, :3].astype(np.float64)
                 scale = np.abs(ref).max()
                 diff = np.abs(sa[k][:, :3] - ref).max()
+                sp = spread[a.sim.N][k]
                 print("persistent member N=%d %s: vs lone %.3e, lone vs lone %.3e, scale %.3e"
-                      % (a.sim.N, k, diff, spread[k], scale))
-                assert diff <= max(30 * spread[k], 2e-3 * scale), k
+                      % (a.sim.N, k, diff, sp, scale))
+                assert diff <= max(30 * sp, 2e-3 * scale), k
             assert np.isfinite(sa["aux"]).all()
         # back to the branch form and on again: the members stay engines throughout
         ens.set_persistent(False)
@@ -156,7 +175,7 @@ def test_persistent_round_steps_members_as_alone(ccmod):
             assert np.isfinite(nb.read_state()["pos"]).all()
         ens.close()
     finally:
-        for nb in members + lone + [lone2]:
+        for nb in members + lone:
             nb.close()
 
 
@@ -225,30 +244,29 @@ def test_persistent_round_with_the_second_box_up(ccmod):
     sizes = [16384, 32768]
     members = [settled(ccmod, N) for N in sizes]
     lone = [settled(ccmod, N) for N in sizes]
-    lone2 = settled(ccmod, 16384)
     try:
-        for nb in members + lone + [lone2]:
+        for nb in members + lone:
             two_boxes(nb)
         ens = ccmod.Ensemble(members)
         ens.set_persistent(True)
         ens.steps(16)
         ens.sync()
-        for nb in lone + [lone2]:
+        for nb in lone:
             nb.steps(16)
             nb.sync()
         assert all(nb.uniforms().boxB > 0.5 for nb in members)
-        l2 = lone2.read_state()
-        spread = {k: np.abs(l2[k][:, :3] - lone[0].read_state()[k][:, :3]).max() for k in ("pos", "vel")}
+        spread = twin_spread(ccmod, sizes, lone, 16, prepare=two_boxes)
         for a, b in zip(members, lone):
             sa, sb = a.read_state(), b.read_state()
             for k in ("pos", "vel"):
                 ref = sb[k][:, :3].astype(np.float64)
                 scale = np.abs(ref).max()
                 diff = np.abs(sa[k][:, :3] - ref).max()
+                sp = spread[a.sim.N][k]
                 print("two boxes, persistent member N=%d %s: vs lone %.3e, lone vs lone %.3e, scale %.3e"
-                      % (a.sim.N, k, diff, spread[k], scale))
-                assert diff <= max(30 * spread[k], 2e-3 * scale), k
+                      % (a.sim.N, k, diff, sp, scale))
+                assert diff <= max(30 * sp, 2e-3 * scale), k
         ens.close()
     finally:
-        for nb in members + lone + [lone2]:
+        for nb in members + lone:
             nb.close()
