@@ -63,6 +63,7 @@ sys.path.insert(0, ROOT)
 ALG_BYTES_SIM = 92          # bytes per particle per contact-step launch
 L2_FLUSH_BYTES = 256 << 20
 MIN_SAMPLES = 8                # contact-step launches timed inside the timed region, at least
+ENS_ROUNDS = 4                 # 8-step rounds one ensemble graph holds (ccs_ensemble_steps)
 # the metric both arms report under (the driver divides their values only when the strings agree)
 METRIC = "particle-steps/s @262k, plain vs NN-corrected P\u00b3M at \u22641e-3 force error"
 
@@ -453,8 +454,14 @@ def run_ensemble(args, log, rank=0, world=1):
         ens.close()
         log("ensemble autotuner: %s" % tuned)
     blocks = max(1, args.ens_steps // 8)
+    # the library holds ENS_ROUNDS rounds a graph, keyed by the members' parities (the branch form's also by a
+    # ping that alternates per graph): two full graphs and the last, shorter one cover every graph the timed
+    # rounds replay
+    warm = 8 * (2 * ENS_ROUNDS + blocks % ENS_ROUNDS)
     streams = [torch.cuda.ExternalStream(nb.device_buffers().stream) for nb in runs]
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in runs]
+    for nb in runs:   # each member's block graphs (both ping parities) captured before the timing
+        nb.steps(16)
     torch.cuda.synchronize()
     barrier()
     w0 = time.perf_counter()
@@ -473,7 +480,7 @@ def run_ensemble(args, log, rank=0, world=1):
     total = sum_over_ranks(sum(nb.sim.N for nb in runs) * 8 * blocks)
     # the same number of steps again, every round one graph holding all instances' blocks (ccs_ensemble)
     ens = cc.Ensemble(runs)
-    ens.steps(8)                                          # capture the round's graphs
+    ens.steps(warm)                                       # capture every graph the timed rounds replay
     ens.sync()
     torch.cuda.synchronize()
     barrier()
@@ -484,7 +491,7 @@ def run_ensemble(args, log, rank=0, world=1):
     # and again with every round one persistent launch over all instances' grids and contact steps
     # (ccs_ensemble_set_persistent), after the instances' mesh chains
     ens.set_persistent(True)
-    ens.steps(8)                                          # capture the round's graphs
+    ens.steps(warm)                                       # capture every graph the timed rounds replay
     ens.step_ms()                                         # (waits; the sums start at the timed rounds)
     torch.cuda.synchronize()
     barrier()
