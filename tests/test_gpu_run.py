@@ -84,19 +84,19 @@ def test_small_impact_run_keeps_its_books(ccmod):
     oc = OracleRun(opt)
     oc.run_to(T_END)
     o, oref = oc.report, oc.ref
-    print("GPU: L %.6f (first look %.6f) balance %.4f drift %.3e largest %.4f | oracle: L %.6f balance %.4f "
+    print("GPU: L %.6f (first look %.6f) balance %.3e drift %.3e largest %.4f | oracle: L %.6f balance %.3e "
           "largest %.4f | steps %d" % (g.L, gref["L"], balance(g, gref), g.drift, g.largest, o.L,
                                        balance(o, oref), o.largest, steps))
     # the same schedule on both sides
     assert steps == oc.sim.stepNo and t == oc.sim.t and soft == oc.sim.soft == 1
-    # the books, kept to a fraction of a percent
+    # the books, to 0.1 % (measured: L 8.6e-5 of the first look, energy balance 5e-4, momentum drift 1e-5)
     assert abs(g.L - gref["L"]) / gref["L"] < 1e-3
-    assert abs(balance(g, gref)) < 1e-2
+    assert abs(balance(g, gref)) < 1e-3
     assert g.drift < 1e-4
     # and the same run in aggregate
     assert abs(g.L - o.L) / o.L < 1e-3
     assert abs(g.largest - o.largest) < 0.01
-    assert abs(balance(g, gref) - balance(o, oref)) < 5e-3
+    assert abs(balance(g, gref) - balance(o, oref)) < 1e-3
     # the device's binary64 books agree with the host analysis's
     assert abs(books["M"] - g.M) < 1e-9
     assert abs(np.sqrt(books["Lx"] ** 2 + books["Ly"] ** 2 + books["Lz"] ** 2) - g.L) < 1e-6 * g.L
